@@ -1,0 +1,397 @@
+"""Benchmark of the FP32 lyotropic Model::Step() on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--size L] [--model lyotropic|nematic] [--precision fp32|fp64]
+
+Workload (default): the lyotropic model on a periodic 4096 x 4096 lattice in
+FP32 - the throughput target named for this path - with the physics of the
+256^2 CPU configuration (rho=40, tau=1.5, CC=0.1, AA=0.1, KK=0.05, LL=0.05,
+GammaQ=0.3, GammaP=0.1, xi=0.7, zeta=0.01, npc=1), director angle i.i.d.
+U[0, pi) with S=1, phi a tanh disk of radius L/4. Seeded synthetic input.
+
+A step is one Model::Step() over the whole lattice (one fused kernel
+launch). `value` is site-updates/s with the state resident in HBM, timed
+with CUDA events on the library's stream; the 805 MB state per buffer is
+larger than the 126 MB L2, so no flush is needed. `e2e` goes through the C
+ABI with host buffers: each e2e step uploads the state from pinned host
+memory, runs 100 steps (the output interval of the configuration) and
+downloads the primary frame fields (ff, QQxx, QQyx, phi).
+
+With --gpus N (torchrun), every rank advances its own lattice of the same
+size (independent runs, weak scaling, no collective on the data path); time
+is the max over ranks.
+
+--impl reference times the reference's own OpenMP build of the same step
+(oracle/_ref, compiled from the reference sources) on the host cores, on a
+bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "site-updates/s"
+UNIT = "site-updates/s"
+NINFO = 100
+
+LYO_C1 = dict(GammaQ=0.3, GammaP=0.1, xi=0.7, tauNem=1.5, tauIso=1.5, rho=40.0,
+              friction=0.0, AA=0.1, CC=0.1, LL=0.05, KK=0.05, zeta=0.01,
+              zetaI=0.0, conc=1.0, npc=1)
+NEM_C2 = dict(Gamma=0.3, xi=0.7, tau=1.5, rho=40.0, friction=0.0, CC=0.1,
+              LL=0.05, zeta=0.02, npc=1)
+
+
+def algorithmic_bytes(model: str, precision: str) -> int:
+    """Primary state read once and written once per site-update:
+    (9 populations + Qxx + Qyx [+ phi]) x 2 x element size."""
+    planes = 12 if model == "lyotropic" else 11
+    return planes * 2 * (4 if precision == "fp32" else 8)
+
+
+def measured_hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_per_site(model: str, precision: str):
+    """DRAM bytes per site-update of the fused kernel from the committed ncu
+    summary (profiles/fused_step_traffic.json), or None."""
+    path = os.path.join(ROOT, "profiles", "fused_step_traffic.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d[f"{model}_{precision}"]["dram_bytes_per_site"])
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def synthetic_state(model: str, L: int, seed: int):
+    from oracle.oracle import LYOTROPIC, NEMATIC, synthetic_state as st
+    return st(LYOTROPIC if model == "lyotropic" else NEMATIC, L, L, seed=seed,
+              radius=L / 4)
+
+
+def pinned_copy(a: np.ndarray):
+    import torch
+    t = torch.empty(a.size, dtype=torch.float64, pin_memory=True)
+    out = t.numpy()
+    out[:] = a.reshape(-1)
+    return out, t
+
+
+def dist_setup(n: int):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        import torch
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return rank, world, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_reference_run(model: str, L: int, steps: int, warmup: int, budget_s: float):
+    """Time the reference's own build (oracle/_ref) or, if that library is
+    absent, the C restatement, on all host cores. Returns (site-updates/s,
+    kind, cores, sample description)."""
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    mcode = O.LYOTROPIC if model == "lyotropic" else O.NEMATIC
+    params = LYO_C1 if model == "lyotropic" else NEM_C2
+    # the reference keeps ~550 bytes per site; shrink the lattice if the
+    # host cannot hold it
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+    except Exception:
+        avail = 64 << 30
+    Ls = L
+    while Ls > 256 and Ls * Ls * 600 > 0.5 * avail:
+        Ls //= 2
+    st = synthetic_state(model, Ls, seed=1)
+    if O.ref_available():
+        m = O.RefOracle(mcode, params, Ls, Ls, 0)
+        for k, v in st.items():
+            m.set(k, v)
+        kind, threads = "reference", cores
+        run = lambda n: m.time_steps(n, threads)
+    else:
+        m = O.PortOracle(mcode, params, Ls, Ls, 0)
+        for k, v in st.items():
+            m.set(k, v)
+        kind, threads = "port", 1
+
+        def run(n):
+            t0 = time.perf_counter()
+            m.step(n)
+            return time.perf_counter() - t0
+    for _ in range(warmup):
+        run(1)
+    times = []
+    t_start = time.perf_counter()
+    for _ in range(steps):
+        times.append(run(1))
+        if time.perf_counter() - t_start > budget_s:
+            break
+    per_step = statistics.median(times)
+    rate = Ls * Ls / per_step
+    sample = (f"{model} {Ls}x{Ls} periodic FP64, {len(times)} timed Step() calls "
+              f"after {warmup} warm-up, median step {per_step:.3f} s")
+    return rate, kind, threads, sample
+
+
+def run_reference(args):
+    rank, world, _ = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), 0
+    if rank != 0:
+        return 0
+    rate, kind, cores, sample = cpu_reference_run(args.model, args.size, args.steps,
+                                                  max(1, min(args.warmup, 2)), 240.0)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded)",
+        "config": {"workload": f"{args.model} {args.size}x{args.size} periodic", "model": args.model,
+                   "LX": args.size, "LY": args.size, "precision": "fp64 (reference build)"},
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+
+    import mass_hd_b200 as M
+
+    rank, world, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    model = args.model
+    mcode = M.LYOTROPIC if model == "lyotropic" else M.NEMATIC
+    params = LYO_C1 if model == "lyotropic" else NEM_C2
+    prec = M.FP32 if args.precision == "fp32" else M.FP64
+    L = args.size
+    sites = L * L
+
+    st = synthetic_state(model, L, seed=1 + rank)
+    lat = M.Lattice(mcode, params, L, L, 0, prec)
+    lat.upload_state(st)
+    stream = torch.cuda.ExternalStream(lat.stream)
+
+    # warm-up (also runs the tile autotuner before the first step)
+    for _ in range(max(args.warmup, 3)):
+        lat.step(1)
+    lat.synchronize()
+
+    sampler = ClockSampler(local) if rank == 0 else None
+    barrier(world)
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        lat.step(1)
+    e1.record(stream)
+    e1.synchronize()
+    lat.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = e0.elapsed_time(e1)
+    clocks = sampler.stop() if sampler else None
+    ms = max_over_ranks(ms, world)
+    ms_per_step = ms / args.steps
+    value = sites * world / (ms_per_step / 1e3)
+    launches = args.steps * lat.launches_per_step
+
+    # roofline of the dominant kernel (one fused launch per step)
+    bps = algorithmic_bytes(model, args.precision)
+    peak, peak_kind = measured_hbm_peak()
+    achieved = sites * bps / (ms_per_step / 1e3) / 1e9
+    tps = traffic_per_site(model, args.precision)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind,
+                "bytes_per_site": bps,
+                "traffic": (tps * sites if tps is not None else None)}
+
+    # end-to-end through the C ABI with pinned host buffers
+    e2e = None
+    host = {}
+    keep = []
+    for k in (("ff", "QQxx", "QQyx", "phi") if model == "lyotropic" else ("ff", "QQxx", "QQyx")):
+        arr, t = pinned_copy(st[k])
+        host[k] = arr
+        keep.append(t)
+    outs = {}
+    for k, a in host.items():
+        o, t = pinned_copy(np.zeros_like(a))
+        outs[k] = o
+        keep.append(t)
+    h2d = sum(a.nbytes for a in host.values())
+    d2h = sum(a.nbytes for a in outs.values())
+
+    def e2e_step():
+        lat.upload(host["ff"], host["QQxx"], host["QQyx"], host.get("phi"))
+        lat.step(NINFO)
+        for k, o in outs.items():
+            lat.get_into(k, o)
+
+    e2e_step()     # warm-up
+    n_e2e = 3
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
+        e2e_step()
+    dt = time.perf_counter() - t0
+    dt = max_over_ranks(dt, world)
+    e2e = {"value": sites * NINFO * n_e2e * world / dt, "unit": UNIT,
+           "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+           "steps_per_e2e_step": NINFO, "e2e_steps": n_e2e,
+           "note": "per e2e step: upload state from pinned host memory, 100 Step() calls, "
+                   "download ff/QQxx/QQyx/phi; host wall clock around synchronous C-ABI calls"}
+    launches_e2e = n_e2e * NINFO * lat.launches_per_step
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, kind, cores, sample = cpu_reference_run(model, L, 5, 1, 20.0)
+        cpu = {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+
+    tile = list(lat.tile()) if lat.uses_fused else None
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.precision == "fp32" else "f64",
+            "data": "synthetic (seeded random director S=1, tanh phi disk R=L/4)",
+            "config": {"workload": f"{model} {args.precision.upper()} {L}x{L} periodic, "
+                                   f"256^2-config physics, npc=1",
+                       "model": model, "LX": L, "LY": L, "precision": args.precision,
+                       "lattices": world,
+                       "parallelism": "independent lattice per GPU" if world > 1 else "single GPU",
+                       "l2": f"state {sites * bps // 2 / 1e6:.0f} MB per buffer > 126 MB L2, no flush",
+                       "tile": tile},
+            "gpu_launches": launches,
+            "gpu_launches_e2e": launches_e2e,
+            "roofline": roofline,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    lat.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--size", type=int, default=4096)
+    ap.add_argument("--model", default="lyotropic", choices=["lyotropic", "nematic"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

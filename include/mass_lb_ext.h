@@ -1,0 +1,44 @@
+/* mass_lb_ext.h - entry points of the sm_100a MASS step library that have
+ * no counterpart in the reference (the reference is a CPU-only program with
+ * no FFI): tile tuning of the fused FP32 kernel and introspection. They
+ * extend the handle API of mass_lb.h and follow its conventions (0 or a
+ * negative mass_lb_status, text in mass_lb_last_error()). */
+#ifndef MASS_LB_EXT_H_
+#define MASS_LB_EXT_H_
+
+#include "mass_lb.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Upload one primary field (MASS_LB_FF, QQXX, QQYX or PHI) from host memory,
+ * same layout as mass_lb_upload. Does not reset the recorded totals. */
+int mass_lb_upload_field(mass_lb_handle* h, int field, const double* src);
+
+/* Tile of the fused FP32 kernel: `threads` lattice columns per CTA strip
+ * (64, 128 or 256; NT - 8 of them are output columns) and `rows` lattice
+ * rows per CTA chunk. set_tile(h, 0, 0) re-enables the autotuner, which
+ * otherwise runs once before the first step (timing every candidate tile on
+ * the live state without advancing it). The environment variable
+ * MASS_LB_TILE="threads,rows" fixes the tile at handle creation.
+ * EUNSUPPORTED when the handle does not use the fused kernel. */
+int mass_lb_get_tile(mass_lb_handle* h, int* threads, int* rows);
+int mass_lb_set_tile(mass_lb_handle* h, int threads, int rows);
+int mass_lb_autotune(mass_lb_handle* h);
+
+/* 1 if mass_lb_step runs the fused FP32 kernel (FP32, periodic lattice,
+ * npc = 1, LY % 4 == 0, LY >= 64), else 0. */
+int mass_lb_uses_fused(mass_lb_handle* h);
+
+/* Device view of the fused FP32 state (read-only for the caller): `*planes`
+ * receives the base of NP float planes of LX*LY values each (g0..g8 as
+ * deviations from t_v*rho, then Qxx, Qyx and, for lyotropic, phi), valid
+ * until the next mass_lb_step / upload call. */
+int mass_lb_device_state(mass_lb_handle* h, void** planes, long long* plane_stride,
+                         int* nplanes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,778 @@
+// C ABI (include/mass_lb.h): handle lifetime, host <-> device transfers,
+// step dispatch (FP64 unfused / FP32 fused / FP32 unfused for walls), the
+// fused-kernel autotuner and the runtime-check reductions.
+#include "mass_lb.h"
+#include "mass_lb_ext.h"
+
+#include "lb_common.cuh"
+#include "unfused.h"
+#include "fused32.cuh"
+#include "reduce.cuh"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace mlb;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg)
+{
+  g_err = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where)
+{
+  return fail(MASS_LB_ECUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CU(call, where) do { const cudaError_t e_ = (call); \
+  if(e_ != cudaSuccess) return cuda_fail(e_, where); } while(0)
+
+const char* kFieldNames[MASS_LB_NUM_FIELDS] = {
+  "ff", "QQxx", "QQyx", "phi", "n", "ux", "uy", "ux_phi", "uy_phi", "HHxx",
+  "HHyx", "MU", "dxQQxx", "dyQQxx", "dxQQyx", "dyQQyx", "sigmaXX", "sigmaYY",
+  "sigmaYX", "sigmaXY", "sigma_bulk", "sigma_elastic_xx", "sigma_elastic_yx",
+  "sigma_phase_field_xx", "sigma_phase_field_yx", "sigma_active_xx",
+  "sigma_active_yx", "fn", "QNxx", "QNyx", "phn"};
+
+constexpr long long kStageSites = 1ll << 22;   // sites per transfer chunk
+
+// --------------------------------------------------------------------------
+// host <-> device conversion kernels (one chunk of whole rows at a time)
+
+// host AoS doubles [k][v] (k relative to chunk start) -> device planes
+template<typename T>
+__global__ void k_put_ff(const double* __restrict__ st, T* ff, long long plane,
+                         int x0, int nrows, int LY, int g, int EY, double rest)
+{
+  const long long n = static_cast<long long>(nrows)*LY;
+  for(long long k = blockIdx.x*256ll + threadIdx.x; k < n; k += 256ll*gridDim.x)
+  {
+    const int x = x0 + static_cast<int>(k / LY), y = static_cast<int>(k % LY);
+    const long long e = (y + g) + static_cast<long long>(EY)*(x + g);
+#pragma unroll
+    for(int v = 0; v < 9; ++v)
+      ff[v*plane + e] = static_cast<T>(st[9*k + v] - Tv(v)*rest);
+  }
+}
+
+template<typename T>
+__global__ void k_get_ff(double* __restrict__ st, const T* ff, long long plane,
+                         int x0, int nrows, int LY, int g, int EY, double rest)
+{
+  const long long n = static_cast<long long>(nrows)*LY;
+  for(long long k = blockIdx.x*256ll + threadIdx.x; k < n; k += 256ll*gridDim.x)
+  {
+    const int x = x0 + static_cast<int>(k / LY), y = static_cast<int>(k % LY);
+    const long long e = (y + g) + static_cast<long long>(EY)*(x + g);
+#pragma unroll
+    for(int v = 0; v < 9; ++v)
+      st[9*k + v] = static_cast<double>(ff[v*plane + e]) + Tv(v)*rest;
+  }
+}
+
+template<typename T>
+__global__ void k_put_scalar(const double* __restrict__ st, T* a, int x0, int nrows,
+                             int LY, int g, int EY)
+{
+  const long long n = static_cast<long long>(nrows)*LY;
+  for(long long k = blockIdx.x*256ll + threadIdx.x; k < n; k += 256ll*gridDim.x)
+  {
+    const int x = x0 + static_cast<int>(k / LY), y = static_cast<int>(k % LY);
+    a[(y + g) + static_cast<long long>(EY)*(x + g)] = static_cast<T>(st[k]);
+  }
+}
+
+template<typename T>
+__global__ void k_get_scalar(double* __restrict__ st, const T* a, int x0, int nrows,
+                             int LY, int g, int EY, double add)
+{
+  const long long n = static_cast<long long>(nrows)*LY;
+  for(long long k = blockIdx.x*256ll + threadIdx.x; k < n; k += 256ll*gridDim.x)
+  {
+    const int x = x0 + static_cast<int>(k / LY), y = static_cast<int>(k % LY);
+    st[k] = static_cast<double>(a[(y + g) + static_cast<long long>(EY)*(x + g)]) + add;
+  }
+}
+
+inline int blocks_for(long long n)
+{
+  long long b = (n + 255)/256;
+  return static_cast<int>(std::min<long long>(std::max<long long>(b, 1), 4096));
+}
+
+} // namespace
+
+// --------------------------------------------------------------------------
+
+struct mass_lb_handle
+{
+  int device = 0;
+  int precision = MASS_LB_FP64;
+  int model = LYO;
+  unsigned LX = 0, LY = 0, bc = 0;
+  int wall = 0;              // 1 if the lattice carries a ghost ring
+  Params P{};
+  Dims d{};
+  cudaStream_t stream = nullptr;
+  bool fused = false;
+
+  State<double> s64{};       // FP64 (any bc)
+  State<float> s32{};        // FP32 with walls
+  std::vector<void*> allocs;
+
+  // FP32 fused periodic state: NP planes each, ping-pong
+  float* cur = nullptr;
+  float* nxt = nullptr;
+  float* diag = nullptr;     // NDIAG planes, allocated on first use
+  bool has_prev = false;     // nxt holds the state before the last step
+  FusedConfig cfg{128, 256};
+  bool tuned = false;
+
+  double* stage = nullptr;   // device staging (kStageSites*9 doubles)
+  double* red_scratch = nullptr;
+  double* red_out = nullptr; // 3 doubles
+  int* err = nullptr;
+
+  double ftot = 0, ptot = 0;
+  unsigned long long steps = 0;
+};
+
+namespace {
+
+struct DeviceGuard
+{
+  int prev = -1;
+  explicit DeviceGuard(int dev)
+  {
+    cudaGetDevice(&prev);
+    if(prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard()
+  {
+    int now = -1;
+    cudaGetDevice(&now);
+    if(prev >= 0 && now != prev) cudaSetDevice(prev);
+  }
+};
+
+template<typename T>
+int dalloc(mass_lb_handle* h, T** p, size_t n)
+{
+  void* q = nullptr;
+  const cudaError_t e = cudaMalloc(&q, n*sizeof(T) > 0 ? n*sizeof(T) : 1);
+  if(e != cudaSuccess)
+  {
+    cudaGetLastError();
+    return fail(MASS_LB_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  }
+  h->allocs.push_back(q);
+  *p = static_cast<T*>(q);
+  return 0;
+}
+
+int nplanes(const mass_lb_handle* h) { return h->model == LYO ? 12 : 11; }
+
+template<typename T>
+int alloc_state(mass_lb_handle* h, State<T>& s)
+{
+  const size_t NE = static_cast<size_t>(h->d.NE);
+  T** lb[4] = {&s.ff, &s.fn, &s.ff_tmp, &s.fn_tmp};
+  for(auto p : lb) if(int r = dalloc(h, p, 9*NE)) return r;
+  std::vector<T**> sc = {&s.Qxx, &s.Qyx, &s.QNxx, &s.QNyx, &s.n, &s.ux, &s.uy,
+                         &s.Hxx, &s.Hyx, &s.dxQxx, &s.dyQxx, &s.dxQyx, &s.dyQyx,
+                         &s.sXX, &s.sYY, &s.sYX, &s.sXY};
+  if(h->model == LYO)
+  {
+    T** extra[6] = {&s.phi, &s.phn, &s.phi_tmp, &s.uxp, &s.uyp, &s.MU};
+    for(int i = 0; i < 6; ++i) sc.push_back(extra[i]);
+    for(int i = 0; i < 7; ++i) sc.push_back(&s.diag[i]);
+  }
+  for(auto p : sc) if(int r = dalloc(h, p, NE)) return r;
+  return 0;
+}
+
+template<typename T>
+int zero_state(mass_lb_handle* h, State<T>& s)
+{
+  const size_t NE = static_cast<size_t>(h->d.NE);
+  T* lb[4] = {s.ff, s.fn, s.ff_tmp, s.fn_tmp};
+  for(T* p : lb) CU(cudaMemsetAsync(p, 0, 9*NE*sizeof(T), h->stream), "memset");
+  std::vector<T*> sc = {s.Qxx, s.Qyx, s.QNxx, s.QNyx, s.n, s.ux, s.uy, s.Hxx, s.Hyx,
+                        s.dxQxx, s.dyQxx, s.dxQyx, s.dyQyx, s.sXX, s.sYY, s.sYX, s.sXY};
+  if(h->model == LYO)
+  {
+    T* extra[6] = {s.phi, s.phn, s.phi_tmp, s.uxp, s.uyp, s.MU};
+    for(int i = 0; i < 6; ++i) sc.push_back(extra[i]);
+    for(int i = 0; i < 7; ++i) sc.push_back(s.diag[i]);
+  }
+  for(T* p : sc) CU(cudaMemsetAsync(p, 0, NE*sizeof(T), h->stream), "memset");
+  return 0;
+}
+
+FusedArgs fused_args(mass_lb_handle* h, const float* in, float* out, bool diag)
+{
+  FusedArgs a{};
+  a.in = in;
+  a.out = out;
+  a.diag = diag ? h->diag : nullptr;
+  a.err = h->err;
+  a.LX = static_cast<int>(h->LX);
+  a.LY = static_cast<int>(h->LY);
+  a.plane = static_cast<long long>(h->LX)*h->LY;
+  const Params& P = h->P;
+  a.p = P32{static_cast<float>(P.rho), static_cast<float>(P.GammaQ),
+            static_cast<float>(P.GammaP), static_cast<float>(P.xi),
+            static_cast<float>(P.tauNem), static_cast<float>(P.tauIso),
+            static_cast<float>(P.friction), static_cast<float>(P.AA),
+            static_cast<float>(P.CC), static_cast<float>(P.LL),
+            static_cast<float>(P.KK), static_cast<float>(P.zeta),
+            static_cast<float>(P.zetaI), static_cast<float>(P.conc)};
+  return a;
+}
+
+int check_err_flag(mass_lb_handle* h)
+{
+  int e = 0;
+  CU(cudaMemcpyAsync(&e, h->err, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "err flag");
+  CU(cudaStreamSynchronize(h->stream), "sync");
+  if(e) return fail(MASS_LB_ECUDA, "fused step: a bounded wait on a bulk copy timed out");
+  return 0;
+}
+
+// Candidate tiles for the autotuner: strip widths that fit the lattice and
+// chunk heights from 32 rows to the whole lattice.
+std::vector<FusedConfig> tile_candidates(const mass_lb_handle* h)
+{
+  std::vector<FusedConfig> c;
+  for(int nt : {32, 64, 128, 256})
+  {
+    if(!fused_supported(static_cast<int>(h->LX), static_cast<int>(h->LY), nt)) continue;
+    for(int rows : {32, 64, 128, 256, 512, 1024})
+    {
+      if(rows > static_cast<int>(h->LX) && rows != 32) continue;
+      c.push_back(FusedConfig{nt, std::min(rows, static_cast<int>(h->LX))});
+    }
+  }
+  return c;
+}
+
+int autotune(mass_lb_handle* h)
+{
+  const auto cands = tile_candidates(h);
+  if(cands.empty()) return fail(MASS_LB_EUNSUPPORTED, "no fused tile fits this lattice");
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0), "event");
+  CU(cudaEventCreate(&e1), "event");
+  float best = 1e30f;
+  FusedConfig bestc = cands.front();
+  // time cur -> nxt without swapping: the state is not advanced
+  for(const FusedConfig& c : cands)
+  {
+    const FusedArgs a = fused_args(h, h->cur, h->nxt, false);
+    if(launch_fused_step(a, h->model, c, false, h->stream) != cudaSuccess) continue;
+    CU(cudaEventRecord(e0, h->stream), "event");
+    const int reps = 3;
+    for(int r = 0; r < reps; ++r) launch_fused_step(a, h->model, c, false, h->stream);
+    CU(cudaEventRecord(e1, h->stream), "event");
+    CU(cudaEventSynchronize(e1), "event sync");
+    float ms = 0;
+    CU(cudaEventElapsedTime(&ms, e0, e1), "event time");
+    if(std::getenv("MASS_LB_TUNE_LOG"))
+      std::fprintf(stderr, "mass_lb autotune: threads %d rows %d: %.4f ms/step\n",
+                   c.nt, c.rows, ms/reps);
+    if(ms < best) { best = ms; bestc = c; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  h->cfg = bestc;
+  h->tuned = true;
+  h->has_prev = false;   // nxt was used as scratch
+  if(int r = check_err_flag(h)) return r;
+  return 0;
+}
+
+int ensure_diag_buffer(mass_lb_handle* h)
+{
+  if(h->diag) return 0;
+  return dalloc(h, &h->diag, static_cast<size_t>(NDIAG)*h->LX*h->LY);
+}
+
+} // namespace
+
+// ==========================================================================
+
+extern "C" {
+
+int mass_lb_abi_version(void) { return MASS_LB_ABI_VERSION; }
+
+const char* mass_lb_last_error(void) { return g_err.c_str(); }
+
+const char* mass_lb_field_name(int field)
+{
+  if(field < 0 || field >= MASS_LB_NUM_FIELDS) return nullptr;
+  return kFieldNames[field];
+}
+
+int mass_lb_create(const mass_lb_params* params, unsigned LX, unsigned LY,
+                   unsigned bc, int precision, mass_lb_handle** out)
+{
+  if(!params || !out) return fail(MASS_LB_EINVAL, "null argument");
+  *out = nullptr;
+  if(LX == 0 || LY == 0) return fail(MASS_LB_EINVAL, "empty lattice");
+  if(params->model != MASS_LB_LYOTROPIC && params->model != MASS_LB_NEMATIC)
+    return fail(MASS_LB_EINVAL, "unknown model");
+  if(precision != MASS_LB_FP64 && precision != MASS_LB_FP32)
+    return fail(MASS_LB_EINVAL, "unknown precision");
+  if(params->npc < 1) return fail(MASS_LB_EINVAL, "npc must be >= 1");
+  int ndev = 0;
+  if(cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+  {
+    cudaGetLastError();
+    return fail(MASS_LB_ENODEV, "no CUDA device");
+  }
+  int dev = 0;
+  CU(cudaGetDevice(&dev), "cudaGetDevice");
+  cudaDeviceProp prop;
+  CU(cudaGetDeviceProperties(&prop, dev), "cudaGetDeviceProperties");
+  if(prop.major != 10)
+    return fail(MASS_LB_ENODEV, "this library is built for sm_100a (B200) only");
+
+  auto* h = new mass_lb_handle();
+  h->device = dev;
+  h->precision = precision;
+  h->model = params->model;
+  h->LX = LX; h->LY = LY;
+  h->bc = bc;
+  // Which bc values carry walls: lyotropic 1..4 (src/models/lyotropic.cpp:388-498),
+  // nematic 1 (src/models/nematic.cpp:259-368). Every other non-zero value is
+  // the periodic ghost layer, which computes exactly what bc = 0 computes.
+  h->wall = (h->model == LYO) ? (bc >= 1 && bc <= 4) : (bc == 1);
+  if(h->wall && (LX < 2 || LY < 2))
+  {
+    delete h;
+    return fail(MASS_LB_EINVAL, "wall boundaries need LX, LY >= 2");
+  }
+  std::memcpy(&h->P, params, sizeof(Params));
+  static_assert(sizeof(Params) == sizeof(mass_lb_params), "param layout");
+  const int g = h->wall ? 1 : 0;
+  h->d = Dims{static_cast<int>(LX), static_cast<int>(LY), g,
+              static_cast<int>(LX) + 2*g, static_cast<int>(LY) + 2*g,
+              static_cast<long long>(LX + 2*g)*(LY + 2*g)};
+
+  auto bail = [&](int r) { mass_lb_destroy(h); return r; };
+  if(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(fail(MASS_LB_ECUDA, "stream create"));
+
+  if(int r = dalloc(h, &h->err, 1)) return bail(r);
+  if(int r = dalloc(h, &h->red_scratch, sums_scratch_doubles())) return bail(r);
+  if(int r = dalloc(h, &h->red_out, 3)) return bail(r);
+  const long long stage_sites = std::min<long long>(kStageSites, static_cast<long long>(LX)*LY);
+  if(int r = dalloc(h, &h->stage, 9*stage_sites)) return bail(r);
+
+  if(precision == MASS_LB_FP64)
+  {
+    if(int r = alloc_state(h, h->s64)) return bail(r);
+    if(int r = zero_state(h, h->s64)) return bail(r);
+  }
+  else
+  {
+    h->fused = !h->wall && h->P.npc == 1 &&
+               fused_supported(static_cast<int>(LX), static_cast<int>(LY), 64);
+    if(h->fused)
+    {
+      const size_t n = static_cast<size_t>(nplanes(h))*LX*LY;
+      if(int r = dalloc(h, &h->cur, n)) return bail(r);
+      if(int r = dalloc(h, &h->nxt, n)) return bail(r);
+      if(cudaMemsetAsync(h->cur, 0, n*sizeof(float), h->stream) != cudaSuccess ||
+         cudaMemsetAsync(h->nxt, 0, n*sizeof(float), h->stream) != cudaSuccess)
+        return bail(fail(MASS_LB_ECUDA, "memset"));
+      if(const char* env = std::getenv("MASS_LB_TILE"))
+      {
+        int nt = 0, rows = 0;
+        if(std::sscanf(env, "%d,%d", &nt, &rows) == 2 &&
+           fused_supported(static_cast<int>(LX), static_cast<int>(LY), nt) && rows > 0)
+        {
+          h->cfg = FusedConfig{nt, rows};
+          h->tuned = true;
+        }
+      }
+      if(!h->tuned)
+      {
+        // a width that always fits; the autotuner refines it on the first step
+        h->cfg = FusedConfig{LY >= 128 ? 128 : 64, static_cast<int>(std::min(LX, 256u))};
+      }
+    }
+    else
+    {
+      if(int r = alloc_state(h, h->s32)) return bail(r);
+      if(int r = zero_state(h, h->s32)) return bail(r);
+    }
+  }
+  if(cudaMemsetAsync(h->err, 0, sizeof(int), h->stream) != cudaSuccess ||
+     cudaStreamSynchronize(h->stream) != cudaSuccess)
+    return bail(fail(MASS_LB_ECUDA, "init"));
+  *out = h;
+  return MASS_LB_OK;
+}
+
+void mass_lb_destroy(mass_lb_handle* h)
+{
+  if(!h) return;
+  DeviceGuard g(h->device);
+  if(h->stream) cudaStreamSynchronize(h->stream);
+  for(void* p : h->allocs) cudaFree(p);
+  if(h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+static int put_field(mass_lb_handle* h, int field, const double* src)
+{
+  const int LY = static_cast<int>(h->LY);
+  const long long rows_per = std::max<long long>(1, kStageSites/LY);
+  const bool f64 = h->precision == MASS_LB_FP64;
+  const bool isff = field == MASS_LB_FF;
+  const int comps = isff ? 9 : 1;
+  const double rest = f64 ? 0.0 : h->P.rho;
+  for(long long x0 = 0; x0 < h->LX; x0 += rows_per)
+  {
+    const int nrows = static_cast<int>(std::min<long long>(rows_per, h->LX - x0));
+    const long long n = static_cast<long long>(nrows)*LY;
+    CU(cudaMemcpyAsync(h->stage, src + x0*LY*comps, n*comps*sizeof(double),
+                       cudaMemcpyHostToDevice, h->stream), "upload copy");
+    const int nb = blocks_for(n);
+    if(h->fused)
+    {
+      const long long plane = static_cast<long long>(h->LX)*h->LY;
+      float* base = h->cur;
+      if(isff)
+        k_put_ff<float><<<nb, 256, 0, h->stream>>>(h->stage, base, plane, x0, nrows, LY, 0, LY, rest);
+      else
+      {
+        const int p = field == MASS_LB_QQXX ? 9 : field == MASS_LB_QQYX ? 10 : 11;
+        k_put_scalar<float><<<nb, 256, 0, h->stream>>>(h->stage, base + p*plane, x0, nrows, LY, 0, LY);
+      }
+    }
+    else if(f64)
+    {
+      State<double>& s = h->s64;
+      double* a = field == MASS_LB_QQXX ? s.Qxx : field == MASS_LB_QQYX ? s.Qyx : s.phi;
+      if(isff) k_put_ff<double><<<nb, 256, 0, h->stream>>>(h->stage, s.ff, h->d.NE, x0, nrows, LY, h->d.g, h->d.EY, 0.0);
+      else k_put_scalar<double><<<nb, 256, 0, h->stream>>>(h->stage, a, x0, nrows, LY, h->d.g, h->d.EY);
+    }
+    else
+    {
+      State<float>& s = h->s32;
+      float* a = field == MASS_LB_QQXX ? s.Qxx : field == MASS_LB_QQYX ? s.Qyx : s.phi;
+      if(isff) k_put_ff<float><<<nb, 256, 0, h->stream>>>(h->stage, s.ff, h->d.NE, x0, nrows, LY, h->d.g, h->d.EY, rest);
+      else k_put_scalar<float><<<nb, 256, 0, h->stream>>>(h->stage, a, x0, nrows, LY, h->d.g, h->d.EY);
+    }
+    CU(cudaGetLastError(), "upload kernel");
+  }
+  return 0;
+}
+
+int mass_lb_upload_field(mass_lb_handle* h, int field, const double* src)
+{
+  if(!h || !src) return fail(MASS_LB_EINVAL, "null argument");
+  if(field != MASS_LB_FF && field != MASS_LB_QQXX && field != MASS_LB_QQYX && field != MASS_LB_PHI)
+    return fail(MASS_LB_EINVAL, "only ff, QQxx, QQyx, phi can be uploaded");
+  if(field == MASS_LB_PHI && h->model != LYO)
+    return fail(MASS_LB_EUNSUPPORTED, "the nematic model has no phi");
+  DeviceGuard g(h->device);
+  if(int r = put_field(h, field, src)) return r;
+  h->has_prev = false;
+  CU(cudaStreamSynchronize(h->stream), "upload sync");
+  return 0;
+}
+
+int mass_lb_upload(mass_lb_handle* h, const double* ff, const double* QQxx,
+                   const double* QQyx, const double* phi)
+{
+  if(!h || !ff || !QQxx || !QQyx) return fail(MASS_LB_EINVAL, "null argument");
+  if(h->model == LYO && !phi) return fail(MASS_LB_EINVAL, "lyotropic needs phi");
+  DeviceGuard g(h->device);
+  if(int r = put_field(h, MASS_LB_FF, ff)) return r;
+  if(int r = put_field(h, MASS_LB_QQXX, QQxx)) return r;
+  if(int r = put_field(h, MASS_LB_QQYX, QQyx)) return r;
+  if(h->model == LYO)
+    if(int r = put_field(h, MASS_LB_PHI, phi)) return r;
+  h->has_prev = false;
+  h->steps = 0;
+  // reference totals (ftot, ptot), as Configure() accumulates them
+  double fs = 0, ps = 0;
+  int bad = 0;
+  if(int r = mass_lb_checks(h, &fs, &ps, &bad)) return r;
+  h->ftot = fs;
+  h->ptot = ps;
+  return 0;
+}
+
+int mass_lb_step(mass_lb_handle* h, unsigned nsteps)
+{
+  if(!h) return fail(MASS_LB_EINVAL, "null handle");
+  if(nsteps == 0) return 0;
+  DeviceGuard g(h->device);
+  if(h->precision == MASS_LB_FP64)
+  {
+    if(step_unfused_f64(h->d, h->P, h->s64, h->wall ? static_cast<int>(h->bc) : 0,
+                        nsteps, true, h->stream) != 0)
+      return cuda_fail(cudaGetLastError(), "fp64 step");
+  }
+  else if(!h->fused)
+  {
+    if(step_unfused_f32(h->d, h->P, h->s32, h->wall ? static_cast<int>(h->bc) : 0,
+                        nsteps, true, h->stream) != 0)
+      return cuda_fail(cudaGetLastError(), "fp32 step");
+  }
+  else
+  {
+    if(!h->tuned)
+      if(int r = autotune(h)) return r;
+    for(unsigned i = 0; i < nsteps; ++i)
+    {
+      const FusedArgs a = fused_args(h, h->cur, h->nxt, false);
+      CU(launch_fused_step(a, h->model, h->cfg, false, h->stream), "fused step");
+      std::swap(h->cur, h->nxt);
+    }
+    h->has_prev = true;
+  }
+  h->steps += nsteps;
+  return 0;
+}
+
+static int get_primary(mass_lb_handle* h, int field, double* out)
+{
+  const int LY = static_cast<int>(h->LY);
+  const long long rows_per = std::max<long long>(1, kStageSites/LY);
+  const bool isff = field == MASS_LB_FF || field == MASS_LB_FN;
+  const int comps = isff ? 9 : 1;
+  for(long long x0 = 0; x0 < h->LX; x0 += rows_per)
+  {
+    const int nrows = static_cast<int>(std::min<long long>(rows_per, h->LX - x0));
+    const long long n = static_cast<long long>(nrows)*LY;
+    const int nb = blocks_for(n);
+    if(h->fused)
+    {
+      const long long plane = static_cast<long long>(h->LX)*h->LY;
+      if(field <= MASS_LB_PHI)
+      {
+        if(isff) k_get_ff<float><<<nb, 256, 0, h->stream>>>(h->stage, h->cur, plane, x0, nrows, LY, 0, LY, h->P.rho);
+        else
+        {
+          const int p = field == MASS_LB_QQXX ? 9 : field == MASS_LB_QQYX ? 10 : 11;
+          k_get_scalar<float><<<nb, 256, 0, h->stream>>>(h->stage, h->cur + p*plane, x0, nrows, LY, 0, LY, 0.0);
+        }
+      }
+      else
+      {
+        // derived fields from the replayed diagnostics, mass_lb_field order
+        const int p = field - MASS_LB_N;
+        k_get_scalar<float><<<nb, 256, 0, h->stream>>>(h->stage, h->diag + p*plane, x0, nrows, LY, 0, LY, 0.0);
+      }
+    }
+    else if(h->precision == MASS_LB_FP64)
+    {
+      State<double>& s = h->s64;
+      const Dims& d = h->d;
+      const double* a = nullptr;
+      switch(field)
+      {
+        case MASS_LB_QQXX: a = s.Qxx; break;  case MASS_LB_QQYX: a = s.Qyx; break;
+        case MASS_LB_PHI: a = s.phi; break;   case MASS_LB_N: a = s.n; break;
+        case MASS_LB_UX: a = s.ux; break;     case MASS_LB_UY: a = s.uy; break;
+        case MASS_LB_UX_PHI: a = s.uxp; break; case MASS_LB_UY_PHI: a = s.uyp; break;
+        case MASS_LB_HHXX: a = s.Hxx; break;  case MASS_LB_HHYX: a = s.Hyx; break;
+        case MASS_LB_MU: a = s.MU; break;
+        case MASS_LB_DXQQXX: a = s.dxQxx; break; case MASS_LB_DYQQXX: a = s.dyQxx; break;
+        case MASS_LB_DXQQYX: a = s.dxQyx; break; case MASS_LB_DYQQYX: a = s.dyQyx; break;
+        case MASS_LB_SIGMAXX: a = s.sXX; break; case MASS_LB_SIGMAYY: a = s.sYY; break;
+        case MASS_LB_SIGMAYX: a = s.sYX; break; case MASS_LB_SIGMAXY: a = s.sXY; break;
+        case MASS_LB_QNXX: a = s.QNxx; break; case MASS_LB_QNYX: a = s.QNyx; break;
+        case MASS_LB_PHN: a = s.phn; break;
+        default:
+          if(field >= MASS_LB_SIGMA_BULK && field <= MASS_LB_SIGMA_ACTIVE_YX)
+            a = s.diag[field - MASS_LB_SIGMA_BULK];
+      }
+      if(field == MASS_LB_FF) k_get_ff<double><<<nb, 256, 0, h->stream>>>(h->stage, s.ff, d.NE, x0, nrows, LY, d.g, d.EY, 0.0);
+      else if(field == MASS_LB_FN) k_get_ff<double><<<nb, 256, 0, h->stream>>>(h->stage, s.fn, d.NE, x0, nrows, LY, d.g, d.EY, 0.0);
+      else k_get_scalar<double><<<nb, 256, 0, h->stream>>>(h->stage, a, x0, nrows, LY, d.g, d.EY, 0.0);
+    }
+    else
+    {
+      State<float>& s = h->s32;
+      const Dims& d = h->d;
+      const float* a = nullptr;
+      double add = 0.0;
+      switch(field)
+      {
+        case MASS_LB_QQXX: a = s.Qxx; break;  case MASS_LB_QQYX: a = s.Qyx; break;
+        case MASS_LB_PHI: a = s.phi; break;   case MASS_LB_N: a = s.n; add = h->P.rho; break;
+        case MASS_LB_UX: a = s.ux; break;     case MASS_LB_UY: a = s.uy; break;
+        case MASS_LB_UX_PHI: a = s.uxp; break; case MASS_LB_UY_PHI: a = s.uyp; break;
+        case MASS_LB_HHXX: a = s.Hxx; break;  case MASS_LB_HHYX: a = s.Hyx; break;
+        case MASS_LB_MU: a = s.MU; break;
+        case MASS_LB_DXQQXX: a = s.dxQxx; break; case MASS_LB_DYQQXX: a = s.dyQxx; break;
+        case MASS_LB_DXQQYX: a = s.dxQyx; break; case MASS_LB_DYQQYX: a = s.dyQyx; break;
+        case MASS_LB_SIGMAXX: a = s.sXX; break; case MASS_LB_SIGMAYY: a = s.sYY; break;
+        case MASS_LB_SIGMAYX: a = s.sYX; break; case MASS_LB_SIGMAXY: a = s.sXY; break;
+        default:
+          if(field >= MASS_LB_SIGMA_BULK && field <= MASS_LB_SIGMA_ACTIVE_YX)
+            a = s.diag[field - MASS_LB_SIGMA_BULK];
+      }
+      if(field == MASS_LB_FF) k_get_ff<float><<<nb, 256, 0, h->stream>>>(h->stage, s.ff, d.NE, x0, nrows, LY, d.g, d.EY, h->P.rho);
+      else k_get_scalar<float><<<nb, 256, 0, h->stream>>>(h->stage, a, x0, nrows, LY, d.g, d.EY, add);
+    }
+    CU(cudaGetLastError(), "download kernel");
+    CU(cudaMemcpyAsync(out + x0*LY*comps, h->stage, n*comps*sizeof(double),
+                       cudaMemcpyDeviceToHost, h->stream), "download copy");
+  }
+  CU(cudaStreamSynchronize(h->stream), "download sync");
+  return 0;
+}
+
+int mass_lb_download(mass_lb_handle* h, int field, double* out)
+{
+  if(!h || !out) return fail(MASS_LB_EINVAL, "null argument");
+  if(field < 0 || field >= MASS_LB_NUM_FIELDS) return fail(MASS_LB_EINVAL, "bad field id");
+  const bool phase_field = field == MASS_LB_PHI || field == MASS_LB_UX_PHI ||
+    field == MASS_LB_UY_PHI || field == MASS_LB_MU || field == MASS_LB_PHN ||
+    (field >= MASS_LB_SIGMA_BULK && field <= MASS_LB_SIGMA_ACTIVE_YX);
+  if(h->model != LYO && phase_field)
+    return fail(MASS_LB_EUNSUPPORTED, "field does not exist in the nematic model");
+  if(h->precision == MASS_LB_FP32 && field >= MASS_LB_FN)
+    return fail(MASS_LB_EUNSUPPORTED, "step-internal predictor fields are FP64-mode only");
+  DeviceGuard g(h->device);
+  if(h->fused && field >= MASS_LB_N && field <= MASS_LB_SIGMA_ACTIVE_YX)
+  {
+    if(!h->has_prev)
+      return fail(MASS_LB_EUNSUPPORTED, "derived fields need a step since the last upload");
+    if(int r = ensure_diag_buffer(h)) return r;
+    // replay the last step from the retained input with the diagnostic
+    // outputs on (the replay does not write the state)
+    const FusedArgs a = fused_args(h, h->nxt, h->cur, true);
+    CU(launch_fused_step(a, h->model, h->cfg, true, h->stream), "diag replay");
+    if(int r = check_err_flag(h)) return r;
+  }
+  return get_primary(h, field, out);
+}
+
+int mass_lb_checks(mass_lb_handle* h, double* fsum, double* phisum, int* nonfinite)
+{
+  if(!h) return fail(MASS_LB_EINVAL, "null handle");
+  DeviceGuard g(h->device);
+  cudaError_t e;
+  if(h->fused)
+  {
+    const long long plane = static_cast<long long>(h->LX)*h->LY;
+    SumView<float> v{h->cur, h->cur + 9*plane, h->cur + 10*plane,
+                     h->model == LYO ? h->cur + 11*plane : nullptr, plane,
+                     static_cast<int>(h->LX), static_cast<int>(h->LY), 0,
+                     static_cast<int>(h->LY), h->P.rho};
+    e = launch_sums_f32(v, h->red_scratch, h->red_out, h->stream);
+  }
+  else if(h->precision == MASS_LB_FP64)
+  {
+    const State<double>& s = h->s64;
+    SumView<double> v{s.ff, s.Qxx, s.Qyx, h->model == LYO ? s.phi : nullptr, h->d.NE,
+                      h->d.LX, h->d.LY, h->d.g, h->d.EY, 0.0};
+    e = launch_sums_f64(v, h->red_scratch, h->red_out, h->stream);
+  }
+  else
+  {
+    const State<float>& s = h->s32;
+    SumView<float> v{s.ff, s.Qxx, s.Qyx, h->model == LYO ? s.phi : nullptr, h->d.NE,
+                     h->d.LX, h->d.LY, h->d.g, h->d.EY, h->P.rho};
+    e = launch_sums_f32(v, h->red_scratch, h->red_out, h->stream);
+  }
+  if(e != cudaSuccess) return cuda_fail(e, "sums");
+  double r[3];
+  CU(cudaMemcpyAsync(r, h->red_out, sizeof(r), cudaMemcpyDeviceToHost, h->stream), "sums copy");
+  CU(cudaStreamSynchronize(h->stream), "sums sync");
+  if(h->fused)
+    if(int rc = check_err_flag(h)) return rc;
+  if(fsum) *fsum = r[0];
+  if(phisum) *phisum = r[1];
+  if(nonfinite) *nonfinite = r[2] != 0.0 ? 1 : 0;
+  return 0;
+}
+
+int mass_lb_initial_totals(mass_lb_handle* h, double* ftot, double* ptot)
+{
+  if(!h) return fail(MASS_LB_EINVAL, "null handle");
+  if(ftot) *ftot = h->ftot;
+  if(ptot) *ptot = h->ptot;
+  return 0;
+}
+
+int mass_lb_synchronize(mass_lb_handle* h)
+{
+  if(!h) return fail(MASS_LB_EINVAL, "null handle");
+  DeviceGuard g(h->device);
+  CU(cudaStreamSynchronize(h->stream), "sync");
+  if(h->fused) return check_err_flag(h);
+  return 0;
+}
+
+void* mass_lb_stream(mass_lb_handle* h) { return h ? static_cast<void*>(h->stream) : nullptr; }
+
+int mass_lb_launches_per_step(mass_lb_handle* h)
+{
+  if(!h) return fail(MASS_LB_EINVAL, "null handle");
+  if(h->fused) return 1;
+  return launches_unfused(h->model, h->wall ? static_cast<int>(h->bc) : 0, h->P.npc);
+}
+
+// ---- mass_lb_ext.h ------------------------------------------------------
+
+int mass_lb_get_tile(mass_lb_handle* h, int* threads, int* rows)
+{
+  if(!h) return fail(MASS_LB_EINVAL, "null handle");
+  if(!h->fused) return fail(MASS_LB_EUNSUPPORTED, "not using the fused kernel");
+  if(threads) *threads = h->cfg.nt;
+  if(rows) *rows = h->cfg.rows;
+  return 0;
+}
+
+int mass_lb_set_tile(mass_lb_handle* h, int threads, int rows)
+{
+  if(!h) return fail(MASS_LB_EINVAL, "null handle");
+  if(!h->fused) return fail(MASS_LB_EUNSUPPORTED, "not using the fused kernel");
+  if(threads == 0 && rows == 0) { h->tuned = false; return 0; }
+  if(!fused_supported(static_cast<int>(h->LX), static_cast<int>(h->LY), threads) || rows <= 0)
+    return fail(MASS_LB_EINVAL, "tile does not fit this lattice");
+  h->cfg = FusedConfig{threads, rows};
+  h->tuned = true;
+  return 0;
+}
+
+int mass_lb_autotune(mass_lb_handle* h)
+{
+  if(!h) return fail(MASS_LB_EINVAL, "null handle");
+  if(!h->fused) return 0;
+  DeviceGuard g(h->device);
+  return autotune(h);
+}
+
+int mass_lb_uses_fused(mass_lb_handle* h) { return h && h->fused ? 1 : 0; }
+
+int mass_lb_device_state(mass_lb_handle* h, void** planes, long long* plane_stride,
+                         int* nplanes_out)
+{
+  if(!h || !planes) return fail(MASS_LB_EINVAL, "null argument");
+  if(!h->fused) return fail(MASS_LB_EUNSUPPORTED, "device state view is FP32-fused only");
+  *planes = h->cur;
+  if(plane_stride) *plane_stride = static_cast<long long>(h->LX)*h->LY;
+  if(nplanes_out) *nplanes_out = nplanes(h);
+  return 0;
+}
+
+} // extern "C"

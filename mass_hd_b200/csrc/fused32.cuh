@@ -1,0 +1,73 @@
+// FP32 fused periodic step: one kernel launch advances the whole lattice by
+// one Model::Step() (predictor UpdateQuantities + UpdateFields, Move, and
+// npc = 1 corrector UpdateQuantities + UpdateFields).
+#pragma once
+
+#include "lb_common.cuh"
+
+namespace mlb {
+
+// Parameters in FP32 (nematic: Gamma -> GammaQ, tau -> tauNem = tauIso).
+struct P32
+{
+  float rho, GammaQ, GammaP, xi, tauNem, tauIso, friction;
+  float AA, CC, LL, KK, zeta, zetaI, conc;
+};
+
+// Diagnostic outputs of the corrector UpdateQuantities (the values the
+// reference holds in n, ux, ..., sigma_active_yx after Step()), written only
+// by the replay launch. Planes of LX*LY floats, in mass_lb_field order
+// MASS_LB_N .. MASS_LB_SIGMA_ACTIVE_YX (23 planes).
+enum { NDIAG = 23 };
+
+// Parameters and literals pre-broadcast to pairs for the packed FP32x2
+// kernel (read straight from the constant bank as 64-bit operands).
+struct PairParams
+{
+  float2 rho, GammaQ, GammaP, xi2, xi, tauIso, dtau, friction;
+  float2 AA, hAA, nCC, hCC, LL, nLL2, KK, hKK, nKK, zeta, zetaI, conc;
+  float2 one, neg1, two, half, nhalf, quarter, nquarter, nfour, ntwo;
+  float2 third, twelfth, ninth, th36, zero;
+};
+
+struct FusedArgs
+{
+  const float* in;     // NP planes of LX*LY: g0..g8, Qxx, Qyx[, phi]
+  float* out;          // same layout
+  float* diag;         // NDIAG planes (DIAG launches only)
+  int* err;            // bit 0: a bounded wait gave up
+  int LX, LY;
+  long long plane;     // LX*LY
+  int nstrips;         // ceil(LY / (NT - 8))
+  int rows;            // rows per CTA chunk
+  P32 p;
+  PairParams pp;       // filled by the warp-strip launcher
+};
+
+// Tile shapes the autotuner may pick.
+//   nt = 64, 128, 256: CTA-strip kernel (fused32.cu), nt threads = nt
+//        columns per strip, one column per thread;
+//   nt = 32: warp-strip kernel (fused_warp.cu), every warp an independent
+//        64-column strip, two columns per lane in packed FP32x2.
+struct FusedConfig
+{
+  int nt;
+  int rows;  // rows per CTA (or warp) chunk
+};
+
+// Warp-strip kernel launch (fused_warp.cu).
+cudaError_t launch_fused_warp_step(const FusedArgs& a, int model, int rows, bool diag,
+                                   cudaStream_t st);
+
+// Launch one fused step (template dispatch on nt / model / diag).
+cudaError_t launch_fused_step(const FusedArgs& a, int model, FusedConfig cfg,
+                              bool diag, cudaStream_t st);
+
+// Dynamic shared memory one CTA of the given width needs.
+size_t fused_smem_bytes(int nt, int model);
+
+// True if the fused kernel can run this lattice: LY % 4 == 0 (16-byte
+// aligned row segments for the bulk copies), LY >= max(nt, 64), LX >= 1.
+bool fused_supported(int LX, int LY, int nt);
+
+} // namespace mlb

@@ -1,0 +1,675 @@
+// FP32 fused periodic step, warp-strip variant (two lattice columns per
+// lane, packed FP32x2 arithmetic).
+//
+// Same algorithm as fused32.cu - one launch is one Model::Step() with npc = 1
+// (src/models/lyotropic.cpp:500-525, src/models/nematic.cpp:370-395) - with a
+// different decomposition:
+//  * every warp owns an independent strip of 64 columns (56 output columns
+//    and a 4-column halo on each side) and marches along x on its own; there
+//    is no CTA-wide barrier,
+//  * lane l holds columns 2l and 2l+1 as one float2 and computes both with
+//    the sm_100 packed FFMA2/FADD2/FMUL2 instructions,
+//  * y-neighbours of computed values come from the adjacent lane by
+//    __shfl_up/down; x-neighbours are rows this lane produced earlier,
+//  * stages run 0 (B: predictor UpdateQuantities), 1 (C: predictor
+//    UpdateFields + y-part of Move), 2 (D: corrector UpdateQuantities, x-part
+//    of Move) and 3 (E: corrector UpdateFields) rows behind the newest row,
+//  * D folds the corrector's fn - ff/(2 tau) per population one row early,
+//    so E carries 9 instead of 18 values per site,
+//  * input rows arrive in a per-warp ring by 1D bulk copies (TMA) with one
+//    mbarrier per slot; every wait is bounded (bit 0 of *err on time-out).
+#include "fused32.cuh"
+
+#include <cstdint>
+
+namespace mlb {
+namespace {
+
+constexpr int RING = 6;     // input rows per warp in shared memory
+constexpr int PADY = 4;     // ring row padding (floats, each side)
+constexpr int COLS = 64;    // columns per warp strip
+constexpr int WOUT = COLS - 8;
+constexpr int RWW = COLS + 2*PADY;   // ring row stride (floats)
+constexpr int WPB = 4;      // warps per CTA
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_barrier_init()
+{
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async()
+{
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+               :: "r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+  asm volatile(
+    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+    :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+  uint32_t ok;
+  asm volatile(
+    "{\n\t.reg .pred p;\n\t"
+    "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+    "selp.u32 %0, 1, 0, p;\n\t}"
+    : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity)
+{
+  if(mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while(!mbar_try_wait(bar, parity))
+    if(clock64() - t0 > (1ll << 31)) return false;
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// packed pair arithmetic (columns 2l and 2l+1)
+
+struct f2 { float2 v; };
+__device__ __forceinline__ f2 mk(float a, float b) { return f2{make_float2(a, b)}; }
+__device__ __forceinline__ f2 bc(float s) { return f2{make_float2(s, s)}; }
+__device__ __forceinline__ f2 operator+(f2 a, f2 b) { return f2{__fadd2_rn(a.v, b.v)}; }
+__device__ __forceinline__ f2 operator*(f2 a, f2 b) { return f2{__fmul2_rn(a.v, b.v)}; }
+__device__ __forceinline__ f2 fma(f2 a, f2 b, f2 c) { return f2{__ffma2_rn(a.v, b.v, c.v)}; }
+__device__ __forceinline__ f2 operator-(f2 a, f2 b) { return f2{__ffma2_rn(b.v, make_float2(-1.f, -1.f), a.v)}; }
+__device__ __forceinline__ f2 neg(f2 a) { return f2{__fmul2_rn(a.v, make_float2(-1.f, -1.f))}; }
+__device__ __forceinline__ f2 K(float c) { return bc(c); }
+__device__ __forceinline__ f2 W2(const float2& c) { return f2{c}; }
+
+__device__ __forceinline__ float rcp_approx(float x)
+{
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+// 1/x: hardware estimate refined by one Newton step
+__device__ __forceinline__ f2 rcp2(f2 x, const PairParams& P)
+{
+  const f2 r0 = mk(rcp_approx(x.v.x), rcp_approx(x.v.y));
+  const f2 e = fma(neg(x), r0, W2(P.one));
+  return fma(r0, e, r0);
+}
+
+__device__ __forceinline__ f2 lds2(const float* p) { return f2{*reinterpret_cast<const float2*>(p)}; }
+
+// neighbour along +y / -y of a pair held by every lane
+__device__ __forceinline__ f2 yplus(f2 a)
+{
+  return mk(a.v.y, __shfl_down_sync(0xffffffffu, a.v.x, 1));
+}
+__device__ __forceinline__ f2 yminus(f2 a)
+{
+  return mk(__shfl_up_sync(0xffffffffu, a.v.y, 1), a.v.x);
+}
+
+using PP = PairParams;
+
+__host__ PairParams make_pp(const P32& p, int model)
+{
+  auto b = [](float x) { return make_float2(x, x); };
+  PairParams q;
+  q.rho = b(p.rho); q.GammaQ = b(p.GammaQ); q.GammaP = b(p.GammaP);
+  q.xi2 = b(2.f*p.xi); q.xi = b(p.xi);
+  q.tauIso = b(model == LYO ? p.tauIso : p.tauNem);
+  q.dtau = b(model == LYO ? p.tauNem - p.tauIso : 0.f);
+  q.friction = b(p.friction);
+  q.AA = b(p.AA); q.hAA = b(0.5f*p.AA);
+  q.nCC = b(-p.CC); q.hCC = b(0.5f*p.CC);
+  q.LL = b(p.LL); q.nLL2 = b(-2.f*p.LL);
+  q.KK = b(p.KK); q.hKK = b(0.5f*p.KK); q.nKK = b(-p.KK);
+  q.zeta = b(p.zeta); q.zetaI = b(p.zetaI); q.conc = b(p.conc);
+  q.one = b(1.f); q.neg1 = b(-1.f); q.two = b(2.f); q.half = b(0.5f);
+  q.nhalf = b(-0.5f); q.quarter = b(0.25f); q.nquarter = b(-0.25f);
+  q.nfour = b(-4.f); q.ntwo = b(-2.f); q.third = b(1.f/3.f);
+  q.twelfth = b(1.f/12.f); q.ninth = b(1.f/9.f); q.th36 = b(1.f/36.f);
+  q.zero = b(0.f);
+  return q;
+}
+
+// UpdateQuantities outputs of one row pair.
+// x-neighbour set: ux, uy, sXX, sYX, uxp, MU; y-neighbour set: ux, uy, sXY,
+// sYY, uyp, MU; centre only: dn, Hxx, Hyx, dQ.
+struct UQ2o
+{
+  f2 dn, ux, uy, uxp, uyp, MU, Hxx, Hyx, dxQxx, dyQxx, dxQyx, dyQyx, sXX, sYY, sXY, sYX;
+};
+struct UQx
+{
+  f2 ux, uy, sXX, sYX, uxp, MU;
+};
+__device__ __forceinline__ UQx xset(const UQ2o& a)
+{
+  return UQx{a.ux, a.uy, a.sXX, a.sYX, a.uxp, a.MU};
+}
+
+// Qa/Qb/Ph: centre, +x, -x, +y, -y
+template<int MODEL>
+__device__ __forceinline__ void uq_pair(const PP& P, const f2 g[9], const f2 Qa[5],
+                                        const f2 Qb[5], const f2 Ph[5], UQ2o& o,
+                                        f2* dg)
+{
+  const f2 dn = ((g[0] + g[1]) + (g[2] + g[3])) + ((g[4] + g[5]) + (g[6] + g[7])) + g[8];
+  const f2 nn = W2(P.rho) + dn;
+  const f2 inv = rcp2(nn, P);
+  const f2 d56 = g[5] - g[6];
+  const f2 jx = (g[1] - g[2]) + (d56 + (g[8] - g[7]));
+  const f2 jy = (g[3] - g[4]) + (d56 + (g[7] - g[8]));
+  const f2 vx = jx*inv, vy = jy*inv;
+
+  const f2 Qxx = Qa[0], Qyx = Qb[0];
+  const f2 lQxx = fma(W2(P.nfour), Qxx, (Qa[1] + Qa[2]) + (Qa[3] + Qa[4]));
+  const f2 lQyx = fma(W2(P.nfour), Qyx, (Qb[1] + Qb[2]) + (Qb[3] + Qb[4]));
+  const f2 dxQxx = W2(P.half)*(Qa[1] - Qa[2]), dyQxx = W2(P.half)*(Qa[3] - Qa[4]);
+  const f2 dxQyx = W2(P.half)*(Qb[1] - Qb[2]), dyQyx = W2(P.half)*(Qb[3] - Qb[4]);
+  const f2 S2 = fma(Qxx, Qxx, Qyx*Qyx);
+  // cterm = CC*term with term = -S2 (lyotropic) or 1 - S2 (nematic)
+  const f2 cterm = MODEL == LYO ? W2(P.nCC)*S2 : fma(W2(P.nCC), S2, neg(W2(P.nCC)));
+  const f2 Hxx = fma(cterm, Qxx, W2(P.LL)*lQxx);
+  const f2 Hyx = fma(cterm, Qyx, W2(P.LL)*lQyx);
+  const f2 el = W2(P.LL)*(fma(dyQxx, dyQxx, dyQyx*dyQyx) - fma(dxQxx, dxQxx, dxQyx*dxQyx));
+  const f2 elS = W2(P.nLL2)*fma(dxQxx, dyQxx, dxQyx*dyQyx);
+  const f2 sigmaA = W2(P.two)*fma(Qxx, Hyx, neg(Qyx*Hxx));
+  const f2 QQ = Qxx*Qyx;
+  const f2 flowF = W2(P.xi2)*fma(fma(Qxx, Qxx, W2(P.neg1)), Hxx, QQ*Hyx);
+  const f2 flowS = W2(P.xi2)*fma(QQ, Hxx, fma(Qyx, Qyx, W2(P.neg1))*Hyx);
+  // sigmaB's nematic/lyotropic common part: 0.5 CC term^2 = 0.5 cterm^2/CC;
+  // written as hCC*term*term with term recomputed from S2
+  const f2 term = MODEL == LYO ? neg(S2) : W2(P.one) - S2;
+  const f2 bulkQ = W2(P.hCC)*(term*term);
+
+  o.dn = dn; o.ux = vx; o.uy = vy;
+  o.Hxx = Hxx; o.Hyx = Hyx;
+  o.dxQxx = dxQxx; o.dyQxx = dyQxx; o.dxQyx = dxQyx; o.dyQyx = dyQyx;
+
+  if constexpr (MODEL == LYO)
+  {
+    const f2 p = Ph[0];
+    const f2 omp = W2(P.one) - p;
+    const f2 lp = fma(W2(P.nfour), p, (Ph[1] + Ph[2]) + (Ph[3] + Ph[4]));
+    const f2 dxPhi = W2(P.half)*(Ph[1] - Ph[2]), dyPhi = W2(P.half)*(Ph[3] - Ph[4]);
+    const f2 pq = p*omp;
+    const f2 mu = fma(W2(P.AA)*pq, fma(W2(P.ntwo), p, W2(P.one)), W2(P.nKK)*lp);
+    const f2 sigmaB = fma(W2(P.hAA)*pq, pq, bulkQ) - mu*p;
+    const f2 act = W2(P.zeta)*omp;
+    const f2 pf = W2(P.hKK)*fma(dyPhi, dyPhi, neg(dxPhi*dxPhi));
+    const f2 pfS = W2(P.nKK)*(dxPhi*dyPhi);
+    const f2 sigmaF = fma(neg(act), Qxx, flowF) + (pf + el);
+    const f2 sigmaS = fma(neg(act), Qyx, flowS) + (pfS + elS);
+    const f2 bi = sigmaB + W2(P.zetaI)*(W2(P.conc) - p);
+    o.uxp = vx*p; o.uyp = vy*p; o.MU = mu;
+    o.sXX = bi + sigmaF;
+    o.sYY = bi - sigmaF;
+    o.sXY = sigmaS + sigmaA;
+    o.sYX = sigmaS - sigmaA;
+    if(dg)
+    {
+      dg[0] = bi;
+      dg[1] = fma(act, Qxx, sigmaF - pf);
+      // zeta*Qxx in the yx component as the reference has it
+      // (src/models/lyotropic.cpp:242)
+      dg[2] = fma(act, Qxx, sigmaS - pfS);
+      dg[3] = pf;
+      dg[4] = pfS;
+      dg[5] = neg(act*Qxx);
+      dg[6] = neg(act*Qyx);
+    }
+  }
+  else
+  {
+    const f2 sigmaF = fma(neg(W2(P.zeta)), Qxx, flowF) + el;
+    const f2 sigmaS = fma(neg(W2(P.zeta)), Qyx, flowS) + elS;
+    o.uxp = W2(P.zero); o.uyp = W2(P.zero); o.MU = W2(P.zero);
+    o.sXX = bulkQ + sigmaF;
+    o.sYY = bulkQ - sigmaF;
+    o.sXY = sigmaS + sigmaA;
+    o.sYX = sigmaS - sigmaA;
+  }
+}
+
+// y-neighbour values (+y, -y) of the y-set of a row, fetched from the
+// neighbouring lanes
+struct YN
+{
+  f2 uxp_, uxm, uyp_, uym, sxyp, sxym, syyp, syym, uypp, uypm, mup, mum;
+};
+template<int MODEL>
+__device__ __forceinline__ YN ynbrs(const UQ2o& c)
+{
+  YN y;
+  y.uxp_ = yplus(c.ux); y.uxm = yminus(c.ux);
+  y.uyp_ = yplus(c.uy); y.uym = yminus(c.uy);
+  y.sxyp = yplus(c.sXY); y.sxym = yminus(c.sXY);
+  y.syyp = yplus(c.sYY); y.syym = yminus(c.sYY);
+  if constexpr (MODEL == LYO)
+  {
+    y.uypp = yplus(c.uyp); y.uypm = yminus(c.uyp);
+    y.mup = yplus(c.MU); y.mum = yminus(c.MU);
+  }
+  else
+  {
+    y.uypp = y.uypm = y.mup = y.mum = K(0.f);
+  }
+  return y;
+}
+
+// The flow part shared by both UpdateFields: Beris-Edwards D, force F,
+// Cahn-Hilliard Dp, equilibrium deviation fe and forcing term per direction.
+struct UFcore
+{
+  f2 Dxx, Dyx, Dp, fe[9], F[9];
+};
+
+template<int MODEL>
+__device__ __forceinline__ void uf_core(const PP& P, const UQ2o& c, const UQx& xp,
+                                        const UQx& xm, const YN& y, f2 Qxx, f2 Qyx,
+                                        UFcore& u)
+{
+  const f2 dxux = W2(P.half)*(xp.ux - xm.ux), dyux = W2(P.half)*(y.uxp_ - y.uxm);
+  const f2 dxuy = W2(P.half)*(xp.uy - xm.uy), dyuy = W2(P.half)*(y.uyp_ - y.uym);
+  const f2 dxSxx = W2(P.half)*(xp.sXX - xm.sXX), dySxy = W2(P.half)*(y.sxyp - y.sxym);
+  const f2 dxSyx = W2(P.half)*(xp.sYX - xm.sYX), dySyy = W2(P.half)*(y.syyp - y.syym);
+  const f2 expansion = dxux + dyuy;
+  const f2 shear = W2(P.half)*(dxuy + dyux);
+  const f2 vorticity = W2(P.half)*(dxuy - dyux);
+  const f2 Qs2 = W2(P.two)*(Qyx*shear);
+  const f2 traceQL = fma(Qxx, dxux - dyuy, Qs2);
+  const f2 vx = c.ux, vy = c.uy;
+  const f2 v2 = W2(P.two)*vorticity;
+  // Dxx = G Hxx - vx dxQxx - vy dyQxx - 2 w Qyx + xi((Qxx+1)(2 dxux - trQL) + 2 Qyx shear - expansion)
+  const f2 bx = fma(Qxx + W2(P.one), fma(W2(P.two), dxux, neg(traceQL)), Qs2 - expansion);
+  u.Dxx = fma(W2(P.GammaQ), c.Hxx, fma(W2(P.xi), bx, neg(fma(vx, c.dxQxx, fma(vy, c.dyQxx, v2*Qyx)))));
+  // Dyx = G Hyx - vx dxQyx - vy dyQyx + 2 w Qxx + xi(Qyx(expansion - trQL) + 2 shear)
+  const f2 by = fma(Qyx, expansion - traceQL, W2(P.two)*shear);
+  u.Dyx = fma(W2(P.GammaQ), c.Hyx, fma(W2(P.xi), by, fma(v2, Qxx, neg(fma(vx, c.dxQyx, vy*c.dyQyx)))));
+  const f2 Fx = (dxSxx + dySxy) - W2(P.friction)*vx;
+  const f2 Fy = (dxSyx + dySyy) - W2(P.friction)*vy;
+  if constexpr (MODEL == LYO)
+  {
+    const f2 lMU = fma(W2(P.nfour), c.MU, (xp.MU + xm.MU) + (y.mup + y.mum));
+    const f2 pFlux = W2(P.half)*((xp.uxp - xm.uxp) + (y.uypp - y.uypm));
+    u.Dp = fma(W2(P.GammaP), lMU, neg(pFlux));
+  }
+  else u.Dp = W2(P.zero);
+
+  const f2 dn = c.dn;
+  const f2 nn = W2(P.rho) + dn;
+  const f2 jx = nn*vx, jy = nn*vy;
+  const f2 kxx = jx*vx, kyy = jy*vy, kxy = jx*vy, k2 = kxx + kyy;
+  const f2 dn9 = W2(P.ninth)*dn, dn36 = W2(P.th36)*dn;
+  const f2 a1 = fma(W2(P.nhalf), kyy, dn9), a3 = fma(W2(P.nhalf), kxx, dn9);
+  const f2 b5 = fma(W2(P.quarter), kxy, dn36), b7 = fma(W2(P.nquarter), kxy, dn36);
+  u.fe[1] = fma(k2 + jx, W2(P.third), a1);
+  u.fe[2] = fma(k2 - jx, W2(P.third), a1);
+  u.fe[3] = fma(k2 + jy, W2(P.third), a3);
+  u.fe[4] = fma(k2 - jy, W2(P.third), a3);
+  const f2 s = jx + jy, d = jx - jy;
+  u.fe[5] = fma(k2 + s, W2(P.twelfth), b5);
+  u.fe[6] = fma(k2 - s, W2(P.twelfth), b5);
+  u.fe[7] = fma(k2 - d, W2(P.twelfth), b7);
+  u.fe[8] = fma(k2 + d, W2(P.twelfth), b7);
+  u.fe[0] = dn - (((u.fe[1] + u.fe[2]) + (u.fe[3] + u.fe[4])) + ((u.fe[5] + u.fe[6]) + (u.fe[7] + u.fe[8])));
+  u.F[0] = W2(P.zero);
+  u.F[1] = W2(P.third)*Fx; u.F[2] = neg(u.F[1]);
+  u.F[3] = W2(P.third)*Fy; u.F[4] = neg(u.F[3]);
+  u.F[5] = W2(P.twelfth)*(Fx + Fy); u.F[6] = neg(u.F[5]);
+  u.F[7] = W2(P.twelfth)*(Fy - Fx); u.F[8] = neg(u.F[7]);
+}
+
+template<int MODEL>
+__device__ __forceinline__ f2 itau_of(const PP& P, f2 p)
+{
+  return MODEL == LYO ? rcp2(fma(W2(P.dtau), p, W2(P.tauIso)), P) : rcp2(W2(P.tauIso), P);
+}
+
+template<int MODEL, bool DIAG>
+__global__ void __launch_bounds__(32*WPB, 2)
+fused_warp_kernel(const __grid_constant__ FusedArgs a, const int nitems)
+{
+  constexpr int NP = MODEL == LYO ? 12 : 11;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* ring = reinterpret_cast<float*>(smem_raw) + warp*(RING*NP*RWW);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(
+    smem_raw + WPB*RING*NP*RWW*sizeof(float)) + warp*RING;
+
+  const int item = blockIdx.x*WPB + warp;
+  if(item >= nitems) return;
+  const int strip = item % a.nstrips;
+  const int chunk = item / a.nstrips;
+  const int y0 = strip*WOUT;
+  const int x0 = chunk*a.rows;
+  const int rows = min(a.rows, a.LX - x0);
+  const int LX = a.LX, LY = a.LY;
+  const int nload = rows + 8;            // rows x0-4 .. x0+rows+3
+  const int ystart = (y0 - 4 + LY) % LY;
+  const PP& P = a.pp;
+
+  if(lane == 0)
+  {
+    for(int s = 0; s < RING; ++s) mbar_init(&mbar[s], 1);
+    fence_barrier_init();
+  }
+  __syncwarp();
+
+  auto issue = [&](int rr) {
+    const int slot = rr % RING;
+    uint64_t* bar = &mbar[slot];
+    mbar_expect_tx(bar, NP*COLS*4);
+    const int gx = ((x0 - 4 + rr) % LX + LX) % LX;
+    for(int p = 0; p < NP; ++p)
+    {
+      const float* src = a.in + p*a.plane + static_cast<long long>(gx)*LY;
+      float* dst = ring + (slot*NP + p)*RWW + PADY;
+      int start = ystart, rem = COLS;
+      while(rem > 0)
+      {
+        const int len = min(rem, LY - start);
+        bulk_load(dst, src + start, static_cast<uint32_t>(len*4), bar);
+        dst += len;
+        rem -= len;
+        start = 0;
+      }
+    }
+  };
+
+  int issued = 0;
+  if(lane == 0)
+  {
+    const int n0 = min(RING, nload);
+    for(int rr = 0; rr < n0; ++rr) issue(rr);
+    issued = n0;
+  }
+  bool abort = !mbar_wait_bounded(&mbar[0], 0) || !mbar_wait_bounded(&mbar[1], 0);
+
+  const int c2 = PADY + 2*lane;            // this lane's first column in a ring row
+  const int yg = y0 - 4 + 2*lane;          // global column of .x (pre-wrap)
+  const bool lane_out = lane >= 2 && lane < 30;
+  const bool colx_ok = lane_out && yg < LY;
+  const bool coly_ok = lane_out && yg + 1 < LY;
+
+  UQ2o q1c{}, q2c{};
+  UQx q1m{}, q2m{};
+  f2 qa1[3], qa2[3], qn1[3], qn2[3];
+  f2 d1[6], d2a[6], d2b[6];   // pops delayed 1 / 2 rows: ff v=0,3,4 | fn v=0,3,4 ; ff v=1,5,8 | fn v=1,5,8
+  f2 hcar[9];                 // fn - ff/(2 tau) of the row E processes next
+#pragma unroll
+  for(int k = 0; k < 3; ++k) { qa1[k] = qa2[k] = qn1[k] = qn2[k] = W2(P.zero); }
+#pragma unroll
+  for(int k = 0; k < 6; ++k) { d1[k] = d2a[k] = d2b[k] = W2(P.zero); }
+#pragma unroll
+  for(int v = 0; v < 9; ++v) hcar[v] = W2(P.zero);
+
+  const int nit = rows + 6;
+  for(int i = 0; i < nit; ++i)
+  {
+    if(i + 2 < nload)
+    {
+      const int rr = i + 2;
+      if(!mbar_wait_bounded(&mbar[rr % RING], (rr / RING) & 1)) abort = true;
+    }
+    if(__any_sync(0xffffffffu, abort)) break;
+    const float* Rm = ring + ((i    ) % RING)*NP*RWW;   // row b-1
+    const float* R0 = ring + ((i + 1) % RING)*NP*RWW;   // row b
+    const float* Rp = ring + ((i + 2) % RING)*NP*RWW;   // row b+1
+
+    // ---- B: predictor UpdateQuantities at row b ----
+    UQ2o nq1;
+    {
+      f2 g[9];
+#pragma unroll
+      for(int v = 0; v < 9; ++v) g[v] = lds2(R0 + v*RWW + c2);
+      f2 Qa[5], Qb[5], Ph[5];
+      const float* q0 = R0 + 9*RWW + c2;
+      Qa[0] = lds2(q0); Qa[1] = lds2(Rp + 9*RWW + c2); Qa[2] = lds2(Rm + 9*RWW + c2);
+      Qa[3] = mk(Qa[0].v.y, q0[2]); Qa[4] = mk(q0[-1], Qa[0].v.x);
+      const float* q1 = R0 + 10*RWW + c2;
+      Qb[0] = lds2(q1); Qb[1] = lds2(Rp + 10*RWW + c2); Qb[2] = lds2(Rm + 10*RWW + c2);
+      Qb[3] = mk(Qb[0].v.y, q1[2]); Qb[4] = mk(q1[-1], Qb[0].v.x);
+      if constexpr (MODEL == LYO)
+      {
+        const float* q2 = R0 + 11*RWW + c2;
+        Ph[0] = lds2(q2); Ph[1] = lds2(Rp + 11*RWW + c2); Ph[2] = lds2(Rm + 11*RWW + c2);
+        Ph[3] = mk(Ph[0].v.y, q2[2]); Ph[4] = mk(q2[-1], Ph[0].v.x);
+      }
+      else
+      {
+#pragma unroll
+        for(int k = 0; k < 5; ++k) Ph[k] = W2(P.zero);
+      }
+      uq_pair<MODEL>(P, g, Qa, Qb, Ph, nq1, nullptr);
+    }
+
+    // ---- C: predictor UpdateFields at row b-1, then y-part of Move ----
+    f2 nQ[3], nQN[3], pf[9], pn[9];
+    {
+      const YN y = ynbrs<MODEL>(q1c);
+      const f2 Qxx = lds2(Rm + 9*RWW + c2), Qyx = lds2(Rm + 10*RWW + c2);
+      const f2 p = MODEL == LYO ? lds2(Rm + 11*RWW + c2) : W2(P.zero);
+      UFcore u;
+      uf_core<MODEL>(P, q1c, xset(nq1), q1m, y, Qxx, Qyx, u);
+      const f2 itau = itau_of<MODEL>(P, p);
+#pragma unroll
+      for(int v = 0; v < 9; ++v)
+      {
+        const f2 g = lds2(Rm + v*RWW + c2);
+        const f2 coll = fma(u.fe[v] - g, itau, u.F[v]);
+        pn[v] = fma(W2(P.half), coll, g);
+        pf[v] = MODEL == LYO ? g + coll : fma(W2(P.half), coll, pn[v]);
+      }
+      nQN[0] = fma(W2(P.half), u.Dxx, Qxx);
+      nQN[1] = fma(W2(P.half), u.Dyx, Qyx);
+      if constexpr (MODEL == LYO)
+      {
+        nQ[0] = Qxx + u.Dxx;
+        nQ[1] = Qyx + u.Dyx;
+        nQN[2] = fma(W2(P.half), u.Dp, p);
+        nQ[2] = p + u.Dp;
+      }
+      else
+      {
+        nQ[0] = fma(W2(P.half), u.Dxx, nQN[0]);
+        nQ[1] = fma(W2(P.half), u.Dyx, nQN[1]);
+        nQN[2] = nQ[2] = W2(P.zero);
+      }
+      // stream along y: directions with cy = +1 move one column up, cy = -1 down
+#pragma unroll
+      for(int v = 3; v < 9; ++v)
+      {
+        if(CYv(v) > 0) { pf[v] = yminus(pf[v]); pn[v] = yminus(pn[v]); }
+        else if(CYv(v) < 0) { pf[v] = yplus(pf[v]); pn[v] = yplus(pn[v]); }
+      }
+    }
+
+    // ---- D: corrector UpdateQuantities at row s = b-2 (x-part of Move) ----
+    UQ2o nq2;
+    f2 hn[9];
+    {
+      // direction v at (s, y) left row s - cx: cx = -1 is the row C just
+      // produced, cx = 0 the previous one, cx = +1 the one before that
+      f2 fs[9], ns[9];
+      fs[2] = pf[2]; fs[6] = pf[6]; fs[7] = pf[7];
+      ns[2] = pn[2]; ns[6] = pn[6]; ns[7] = pn[7];
+      fs[0] = d1[0]; fs[3] = d1[1]; fs[4] = d1[2];
+      ns[0] = d1[3]; ns[3] = d1[4]; ns[4] = d1[5];
+      fs[1] = d2b[0]; fs[5] = d2b[1]; fs[8] = d2b[2];
+      ns[1] = d2b[3]; ns[5] = d2b[4]; ns[8] = d2b[5];
+      f2 Qa[5], Qb[5], Ph[5];
+      Qa[0] = qa1[0]; Qa[1] = nQ[0]; Qa[2] = qa2[0]; Qa[3] = yplus(qa1[0]); Qa[4] = yminus(qa1[0]);
+      Qb[0] = qa1[1]; Qb[1] = nQ[1]; Qb[2] = qa2[1]; Qb[3] = yplus(qa1[1]); Qb[4] = yminus(qa1[1]);
+      if constexpr (MODEL == LYO)
+      {
+        Ph[0] = qa1[2]; Ph[1] = nQ[2]; Ph[2] = qa2[2]; Ph[3] = yplus(qa1[2]); Ph[4] = yminus(qa1[2]);
+      }
+      else
+      {
+#pragma unroll
+        for(int k = 0; k < 5; ++k) Ph[k] = W2(P.zero);
+      }
+      f2 dg[7];
+      uq_pair<MODEL>(P, fs, Qa, Qb, Ph, nq2, DIAG ? dg : nullptr);
+      const f2 hitau = W2(P.nhalf)*itau_of<MODEL>(P, qa1[2]);
+#pragma unroll
+      for(int v = 0; v < 9; ++v) hn[v] = fma(hitau, fs[v], ns[v]);
+      if constexpr (DIAG)
+      {
+        const int xs = x0 - 5 + i;
+        if(xs >= x0 && xs < x0 + rows)
+        {
+          const long long pl = a.plane;
+          float* o = a.diag + static_cast<long long>(xs)*LY + yg;
+          const f2 vals[16] = {W2(P.rho) + nq2.dn, nq2.ux, nq2.uy, nq2.uxp, nq2.uyp, nq2.Hxx,
+                               nq2.Hyx, nq2.MU, nq2.dxQxx, nq2.dyQxx, nq2.dxQyx, nq2.dyQyx,
+                               nq2.sXX, nq2.sYY, nq2.sYX, nq2.sXY};
+#pragma unroll
+          for(int k = 0; k < 16; ++k)
+          {
+            if(colx_ok) o[k*pl] = vals[k].v.x;
+            if(coly_ok) o[k*pl + 1] = vals[k].v.y;
+          }
+          if constexpr (MODEL == LYO)
+          {
+#pragma unroll
+            for(int k = 0; k < 7; ++k)
+            {
+              if(colx_ok) o[(16 + k)*pl] = dg[k].v.x;
+              if(coly_ok) o[(16 + k)*pl + 1] = dg[k].v.y;
+            }
+          }
+        }
+      }
+    }
+
+    // ---- E: corrector UpdateFields at row b-3, store ----
+    if constexpr (!DIAG)
+    {
+      const YN y = ynbrs<MODEL>(q2c);
+      UFcore u;
+      uf_core<MODEL>(P, q2c, xset(nq2), q2m, y, qa2[0], qa2[1], u);
+      const f2 itau = itau_of<MODEL>(P, qa2[2]);
+      const f2 hitau = W2(P.half)*itau;
+      f2 gout[9];
+#pragma unroll
+      for(int v = 0; v < 9; ++v)
+        gout[v] = fma(W2(P.half), u.F[v], fma(hitau, u.fe[v], hcar[v]));
+      const f2 Qo0 = fma(W2(P.half), u.Dxx, qn2[0]);
+      const f2 Qo1 = fma(W2(P.half), u.Dyx, qn2[1]);
+      const f2 Qo2 = fma(W2(P.half), u.Dp, qn2[2]);
+      const int xo = x0 - 6 + i;
+      if(i >= 6 && xo < x0 + rows)
+      {
+        const long long pl = a.plane;
+        float* o = a.out + static_cast<long long>(xo)*LY + yg;
+        if(colx_ok && coly_ok)
+        {
+#pragma unroll
+          for(int v = 0; v < 9; ++v) *reinterpret_cast<float2*>(o + v*pl) = gout[v].v;
+          *reinterpret_cast<float2*>(o + 9*pl) = Qo0.v;
+          *reinterpret_cast<float2*>(o + 10*pl) = Qo1.v;
+          if constexpr (MODEL == LYO) *reinterpret_cast<float2*>(o + 11*pl) = Qo2.v;
+        }
+        else if(colx_ok)
+        {
+#pragma unroll
+          for(int v = 0; v < 9; ++v) o[v*pl] = gout[v].v.x;
+          o[9*pl] = Qo0.v.x;
+          o[10*pl] = Qo1.v.x;
+          if constexpr (MODEL == LYO) o[11*pl] = Qo2.v.x;
+        }
+      }
+    }
+
+    // ---- advance the row windows ----
+    q1m = xset(q1c); q1c = nq1;
+    q2m = xset(q2c); q2c = nq2;
+#pragma unroll
+    for(int k = 0; k < 3; ++k)
+    {
+      qa2[k] = qa1[k]; qa1[k] = nQ[k];
+      qn2[k] = qn1[k]; qn1[k] = nQN[k];
+    }
+#pragma unroll
+    for(int k = 0; k < 6; ++k) d2b[k] = d2a[k];
+    d2a[0] = pf[1]; d2a[1] = pf[5]; d2a[2] = pf[8];
+    d2a[3] = pn[1]; d2a[4] = pn[5]; d2a[5] = pn[8];
+    d1[0] = pf[0]; d1[1] = pf[3]; d1[2] = pf[4];
+    d1[3] = pn[0]; d1[4] = pn[3]; d1[5] = pn[4];
+#pragma unroll
+    for(int v = 0; v < 9; ++v) hcar[v] = hn[v];
+
+    __syncwarp();
+    if(lane == 0 && issued < nload && issued <= i + RING)
+    {
+      fence_proxy_async();
+      issue(issued);
+      ++issued;
+    }
+  }
+
+  if(abort && lane == 0)
+  {
+    atomicOr(a.err, 1);
+    for(int rr = 0; rr < issued; ++rr)
+      mbar_wait_bounded(&mbar[rr % RING], (rr / RING) & 1);
+  }
+}
+
+template<int MODEL>
+constexpr size_t smem_bytes()
+{
+  return static_cast<size_t>(WPB)*RING*(MODEL == LYO ? 12 : 11)*RWW*sizeof(float) +
+         static_cast<size_t>(WPB)*RING*sizeof(uint64_t);
+}
+
+template<int MODEL, bool DIAG>
+cudaError_t launch_t(const FusedArgs& a, int rows, cudaStream_t st)
+{
+  auto kern = fused_warp_kernel<MODEL, DIAG>;
+  static unsigned long long attr_set = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const unsigned long long bit = 1ull << (dev & 63);
+  if(!(attr_set & bit))
+  {
+    const cudaError_t e = cudaFuncSetAttribute(
+      kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem_bytes<MODEL>()));
+    if(e != cudaSuccess) return e;
+    attr_set |= bit;
+  }
+  FusedArgs b = a;
+  b.rows = rows;
+  b.nstrips = (a.LY + WOUT - 1)/WOUT;
+  b.pp = make_pp(a.p, MODEL);
+  const int nchunks = (a.LX + rows - 1)/rows;
+  const int nitems = b.nstrips*nchunks;
+  const dim3 grid((nitems + WPB - 1)/WPB);
+  kern<<<grid, 32*WPB, smem_bytes<MODEL>(), st>>>(b, nitems);
+  return cudaGetLastError();
+}
+
+} // namespace
+
+cudaError_t launch_fused_warp_step(const FusedArgs& a, int model, int rows, bool diag,
+                                   cudaStream_t st)
+{
+  if(model == LYO)
+    return diag ? launch_t<LYO, true>(a, rows, st) : launch_t<LYO, false>(a, rows, st);
+  return diag ? launch_t<NEM, true>(a, rows, st) : launch_t<NEM, false>(a, rows, st);
+}
+
+} // namespace mlb

@@ -1,0 +1,676 @@
+// Unfused step kernels: one sweep per reference loop.
+//
+//   UpdateQuantities  -> uq_kernel   (src/models/lyotropic.cpp:168-247,
+//                                     src/models/nematic.cpp:76-130)
+//   UpdateFields      -> uf_kernel   (src/models/lyotropic.cpp:249-341,
+//                                     src/models/nematic.cpp:132-226)
+//   Move              -> move_kernel (src/models/lyotropic.cpp:371-386),
+//                        written as a pull over the extended torus, which
+//                        assigns every target exactly the value the
+//                        reference's push assigns it
+//   BoundaryConditions*-> bc_*_kernel (src/fields.hpp:620-930)
+//
+// Two instantiations:
+//   T = double, DEV = false : the FP64 oracle mode. This file is compiled
+//     with --fmad=false and every expression keeps the reference's operand
+//     order, so each value is rounded exactly as the reference's x86-64
+//     build rounds it.
+//   T = float,  DEV = true  : FP32 on wall lattices (the fused kernel covers
+//     periodic ones). Populations are stored as deviations g_v = f_v - t_v*rho
+//     from the rest state, so the O(1e-3) flow signal is not lost against
+//     rho = 40 in a 24-bit mantissa.
+#include "lb_common.cuh"
+#include "unfused.h"
+
+#include <utility>
+
+namespace mlb {
+namespace {
+
+template<typename T>
+struct Nbr
+{
+  long long e, e1, e2, e3, e4;  // self, +x, -x, +y, -y
+};
+
+template<typename T>
+__device__ __forceinline__ Nbr<T> neighbours(const Dims& d, int X, int Y)
+{
+  Nbr<T> n;
+  const int Xp = X + 1 == d.EX ? 0 : X + 1, Xm = X == 0 ? d.EX - 1 : X - 1;
+  const int Yp = Y + 1 == d.EY ? 0 : Y + 1, Ym = Y == 0 ? d.EY - 1 : Y - 1;
+  n.e  = Y  + (long long)d.EY*X;
+  n.e1 = Y  + (long long)d.EY*Xp;
+  n.e2 = Y  + (long long)d.EY*Xm;
+  n.e3 = Yp + (long long)d.EY*X;
+  n.e4 = Ym + (long long)d.EY*X;
+  return n;
+}
+
+// 5-point stencils (src/lb.hpp:79, :89, :134); `+0*stencil` adds +0
+template<typename T>
+__device__ __forceinline__ T dX(const T* __restrict__ a, const Nbr<T>& n)
+{ return T(.5)*(a[n.e1]-a[n.e2]) + T(0); }
+template<typename T>
+__device__ __forceinline__ T dY(const T* __restrict__ a, const Nbr<T>& n)
+{ return T(.5)*(a[n.e3]-a[n.e4]) + T(0); }
+template<typename T>
+__device__ __forceinline__ T lap(const T* __restrict__ a, const Nbr<T>& n)
+{ return a[n.e1]+a[n.e2]+a[n.e3]+a[n.e4] - T(4)*a[n.e] + T(0); }
+
+// Equilibrium (src/lb.hpp:24-41). DEV: deviation from t_v*rho, given the
+// density deviation dn = nn - rho (t_v*dn + the velocity terms times nn).
+template<typename T, bool DEV>
+__device__ __forceinline__ void equilibrium(T vx, T vy, T nn, T dn, T fe[9])
+{
+  const T v2 = vx*vx + vy*vy;
+  if constexpr (!DEV)
+  {
+    fe[1] = nn*(T(1./9.) + T(1./3.)*vx + T(1./3.)*v2 - T(1./2.)*vy*vy);
+    fe[2] = nn*(T(1./9.) - T(1./3.)*vx + T(1./3.)*v2 - T(1./2.)*vy*vy);
+    fe[3] = nn*(T(1./9.) + T(1./3.)*vy - T(1./2.)*vx*vx + T(1./3.)*v2);
+    fe[4] = nn*(T(1./9.) - T(1./3.)*vy - T(1./2.)*vx*vx + T(1./3.)*v2);
+    fe[5] = nn*(T(1./36.) + T(1./12.)*vx + T(1./12.)*vy + T(1./12.)*v2 + T(1./4.)*vx*vy);
+    fe[6] = nn*(T(1./36.) - T(1./12.)*vx - T(1./12.)*vy + T(1./12.)*v2 + T(1./4.)*vx*vy);
+    fe[7] = nn*(T(1./36.) - T(1./12.)*vx + T(1./12.)*vy + T(1./12.)*v2 - T(1./4.)*vx*vy);
+    fe[8] = nn*(T(1./36.) + T(1./12.)*vx - T(1./12.)*vy + T(1./12.)*v2 - T(1./4.)*vx*vy);
+    fe[0] = nn-fe[1]-fe[2]-fe[3]-fe[4]-fe[5]-fe[6]-fe[7]-fe[8];
+  }
+  else
+  {
+    fe[1] = T(1./9.)*dn + nn*( T(1./3.)*vx + T(1./3.)*v2 - T(1./2.)*vy*vy);
+    fe[2] = T(1./9.)*dn + nn*(-T(1./3.)*vx + T(1./3.)*v2 - T(1./2.)*vy*vy);
+    fe[3] = T(1./9.)*dn + nn*( T(1./3.)*vy - T(1./2.)*vx*vx + T(1./3.)*v2);
+    fe[4] = T(1./9.)*dn + nn*(-T(1./3.)*vy - T(1./2.)*vx*vx + T(1./3.)*v2);
+    fe[5] = T(1./36.)*dn + nn*( T(1./12.)*vx + T(1./12.)*vy + T(1./12.)*v2 + T(1./4.)*vx*vy);
+    fe[6] = T(1./36.)*dn + nn*(-T(1./12.)*vx - T(1./12.)*vy + T(1./12.)*v2 + T(1./4.)*vx*vy);
+    fe[7] = T(1./36.)*dn + nn*(-T(1./12.)*vx + T(1./12.)*vy + T(1./12.)*v2 - T(1./4.)*vx*vy);
+    fe[8] = T(1./36.)*dn + nn*( T(1./12.)*vx - T(1./12.)*vy + T(1./12.)*v2 - T(1./4.)*vx*vy);
+    fe[0] = dn-fe[1]-fe[2]-fe[3]-fe[4]-fe[5]-fe[6]-fe[7]-fe[8];
+  }
+}
+
+template<typename T, bool DEV, int MODEL, bool DIAG>
+__global__ void __launch_bounds__(256)
+uq_kernel(Dims d, Params P, State<T> s)
+{
+  const int y = blockIdx.x*blockDim.x + threadIdx.x;
+  const int x = blockIdx.y*blockDim.y + threadIdx.y;
+  if(x >= d.LX || y >= d.LY) return;
+  const Nbr<T> nb = neighbours<T>(d, x + d.g, y + d.g);
+  const long long e = nb.e, NE = d.NE;
+  const T* __restrict__ F = s.ff;
+  const T f0 = F[e], f1 = F[NE+e], f2 = F[2*NE+e], f3 = F[3*NE+e], f4 = F[4*NE+e],
+          f5 = F[5*NE+e], f6 = F[6*NE+e], f7 = F[7*NE+e], f8 = F[8*NE+e];
+  const T Qxx = s.Qxx[e], Qyx = s.Qyx[e];
+
+  T nn, dn;
+  if constexpr (DEV) { dn = f0 + f1 + f2 + f3 + f4 + f5 + f6 + f7 + f8; nn = T(P.rho) + dn; }
+  else { nn = f0 + f1 + f2 + f3 + f4 + f5 + f6 + f7 + f8; dn = nn; }
+  const T vx = (f1 - f2 + f5 - f6 - f7 + f8)/nn;
+  const T vy = (f3 - f4 + f5 - f6 + f7 - f8)/nn;
+
+  const T del2Qxx = lap(s.Qxx, nb);
+  const T dxQxx = dX(s.Qxx, nb);
+  const T dyQxx = dY(s.Qxx, nb);
+  const T del2Qyx = lap(s.Qyx, nb);
+  const T dxQyx = dX(s.Qyx, nb);
+  const T dyQyx = dY(s.Qyx, nb);
+
+  const T CC = T(P.CC), LL = T(P.LL), xi = T(P.xi), zeta = T(P.zeta);
+
+  s.n[e] = DEV ? dn : nn;   // DEV mode keeps the density deviation
+  s.ux[e] = vx;
+  s.uy[e] = vy;
+  s.dxQxx[e] = dxQxx;
+  s.dxQyx[e] = dxQyx;
+  s.dyQxx[e] = dyQxx;
+  s.dyQyx[e] = dyQyx;
+
+  if constexpr (MODEL == LYO)
+  {
+    const T AA = T(P.AA), KK = T(P.KK), zetaI = T(P.zetaI), conc = T(P.conc);
+    const T p = s.phi[e];
+    const T del2p = lap(s.phi, nb);
+    const T dxPhi = dX(s.phi, nb);
+    const T dyPhi = dY(s.phi, nb);
+    const T term = T(0) - Qxx*Qxx - Qyx*Qyx;
+    const T Hxx = CC*term*Qxx + LL*del2Qxx;
+    const T Hyx = CC*term*Qyx + LL*del2Qyx;
+    const T mu = AA*p*(T(1)-p)*(T(1)-T(2)*p) + T(0)*CC*term - KK*del2p;
+    const T sigmaB = T(.5)*AA*p*p*(T(1)-p)*(T(1)-p) + T(.5)*CC*term*term - mu*p;
+    const T sigmaF = T(2)*xi*( (Qxx*Qxx-T(1))*Hxx + Qxx*Qyx*Hyx )
+      - zeta*Qxx*(T(1)-p) + T(.5)*KK*(dyPhi*dyPhi-dxPhi*dxPhi)
+      + LL*(dyQxx*dyQxx+dyQyx*dyQyx-dxQxx*dxQxx-dxQyx*dxQyx);
+    const T sigmaS = T(2)*xi*(Qyx*Qxx*Hxx + (Qyx*Qyx-T(1))*Hyx)
+      - zeta*Qyx*(T(1)-p) - KK*dxPhi*dyPhi
+      - T(2)*LL*(dxQxx*dyQxx+dxQyx*dyQyx);
+    const T sigmaA = T(2)*(Qxx*Hyx - Qyx*Hxx);
+
+    s.uxp[e] = vx*p;
+    s.uyp[e] = vy*p;
+    s.Hxx[e] = Hxx;
+    s.Hyx[e] = Hyx;
+    s.MU[e] = mu;
+    s.sXX[e] = sigmaF + sigmaB + zetaI*(conc-p);
+    s.sYY[e] = -sigmaF + sigmaB + zetaI*(conc-p);
+    s.sXY[e] = sigmaS + sigmaA;
+    s.sYX[e] = sigmaS - sigmaA;
+    if constexpr (DIAG)
+    {
+      s.diag[0][e] = sigmaB + zetaI*(conc-p);
+      s.diag[1][e] = sigmaF - T(.5)*KK*(dyPhi*dyPhi-dxPhi*dxPhi) + zeta*Qxx*(T(1)-p);
+      // the reference uses zeta*Qxx here too (src/models/lyotropic.cpp:242)
+      s.diag[2][e] = sigmaS + KK*dxPhi*dyPhi + zeta*Qxx*(T(1)-p);
+      s.diag[3][e] = T(.5)*KK*(dyPhi*dyPhi-dxPhi*dxPhi);
+      s.diag[4][e] = -KK*dxPhi*dyPhi;
+      s.diag[5][e] = -zeta*Qxx*(T(1)-p);
+      s.diag[6][e] = -zeta*Qyx*(T(1)-p);
+    }
+  }
+  else
+  {
+    const T term = T(1.) - Qxx*Qxx - Qyx*Qyx;
+    const T Hxx = CC*term*Qxx + LL*del2Qxx;
+    const T Hyx = CC*term*Qyx + LL*del2Qyx;
+    const T sigmaB = T(.5)*CC*term*term;
+    const T sigmaF = T(2)*xi*( (Qxx*Qxx-T(1.))*Hxx + Qxx*Qyx*Hyx )
+      - zeta*Qxx
+      + LL*(dyQxx*dyQxx+dyQyx*dyQyx-dxQxx*dxQxx-dxQyx*dxQyx);
+    const T sigmaS = T(2)*xi*(Qyx*Qxx*Hxx + (Qyx*Qyx-T(1))*Hyx) - zeta*Qyx
+      - T(2)*LL*(dxQxx*dyQxx+dxQyx*dyQyx);
+    const T sigmaA = T(2)*(Qxx*Hyx - Qyx*Hxx);
+    s.Hxx[e] = Hxx;
+    s.Hyx[e] = Hyx;
+    s.sXX[e] = sigmaF + sigmaB;
+    s.sYY[e] = -sigmaF + sigmaB;
+    s.sXY[e] = sigmaS + sigmaA;
+    s.sYX[e] = sigmaS - sigmaA;
+  }
+}
+
+template<typename T, bool DEV, int MODEL, bool FIRST>
+__global__ void __launch_bounds__(256)
+uf_kernel(Dims d, Params P, State<T> s)
+{
+  const int y = blockIdx.x*blockDim.x + threadIdx.x;
+  const int x = blockIdx.y*blockDim.y + threadIdx.y;
+  if(x >= d.LX || y >= d.LY) return;
+  const Nbr<T> nb = neighbours<T>(d, x + d.g, y + d.g);
+  const long long e = nb.e, NE = d.NE;
+
+  const T nstore = s.n[e];
+  const T nn = DEV ? T(P.rho) + nstore : nstore;
+  const T dn = nstore;
+  const T vx = s.ux[e];
+  const T vy = s.uy[e];
+  const T Qxx = s.Qxx[e];
+  const T Qyx = s.Qyx[e];
+  const T Hxx = s.Hxx[e];
+  const T Hyx = s.Hyx[e];
+  const T dxQxx = s.dxQxx[e];
+  const T dyQxx = s.dyQxx[e];
+  const T dxQyx = s.dxQyx[e];
+  const T dyQyx = s.dyQyx[e];
+
+  const T dxux = dX(s.ux, nb);
+  const T dyux = dY(s.ux, nb);
+  const T dxuy = dX(s.uy, nb);
+  const T dyuy = dY(s.uy, nb);
+  const T dxSxx = dX(s.sXX, nb);
+  const T dySxy = dY(s.sXY, nb);
+  const T dxSyx = dX(s.sYX, nb);
+  const T dySyy = dY(s.sYY, nb);
+
+  const T GammaQ = T(P.GammaQ), xi = T(P.xi), friction = T(P.friction);
+
+  const T expansion = dxux + dyuy;
+  const T shear     = T(.5)*(dxuy + dyux);
+  const T vorticity = T(.5)*(dxuy - dyux);
+  const T traceQL   = Qxx*(dxux - dyuy) + T(2)*Qyx*shear;
+
+  const T Dxx = GammaQ*Hxx - vx*dxQxx - vy*dyQxx - T(2)*vorticity*Qyx
+    + xi*((Qxx+T(1))*(T(2)*dxux-traceQL) +T(2)*Qyx*shear -expansion);
+  const T Dyx = GammaQ*Hyx - vx*dxQyx - vy*dyQyx + T(2)*vorticity*Qxx
+    + xi*( Qyx*(expansion-traceQL) + T(2)*shear);
+
+  const T Fx = dxSxx + dySxy - friction*vx;
+  const T Fy = dxSyx + dySyy - friction*vy;
+
+  T fe[9];
+  equilibrium<T, DEV>(vx, vy, nn, dn, fe);
+
+  T* __restrict__ FF = s.ff;
+  T* __restrict__ FN = s.fn;
+
+  if constexpr (MODEL == LYO)
+  {
+    const T p = s.phi[e];
+    const T del2mu = lap(s.MU, nb);
+    const T pFlux = dX(s.uxp, nb) + dY(s.uyp, nb);
+    // conserve_phi is false in the reference (src/models/lyotropic.hpp:46)
+    const T Dp = T(P.GammaP)*del2mu - pFlux - T(0);
+    const T tau = T(P.tauNem)*p + T(P.tauIso)*(T(1)-p);
+    if constexpr (FIRST)
+    {
+      s.QNxx[e] = s.Qxx[e] + T(.5)*Dxx;
+      s.QNyx[e] = s.Qyx[e] + T(.5)*Dyx;
+      s.phn[e]  = s.phi[e] + T(.5)*Dp;
+      s.Qxx[e]  = s.Qxx[e] + Dxx;
+      s.Qyx[e]  = s.Qyx[e] + Dyx;
+      s.phi_tmp[e] = s.phi[e] + Dp;
+#pragma unroll
+      for(int v=0; v<9; ++v)
+      {
+        const T f = FF[v*NE+e];
+        const T force = T(Wv(v))*(Fx*T(CXv(v)) + Fy*T(CYv(v)));
+        FN[v*NE+e] = f + T(.5)*((fe[v]-f)/tau + force);
+        FF[v*NE+e] = f +      ((fe[v]-f)/tau + force);
+      }
+    }
+    else
+    {
+      s.Qxx[e] = s.QNxx[e] + T(.5)*Dxx;
+      s.Qyx[e] = s.QNyx[e] + T(.5)*Dyx;
+      s.phi_tmp[e] = s.phn[e] + T(.5)*Dp;
+#pragma unroll
+      for(int v=0; v<9; ++v)
+      {
+        const T f = FF[v*NE+e];
+        const T force = T(Wv(v))*(Fx*T(CXv(v)) + Fy*T(CYv(v)));
+        FF[v*NE+e] = FN[v*NE+e] + T(.5)*((fe[v]-f)/tau + force);
+      }
+    }
+  }
+  else
+  {
+    const T tau = T(P.tauNem);
+    if constexpr (FIRST)
+    {
+      const T qn_xx = s.Qxx[e] + T(.5)*Dxx + T(0);
+      const T qn_yx = s.Qyx[e] + T(.5)*Dyx + T(0);
+      s.QNxx[e] = qn_xx;
+      s.QNyx[e] = qn_yx;
+      s.Qxx[e] = qn_xx + T(.5)*Dxx;
+      s.Qyx[e] = qn_yx + T(.5)*Dyx;
+#pragma unroll
+      for(int v=0; v<9; ++v)
+      {
+        const T f = FF[v*NE+e];
+        const T force = T(Wv(v))*(Fx*T(CXv(v)) + Fy*T(CYv(v)));
+        const T fnv = f + T(.5)*((fe[v]-f)/tau + force) + T(0);
+        FN[v*NE+e] = fnv;
+        FF[v*NE+e] = fnv + T(.5)*((fe[v]-f)/tau + force);
+      }
+    }
+    else
+    {
+      s.Qxx[e] = s.QNxx[e] + T(.5)*Dxx;
+      s.Qyx[e] = s.QNyx[e] + T(.5)*Dyx;
+#pragma unroll
+      for(int v=0; v<9; ++v)
+      {
+        const T f = FF[v*NE+e];
+        const T force = T(Wv(v))*(Fx*T(CXv(v)) + Fy*T(CYv(v)));
+        FF[v*NE+e] = FN[v*NE+e] + T(.5)*((fe[v]-f)/tau + force);
+      }
+    }
+  }
+}
+
+// Streaming as a pull over every extended site.
+template<typename T>
+__global__ void __launch_bounds__(256)
+move_kernel(Dims d, const T* __restrict__ ff, const T* __restrict__ fn,
+            T* __restrict__ ff_out, T* __restrict__ fn_out)
+{
+  const int Y = blockIdx.x*blockDim.x + threadIdx.x;
+  const int X = blockIdx.y*blockDim.y + threadIdx.y;
+  if(X >= d.EX || Y >= d.EY) return;
+  const long long e = Y + (long long)d.EY*X, NE = d.NE;
+#pragma unroll
+  for(int v=0; v<9; ++v)
+  {
+    const int Xs = wrapi(X - CXv(v), d.EX), Ys = wrapi(Y - CYv(v), d.EY);
+    const long long src = Ys + (long long)d.EY*Xs;
+    ff_out[v*NE+e] = ff[v*NE+src];
+    fn_out[v*NE+e] = fn[v*NE+src];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Wall boundary conditions on the ghost ring (g = 1), src/fields.hpp:620-930.
+// Wall and corner ids are their direction numbers (src/geometry.hpp:146-193).
+
+enum { W_RIGHT = 1, W_LEFT = 2, W_BACK = 3, W_FRONT = 4 };
+enum { C_RIGHTBACK = 5, C_LEFTFRONT = 6, C_LEFTBACK = 7, C_RIGHTFRONT = 8 };
+
+__constant__ int c_refl[9][9] = {
+  {0, 2, 1, 4, 3, 6, 5, 8, 7},
+  {0, 2, 1, 3, 4, 7, 8, 5, 6},
+  {0, 2, 1, 3, 4, 7, 8, 5, 6},
+  {0, 1, 2, 4, 3, 8, 7, 6, 5},
+  {0, 1, 2, 4, 3, 8, 7, 6, 5},
+  {0, 4, 3, 2, 1, 6, 5, 7, 8},
+  {0, 4, 3, 2, 1, 6, 5, 7, 8},
+  {0, 3, 4, 1, 2, 5, 6, 8, 7},
+  {0, 3, 4, 1, 2, 5, 6, 8, 7}};
+__constant__ int c_proj[9][9] = {
+  {0, 0, 0, 0, 0, 0, 0, 0, 0},
+  {0, 0, 0, 3, 4, 3, 4, 3, 4},
+  {0, 0, 0, 3, 4, 3, 4, 3, 4},
+  {0, 1, 2, 0, 0, 1, 2, 2, 1},
+  {0, 1, 2, 0, 0, 1, 2, 2, 1},
+  {0, 5, 6, 5, 6, 5, 6, 0, 0},
+  {0, 1, 2, 4, 3, 8, 7, 6, 5},
+  {0, 8, 7, 7, 8, 0, 0, 7, 8},
+  {0, 8, 7, 7, 8, 0, 0, 7, 8}};
+
+struct XY { int X, Y; };
+
+__device__ __forceinline__ XY wall_xy(const Dims& d, int w, int k)
+{
+  switch(w)
+  {
+    case W_LEFT:  return {0, k + 1};
+    case W_RIGHT: return {d.EX - 1, k + 1};
+    case W_FRONT: return {k + 1, 0};
+    default:      return {k + 1, d.EY - 1};
+  }
+}
+__device__ __forceinline__ XY corner_xy(const Dims& d, int c)
+{
+  switch(c)
+  {
+    case C_LEFTFRONT:  return {0, 0};
+    case C_RIGHTFRONT: return {d.EX - 1, 0};
+    case C_LEFTBACK:   return {0, d.EY - 1};
+    default:           return {d.EX - 1, d.EY - 1};
+  }
+}
+__device__ __forceinline__ XY step_xy(const Dims& d, XY a, int v)
+{
+  return {wrapi(a.X + CXv(v), d.EX), wrapi(a.Y + CYv(v), d.EY)};
+}
+__device__ __forceinline__ long long at(const Dims& d, XY a)
+{
+  return a.Y + (long long)d.EY*a.X;
+}
+__device__ __forceinline__ bool incoming(int v, int w)
+{
+  return CXv(w)*CXv(v) == -1 || CYv(w)*CYv(v) == -1;
+}
+
+// one scalar ghost value from inward direction `in`
+template<typename T>
+__device__ __forceinline__ void s_apply(const Dims& d, T* a, XY i, int in, int kind)
+{
+  const XY j = step_xy(d, i, in);
+  if(kind == BC_NEUMANN) a[at(d, i)] = a[at(d, j)];
+  else if(kind == BC_DIRICHLET0) a[at(d, i)] = T(2)*T(0) - a[at(d, j)];
+  else a[at(d, i)] = T(2)*a[at(d, j)] - a[at(d, step_xy(d, j, in))];
+}
+
+// Scalar fields. Phase 1: walls (they read domain values only); phase 2:
+// corners (channel corners read the left/right ghosts written in phase 1).
+template<typename T>
+__global__ void __launch_bounds__(1024)
+bc_scalar_kernel(Dims d, ScalarBC<T> job)
+{
+  const int LX = d.LX, LY = d.LY;
+  const int nwall = 2*LY + 2*LX;
+  for(int idx = threadIdx.x; idx < nwall; idx += blockDim.x)
+  {
+    int w, k;
+    if(idx < LY) { w = W_LEFT; k = idx; }
+    else if(idx < 2*LY) { w = W_RIGHT; k = idx - LY; }
+    else if(idx < 2*LY + LX) { w = W_FRONT; k = idx - 2*LY; }
+    else { w = W_BACK; k = idx - 2*LY - LX; }
+    const XY i = wall_xy(d, w, k);
+    const bool pbc = job.mode == BCM_PBC ||
+                     (job.mode == BCM_CHANNEL && (w == W_LEFT || w == W_RIGHT));
+    for(int f = 0; f < job.nf; ++f)
+    {
+      T* a = job.f[f];
+      if(pbc)
+      {
+        const XY o = wall_xy(d, OPPv(w), k);
+        a[at(d, i)] = a[at(d, step_xy(d, o, w))];
+      }
+      else s_apply(d, a, i, OPPv(w), job.kind[f]);
+    }
+  }
+  __syncthreads();
+  if(threadIdx.x < 4)
+  {
+    // order of the reference's corner calls does not matter: each corner
+    // reads a wall ghost or a domain site, never another corner
+    const int cs[4] = {C_RIGHTBACK, C_RIGHTFRONT, C_LEFTBACK, C_LEFTFRONT};
+    const int c = cs[threadIdx.x];
+    const XY i = corner_xy(d, c);
+    for(int f = 0; f < job.nf; ++f)
+    {
+      T* a = job.f[f];
+      if(job.mode == BCM_PBC)
+        a[at(d, i)] = a[at(d, step_xy(d, corner_xy(d, OPPv(c)), c))];
+      else if(job.mode == BCM_CHANNEL)
+      {
+        const int w = (c == C_RIGHTBACK || c == C_LEFTBACK) ? W_BACK : W_FRONT;
+        s_apply(d, a, i, OPPv(w), job.kind[f]);
+      }
+      else s_apply(d, a, i, OPPv(c), job.kind[f]);
+    }
+  }
+}
+
+template<typename T>
+__device__ __forceinline__ void f_pbc_node(const Dims& d, T* f, XY dst, XY src)
+{
+  const long long a = at(d, dst), b = at(d, src);
+#pragma unroll
+  for(int v=0; v<9; ++v) f[v*d.NE + a] = f[v*d.NE + b];
+}
+
+template<typename T>
+__device__ __forceinline__ void f_wall(const Dims& d, T* f, int w, int k, bool noslip)
+{
+  const XY i = wall_xy(d, w, k);
+  const long long ki = at(d, i);
+#pragma unroll
+  for(int v=0; v<9; ++v)
+    if(incoming(v, w))
+    {
+      if(noslip) f[v*d.NE + ki] = f[OPPv(v)*d.NE + at(d, step_xy(d, i, v))];
+      else f[v*d.NE + ki] = f[c_refl[w][v]*d.NE + at(d, step_xy(d, i, OPPv(w)))];
+    }
+}
+
+// Population fields ff and fn. Phase 1: left/right walls, and every wall
+// whose update reads domain values only; phase 2: front/back no-slip walls
+// (their diagonal bounce reads the left/right ghosts, which the reference
+// has already updated by then); phase 3: corners.
+template<typename T>
+__global__ void __launch_bounds__(1024)
+bc_lb_kernel(Dims d, T* ff, T* fn, int kind)
+{
+  const int LX = d.LX, LY = d.LY;
+  T* arrs[2] = {ff, fn};
+  // phase 1
+  for(int idx = threadIdx.x; idx < 2*LY + 2*LX; idx += blockDim.x)
+  {
+    int w, k;
+    if(idx < LY) { w = W_LEFT; k = idx; }
+    else if(idx < 2*LY) { w = W_RIGHT; k = idx - LY; }
+    else if(idx < 2*LY + LX) { w = W_FRONT; k = idx - 2*LY; }
+    else { w = W_BACK; k = idx - 2*LY - LX; }
+    const bool lr = (w == W_LEFT || w == W_RIGHT);
+    for(int a = 0; a < 2; ++a)
+    {
+      T* f = arrs[a];
+      if(kind == LBK_PBC || ((kind == LBK_FREESLIP_CHANNEL || kind == LBK_NOSLIP_CHANNEL) && lr))
+        f_pbc_node(d, f, wall_xy(d, w, k), step_xy(d, wall_xy(d, OPPv(w), k), w));
+      else if(kind == LBK_FREESLIP_CHANNEL || kind == LBK_FREESLIP_BOX)
+        f_wall(d, f, w, k, false);
+      else if(kind == LBK_NOSLIP_BOX && lr)
+        f_wall(d, f, w, k, true);
+    }
+  }
+  __syncthreads();
+  // phase 2
+  if(kind == LBK_NOSLIP_CHANNEL || kind == LBK_NOSLIP_BOX)
+  {
+    for(int idx = threadIdx.x; idx < 2*LX; idx += blockDim.x)
+    {
+      const int w = idx < LX ? W_FRONT : W_BACK;
+      const int k = idx < LX ? idx : idx - LX;
+      for(int a = 0; a < 2; ++a) f_wall(d, arrs[a], w, k, true);
+    }
+  }
+  __syncthreads();
+  // phase 3
+  if(threadIdx.x < 4)
+  {
+    const int cs[4] = {C_RIGHTBACK, C_RIGHTFRONT, C_LEFTBACK, C_LEFTFRONT};
+    const int c = cs[threadIdx.x];
+    const XY i = corner_xy(d, c);
+    for(int a = 0; a < 2; ++a)
+    {
+      T* f = arrs[a];
+      if(kind == LBK_PBC)
+        f_pbc_node(d, f, i, step_xy(d, corner_xy(d, OPPv(c)), c));
+      else if(kind == LBK_FREESLIP_CHANNEL)
+      {
+        const int w = (c == C_RIGHTBACK || c == C_LEFTBACK) ? W_BACK : W_FRONT;
+        const int p = c_proj[w][c];
+        const int v = OPPv(c);
+        const XY l = step_xy(d, corner_xy(d, c_refl[p][c]), p);
+        f[v*d.NE + at(d, i)] = f[v*d.NE + at(d, l)];
+      }
+      else
+      {
+        const int v = OPPv(c);
+        f[v*d.NE + at(d, i)] = f[c*d.NE + at(d, step_xy(d, i, v))];
+      }
+    }
+  }
+}
+
+inline dim3 site_grid(int nx, int ny, dim3 blk)
+{
+  return dim3((ny + blk.x - 1)/blk.x, (nx + blk.y - 1)/blk.y);
+}
+
+template<typename T, bool DEV, int MODEL>
+int step_impl(const Dims& d, const Params& P, State<T>& s, int bc,
+              unsigned nsteps, bool diag_last, cudaStream_t st)
+{
+  const dim3 blk(64, 4);
+  const dim3 grd = site_grid(d.LX, d.LY, blk);
+  const dim3 egrd = site_grid(d.EX, d.EY, blk);
+  const int lbk = lb_kind(MODEL, bc);
+  const int bcm_fields = bc_mode(MODEL, bc);
+
+  auto fields_bc = [&]() {
+    if(!bc) return;
+    ScalarBC<T> j{};
+    j.mode = bcm_fields;
+    j.f[0] = s.Qxx; j.f[1] = s.Qyx; j.nf = 2;
+    if(MODEL == LYO) { j.f[2] = s.phi; j.nf = 3; }
+    for(int i = 0; i < j.nf; ++i) j.kind[i] = BC_NEUMANN;
+    bc_scalar_kernel<T><<<1, 1024, 0, st>>>(d, j);
+  };
+  auto fields2_bc = [&]() {
+    if(!bc) return;
+    ScalarBC<T> j{};
+    j.mode = bcm_fields;
+    if(MODEL == LYO)
+    {
+      T* fs[9] = {s.uy, s.ux, s.uyp, s.uxp, s.MU, s.sXX, s.sYY, s.sYX, s.sXY};
+      const int ks[9] = {BC_COPYDERIV, BC_COPYDERIV, BC_DIRICHLET0, BC_DIRICHLET0,
+                         BC_NEUMANN, BC_NEUMANN, BC_NEUMANN, BC_NEUMANN, BC_NEUMANN};
+      for(int i = 0; i < 9; ++i) { j.f[i] = fs[i]; j.kind[i] = ks[i]; }
+      j.nf = 9;
+    }
+    else
+    {
+      // nematic walls use Neumann for u as well (src/models/nematic.cpp:338-357)
+      T* fs[6] = {s.ux, s.uy, s.sXX, s.sYY, s.sYX, s.sXY};
+      for(int i = 0; i < 6; ++i) { j.f[i] = fs[i]; j.kind[i] = BC_NEUMANN; }
+      j.nf = 6;
+    }
+    bc_scalar_kernel<T><<<1, 1024, 0, st>>>(d, j);
+  };
+
+  for(unsigned it = 0; it < nsteps; ++it)
+  {
+    fields_bc();
+    uq_kernel<T, DEV, MODEL, false><<<grd, blk, 0, st>>>(d, P, s);
+    fields2_bc();
+    uf_kernel<T, DEV, MODEL, true><<<grd, blk, 0, st>>>(d, P, s);
+    if(MODEL == LYO) std::swap(s.phi, s.phi_tmp);
+    if(bc) bc_lb_kernel<T><<<1, 1024, 0, st>>>(d, s.ff, s.fn, lbk);
+    move_kernel<T><<<egrd, blk, 0, st>>>(d, s.ff, s.fn, s.ff_tmp, s.fn_tmp);
+    std::swap(s.ff, s.ff_tmp);
+    std::swap(s.fn, s.fn_tmp);
+    for(unsigned c = 1; c <= P.npc; ++c)
+    {
+      const bool diag = diag_last && it + 1 == nsteps && c == P.npc;
+      fields_bc();
+      if(diag) uq_kernel<T, DEV, MODEL, true><<<grd, blk, 0, st>>>(d, P, s);
+      else uq_kernel<T, DEV, MODEL, false><<<grd, blk, 0, st>>>(d, P, s);
+      fields2_bc();
+      uf_kernel<T, DEV, MODEL, false><<<grd, blk, 0, st>>>(d, P, s);
+      if(MODEL == LYO) std::swap(s.phi, s.phi_tmp);
+    }
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+} // namespace
+
+int lb_kind(int model, int bc)
+{
+  if(model == LYO)
+  {
+    switch(bc)
+    {
+      case 1: return LBK_FREESLIP_CHANNEL;
+      case 2: return LBK_NOSLIP_CHANNEL;
+      case 3: return LBK_FREESLIP_BOX;
+      case 4: return LBK_NOSLIP_BOX;
+      default: return LBK_PBC;
+    }
+  }
+  return bc == 1 ? LBK_FREESLIP_CHANNEL : LBK_PBC;
+}
+
+int bc_mode(int model, int bc)
+{
+  if(model == LYO)
+    return (bc == 1 || bc == 2) ? BCM_CHANNEL : (bc == 3 || bc == 4) ? BCM_BOX : BCM_PBC;
+  return bc == 1 ? BCM_CHANNEL : BCM_PBC;
+}
+
+int launches_unfused(int model, int bc, unsigned npc)
+{
+  // predictor: [bc] uq [bc] uf [bc] move ; corrector: [bc] uq [bc] uf
+  const int w = bc ? 1 : 0;
+  (void)model;
+  return (2 + 3*w + 1) + (int)npc*(2 + 2*w);
+}
+
+int step_unfused_f64(const Dims& d, const Params& P, State<double>& s, int bc,
+                     unsigned nsteps, bool diag_last, cudaStream_t st)
+{
+  return P.model == LYO ? step_impl<double, false, LYO>(d, P, s, bc, nsteps, diag_last, st)
+                        : step_impl<double, false, NEM>(d, P, s, bc, nsteps, diag_last, st);
+}
+
+int step_unfused_f32(const Dims& d, const Params& P, State<float>& s, int bc,
+                     unsigned nsteps, bool diag_last, cudaStream_t st)
+{
+  return P.model == LYO ? step_impl<float, true, LYO>(d, P, s, bc, nsteps, diag_last, st)
+                        : step_impl<float, true, NEM>(d, P, s, bc, nsteps, diag_last, st);
+}
+
+} // namespace mlb

@@ -1,0 +1,37 @@
+// Host entry points of the unfused step kernels (unfused.cu).
+#pragma once
+
+#include "lb_common.cuh"
+
+namespace mlb {
+
+// scalar ghost kinds (src/fields.hpp:705-778)
+enum { BC_NEUMANN = 0, BC_DIRICHLET0 = 1, BC_COPYDERIV = 2 };
+// scalar ghost layouts: channel (pbc left/right), box, full pbc
+enum { BCM_CHANNEL = 0, BCM_BOX = 1, BCM_PBC = 2 };
+// population ghost layouts (src/fields.hpp:792-930)
+enum { LBK_PBC = 0, LBK_FREESLIP_CHANNEL = 1, LBK_NOSLIP_CHANNEL = 2,
+       LBK_FREESLIP_BOX = 3, LBK_NOSLIP_BOX = 4 };
+
+template<typename T>
+struct ScalarBC
+{
+  T* f[9];
+  int kind[9];
+  int nf;
+  int mode;
+};
+
+int lb_kind(int model, int bc);
+int bc_mode(int model, int bc);
+int launches_unfused(int model, int bc, unsigned npc);
+
+// Advance `nsteps` steps; swaps the ping-pong pointers held in `s`.
+// diag_last: the last corrector UpdateQuantities also writes the seven
+// diagnostic stress fields.
+int step_unfused_f64(const Dims& d, const Params& P, State<double>& s, int bc,
+                     unsigned nsteps, bool diag_last, cudaStream_t st);
+int step_unfused_f32(const Dims& d, const Params& P, State<float>& s, int bc,
+                     unsigned nsteps, bool diag_last, cudaStream_t st);
+
+} // namespace mlb

@@ -1,0 +1,252 @@
+"""Python front-end of libmass_lb.so (include/mass_lb.h) through ctypes.
+
+This mirrors the reference's model interface for one lattice: construct with
+the runcard parameters and (LX, LY, BC) as declare_model's factory does
+(src/models.hpp:197-205), upload the configured state, `step()` as
+Model::Step(), read fields by their reference member names, and
+`runtime_checks()` with the semantics of Model::RuntimeChecks()
+(src/models/lyotropic.cpp:527-549): an error when |sum f - ftot| > 1.
+
+There is no CPU fallback: if the CUDA library is missing or no sm_100 device
+is present, construction raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libmass_lb.so")
+
+LYOTROPIC, NEMATIC = 0, 1
+FP64, FP32 = 0, 1
+
+FIELDS = ("ff", "QQxx", "QQyx", "phi", "n", "ux", "uy", "ux_phi", "uy_phi",
+          "HHxx", "HHyx", "MU", "dxQQxx", "dyQQxx", "dxQQyx", "dyQQyx",
+          "sigmaXX", "sigmaYY", "sigmaYX", "sigmaXY", "sigma_bulk",
+          "sigma_elastic_xx", "sigma_elastic_yx", "sigma_phase_field_xx",
+          "sigma_phase_field_yx", "sigma_active_xx", "sigma_active_yx", "fn",
+          "QNxx", "QNyx", "phn")
+FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
+
+STATUS = {0: "OK", -1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "EUNSUPPORTED",
+          -5: "ENOTFINITE", -6: "ENODEV"}
+
+
+class MassLBError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Params(C.Structure):
+    _fields_ = [("model", C.c_int)] + [
+        (n, C.c_double) for n in ("GammaQ", "GammaP", "xi", "tauNem", "tauIso",
+                                  "rho", "friction", "AA", "CC", "LL", "KK",
+                                  "zeta", "zetaI", "conc")
+    ] + [("npc", C.c_uint)]
+
+
+_lib = None
+
+
+def library_path() -> str:
+    return LIB_PATH
+
+
+def load_library(build_if_missing: bool = False):
+    """Load libmass_lb.so (raises if it is absent and not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        if build_if_missing:
+            from . import build as _b
+            _b.build()
+        else:
+            raise MassLBError(-6, f"{LIB_PATH} is missing; run python -m mass_hd_b200.build")
+    lib = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    dp = C.POINTER(C.c_double)
+    ip = C.POINTER(C.c_int)
+    sig = {
+        "mass_lb_abi_version": (C.c_int, []),
+        "mass_lb_last_error": (C.c_char_p, []),
+        "mass_lb_field_name": (C.c_char_p, [C.c_int]),
+        "mass_lb_create": (C.c_int, [C.POINTER(Params), C.c_uint, C.c_uint, C.c_uint,
+                                     C.c_int, C.POINTER(vp)]),
+        "mass_lb_destroy": (None, [vp]),
+        "mass_lb_upload": (C.c_int, [vp, dp, dp, dp, dp]),
+        "mass_lb_upload_field": (C.c_int, [vp, C.c_int, dp]),
+        "mass_lb_step": (C.c_int, [vp, C.c_uint]),
+        "mass_lb_download": (C.c_int, [vp, C.c_int, dp]),
+        "mass_lb_checks": (C.c_int, [vp, dp, dp, ip]),
+        "mass_lb_initial_totals": (C.c_int, [vp, dp, dp]),
+        "mass_lb_synchronize": (C.c_int, [vp]),
+        "mass_lb_stream": (vp, [vp]),
+        "mass_lb_launches_per_step": (C.c_int, [vp]),
+        "mass_lb_get_tile": (C.c_int, [vp, ip, ip]),
+        "mass_lb_set_tile": (C.c_int, [vp, C.c_int, C.c_int]),
+        "mass_lb_autotune": (C.c_int, [vp]),
+        "mass_lb_uses_fused": (C.c_int, [vp]),
+        "mass_lb_device_state": (C.c_int, [vp, C.POINTER(vp), C.POINTER(C.c_longlong), ip]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(code: int):
+    if code != 0:
+        raise MassLBError(code, load_library().mass_lb_last_error().decode())
+
+
+def make_params(model: int, params: dict) -> Params:
+    """Runcard names -> mass_lb_params. Lyotropic: GammaQ, GammaP, xi,
+    tauNem, tauIso, rho, friction, AA, CC, LL, KK, zeta, zetaI, conc, npc.
+    Nematic: Gamma, xi, tau, rho, friction, CC, LL, zeta, npc (Q_kBT and
+    u_kBT must be 0)."""
+    p = Params()
+    p.model = model
+    g = lambda k, d=0.0: float(params.get(k, d))
+    if model == LYOTROPIC:
+        for k in ("GammaQ", "GammaP", "xi", "tauNem", "tauIso", "friction",
+                  "AA", "CC", "LL", "KK", "zeta", "zetaI", "conc"):
+            setattr(p, k, g(k))
+        p.rho = g("rho", 40.0)
+    else:
+        if g("Q_kBT") != 0.0 or g("u_kBT") != 0.0:
+            raise MassLBError(-4, "thermal fluctuations (Q_kBT, u_kBT) are not supported")
+        p.GammaQ = g("Gamma")
+        p.xi = g("xi")
+        p.tauNem = p.tauIso = g("tau")
+        p.rho = g("rho", 40.0)
+        p.friction = g("friction")
+        p.CC = g("CC")
+        p.LL = g("LL")
+        p.zeta = g("zeta")
+    p.npc = int(params.get("npc", 1))
+    return p
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Lattice:
+    """One lattice on the current CUDA device (see module docstring)."""
+
+    def __init__(self, model: int, params: dict, LX: int, LY: int, bc: int = 0,
+                 precision: int = FP64):
+        lib = load_library()
+        self.model, self.LX, self.LY, self.bc, self.precision = model, LX, LY, bc, precision
+        self._params = make_params(model, params)
+        h = C.c_void_p()
+        _check(lib.mass_lb_create(C.byref(self._params), LX, LY, bc, precision, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            load_library().mass_lb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- state -------------------------------------------------------------
+    def upload(self, ff, QQxx, QQyx, phi=None):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (ff, QQxx, QQyx)]
+        ph = None if phi is None else np.ascontiguousarray(phi, dtype=np.float64)
+        N = self.LX * self.LY
+        assert arrs[0].size == 9 * N and arrs[1].size == N and arrs[2].size == N
+        _check(load_library().mass_lb_upload(self.h, _dp(arrs[0]), _dp(arrs[1]), _dp(arrs[2]),
+                                             _dp(ph) if ph is not None else None))
+
+    def upload_state(self, state: dict):
+        self.upload(state["ff"], state["QQxx"], state["QQyx"], state.get("phi"))
+
+    def upload_field(self, name: str, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        _check(load_library().mass_lb_upload_field(self.h, FIELD_ID[name], _dp(a)))
+
+    def get(self, name: str) -> np.ndarray:
+        n = self.LX * self.LY * (9 if name in ("ff", "fn") else 1)
+        out = np.empty(n, dtype=np.float64)
+        _check(load_library().mass_lb_download(self.h, FIELD_ID[name], _dp(out)))
+        return out.reshape(-1, 9) if name in ("ff", "fn") else out
+
+    def get_into(self, name: str, out: np.ndarray) -> np.ndarray:
+        assert out.dtype == np.float64 and out.flags.c_contiguous
+        _check(load_library().mass_lb_download(self.h, FIELD_ID[name], _dp(out)))
+        return out
+
+    def step(self, n: int = 1):
+        _check(load_library().mass_lb_step(self.h, n))
+
+    def synchronize(self):
+        _check(load_library().mass_lb_synchronize(self.h))
+
+    def checks(self):
+        f, p, bad = C.c_double(), C.c_double(), C.c_int()
+        _check(load_library().mass_lb_checks(self.h, C.byref(f), C.byref(p), C.byref(bad)))
+        return f.value, p.value, bool(bad.value)
+
+    def initial_totals(self):
+        f, p = C.c_double(), C.c_double()
+        _check(load_library().mass_lb_initial_totals(self.h, C.byref(f), C.byref(p)))
+        return f.value, p.value
+
+    def runtime_checks(self):
+        """Model::RuntimeChecks(): raise when the population sum drifted by
+        more than 1 from its value at upload (src/models/lyotropic.cpp:529-536)
+        or the state holds NaN/Inf."""
+        f, p, bad = self.checks()
+        ftot, _ = self.initial_totals()
+        if bad:
+            raise MassLBError(-5, "nan found in the lattice state")
+        if abs(ftot - f) > 1:
+            raise MassLBError(-5, f"f is not conserved ({ftot}/{f})")
+        return f, p
+
+    # -- introspection -------------------------------------------------------
+    @property
+    def stream(self) -> int:
+        return load_library().mass_lb_stream(self.h) or 0
+
+    @property
+    def launches_per_step(self) -> int:
+        return load_library().mass_lb_launches_per_step(self.h)
+
+    @property
+    def uses_fused(self) -> bool:
+        return bool(load_library().mass_lb_uses_fused(self.h))
+
+    def tile(self):
+        a, b = C.c_int(), C.c_int()
+        _check(load_library().mass_lb_get_tile(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def set_tile(self, threads: int, rows: int):
+        _check(load_library().mass_lb_set_tile(self.h, threads, rows))
+
+    def autotune(self):
+        _check(load_library().mass_lb_autotune(self.h))
+
+    def device_state(self):
+        p, stride, n = C.c_void_p(), C.c_longlong(), C.c_int()
+        _check(load_library().mass_lb_device_state(self.h, C.byref(p), C.byref(stride), C.byref(n)))
+        return p.value, stride.value, n.value

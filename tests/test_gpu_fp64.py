@@ -1,0 +1,138 @@
+"""FP64 oracle mode on the GPU against the reference.
+
+The FP64 mode keeps the reference's evaluation order with no FMA
+contraction, so it must agree with the reference's double-precision build
+bit for bit: against the golden fixtures the reference itself produced, and
+against the CPU restatement on fresh seeded states for 100 steps (the
+north-star bound is <= 1e-10 relative L2 per field; the test asserts exact
+equality and reports the bound).
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.helpers import LYO_ALL, LYO_C1, NEM_ALL, NEM_C2, golden_cases, load_golden, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+import mass_hd_b200 as M  # noqa: E402
+
+
+@pytest.mark.parametrize("path", golden_cases(), ids=lambda p: p.split("/")[-1][:-4])
+def test_fp64_matches_reference_golden(path):
+    meta, z = load_golden(path)
+    L = M.Lattice(meta["model"], meta["params"], meta["LX"], meta["LY"], meta["bc"], M.FP64)
+    L.upload(z["in_ff"], z["in_QQxx"], z["in_QQyx"], z["in_phi"] if "in_phi" in z.files else None)
+    L.step(meta["steps"])
+    for k in z.files:
+        if not k.startswith("out_"):
+            continue
+        name = k[4:]
+        got = L.get(name)
+        want = z[k]
+        assert np.array_equal(got, want), (name, float(np.max(np.abs(got - want))))
+
+
+CASES = [
+    (O.LYOTROPIC, LYO_C1, 64, 48, 0),
+    (O.LYOTROPIC, LYO_ALL, 37, 29, 0),
+    (O.LYOTROPIC, LYO_ALL, 24, 20, 1),
+    (O.LYOTROPIC, LYO_ALL, 24, 20, 2),
+    (O.LYOTROPIC, LYO_ALL, 24, 20, 3),
+    (O.LYOTROPIC, LYO_ALL, 24, 20, 4),
+    (O.LYOTROPIC, LYO_ALL, 24, 20, 7),
+    (O.NEMATIC, NEM_C2, 64, 48, 0),
+    (O.NEMATIC, NEM_ALL, 24, 20, 1),
+    (O.NEMATIC, NEM_ALL, 24, 20, 3),
+]
+
+
+@pytest.mark.parametrize("model,params,LX,LY,bc", CASES)
+def test_fp64_matches_oracle_100_steps(model, params, LX, LY, bc):
+    st = O.synthetic_state(model, LX, LY, seed=11 + bc, flow=0.01)
+    P = O.PortOracle(model, params, LX, LY, bc)
+    for k, v in st.items():
+        P.set(k, v)
+    P.step(100)
+    L = M.Lattice(model, params, LX, LY, bc, M.FP64)
+    L.upload_state(st)
+    L.step(100)
+    names = ["ff", "QQxx", "QQyx", "ux", "uy", "n", "sigmaXX", "sigmaXY", "sigmaYX", "sigmaYY"]
+    if model == O.LYOTROPIC:
+        names += ["phi", "MU", "sigma_bulk", "sigma_elastic_yx", "sigma_active_xx"]
+    for n in names:
+        got, want = L.get(n), P.get(n)
+        assert rel_l2(got, want) <= 1e-10, n
+        assert np.array_equal(got, want), n
+
+
+def test_fp64_steps_split_equal_single_call():
+    st = O.synthetic_state(O.LYOTROPIC, 32, 32, seed=3, flow=0.01)
+    a = M.Lattice(O.LYOTROPIC, LYO_ALL, 32, 32, 0, M.FP64)
+    b = M.Lattice(O.LYOTROPIC, LYO_ALL, 32, 32, 0, M.FP64)
+    a.upload_state(st)
+    b.upload_state(st)
+    a.step(7)
+    for _ in range(7):
+        b.step(1)
+    for n in ("ff", "QQxx", "phi", "sigma_bulk"):
+        assert np.array_equal(a.get(n), b.get(n))
+
+
+def test_fp64_npc3_matches_oracle():
+    params = dict(LYO_ALL, npc=3)
+    st = O.synthetic_state(O.LYOTROPIC, 20, 16, seed=5, flow=0.01)
+    P = O.PortOracle(O.LYOTROPIC, params, 20, 16, 0)
+    for k, v in st.items():
+        P.set(k, v)
+    P.step(9)
+    L = M.Lattice(O.LYOTROPIC, params, 20, 16, 0, M.FP64)
+    L.upload_state(st)
+    L.step(9)
+    for n in ("ff", "fn", "QQxx", "QNxx", "phi", "phn"):
+        assert np.array_equal(L.get(n), P.get(n)), n
+
+
+def test_fp64_odd_tiny_lattices():
+    for (LX, LY) in ((1, 1), (3, 2), (2, 7), (5, 1)):
+        st = O.synthetic_state(O.LYOTROPIC, LX, LY, seed=LX * 10 + LY, flow=0.01)
+        P = O.PortOracle(O.LYOTROPIC, LYO_ALL, LX, LY, 0)
+        for k, v in st.items():
+            P.set(k, v)
+        P.step(5)
+        L = M.Lattice(O.LYOTROPIC, LYO_ALL, LX, LY, 0, M.FP64)
+        L.upload_state(st)
+        L.step(5)
+        assert np.array_equal(L.get("ff"), P.get("ff")), (LX, LY)
+        assert np.array_equal(L.get("phi"), P.get("phi")), (LX, LY)
+
+
+def test_runtime_checks_conservation_and_nan():
+    st = O.synthetic_state(O.LYOTROPIC, 32, 32, seed=8, flow=0.01)
+    L = M.Lattice(O.LYOTROPIC, LYO_ALL, 32, 32, 0, M.FP64)
+    L.upload_state(st)
+    ftot, ptot = L.initial_totals()
+    assert ftot == pytest.approx(st["ff"].sum(), rel=1e-14)
+    assert ptot == pytest.approx(st["phi"].sum(), rel=1e-13)
+    L.step(50)
+    f, p = L.runtime_checks()
+    assert abs(f - ftot) < 1e-9 * ftot
+    assert abs(p - ptot) < 1e-9 * 32 * 32
+    bad = dict(st)
+    bad["QQxx"] = st["QQxx"].copy()
+    bad["QQxx"][17] = np.nan
+    L.upload_state(bad)
+    _, _, nonfinite = L.checks()
+    assert nonfinite
+    with pytest.raises(M.MassLBError):
+        L.runtime_checks()
+
+
+def test_invalid_arguments_are_errors():
+    with pytest.raises(M.MassLBError):
+        M.Lattice(O.LYOTROPIC, LYO_ALL, 0, 16, 0, M.FP64)
+    L = M.Lattice(O.NEMATIC, NEM_C2, 16, 16, 0, M.FP64)
+    with pytest.raises(M.MassLBError):
+        L.get("phi")
+    with pytest.raises(M.MassLBError):
+        M.Lattice(O.LYOTROPIC, LYO_ALL, 1, 16, 3, M.FP64)   # walls need >= 2
