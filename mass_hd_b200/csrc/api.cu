@@ -407,8 +407,9 @@ int mass_lb_create(const mass_lb_params* params, unsigned LX, unsigned LY,
       }
       if(!h->tuned)
       {
-        // a width that always fits; the autotuner refines it on the first step
-        h->cfg = FusedConfig{LY >= 128 ? 128 : 64, static_cast<int>(std::min(LX, 256u))};
+        // the warp-strip kernel fits every fusable lattice; the autotuner
+        // refines the tile on the first step
+        h->cfg = FusedConfig{32, static_cast<int>(std::min(LX, 128u))};
       }
     }
     else

@@ -25,12 +25,14 @@
 namespace mlb {
 namespace {
 
-constexpr int RING = 6;     // input rows per warp in shared memory
+constexpr int RING = 4;     // input rows per warp in shared memory (power of 2)
 constexpr int PADY = 4;     // ring row padding (floats, each side)
 constexpr int COLS = 64;    // columns per warp strip
 constexpr int WOUT = COLS - 8;
 constexpr int RWW = COLS + 2*PADY;   // ring row stride (floats)
 constexpr int WPB = 4;      // warps per CTA
+constexpr int PW = COLS + 4;         // stride of a delayed-population row
+constexpr int NDP = 12;              // delayed populations (see below)
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
 {
@@ -98,12 +100,12 @@ __device__ __forceinline__ float rcp_approx(float x)
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
   return r;
 }
-// 1/x: hardware estimate refined by one Newton step
+// 1/x from the hardware estimate (relative error within about 1 ulp of
+// FP32 for the normal range used here: densities near rho, tau in [0.5, 10])
 __device__ __forceinline__ f2 rcp2(f2 x, const PairParams& P)
 {
-  const f2 r0 = mk(rcp_approx(x.v.x), rcp_approx(x.v.y));
-  const f2 e = fma(neg(x), r0, W2(P.one));
-  return fma(r0, e, r0);
+  (void)P;
+  return mk(rcp_approx(x.v.x), rcp_approx(x.v.y));
 }
 
 __device__ __forceinline__ f2 lds2(const float* p) { return f2{*reinterpret_cast<const float2*>(p)}; }
@@ -344,9 +346,13 @@ fused_warp_kernel(const __grid_constant__ FusedArgs a, const int nitems)
   constexpr int NP = MODEL == LYO ? 12 : 11;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float* ring = reinterpret_cast<float*>(smem_raw) + warp*(RING*NP*RWW);
+  // per warp: input ring | delayed populations (3 rows) | fn - ff/(2 tau) (2 rows)
+  constexpr int WARP_F = RING*NP*RWW + 3*NDP*PW + 2*9*COLS;
+  float* ring = reinterpret_cast<float*>(smem_raw) + warp*WARP_F;
+  float* dpop = ring + RING*NP*RWW;
+  float* hrow = dpop + 3*NDP*PW;
   uint64_t* mbar = reinterpret_cast<uint64_t*>(
-    smem_raw + WPB*RING*NP*RWW*sizeof(float)) + warp*RING;
+    smem_raw + WPB*WARP_F*sizeof(float)) + warp*RING;
 
   const int item = blockIdx.x*WPB + warp;
   if(item >= nitems) return;
@@ -367,15 +373,22 @@ fused_warp_kernel(const __grid_constant__ FusedArgs a, const int nitems)
   }
   __syncwarp();
 
+  // Bulk-copy input row rr (lattice row x0 - 4 + rr) into its ring slot:
+  // lane 0 posts the byte count, then lanes 0..NP-1 copy one plane each
+  // (called by the whole warp).
+  const float* plane_in = a.in + static_cast<long long>(lane < NP ? lane : 0)*a.plane;
+  int gx_next = ((x0 - 4) % LX + LX) % LX;   // lattice row of the next copy
   auto issue = [&](int rr) {
-    const int slot = rr % RING;
+    const int slot = rr & (RING - 1);
     uint64_t* bar = &mbar[slot];
-    mbar_expect_tx(bar, NP*COLS*4);
-    const int gx = ((x0 - 4 + rr) % LX + LX) % LX;
-    for(int p = 0; p < NP; ++p)
+    if(lane == 0) mbar_expect_tx(bar, NP*COLS*4);
+    __syncwarp();
+    const int gx = gx_next;
+    gx_next = gx_next + 1 == LX ? 0 : gx_next + 1;
+    if(lane < NP)
     {
-      const float* src = a.in + p*a.plane + static_cast<long long>(gx)*LY;
-      float* dst = ring + (slot*NP + p)*RWW + PADY;
+      const float* src = plane_in + static_cast<long long>(gx)*LY;
+      float* dst = ring + (slot*NP + lane)*RWW + PADY;
       int start = ystart, rem = COLS;
       while(rem > 0)
       {
@@ -388,16 +401,12 @@ fused_warp_kernel(const __grid_constant__ FusedArgs a, const int nitems)
     }
   };
 
-  int issued = 0;
-  if(lane == 0)
-  {
-    const int n0 = min(RING, nload);
-    for(int rr = 0; rr < n0; ++rr) issue(rr);
-    issued = n0;
-  }
+  const int n0 = min(RING, nload);
+  for(int rr = 0; rr < n0; ++rr) issue(rr);
+  int issued = n0;
   bool abort = !mbar_wait_bounded(&mbar[0], 0) || !mbar_wait_bounded(&mbar[1], 0);
 
-  const int c2 = PADY + 2*lane;            // this lane's first column in a ring row
+  const int cl = PADY + 2*lane;            // this lane's first column in a ring row
   const int yg = y0 - 4 + 2*lane;          // global column of .x (pre-wrap)
   const bool lane_out = lane >= 2 && lane < 30;
   const bool colx_ok = lane_out && yg < LY;
@@ -406,14 +415,14 @@ fused_warp_kernel(const __grid_constant__ FusedArgs a, const int nitems)
   UQ2o q1c{}, q2c{};
   UQx q1m{}, q2m{};
   f2 qa1[3], qa2[3], qn1[3], qn2[3];
-  f2 d1[6], d2a[6], d2b[6];   // pops delayed 1 / 2 rows: ff v=0,3,4 | fn v=0,3,4 ; ff v=1,5,8 | fn v=1,5,8
-  f2 hcar[9];                 // fn - ff/(2 tau) of the row E processes next
+  // Delayed populations live in shared memory: row slot s (the row C
+  // produced s iterations ago, mod 3), array k: ff v = 0,3,4 (k = 0..2),
+  // fn v = 0,3,4 (3..5), ff v = 1,5,8 (6..8), fn v = 1,5,8 (9..11). C writes
+  // them already shifted along y (column + cy); D reads its own columns.
 #pragma unroll
   for(int k = 0; k < 3; ++k) { qa1[k] = qa2[k] = qn1[k] = qn2[k] = W2(P.zero); }
-#pragma unroll
-  for(int k = 0; k < 6; ++k) { d1[k] = d2a[k] = d2b[k] = W2(P.zero); }
-#pragma unroll
-  for(int v = 0; v < 9; ++v) hcar[v] = W2(P.zero);
+  int s3 = 0;                              // i mod 3
+  float* orow = a.out + static_cast<long long>(x0 - 6)*LY + yg;   // E's output row
 
   const int nit = rows + 6;
   for(int i = 0; i < nit; ++i)
@@ -421,30 +430,33 @@ fused_warp_kernel(const __grid_constant__ FusedArgs a, const int nitems)
     if(i + 2 < nload)
     {
       const int rr = i + 2;
-      if(!mbar_wait_bounded(&mbar[rr % RING], (rr / RING) & 1)) abort = true;
+      if(!mbar_wait_bounded(&mbar[rr & (RING - 1)], (rr / RING) & 1)) abort = true;
     }
     if(__any_sync(0xffffffffu, abort)) break;
-    const float* Rm = ring + ((i    ) % RING)*NP*RWW;   // row b-1
-    const float* R0 = ring + ((i + 1) % RING)*NP*RWW;   // row b
-    const float* Rp = ring + ((i + 2) % RING)*NP*RWW;   // row b+1
+    const float* Rm = ring + ((i    ) & (RING - 1))*NP*RWW;   // row b-1
+    const float* R0 = ring + ((i + 1) & (RING - 1))*NP*RWW;   // row b
+    const float* Rp = ring + ((i + 2) & (RING - 1))*NP*RWW;   // row b+1
+    float* dp_now = dpop + s3*NDP*PW + 2 + 2*lane;                    // row of C, this iteration
+    const float* dp_1 = dpop + (s3 == 0 ? 2 : s3 - 1)*NDP*PW + 2 + 2*lane;   // one iteration ago
+    const float* dp_2 = dpop + (s3 == 2 ? 0 : s3 + 1)*NDP*PW + 2 + 2*lane;   // two iterations ago
 
     // ---- B: predictor UpdateQuantities at row b ----
     UQ2o nq1;
     {
       f2 g[9];
 #pragma unroll
-      for(int v = 0; v < 9; ++v) g[v] = lds2(R0 + v*RWW + c2);
+      for(int v = 0; v < 9; ++v) g[v] = lds2(R0 + v*RWW + cl);
       f2 Qa[5], Qb[5], Ph[5];
-      const float* q0 = R0 + 9*RWW + c2;
-      Qa[0] = lds2(q0); Qa[1] = lds2(Rp + 9*RWW + c2); Qa[2] = lds2(Rm + 9*RWW + c2);
+      const float* q0 = R0 + 9*RWW + cl;
+      Qa[0] = lds2(q0); Qa[1] = lds2(Rp + 9*RWW + cl); Qa[2] = lds2(Rm + 9*RWW + cl);
       Qa[3] = mk(Qa[0].v.y, q0[2]); Qa[4] = mk(q0[-1], Qa[0].v.x);
-      const float* q1 = R0 + 10*RWW + c2;
-      Qb[0] = lds2(q1); Qb[1] = lds2(Rp + 10*RWW + c2); Qb[2] = lds2(Rm + 10*RWW + c2);
+      const float* q1 = R0 + 10*RWW + cl;
+      Qb[0] = lds2(q1); Qb[1] = lds2(Rp + 10*RWW + cl); Qb[2] = lds2(Rm + 10*RWW + cl);
       Qb[3] = mk(Qb[0].v.y, q1[2]); Qb[4] = mk(q1[-1], Qb[0].v.x);
       if constexpr (MODEL == LYO)
       {
-        const float* q2 = R0 + 11*RWW + c2;
-        Ph[0] = lds2(q2); Ph[1] = lds2(Rp + 11*RWW + c2); Ph[2] = lds2(Rm + 11*RWW + c2);
+        const float* q2 = R0 + 11*RWW + cl;
+        Ph[0] = lds2(q2); Ph[1] = lds2(Rp + 11*RWW + cl); Ph[2] = lds2(Rm + 11*RWW + cl);
         Ph[3] = mk(Ph[0].v.y, q2[2]); Ph[4] = mk(q2[-1], Ph[0].v.x);
       }
       else
@@ -459,15 +471,15 @@ fused_warp_kernel(const __grid_constant__ FusedArgs a, const int nitems)
     f2 nQ[3], nQN[3], pf[9], pn[9];
     {
       const YN y = ynbrs<MODEL>(q1c);
-      const f2 Qxx = lds2(Rm + 9*RWW + c2), Qyx = lds2(Rm + 10*RWW + c2);
-      const f2 p = MODEL == LYO ? lds2(Rm + 11*RWW + c2) : W2(P.zero);
+      const f2 Qxx = lds2(Rm + 9*RWW + cl), Qyx = lds2(Rm + 10*RWW + cl);
+      const f2 p = MODEL == LYO ? lds2(Rm + 11*RWW + cl) : W2(P.zero);
       UFcore u;
       uf_core<MODEL>(P, q1c, xset(nq1), q1m, y, Qxx, Qyx, u);
       const f2 itau = itau_of<MODEL>(P, p);
 #pragma unroll
       for(int v = 0; v < 9; ++v)
       {
-        const f2 g = lds2(Rm + v*RWW + c2);
+        const f2 g = lds2(Rm + v*RWW + cl);
         const f2 coll = fma(u.fe[v] - g, itau, u.F[v]);
         pn[v] = fma(W2(P.half), coll, g);
         pf[v] = MODEL == LYO ? g + coll : fma(W2(P.half), coll, pn[v]);
@@ -487,28 +499,43 @@ fused_warp_kernel(const __grid_constant__ FusedArgs a, const int nitems)
         nQ[1] = fma(W2(P.half), u.Dyx, nQN[1]);
         nQN[2] = nQ[2] = W2(P.zero);
       }
-      // stream along y: directions with cy = +1 move one column up, cy = -1 down
+      // stream along y. Directions with cx = -1 (2, 6, 7) are used by D in
+      // this same iteration: shift them by shuffles. The others go to the
+      // delayed-population rows in shared memory, written at column + cy.
+      pf[6] = yplus(pf[6]); pn[6] = yplus(pn[6]);
+      pf[7] = yminus(pf[7]); pn[7] = yminus(pn[7]);
+      const int dv[6] = {0, 3, 4, 1, 5, 8};
 #pragma unroll
-      for(int v = 3; v < 9; ++v)
+      for(int k = 0; k < 6; ++k)
       {
-        if(CYv(v) > 0) { pf[v] = yminus(pf[v]); pn[v] = yminus(pn[v]); }
-        else if(CYv(v) < 0) { pf[v] = yplus(pf[v]); pn[v] = yplus(pn[v]); }
+        const int v = dv[k];
+        float* d0 = dp_now + (k < 3 ? k : k + 3)*PW + CYv(v);
+        float* d1p = dp_now + (k < 3 ? k + 3 : k + 6)*PW + CYv(v);
+        if(CYv(v) == 0)
+        {
+          *reinterpret_cast<float2*>(d0) = pf[v].v;
+          *reinterpret_cast<float2*>(d1p) = pn[v].v;
+        }
+        else
+        {
+          d0[0] = pf[v].v.x; d0[1] = pf[v].v.y;
+          d1p[0] = pn[v].v.x; d1p[1] = pn[v].v.y;
+        }
       }
     }
 
     // ---- D: corrector UpdateQuantities at row s = b-2 (x-part of Move) ----
     UQ2o nq2;
-    f2 hn[9];
     {
       // direction v at (s, y) left row s - cx: cx = -1 is the row C just
       // produced, cx = 0 the previous one, cx = +1 the one before that
       f2 fs[9], ns[9];
       fs[2] = pf[2]; fs[6] = pf[6]; fs[7] = pf[7];
       ns[2] = pn[2]; ns[6] = pn[6]; ns[7] = pn[7];
-      fs[0] = d1[0]; fs[3] = d1[1]; fs[4] = d1[2];
-      ns[0] = d1[3]; ns[3] = d1[4]; ns[4] = d1[5];
-      fs[1] = d2b[0]; fs[5] = d2b[1]; fs[8] = d2b[2];
-      ns[1] = d2b[3]; ns[5] = d2b[4]; ns[8] = d2b[5];
+      fs[0] = lds2(dp_1 + 0*PW); fs[3] = lds2(dp_1 + 1*PW); fs[4] = lds2(dp_1 + 2*PW);
+      ns[0] = lds2(dp_1 + 3*PW); ns[3] = lds2(dp_1 + 4*PW); ns[4] = lds2(dp_1 + 5*PW);
+      fs[1] = lds2(dp_2 + 6*PW); fs[5] = lds2(dp_2 + 7*PW); fs[8] = lds2(dp_2 + 8*PW);
+      ns[1] = lds2(dp_2 + 9*PW); ns[5] = lds2(dp_2 + 10*PW); ns[8] = lds2(dp_2 + 11*PW);
       f2 Qa[5], Qb[5], Ph[5];
       Qa[0] = qa1[0]; Qa[1] = nQ[0]; Qa[2] = qa2[0]; Qa[3] = yplus(qa1[0]); Qa[4] = yminus(qa1[0]);
       Qb[0] = qa1[1]; Qb[1] = nQ[1]; Qb[2] = qa2[1]; Qb[3] = yplus(qa1[1]); Qb[4] = yminus(qa1[1]);
@@ -525,7 +552,8 @@ fused_warp_kernel(const __grid_constant__ FusedArgs a, const int nitems)
       uq_pair<MODEL>(P, fs, Qa, Qb, Ph, nq2, DIAG ? dg : nullptr);
       const f2 hitau = W2(P.nhalf)*itau_of<MODEL>(P, qa1[2]);
 #pragma unroll
-      for(int v = 0; v < 9; ++v) hn[v] = fma(hitau, fs[v], ns[v]);
+      for(int v = 0; v < 9; ++v)
+        *reinterpret_cast<float2*>(hrow + ((i & 1)*9 + v)*COLS + 2*lane) = fma(hitau, fs[v], ns[v]).v;
       if constexpr (DIAG)
       {
         const int xs = x0 - 5 + i;
@@ -566,15 +594,15 @@ fused_warp_kernel(const __grid_constant__ FusedArgs a, const int nitems)
       f2 gout[9];
 #pragma unroll
       for(int v = 0; v < 9; ++v)
-        gout[v] = fma(W2(P.half), u.F[v], fma(hitau, u.fe[v], hcar[v]));
+        gout[v] = fma(W2(P.half), u.F[v],
+                      fma(hitau, u.fe[v], lds2(hrow + (((i + 1) & 1)*9 + v)*COLS + 2*lane)));
       const f2 Qo0 = fma(W2(P.half), u.Dxx, qn2[0]);
       const f2 Qo1 = fma(W2(P.half), u.Dyx, qn2[1]);
       const f2 Qo2 = fma(W2(P.half), u.Dp, qn2[2]);
-      const int xo = x0 - 6 + i;
-      if(i >= 6 && xo < x0 + rows)
+      if(i >= 6)
       {
         const long long pl = a.plane;
-        float* o = a.out + static_cast<long long>(xo)*LY + yg;
+        float* o = orow;
         if(colx_ok && coly_ok)
         {
 #pragma unroll
@@ -603,17 +631,11 @@ fused_warp_kernel(const __grid_constant__ FusedArgs a, const int nitems)
       qa2[k] = qa1[k]; qa1[k] = nQ[k];
       qn2[k] = qn1[k]; qn1[k] = nQN[k];
     }
-#pragma unroll
-    for(int k = 0; k < 6; ++k) d2b[k] = d2a[k];
-    d2a[0] = pf[1]; d2a[1] = pf[5]; d2a[2] = pf[8];
-    d2a[3] = pn[1]; d2a[4] = pn[5]; d2a[5] = pn[8];
-    d1[0] = pf[0]; d1[1] = pf[3]; d1[2] = pf[4];
-    d1[3] = pn[0]; d1[4] = pn[3]; d1[5] = pn[4];
-#pragma unroll
-    for(int v = 0; v < 9; ++v) hcar[v] = hn[v];
+    s3 = s3 == 2 ? 0 : s3 + 1;
+    orow += LY;
 
     __syncwarp();
-    if(lane == 0 && issued < nload && issued <= i + RING)
+    if(issued < nload && issued <= i + RING)
     {
       fence_proxy_async();
       issue(issued);
@@ -621,18 +643,20 @@ fused_warp_kernel(const __grid_constant__ FusedArgs a, const int nitems)
     }
   }
 
-  if(abort && lane == 0)
+  if(abort)
   {
-    atomicOr(a.err, 1);
+    if(lane == 0) atomicOr(a.err, 1);
+    // let every copy this warp issued land before its shared memory is
+    // released
     for(int rr = 0; rr < issued; ++rr)
-      mbar_wait_bounded(&mbar[rr % RING], (rr / RING) & 1);
+      mbar_wait_bounded(&mbar[rr & (RING - 1)], (rr / RING) & 1);
   }
 }
 
 template<int MODEL>
 constexpr size_t smem_bytes()
 {
-  return static_cast<size_t>(WPB)*RING*(MODEL == LYO ? 12 : 11)*RWW*sizeof(float) +
+  return static_cast<size_t>(WPB)*(RING*(MODEL == LYO ? 12 : 11)*RWW + 3*NDP*PW + 2*9*COLS)*sizeof(float) +
          static_cast<size_t>(WPB)*RING*sizeof(uint64_t);
 }
 
