@@ -122,7 +122,12 @@ def gen_json():
             for src, dst in ((pth, f"{tag}_parameters.json"), (fr, f"{tag}_frame3.json")):
                 with open(src) as fi, open(os.path.join(HERE, dst), "w") as fo:
                     fo.write(fi.read())
-        st = {k: r.get(k) for k in (["ff", "QQxx", "QQyx"] + (["phi"] if model == O.LYOTROPIC else []))}
+        names = ["ff", "QQxx", "QQyx"]
+        if model == O.LYOTROPIC:
+            names += ["phi", "sigmaXX", "sigmaXY", "sigmaYX", "sigmaYY", "sigma_bulk",
+                      "sigma_elastic_xx", "sigma_elastic_yx", "sigma_phase_field_xx",
+                      "sigma_phase_field_yx", "sigma_active_xx", "sigma_active_yx"]
+        st = {k: r.get(k) for k in names}
         np.savez_compressed(os.path.join(HERE, f"{tag}_frame3_state.npz"), **st)
         print("wrote json", tag)
 

@@ -1,0 +1,118 @@
+"""End to end through the C++ model plugin and the mass-gpu driver on a GPU.
+
+* FP64 mode on the configuration the reference wrote its golden JSON for:
+  parameters.json and frame3.json must be text-identical to the reference's
+  (same Configure() random stream, bit-exact steps, same JSON writer).
+* Configure() of every initial configuration against the reference's.
+* An FP32 run of the BASELINE initial state (random director, tanh disk)
+  through several output intervals, with the runtime checks on.
+"""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HOST = os.path.join(ROOT, "mass_hd_b200", "host")
+DRIVER = os.path.join(HOST, "_build", "mass-gpu")
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def driver():
+    subprocess.run(["make", "-s", "-C", HOST], check=True)
+    assert os.path.exists(DRIVER)
+
+
+def runcard(path, model, opts):
+    lines = [f"model = {model}"] + [f"{k} = {v}" for k, v in opts.items()]
+    path.write_text("\n".join(lines) + "\n")
+
+
+def run(card, out, *extra):
+    r = subprocess.run([DRIVER, str(card), "-o", str(out), *extra],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    return r
+
+
+LYO = dict(GammaQ=0.3, GammaP=0.1, xi=0.7, tauNem=1.5, tauIso=1.5, rho=40.0,
+           friction=0.0, AA=0.1, CC=0.1, LL=0.05, KK=0.05, zeta=0.01,
+           zetaI=0.0, npc=1)
+NEM = dict(Gamma=0.3, xi=0.7, tau=1.5, rho=40.0, friction=0.0, CC=0.1,
+           LL=0.05, zeta=0.02, npc=1)
+
+
+@pytest.mark.parametrize("tag", ["lyo", "nem"])
+def test_fp64_output_files_identical_to_reference(tmp_path, tag):
+    if tag == "lyo":
+        opts = dict(LYO, config="circle", radius=2.0, level=0.0, conc=1.0, angle=0.0, noise=1.0)
+        model = "lyotropic"
+    else:
+        opts = dict(NEM, angle=0.0, noise=1.0)
+        model = "nematic"
+    opts.update(LX=4, LY=3, nsteps=3, ninfo=1, seed=7, precision="fp64")
+    card = tmp_path / "run.dat"
+    runcard(card, model, opts)
+    run(card, tmp_path / "out")
+    for name, gold in (("parameters.json", f"{tag}_parameters.json"),
+                       ("frame3.json", f"{tag}_frame3.json")):
+        got = (tmp_path / "out" / name).read_text()
+        want = open(os.path.join(GOLDEN, gold)).read()
+        assert got == want, name
+
+
+def load_frame(path):
+    d = json.load(open(path))["data"]
+    return {k: np.asarray(v["value"], dtype=float) for k, v in d.items()}
+
+
+def test_configure_matches_reference(tmp_path):
+    z = np.load(os.path.join(GOLDEN, "configure.npz"))
+    meta = json.loads(str(z["meta"]))
+    for name, m in meta.items():
+        params = dict(m["params"])
+        model = "lyotropic" if m["model"] == 0 else "nematic"
+        params.update(LX=m["LX"], LY=m["LY"], bc=m["bc"], nsteps=0, ninfo=1,
+                      seed=m["seed"], precision="fp64")
+        card = tmp_path / f"{name}.dat"
+        runcard(card, model, params)
+        out = tmp_path / name
+        run(card, out)
+        fr = load_frame(out / "frame0.json")
+        for k in ("ff", "QQxx", "QQyx") + (("phi",) if model == "lyotropic" else ()):
+            want = z[f"{name}__{k}"]
+            got = fr[k].reshape(want.shape)
+            # the frame holds 6 significant digits
+            assert np.allclose(got, want, rtol=2e-6, atol=1e-6), (name, k)
+
+
+def test_fp32_baseline_state_runs_with_checks(tmp_path):
+    opts = dict(LYO, config="random-disk", radius=32.0, width=2.0, conc=1.0, angle=0.0,
+                noise=1.0, LX=128, LY=128, nsteps=300, ninfo=100, seed=3, precision="fp32")
+    card = tmp_path / "run.dat"
+    runcard(card, "lyotropic", opts)
+    r = run(card, tmp_path / "out")
+    assert "fcheck" in r.stdout
+    frames = sorted(p for p in os.listdir(tmp_path / "out") if p.startswith("frame"))
+    assert frames == ["frame0.json", "frame100.json", "frame200.json", "frame300.json"]
+    fr = load_frame(tmp_path / "out" / "frame300.json")
+    for k in ("ff", "QQxx", "phi", "sigmaXX", "sigma_active_yx"):
+        assert np.all(np.isfinite(fr[k])), k
+    # phi is conserved by the flux form; mass to round-off
+    f0 = load_frame(tmp_path / "out" / "frame0.json")
+    assert abs(fr["phi"].sum() - f0["phi"].sum()) < 1e-2
+    assert abs(fr["ff"].sum() - f0["ff"].sum()) < 1e-1
+
+
+def test_step_errors_surface_in_runtime_checks(tmp_path):
+    # an unknown precision is rejected at Initialize() with the model's message
+    opts = dict(LYO, config="circle", radius=2, conc=1, LX=8, LY=8, nsteps=1, precision="fp16")
+    card = tmp_path / "run.dat"
+    runcard(card, "lyotropic", opts)
+    r = subprocess.run([DRIVER, str(card), "-o", str(tmp_path / "o")], capture_output=True, text=True)
+    assert r.returncode == 1 and "precision 'fp16' unknown" in r.stderr
