@@ -38,6 +38,32 @@ int mass_lb_uses_fused(mass_lb_handle* h);
 int mass_lb_device_state(mass_lb_handle* h, void** planes, long long* plane_stride,
                          int* nplanes);
 
+/* Conservation sums of mass_lb_checks (population total, phi total,
+ * non-finite flag) over an FP32 device state such as mass_lb_device_state()
+ * returns, computed WITHOUT allocating device memory. This entry point has
+ * no counterpart in the reference.
+ *
+ * For callers that cannot allocate device memory: a program whose HBM is
+ * owned in full by another allocator (a framework that reserved it up
+ * front, where one more cudaMalloc fails or synchronizes the device), or a
+ * monitoring path that must not pay cudaMalloc/cudaFree synchronization.
+ * Its scratch is a fixed 163,864-byte __device__ array inside the library,
+ * held by every GPU that loads the library until the process exits.
+ *
+ * planes: nplanes (12 lyotropic, 11 nematic) float planes, plane_stride
+ * apart, in the fused layout (g0..g8 as deviations from t_v*rho, Qxx, Qyx,
+ * phi); rho: the rest density. Lattices above 67,108,864 sites (8192^2) are
+ * rejected with MASS_LB_EINVAL. The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) for that device; make that
+ * first call before any stream capture. The array is shared by all calls and
+ * keeps the last call's contents (every call writes all it reads, so
+ * nothing needs clearing); calls that overlap on the GPU race on it. Runs on
+ * `stream` (a cudaStream_t, NULL = default stream) and returns after the
+ * results are on the host. Errors: mass_lb_last_error(). */
+int mass_lb_state_sums_noalloc(const float* planes, long long plane_stride, int nplanes,
+                               unsigned LX, unsigned LY, double rho, void* stream,
+                               double* fsum, double* phisum, int* nonfinite);
+
 #ifdef __cplusplus
 }
 #endif

@@ -310,6 +310,8 @@ int ensure_diag_buffer(mass_lb_handle* h)
 
 // ==========================================================================
 
+void mlb_set_last_error(const std::string& msg) { g_err = msg; }
+
 extern "C" {
 
 int mass_lb_abi_version(void) { return MASS_LB_ABI_VERSION; }
@@ -764,6 +766,7 @@ int mass_lb_autotune(mass_lb_handle* h)
 }
 
 int mass_lb_uses_fused(mass_lb_handle* h) { return h && h->fused ? 1 : 0; }
+
 
 int mass_lb_device_state(mass_lb_handle* h, void** planes, long long* plane_stride,
                          int* nplanes_out)
