@@ -38,6 +38,27 @@ int mass_lb_uses_fused(mass_lb_handle* h);
 int mass_lb_device_state(mass_lb_handle* h, void** planes, long long* plane_stride,
                          int* nplanes);
 
+/* Statistics of the current state with the estimators of the reference's
+ * post-processing (POST/massPy, plot/python/passive_q1_alpha_regime_analysis.py):
+ * <|u|^2>; enstrophy density 0.5<w^2> with w the periodic central-difference
+ * vorticity, over the lattice and over phi > 0.5; the phi > 0.5 area and
+ * its 4-neighbour perimeter; and the +1/2 and -1/2 nematic defects, found as
+ * 4-connected same-sign clusters of sites whose director winding exceeds
+ * 0.4 in magnitude. No counterpart in the reference's C++ (it is the POST
+ * code's arithmetic run on the device). Synchronous. */
+typedef struct {
+  double mean_u2;
+  double enstrophy_density;
+  double enstrophy_density_phi;   /* 0 for the nematic model */
+  double phi_area;                /* sites with phi > 0.5 */
+  double perimeter;               /* exposed edges of the phi > 0.5 region */
+  long long defects_plus;
+  long long defects_minus;
+  long long charged_sites;        /* sites with |charge| > 0.4 */
+} mass_lb_stats;
+
+int mass_lb_statistics(mass_lb_handle* h, mass_lb_stats* out);
+
 /* Conservation sums of mass_lb_checks (population total, phi total,
  * non-finite flag) over an FP32 device state such as mass_lb_device_state()
  * returns, computed WITHOUT allocating device memory. This entry point has

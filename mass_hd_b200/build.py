@@ -32,6 +32,7 @@ UNITS = {
     "fused32.cu": [],
     "fused_warp.cu": [],
     "reduce.cu": [],
+    "stats.cu": [],
     "api.cu": [],
     "noalloc.cu": [],
 }

@@ -8,6 +8,7 @@
 #include "unfused.h"
 #include "fused32.cuh"
 #include "reduce.cuh"
+#include "stats.cuh"
 
 #include <algorithm>
 #include <cstdio>
@@ -138,6 +139,7 @@ struct mass_lb_handle
   bool tuned = false;
 
   double* stage = nullptr;   // device staging (kStageSites*9 doubles)
+  StatScratch stats{};       // statistics scratch, allocated on first use
   double* red_scratch = nullptr;
   double* red_out = nullptr; // 3 doubles
   int* err = nullptr;
@@ -767,6 +769,101 @@ int mass_lb_autotune(mass_lb_handle* h)
 
 int mass_lb_uses_fused(mass_lb_handle* h) { return h && h->fused ? 1 : 0; }
 
+int mass_lb_statistics(mass_lb_handle* h, mass_lb_stats* out)
+{
+  if(!h || !out) return fail(MASS_LB_EINVAL, "null argument");
+  DeviceGuard g(h->device);
+  const long long N = static_cast<long long>(h->LX)*h->LY;
+  if(!h->stats.U)
+  {
+    StatScratch& s = h->stats;
+    if(int r = dalloc(h, &s.U, 2*N)) return r;
+    if(int r = dalloc(h, &s.D, 2*N)) return r;
+    if(int r = dalloc(h, &s.partial, 8*STATS_BLOCKS)) return r;
+    if(int r = dalloc(h, &s.out, 5)) return r;
+    if(int r = dalloc(h, &s.count, 1)) return r;
+    if(int r = dalloc(h, &s.list, N)) return r;
+    s.capacity = static_cast<int>(std::min<long long>(N, 0x7fffffff));
+  }
+  cudaError_t e;
+  if(h->fused)
+  {
+    const long long plane = N;
+    StatView<float> v{h->cur, plane, h->cur + 9*plane, h->cur + 10*plane,
+                      h->model == LYO ? h->cur + 11*plane : nullptr,
+                      static_cast<int>(h->LX), static_cast<int>(h->LY), 0,
+                      static_cast<int>(h->LY), h->P.rho};
+    e = launch_stats_f32(v, h->stats, 0.4, h->stream);
+  }
+  else if(h->precision == MASS_LB_FP64)
+  {
+    const State<double>& s = h->s64;
+    StatView<double> v{s.ff, h->d.NE, s.Qxx, s.Qyx, h->model == LYO ? s.phi : nullptr,
+                       h->d.LX, h->d.LY, h->d.g, h->d.EY, 0.0};
+    e = launch_stats_f64(v, h->stats, 0.4, h->stream);
+  }
+  else
+  {
+    const State<float>& s = h->s32;
+    StatView<float> v{s.ff, h->d.NE, s.Qxx, s.Qyx, h->model == LYO ? s.phi : nullptr,
+                      h->d.LX, h->d.LY, h->d.g, h->d.EY, h->P.rho};
+    e = launch_stats_f32(v, h->stats, 0.4, h->stream);
+  }
+  if(e != cudaSuccess) return cuda_fail(e, "statistics");
+  double sums[5];
+  int count = 0;
+  CU(cudaMemcpyAsync(sums, h->stats.out, sizeof(sums), cudaMemcpyDeviceToHost, h->stream), "stats copy");
+  CU(cudaMemcpyAsync(&count, h->stats.count, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "stats copy");
+  CU(cudaStreamSynchronize(h->stream), "stats sync");
+  if(count > h->stats.capacity) return fail(MASS_LB_ECUDA, "charged-site list overflow");
+  std::vector<int> list(count);
+  if(count)
+  {
+    CU(cudaMemcpy(list.data(), h->stats.list, count*sizeof(int), cudaMemcpyDeviceToHost), "stats list");
+  }
+  // Cluster the charged sites: 4-connected (periodic) same-sign components,
+  // one defect each, as the breadth-first search of defects.py:75-95.
+  std::sort(list.begin(), list.end());
+  std::vector<int> parent(count);
+  for(int i = 0; i < count; ++i) parent[i] = i;
+  auto find = [&](int i) {
+    while(parent[i] != i) { parent[i] = parent[parent[i]]; i = parent[i]; }
+    return i;
+  };
+  const int LX = static_cast<int>(h->LX), LY = static_cast<int>(h->LY);
+  for(int i = 0; i < count; ++i)
+  {
+    const int code = list[i];
+    const bool plus = code >= 0;
+    const long long k = plus ? code : -static_cast<long long>(code) - 1;
+    const int x = static_cast<int>(k / LY), y = static_cast<int>(k % LY);
+    const int nx[4] = {(x + 1) % LX, (x + LX - 1) % LX, x, x};
+    const int ny[4] = {y, y, (y + 1) % LY, (y + LY - 1) % LY};
+    for(int j = 0; j < 4; ++j)
+    {
+      const long long kn = static_cast<long long>(nx[j])*LY + ny[j];
+      const int cn = plus ? static_cast<int>(kn) : -static_cast<int>(kn) - 1;
+      const auto it = std::lower_bound(list.begin(), list.end(), cn);
+      if(it != list.end() && *it == cn)
+      {
+        const int a = find(i), b = find(static_cast<int>(it - list.begin()));
+        if(a != b) parent[a] = b;
+      }
+    }
+  }
+  long long plus = 0, minus = 0;
+  for(int i = 0; i < count; ++i)
+    if(find(i) == i) (list[i] >= 0 ? plus : minus) += 1;
+  out->mean_u2 = sums[0]/N;
+  out->enstrophy_density = .5*sums[1]/N;
+  out->enstrophy_density_phi = sums[3] > 0 ? .5*sums[2]/sums[3] : 0.0;
+  out->phi_area = sums[3];
+  out->perimeter = sums[4];
+  out->defects_plus = plus;
+  out->defects_minus = minus;
+  out->charged_sites = count;
+  return 0;
+}
 
 int mass_lb_device_state(mass_lb_handle* h, void** planes, long long* plane_stride,
                          int* nplanes_out)

@@ -49,6 +49,17 @@ class Params(C.Structure):
     ] + [("npc", C.c_uint)]
 
 
+class Stats(C.Structure):
+    """mass_lb_stats (include/mass_lb_ext.h)."""
+    _fields_ = [("mean_u2", C.c_double), ("enstrophy_density", C.c_double),
+                ("enstrophy_density_phi", C.c_double), ("phi_area", C.c_double),
+                ("perimeter", C.c_double), ("defects_plus", C.c_longlong),
+                ("defects_minus", C.c_longlong), ("charged_sites", C.c_longlong)]
+
+    def as_dict(self) -> dict:
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
 _lib = None
 
 
@@ -92,6 +103,7 @@ def load_library(build_if_missing: bool = False):
         "mass_lb_autotune": (C.c_int, [vp]),
         "mass_lb_uses_fused": (C.c_int, [vp]),
         "mass_lb_device_state": (C.c_int, [vp, C.POINTER(vp), C.POINTER(C.c_longlong), ip]),
+        "mass_lb_statistics": (C.c_int, [vp, C.POINTER(Stats)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -245,6 +257,14 @@ class Lattice:
 
     def autotune(self):
         _check(load_library().mass_lb_autotune(self.h))
+
+    def statistics(self) -> dict:
+        """Flow and defect statistics of the current state (see
+        mass_lb_statistics): mean_u2, enstrophy_density, enstrophy_density_phi,
+        phi_area, perimeter, defects_plus, defects_minus, charged_sites."""
+        st = Stats()
+        _check(load_library().mass_lb_statistics(self.h, C.byref(st)))
+        return st.as_dict()
 
     def device_state(self):
         p, stride, n = C.c_void_p(), C.c_longlong(), C.c_int()
