@@ -85,6 +85,37 @@ int mass_lb_state_sums_noalloc(const float* planes, long long plane_stride, int 
                                unsigned LX, unsigned LY, double rho, void* stream,
                                double* fsum, double* phisum, int* nonfinite);
 
+/* ---- batched ensembles --------------------------------------------------
+ *
+ * Many independent FP32 periodic lattices, of uneven sizes and parameters,
+ * advanced together: one step of every run is ONE persistent kernel launch
+ * whose warps pull (run, strip, chunk) work items from a packed list, largest
+ * run first, through a device counter; per-run parameters sit in constant
+ * memory. Two steps are replayed as one CUDA graph. The reference has no
+ * such call: a parameter sweep there is one `mass` process per runcard, each
+ * calling Model::Step() from Algorithm() (src/main.cpp:132-197) on its own
+ * lattice.
+ *
+ * Each run is an ordinary FP32 handle (mass_lb_ensemble_run), so the
+ * single-lattice calls upload, download, check and measure it; its state
+ * after k ensemble steps is bit-identical to k mass_lb_step calls on the
+ * fused single-lattice path. All runs share one model and use npc = 1; every
+ * LY must be a multiple of 4 and at least 64. At most 192 runs are active on
+ * a device at a time, across all ensembles. */
+typedef struct mass_lb_ensemble mass_lb_ensemble;
+
+int mass_lb_ensemble_create(int nruns, const mass_lb_params* params, const unsigned* LX,
+                            const unsigned* LY, mass_lb_ensemble** out);
+void mass_lb_ensemble_destroy(mass_lb_ensemble* e);
+int mass_lb_ensemble_size(mass_lb_ensemble* e);
+/* the handle of run i (owned by the ensemble; NULL if i is out of range) */
+mass_lb_handle* mass_lb_ensemble_run(mass_lb_ensemble* e, int i);
+/* nsteps steps of every run; returns after they are done. The first call
+ * picks the chunk height by timing (MASS_LB_ENSEMBLE_ROWS=<n> fixes it). */
+int mass_lb_ensemble_step(mass_lb_ensemble* e, unsigned nsteps);
+/* chunk height in rows (0 before the first step) */
+int mass_lb_ensemble_get_rows(mass_lb_ensemble* e);
+
 #ifdef __cplusplus
 }
 #endif

@@ -5,8 +5,8 @@ The product is the C-ABI library ``lib/libmass_lb.so`` (include/mass_lb.h)
 built from ``csrc/`` and the C++ model plugin in ``host/``; ``lb`` is a
 ctypes front-end over the same library.
 """
-from .lb import (FIELDS, FP32, FP64, LYOTROPIC, NEMATIC, Lattice, MassLBError,  # noqa: F401
+from .lb import (FIELDS, FP32, FP64, LYOTROPIC, NEMATIC, Ensemble, Lattice, MassLBError,  # noqa: F401
                  library_path, load_library, make_params)
 
-__all__ = ["FIELDS", "FP32", "FP64", "LYOTROPIC", "NEMATIC", "Lattice",
+__all__ = ["FIELDS", "FP32", "FP64", "LYOTROPIC", "NEMATIC", "Ensemble", "Lattice",
            "MassLBError", "library_path", "load_library", "make_params"]

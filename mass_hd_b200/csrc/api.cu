@@ -11,6 +11,7 @@
 #include "stats.cuh"
 
 #include <algorithm>
+#include <mutex>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -220,6 +221,19 @@ int zero_state(mass_lb_handle* h, State<T>& s)
   return 0;
 }
 
+// FP32 parameters of the fused kernels (the same rounding for single
+// lattices and ensemble runs, so both step bit-identically)
+P32 p32_of(const Params& P)
+{
+  return P32{static_cast<float>(P.rho), static_cast<float>(P.GammaQ),
+             static_cast<float>(P.GammaP), static_cast<float>(P.xi),
+             static_cast<float>(P.tauNem), static_cast<float>(P.tauIso),
+             static_cast<float>(P.friction), static_cast<float>(P.AA),
+             static_cast<float>(P.CC), static_cast<float>(P.LL),
+             static_cast<float>(P.KK), static_cast<float>(P.zeta),
+             static_cast<float>(P.zetaI), static_cast<float>(P.conc)};
+}
+
 FusedArgs fused_args(mass_lb_handle* h, const float* in, float* out, bool diag)
 {
   FusedArgs a{};
@@ -230,14 +244,7 @@ FusedArgs fused_args(mass_lb_handle* h, const float* in, float* out, bool diag)
   a.LX = static_cast<int>(h->LX);
   a.LY = static_cast<int>(h->LY);
   a.plane = static_cast<long long>(h->LX)*h->LY;
-  const Params& P = h->P;
-  a.p = P32{static_cast<float>(P.rho), static_cast<float>(P.GammaQ),
-            static_cast<float>(P.GammaP), static_cast<float>(P.xi),
-            static_cast<float>(P.tauNem), static_cast<float>(P.tauIso),
-            static_cast<float>(P.friction), static_cast<float>(P.AA),
-            static_cast<float>(P.CC), static_cast<float>(P.LL),
-            static_cast<float>(P.KK), static_cast<float>(P.zeta),
-            static_cast<float>(P.zetaI), static_cast<float>(P.conc)};
+  a.p = p32_of(h->P);
   return a;
 }
 
@@ -874,6 +881,273 @@ int mass_lb_device_state(mass_lb_handle* h, void** planes, long long* plane_stri
   if(plane_stride) *plane_stride = static_cast<long long>(h->LX)*h->LY;
   if(nplanes_out) *nplanes_out = nplanes(h);
   return 0;
+}
+
+// ---- ensembles ------------------------------------------------------------
+
+} // extern "C"
+
+struct mass_lb_ensemble
+{
+  int device = 0;
+  int model = LYO;
+  cudaStream_t stream = nullptr;
+  std::vector<mass_lb_handle*> runs;
+  std::vector<int> order;       // runs, largest first
+  EnsRun* d_runs = nullptr;
+  int* d_item_run = nullptr;
+  int* d_counter = nullptr;
+  int* d_err = nullptr;
+  int nitems = 0;
+  int capacity = 0;             // items the device list holds
+  int rows = 0;                 // rows per chunk (0: not tuned yet)
+  int slot0 = -1;
+  int grid = 0;
+  cudaGraphExec_t graph = nullptr;   // two steps: parity 0 then 1
+  std::vector<void*> allocs;
+};
+
+namespace {
+
+std::mutex g_slot_mu;
+std::vector<unsigned char> g_slot_used[64];   // per device: constant-memory slots
+
+int reserve_slots(int dev, int n)
+{
+  std::lock_guard<std::mutex> lock(g_slot_mu);
+  auto& used = g_slot_used[dev & 63];
+  if(used.empty()) used.assign(ENS_MAX_RUNS, 0);
+  for(int s = 0; s + n <= ENS_MAX_RUNS; ++s)
+  {
+    bool free_run = true;
+    for(int k = 0; k < n && free_run; ++k) free_run = !used[s + k];
+    if(free_run)
+    {
+      for(int k = 0; k < n; ++k) used[s + k] = 1;
+      return s;
+    }
+  }
+  return -1;
+}
+
+void release_slots(int dev, int s, int n)
+{
+  std::lock_guard<std::mutex> lock(g_slot_mu);
+  auto& used = g_slot_used[dev & 63];
+  for(int k = 0; k < n && s >= 0; ++k) used[s + k] = 0;
+}
+
+// Pack the work items of every run (largest run first) for chunk height
+// `rows`, and point each run's descriptor at its handle's current buffers
+// (parity 0 reads handle->cur).
+int ens_pack(mass_lb_ensemble* e, int rows)
+{
+  std::vector<EnsRun> desc(e->runs.size());
+  std::vector<int> item_run;
+  for(int r : e->order)
+  {
+    mass_lb_handle* h = e->runs[r];
+    EnsRun& d = desc[r];
+    d.a = h->cur;
+    d.b = h->nxt;
+    d.LX = static_cast<int>(h->LX);
+    d.LY = static_cast<int>(h->LY);
+    d.plane = static_cast<long long>(h->LX)*h->LY;
+    d.nstrips = (d.LY + ENS_WOUT - 1)/ENS_WOUT;
+    d.rows = std::min(rows, d.LX);
+    d.item0 = static_cast<int>(item_run.size());
+    d.slot = e->slot0 + r;
+    const int n = d.nstrips*((d.LX + d.rows - 1)/d.rows);
+    for(int k = 0; k < n; ++k) item_run.push_back(r);
+  }
+  if(static_cast<int>(item_run.size()) > e->capacity)   // sized for rows = 32
+    return fail(MASS_LB_EINVAL, "ensemble item list overflow");
+  e->nitems = static_cast<int>(item_run.size());
+  CU(cudaMemcpyAsync(e->d_runs, desc.data(), desc.size()*sizeof(EnsRun),
+                     cudaMemcpyHostToDevice, e->stream), "ensemble descriptors");
+  CU(cudaMemcpyAsync(e->d_item_run, item_run.data(), item_run.size()*sizeof(int),
+                     cudaMemcpyHostToDevice, e->stream), "ensemble items");
+  return 0;
+}
+
+int ens_launch(mass_lb_ensemble* e, int parity)
+{
+  CU(cudaMemsetAsync(e->d_counter, 0, sizeof(int), e->stream), "ensemble counter");
+  CU(launch_fused_warp_ensemble(e->d_runs, e->d_item_run, e->nitems, e->d_counter, e->d_err,
+                                parity, e->model, e->grid, e->stream), "ensemble step");
+  return 0;
+}
+
+// Choose the chunk height by timing one launch per candidate; the state is
+// read from buffer a and written to b, so it does not advance.
+int ens_autotune(mass_lb_ensemble* e)
+{
+  cudaEvent_t t0, t1;
+  CU(cudaEventCreate(&t0), "event");
+  CU(cudaEventCreate(&t1), "event");
+  float best = 1e30f;
+  int best_rows = 64;
+  const int cand[] = {32, 64, 128, 256};
+  for(int rows : cand)
+  {
+    if(int r = ens_pack(e, rows)) return r;
+    if(int r = ens_launch(e, 0)) return r;
+    CU(cudaEventRecord(t0, e->stream), "event");
+    for(int k = 0; k < 3; ++k)
+      if(int r = ens_launch(e, 0)) return r;
+    CU(cudaEventRecord(t1, e->stream), "event");
+    CU(cudaEventSynchronize(t1), "event");
+    float ms = 0;
+    CU(cudaEventElapsedTime(&ms, t0, t1), "event");
+    if(std::getenv("MASS_LB_TUNE_LOG"))
+      std::fprintf(stderr, "mass_lb ensemble autotune: rows %d: %.4f ms/step\n", rows, ms/3);
+    if(ms < best) { best = ms; best_rows = rows; }
+  }
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  e->rows = best_rows;
+  for(mass_lb_handle* h : e->runs) h->has_prev = false;   // b buffers were scratch
+  return ens_pack(e, e->rows);
+}
+
+} // namespace
+
+extern "C" {
+
+int mass_lb_ensemble_create(int nruns, const mass_lb_params* params, const unsigned* LX,
+                            const unsigned* LY, mass_lb_ensemble** out)
+{
+  if(!params || !LX || !LY || !out) return fail(MASS_LB_EINVAL, "null argument");
+  *out = nullptr;
+  if(nruns < 1) return fail(MASS_LB_EINVAL, "an ensemble needs at least one run");
+  if(nruns > ENS_MAX_RUNS) return fail(MASS_LB_EINVAL, "too many runs for one ensemble");
+  const int model = params[0].model;
+  for(int i = 0; i < nruns; ++i)
+  {
+    if(params[i].model != model) return fail(MASS_LB_EINVAL, "all runs must use one model");
+    if(params[i].npc != 1) return fail(MASS_LB_EUNSUPPORTED, "ensembles need npc = 1");
+    if(!fused_supported(static_cast<int>(LX[i]), static_cast<int>(LY[i]), 32))
+      return fail(MASS_LB_EUNSUPPORTED, "run lattice not supported by the fused kernel "
+                                        "(LY % 4 == 0 and LY >= 64 required)");
+  }
+  auto* e = new mass_lb_ensemble();
+  CU(cudaGetDevice(&e->device), "cudaGetDevice");
+  e->model = model;
+  auto bail = [&](int r) { mass_lb_ensemble_destroy(e); return r; };
+  e->slot0 = reserve_slots(e->device, nruns);
+  if(e->slot0 < 0) return bail(fail(MASS_LB_EUNSUPPORTED, "no free parameter slots on this device"));
+  if(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(fail(MASS_LB_ECUDA, "stream create"));
+  long long items_max = 0;
+  for(int i = 0; i < nruns; ++i)
+  {
+    mass_lb_handle* h = nullptr;
+    if(int r = mass_lb_create(&params[i], LX[i], LY[i], 0, MASS_LB_FP32, &h)) return bail(r);
+    h->tuned = true;   // the ensemble kernel steps this lattice
+    e->runs.push_back(h);
+    const long long strips = (LY[i] + ENS_WOUT - 1)/ENS_WOUT;
+    items_max += strips*((LX[i] + 31)/32);
+    if(ensemble_set_params(e->slot0 + i, p32_of(h->P), model, e->stream) != cudaSuccess)
+      return bail(fail(MASS_LB_ECUDA, "ensemble parameters"));
+  }
+  e->order.resize(nruns);
+  for(int i = 0; i < nruns; ++i) e->order[i] = i;
+  std::stable_sort(e->order.begin(), e->order.end(), [&](int a, int b) {
+    return static_cast<long long>(LX[a])*LY[a] > static_cast<long long>(LX[b])*LY[b];
+  });
+  auto dal = [&](void** p, size_t bytes) {
+    if(cudaMalloc(p, bytes) != cudaSuccess) { cudaGetLastError(); return false; }
+    e->allocs.push_back(*p);
+    return true;
+  };
+  if(!dal(reinterpret_cast<void**>(&e->d_runs), nruns*sizeof(EnsRun)) ||
+     !dal(reinterpret_cast<void**>(&e->d_item_run), items_max*sizeof(int)) ||
+     !dal(reinterpret_cast<void**>(&e->d_counter), sizeof(int)) ||
+     !dal(reinterpret_cast<void**>(&e->d_err), sizeof(int)))
+    return bail(fail(MASS_LB_ENOMEM, "ensemble allocation"));
+  e->capacity = static_cast<int>(items_max);
+  e->grid = ensemble_grid(model);
+  if(e->grid <= 0) return bail(fail(MASS_LB_ECUDA, "ensemble kernel occupancy"));
+  if(cudaMemsetAsync(e->d_err, 0, sizeof(int), e->stream) != cudaSuccess)
+    return bail(fail(MASS_LB_ECUDA, "memset"));
+  if(const char* env = std::getenv("MASS_LB_ENSEMBLE_ROWS"))
+    e->rows = std::max(1, std::atoi(env));
+  *out = e;
+  return 0;
+}
+
+void mass_lb_ensemble_destroy(mass_lb_ensemble* e)
+{
+  if(!e) return;
+  DeviceGuard g(e->device);
+  if(e->stream) cudaStreamSynchronize(e->stream);
+  if(e->graph) cudaGraphExecDestroy(e->graph);
+  for(mass_lb_handle* h : e->runs) mass_lb_destroy(h);
+  for(void* p : e->allocs) cudaFree(p);
+  if(e->slot0 >= 0) release_slots(e->device, e->slot0, static_cast<int>(e->runs.size()));
+  if(e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+}
+
+mass_lb_handle* mass_lb_ensemble_run(mass_lb_ensemble* e, int i)
+{
+  if(!e || i < 0 || i >= static_cast<int>(e->runs.size())) return nullptr;
+  return e->runs[i];
+}
+
+int mass_lb_ensemble_size(mass_lb_ensemble* e)
+{
+  return e ? static_cast<int>(e->runs.size()) : 0;
+}
+
+int mass_lb_ensemble_step(mass_lb_ensemble* e, unsigned nsteps)
+{
+  if(!e) return fail(MASS_LB_EINVAL, "null ensemble");
+  if(nsteps == 0) return 0;
+  DeviceGuard g(e->device);
+  // the run handles may have been uploaded or stepped on their own streams
+  for(mass_lb_handle* h : e->runs) CU(cudaStreamSynchronize(h->stream), "run sync");
+  if(e->rows == 0)
+  {
+    if(int r = ens_autotune(e)) return r;
+  }
+  else if(int r = ens_pack(e, e->rows)) return r;
+  if(!e->graph)
+  {
+    // one replay = two steps: a -> b, then b -> a
+    cudaGraph_t gr = nullptr;
+    CU(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal), "capture");
+    int r1 = ens_launch(e, 0);
+    int r2 = r1 ? r1 : ens_launch(e, 1);
+    const cudaError_t ce = cudaStreamEndCapture(e->stream, &gr);
+    if(r1 || r2) { if(gr) cudaGraphDestroy(gr); return r1 ? r1 : r2; }
+    CU(ce, "end capture");
+    const cudaError_t ie = cudaGraphInstantiate(&e->graph, gr, 0);
+    cudaGraphDestroy(gr);
+    CU(ie, "graph instantiate");
+  }
+  for(unsigned k = 0; k + 1 < nsteps; k += 2)
+    CU(cudaGraphLaunch(e->graph, e->stream), "graph launch");
+  if(nsteps & 1)
+    if(int r = ens_launch(e, 0)) return r;
+  // an odd count leaves every run's state in b; either way the other buffer
+  // holds the state one step back
+  for(mass_lb_handle* h : e->runs)
+  {
+    if(nsteps & 1) std::swap(h->cur, h->nxt);
+    h->has_prev = true;
+    h->steps += nsteps;
+  }
+  CU(cudaStreamSynchronize(e->stream), "ensemble sync");
+  int err = 0;
+  CU(cudaMemcpy(&err, e->d_err, sizeof(int), cudaMemcpyDeviceToHost), "ensemble err");
+  if(err) return fail(MASS_LB_ECUDA, "ensemble step: a bounded wait on a bulk copy timed out");
+  return 0;
+}
+
+int mass_lb_ensemble_get_rows(mass_lb_ensemble* e)
+{
+  return e ? e->rows : 0;
 }
 
 } // extern "C"

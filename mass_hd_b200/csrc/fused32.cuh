@@ -59,6 +59,27 @@ struct FusedConfig
 cudaError_t launch_fused_warp_step(const FusedArgs& a, int model, int rows, bool diag,
                                    cudaStream_t st);
 
+// Ensembles: many lattices advanced by one persistent warp-strip launch.
+constexpr int ENS_MAX_RUNS = 192;     // constant-memory parameter slots per device
+constexpr int ENS_WOUT = 56;          // output columns per warp strip
+
+struct EnsRun
+{
+  float* a;            // state buffers (ping-pong); parity 0 reads a, writes b
+  float* b;
+  int LX, LY;
+  long long plane;
+  int nstrips, rows;   // strips of ENS_WOUT columns, rows per chunk
+  int item0;           // first item of this run in the packed list
+  int slot;            // constant-memory parameter slot
+};
+
+cudaError_t ensemble_set_params(int slot, const P32& p, int model, cudaStream_t st);
+cudaError_t launch_fused_warp_ensemble(const EnsRun* runs, const int* item_run, int nitems,
+                                       int* counter, int* err, int parity, int model, int grid,
+                                       cudaStream_t st);
+int ensemble_grid(int model);   // resident CTAs on this device (0 on error)
+
 // Launch one fused step (template dispatch on nt / model / diag).
 cudaError_t launch_fused_step(const FusedArgs& a, int model, FusedConfig cfg,
                               bool diag, cudaStream_t st);

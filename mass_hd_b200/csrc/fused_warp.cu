@@ -20,6 +20,7 @@
 //    mbarrier per slot; every wait is bounded (bit 0 of *err on time-out).
 #include "fused32.cuh"
 
+#include <algorithm>
 #include <cstdint>
 
 namespace mlb {
@@ -339,39 +340,44 @@ __device__ __forceinline__ f2 itau_of(const PP& P, f2 p)
   return MODEL == LYO ? rcp2(fma(W2(P.dtau), p, W2(P.tauIso)), P) : rcp2(W2(P.tauIso), P);
 }
 
+// One lattice as one work item sees it.
+struct ItemView
+{
+  const float* in;
+  float* out;
+  float* diag;
+  int* err;
+  int LX, LY;
+  long long plane;
+  int rows;
+};
+
+// Per-warp shared memory: input ring | delayed populations (3 rows) |
+// fn - ff/(2 tau) (2 rows); then the ring's mbarriers after all warps.
+template<int MODEL>
+struct WarpSmem
+{
+  static constexpr int NP = MODEL == LYO ? 12 : 11;
+  static constexpr int FLOATS = RING*NP*RWW + 3*NDP*PW + 2*9*COLS;
+};
+
+// Advance one strip chunk (strip `strip`, rows chunk*a.rows ..) of one
+// lattice by a full step. `rowbase` counts the input rows this warp has
+// copied through its ring so far (mbarrier phases continue across items).
+// Returns false if a bounded wait gave up.
 template<int MODEL, bool DIAG>
-__global__ void __launch_bounds__(32*WPB, 2)
-fused_warp_kernel(const __grid_constant__ FusedArgs a, const int nitems)
+__device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P, const int strip,
+                                          const int chunk, float* ring, float* dpop, float* hrow,
+                                          uint64_t* mbar, const int lane, unsigned& rowbase)
 {
   constexpr int NP = MODEL == LYO ? 12 : 11;
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // per warp: input ring | delayed populations (3 rows) | fn - ff/(2 tau) (2 rows)
-  constexpr int WARP_F = RING*NP*RWW + 3*NDP*PW + 2*9*COLS;
-  float* ring = reinterpret_cast<float*>(smem_raw) + warp*WARP_F;
-  float* dpop = ring + RING*NP*RWW;
-  float* hrow = dpop + 3*NDP*PW;
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(
-    smem_raw + WPB*WARP_F*sizeof(float)) + warp*RING;
-
-  const int item = blockIdx.x*WPB + warp;
-  if(item >= nitems) return;
-  const int strip = item % a.nstrips;
-  const int chunk = item / a.nstrips;
   const int y0 = strip*WOUT;
   const int x0 = chunk*a.rows;
   const int rows = min(a.rows, a.LX - x0);
   const int LX = a.LX, LY = a.LY;
   const int nload = rows + 8;            // rows x0-4 .. x0+rows+3
   const int ystart = (y0 - 4 + LY) % LY;
-  const PP& P = a.pp;
-
-  if(lane == 0)
-  {
-    for(int s = 0; s < RING; ++s) mbar_init(&mbar[s], 1);
-    fence_barrier_init();
-  }
-  __syncwarp();
+  const unsigned rb = rowbase;
 
   // Bulk-copy input row rr (lattice row x0 - 4 + rr) into its ring slot:
   // lane 0 posts the byte count, then lanes 0..NP-1 copy one plane each
@@ -379,7 +385,7 @@ fused_warp_kernel(const __grid_constant__ FusedArgs a, const int nitems)
   const float* plane_in = a.in + static_cast<long long>(lane < NP ? lane : 0)*a.plane;
   int gx_next = ((x0 - 4) % LX + LX) % LX;   // lattice row of the next copy
   auto issue = [&](int rr) {
-    const int slot = rr & (RING - 1);
+    const int slot = (rb + rr) & (RING - 1);
     uint64_t* bar = &mbar[slot];
     if(lane == 0) mbar_expect_tx(bar, NP*COLS*4);
     __syncwarp();
@@ -404,7 +410,8 @@ fused_warp_kernel(const __grid_constant__ FusedArgs a, const int nitems)
   const int n0 = min(RING, nload);
   for(int rr = 0; rr < n0; ++rr) issue(rr);
   int issued = n0;
-  bool abort = !mbar_wait_bounded(&mbar[0], 0) || !mbar_wait_bounded(&mbar[1], 0);
+  bool abort = !mbar_wait_bounded(&mbar[rb & (RING - 1)], (rb / RING) & 1) ||
+               !mbar_wait_bounded(&mbar[(rb + 1) & (RING - 1)], ((rb + 1) / RING) & 1);
 
   const int cl = PADY + 2*lane;            // this lane's first column in a ring row
   const int yg = y0 - 4 + 2*lane;          // global column of .x (pre-wrap)
@@ -430,12 +437,12 @@ fused_warp_kernel(const __grid_constant__ FusedArgs a, const int nitems)
     if(i + 2 < nload)
     {
       const int rr = i + 2;
-      if(!mbar_wait_bounded(&mbar[rr & (RING - 1)], (rr / RING) & 1)) abort = true;
+      if(!mbar_wait_bounded(&mbar[(rb + rr) & (RING - 1)], ((rb + rr) / RING) & 1)) abort = true;
     }
     if(__any_sync(0xffffffffu, abort)) break;
-    const float* Rm = ring + ((i    ) & (RING - 1))*NP*RWW;   // row b-1
-    const float* R0 = ring + ((i + 1) & (RING - 1))*NP*RWW;   // row b
-    const float* Rp = ring + ((i + 2) & (RING - 1))*NP*RWW;   // row b+1
+    const float* Rm = ring + ((rb + i    ) & (RING - 1))*NP*RWW;   // row b-1
+    const float* R0 = ring + ((rb + i + 1) & (RING - 1))*NP*RWW;   // row b
+    const float* Rp = ring + ((rb + i + 2) & (RING - 1))*NP*RWW;   // row b+1
     float* dp_now = dpop + s3*NDP*PW + 2 + 2*lane;                    // row of C, this iteration
     const float* dp_1 = dpop + (s3 == 0 ? 2 : s3 - 1)*NDP*PW + 2 + 2*lane;   // one iteration ago
     const float* dp_2 = dpop + (s3 == 2 ? 0 : s3 + 1)*NDP*PW + 2 + 2*lane;   // two iterations ago
@@ -643,20 +650,91 @@ fused_warp_kernel(const __grid_constant__ FusedArgs a, const int nitems)
     }
   }
 
+  rowbase = rb + issued;
   if(abort)
   {
     if(lane == 0) atomicOr(a.err, 1);
     // let every copy this warp issued land before its shared memory is
     // released
     for(int rr = 0; rr < issued; ++rr)
-      mbar_wait_bounded(&mbar[rr & (RING - 1)], (rr / RING) & 1);
+      mbar_wait_bounded(&mbar[(rb + rr) & (RING - 1)], ((rb + rr) / RING) & 1);
+    return false;
+  }
+  return true;
+}
+
+template<int MODEL>
+__device__ __forceinline__ void warp_smem(float*& ring, float*& dpop, float*& hrow,
+                                          uint64_t*& mbar, const int warp, const int lane)
+{
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  constexpr int NP = WarpSmem<MODEL>::NP;
+  ring = reinterpret_cast<float*>(smem_raw) + warp*WarpSmem<MODEL>::FLOATS;
+  dpop = ring + RING*NP*RWW;
+  hrow = dpop + 3*NDP*PW;
+  mbar = reinterpret_cast<uint64_t*>(
+    smem_raw + WPB*WarpSmem<MODEL>::FLOATS*sizeof(float)) + warp*RING;
+  if(lane == 0)
+  {
+    for(int s = 0; s < RING; ++s) mbar_init(&mbar[s], 1);
+    fence_barrier_init();
+  }
+  __syncwarp();
+}
+
+// One lattice: work item = blockIdx.x*WPB + warp.
+template<int MODEL, bool DIAG>
+__global__ void __launch_bounds__(32*WPB, 2)
+fused_warp_kernel(const __grid_constant__ FusedArgs a, const int nitems)
+{
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int item = blockIdx.x*WPB + warp;
+  if(item >= nitems) return;
+  float *ring, *dpop, *hrow;
+  uint64_t* mbar;
+  warp_smem<MODEL>(ring, dpop, hrow, mbar, warp, lane);
+  const ItemView v{a.in, a.out, a.diag, a.err, a.LX, a.LY, a.plane, a.rows};
+  unsigned rowbase = 0;
+  warp_item<MODEL, DIAG>(v, a.pp, item % a.nstrips, item / a.nstrips, ring, dpop, hrow,
+                         mbar, lane, rowbase);
+}
+
+// Ensemble: persistent warps take (run, strip, chunk) items from a packed
+// list through an atomic counter until it runs out. Per-run physics is in
+// constant memory (a slot range per ensemble).
+__constant__ PairParams c_ens_pp[ENS_MAX_RUNS];
+
+template<int MODEL>
+__global__ void __launch_bounds__(32*WPB, 2)
+fused_warp_ensemble_kernel(const EnsRun* __restrict__ runs, const int* __restrict__ item_run,
+                           const int nitems, int* __restrict__ counter, int* err, const int parity)
+{
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float *ring, *dpop, *hrow;
+  uint64_t* mbar;
+  warp_smem<MODEL>(ring, dpop, hrow, mbar, warp, lane);
+  unsigned rowbase = 0;
+  for(;;)
+  {
+    int item = 0;
+    if(lane == 0) item = atomicAdd(counter, 1);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if(item >= nitems) break;
+    const int r = item_run[item];
+    const EnsRun& R = runs[r];
+    const int local = item - R.item0;
+    const ItemView v{parity ? R.b : R.a, parity ? R.a : R.b, nullptr, err, R.LX, R.LY,
+                     R.plane, R.rows};
+    if(!warp_item<MODEL, false>(v, c_ens_pp[R.slot], local % R.nstrips, local / R.nstrips,
+                                ring, dpop, hrow, mbar, lane, rowbase))
+      break;
   }
 }
 
 template<int MODEL>
 constexpr size_t smem_bytes()
 {
-  return static_cast<size_t>(WPB)*(RING*(MODEL == LYO ? 12 : 11)*RWW + 3*NDP*PW + 2*9*COLS)*sizeof(float) +
+  return static_cast<size_t>(WPB)*WarpSmem<MODEL>::FLOATS*sizeof(float) +
          static_cast<size_t>(WPB)*RING*sizeof(uint64_t);
 }
 
@@ -686,7 +764,72 @@ cudaError_t launch_t(const FusedArgs& a, int rows, cudaStream_t st)
   return cudaGetLastError();
 }
 
+template<int MODEL>
+cudaError_t ens_attr()
+{
+  static unsigned long long attr_set = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const unsigned long long bit = 1ull << (dev & 63);
+  if(!(attr_set & bit))
+  {
+    const cudaError_t e = cudaFuncSetAttribute(fused_warp_ensemble_kernel<MODEL>,
+      cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem_bytes<MODEL>()));
+    if(e != cudaSuccess) return e;
+    attr_set |= bit;
+  }
+  return cudaSuccess;
+}
+
+template<int MODEL>
+cudaError_t launch_ens(const EnsRun* runs, const int* item_run, int nitems, int* counter,
+                       int* err, int parity, int grid, cudaStream_t st)
+{
+  const cudaError_t e = ens_attr<MODEL>();
+  if(e != cudaSuccess) return e;
+  fused_warp_ensemble_kernel<MODEL><<<grid, 32*WPB, smem_bytes<MODEL>(), st>>>(
+    runs, item_run, nitems, counter, err, parity);
+  return cudaGetLastError();
+}
+
+template<int MODEL>
+int ens_grid()
+{
+  if(ens_attr<MODEL>() != cudaSuccess) return 0;
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused_warp_ensemble_kernel<MODEL>,
+                                                   32*WPB, smem_bytes<MODEL>()) != cudaSuccess)
+    return 0;
+  return sms*std::max(per_sm, 1);
+}
+
 } // namespace
+
+cudaError_t ensemble_set_params(int slot, const P32& p, int model, cudaStream_t st)
+{
+  if(slot < 0 || slot >= ENS_MAX_RUNS) return cudaErrorInvalidValue;
+  static thread_local PairParams staging[ENS_MAX_RUNS];
+  staging[slot] = make_pp(p, model);
+  const cudaError_t e = cudaMemcpyToSymbolAsync(c_ens_pp, &staging[slot], sizeof(PairParams),
+                                                slot*sizeof(PairParams), cudaMemcpyHostToDevice, st);
+  if(e != cudaSuccess) return e;
+  return cudaStreamSynchronize(st);
+}
+
+cudaError_t launch_fused_warp_ensemble(const EnsRun* runs, const int* item_run, int nitems,
+                                       int* counter, int* err, int parity, int model, int grid,
+                                       cudaStream_t st)
+{
+  return model == LYO ? launch_ens<LYO>(runs, item_run, nitems, counter, err, parity, grid, st)
+                      : launch_ens<NEM>(runs, item_run, nitems, counter, err, parity, grid, st);
+}
+
+int ensemble_grid(int model)
+{
+  return model == LYO ? ens_grid<LYO>() : ens_grid<NEM>();
+}
 
 cudaError_t launch_fused_warp_step(const FusedArgs& a, int model, int rows, bool diag,
                                    cudaStream_t st)

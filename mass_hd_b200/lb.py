@@ -104,6 +104,13 @@ def load_library(build_if_missing: bool = False):
         "mass_lb_uses_fused": (C.c_int, [vp]),
         "mass_lb_device_state": (C.c_int, [vp, C.POINTER(vp), C.POINTER(C.c_longlong), ip]),
         "mass_lb_statistics": (C.c_int, [vp, C.POINTER(Stats)]),
+        "mass_lb_ensemble_create": (C.c_int, [C.c_int, C.POINTER(Params), C.POINTER(C.c_uint),
+                                              C.POINTER(C.c_uint), C.POINTER(vp)]),
+        "mass_lb_ensemble_destroy": (None, [vp]),
+        "mass_lb_ensemble_size": (C.c_int, [vp]),
+        "mass_lb_ensemble_run": (vp, [vp, C.c_int]),
+        "mass_lb_ensemble_step": (C.c_int, [vp, C.c_uint]),
+        "mass_lb_ensemble_get_rows": (C.c_int, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -162,9 +169,20 @@ class Lattice:
         _check(lib.mass_lb_create(C.byref(self._params), LX, LY, bc, precision, C.byref(h)))
         self.h = h
 
+    @classmethod
+    def _borrowed(cls, h, model: int, LX: int, LY: int, params: Params) -> "Lattice":
+        """A view of a handle owned elsewhere (an ensemble run)."""
+        self = cls.__new__(cls)
+        self.model, self.LX, self.LY, self.bc, self.precision = model, LX, LY, 0, FP32
+        self._params = params
+        self.h = C.c_void_p(h)
+        self._owned = False
+        return self
+
     def close(self):
         if getattr(self, "h", None):
-            load_library().mass_lb_destroy(self.h)
+            if getattr(self, "_owned", True):
+                load_library().mass_lb_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -270,3 +288,53 @@ class Lattice:
         p, stride, n = C.c_void_p(), C.c_longlong(), C.c_int()
         _check(load_library().mass_lb_device_state(self.h, C.byref(p), C.byref(stride), C.byref(n)))
         return p.value, stride.value, n.value
+
+
+class Ensemble:
+    """Independent FP32 periodic lattices of uneven sizes and parameters,
+    stepped together by one persistent kernel launch per step
+    (mass_lb_ensemble_*, include/mass_lb_ext.h). `runs[i]` is a Lattice
+    view of run i for upload, get, checks and statistics."""
+
+    def __init__(self, model: int, params: list, sizes: list):
+        lib = load_library()
+        n = len(params)
+        assert n == len(sizes) and n > 0
+        self.model = model
+        arr = (Params * n)(*[make_params(model, p) for p in params])
+        lx = (C.c_uint * n)(*[int(s[0]) for s in sizes])
+        ly = (C.c_uint * n)(*[int(s[1]) for s in sizes])
+        h = C.c_void_p()
+        _check(lib.mass_lb_ensemble_create(n, arr, lx, ly, C.byref(h)))
+        self.h = h
+        self.runs = [Lattice._borrowed(lib.mass_lb_ensemble_run(h, i), model, int(sizes[i][0]),
+                                       int(sizes[i][1]), arr[i]) for i in range(n)]
+
+    def __len__(self):
+        return len(self.runs)
+
+    def step(self, n: int = 1):
+        _check(load_library().mass_lb_ensemble_step(self.h, n))
+
+    @property
+    def rows(self) -> int:
+        return load_library().mass_lb_ensemble_get_rows(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            for r in self.runs:
+                r.h = None
+            load_library().mass_lb_ensemble_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

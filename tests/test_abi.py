@@ -59,3 +59,25 @@ def test_create_rejects_bad_arguments_without_device():
 def test_nematic_rejects_thermal_noise():
     with pytest.raises(M.MassLBError):
         M.make_params(M.NEMATIC, {"Q_kBT": 0.1})
+
+
+def test_ensemble_create_rejects_bad_arguments_without_device():
+    lib = M.load_library()
+    h = ctypes.c_void_p()
+    P = M.lb.Params
+    lx = (ctypes.c_uint * 2)(64, 64)
+    ly = (ctypes.c_uint * 2)(64, 64)
+    two = (P * 2)(M.make_params(0, {}), M.make_params(0, {}))
+    assert lib.mass_lb_ensemble_create(0, two, lx, ly, ctypes.byref(h)) == -1
+    assert lib.mass_lb_ensemble_create(2, None, lx, ly, ctypes.byref(h)) == -1
+    assert lib.mass_lb_ensemble_create(193, two, lx, ly, ctypes.byref(h)) == -1
+    mixed = (P * 2)(M.make_params(0, {}), M.make_params(1, {}))
+    assert lib.mass_lb_ensemble_create(2, mixed, lx, ly, ctypes.byref(h)) == -1
+    npc2 = (P * 2)(M.make_params(0, {"npc": 2}), M.make_params(0, {"npc": 2}))
+    assert lib.mass_lb_ensemble_create(2, npc2, lx, ly, ctypes.byref(h)) == -4
+    bad_ly = (ctypes.c_uint * 2)(64, 62)
+    assert lib.mass_lb_ensemble_create(2, two, lx, bad_ly, ctypes.byref(h)) == -4
+    assert h.value is None
+    assert lib.mass_lb_ensemble_size(None) == 0
+    assert lib.mass_lb_ensemble_run(None, 0) is None
+    assert lib.mass_lb_ensemble_step(None, 1) == -1
