@@ -35,6 +35,8 @@ UNITS = {
     "stats.cu": [],
     "api.cu": [],
     "noalloc.cu": [],
+    "conv_tc.cu": [],
+    "surrogate_ops.cu": [],
 }
 
 

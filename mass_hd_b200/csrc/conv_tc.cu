@@ -1,0 +1,593 @@
+// Implicit-GEMM 3x3 circular convolutions on the sm_100a tensor cores.
+//
+// Forward and input-gradient pass (conv3x3_kernel): D[128 pixels][NOUT] =
+// sum over 9 taps of A_tap[128 pixels][64 ci] * B_tap[NOUT][64 ci]^T. One
+// output tile is half a row of one image (128 consecutive x). A_tap is the
+// tile of the padded input shifted by the tap, fetched by one TMA tile load
+// (128-byte swizzle); all 9 weight taps stay in shared memory for the whole
+// persistent kernel. Warp roles: warp 0 issues TMA loads into a 6-stage
+// ring, warp 1 issues tcgen05.mma (4 x K=16 per tap) into one of two TMEM
+// accumulators, warps 2-5 drain the other accumulator (tcgen05.ld), apply
+// the fused epilogue and store bf16 pixels with their periodic ring copies.
+//
+// Weight gradient (conv3x3_wgrad_kernel): dW_tap[ci][co] = sum over pixels of
+// x(p + tap)[ci] * dy(p)[co]. K runs over pixels, so both operands are read
+// MN-major straight from the NHWC tiles. A CTA owns a pair of taps (M = 2 x
+// 64 input channels, two TMA tiles LBO apart) for a contiguous range of
+// pixel tiles, accumulates in TMEM and adds its partial sums to dW with
+// atomics.
+//
+// Every mbarrier wait is bounded (about a second); on time-out the role sets
+// an error bit, the others stop at their next wait, outstanding MMAs are
+// awaited (bounded) and TMEM is freed before the CTA exits.
+#include "conv_tc.cuh"
+#include "tc_ptx.cuh"
+
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <mutex>
+
+namespace mlb {
+
+using namespace tc;
+
+namespace {
+
+constexpr int CONV_THREADS = 192;     // 6 warps: TMA, MMA, 4 x epilogue
+constexpr int STAGES = 6;
+constexpr uint32_t TILE_BYTES = 128u*128u;   // 128 pixels x 64 bf16
+
+template<int NOUT>
+struct ConvSmem
+{
+  static constexpr uint32_t W_BYTES = 9u*NOUT*128u;          // multiple of 1024
+  static constexpr uint32_t A_OFF = W_BYTES;
+  static constexpr uint32_t BAR_OFF = A_OFF + STAGES*TILE_BYTES;
+  static constexpr int NBAR = 2*STAGES + 6;                  // full, empty, w, tfull[2], tempty[2], done
+  static constexpr uint32_t MISC_OFF = BAR_OFF + NBAR*8;
+  static constexpr uint32_t BIAS_OFF = MISC_OFF + 16;
+  static constexpr uint32_t BYTES = BIAS_OFF + 64*4;
+  static constexpr uint32_t ALLOC = BYTES + 1024;            // room to align the base
+  static constexpr uint32_t TMEM_COLS = NOUT == 64 ? 128 : 32;
+};
+
+__device__ __forceinline__ uint8_t* align1024(uint8_t* p)
+{
+  const uint32_t a = smem_u32(p);
+  return p + ((1024u - (a & 1023u)) & 1023u);
+}
+
+__device__ __forceinline__ size_t padded_index(int n, int yy, int xx, int H, int W)
+{
+  return (static_cast<size_t>(n)*(H + 2) + yy)*static_cast<size_t>(W + 2) + xx;
+}
+
+__device__ __forceinline__ float gelu(float x)
+{
+  return 0.5f*x*(1.f + erff(x*0.70710678118654752f));
+}
+__device__ __forceinline__ float gelu_grad(float x)
+{
+  return 0.5f*(1.f + erff(x*0.70710678118654752f)) + x*0.39894228040143268f*expf(-0.5f*x*x);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16x2(float a, float b)
+{
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<const uint32_t*>(&h);
+}
+
+__device__ __forceinline__ void unpack8(const uint4& u, float* f)
+{
+  const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+  for(int i = 0; i < 4; ++i)
+  {
+    const float2 t = __bfloat1622float2(h[i]);
+    f[2*i] = t.x;
+    f[2*i + 1] = t.y;
+  }
+}
+
+// 64 channels of pixel (n, y, x) -> padded tensor, with its periodic copies
+__device__ __forceinline__ void store_pixel(__nv_bfloat16* base, const float* v, int n, int y,
+                                            int x, int H, int W)
+{
+  uint4 pk[8];
+#pragma unroll
+  for(int k = 0; k < 8; ++k)
+    pk[k] = make_uint4(pack_bf16x2(v[8*k], v[8*k + 1]), pack_bf16x2(v[8*k + 2], v[8*k + 3]),
+                       pack_bf16x2(v[8*k + 4], v[8*k + 5]), pack_bf16x2(v[8*k + 6], v[8*k + 7]));
+  int ys[3] = {y + 1, 0, 0}, xs[3] = {x + 1, 0, 0};
+  int ny = 1, nx = 1;
+  if(y == 0) ys[ny++] = H + 1;
+  if(y == H - 1) ys[ny++] = 0;
+  if(x == 0) xs[nx++] = W + 1;
+  if(x == W - 1) xs[nx++] = 0;
+  for(int i = 0; i < ny; ++i)
+    for(int j = 0; j < nx; ++j)
+    {
+      uint4* dst = reinterpret_cast<uint4*>(base + padded_index(n, ys[i], xs[j], H, W)*64);
+#pragma unroll
+      for(int k = 0; k < 8; ++k) dst[k] = pk[k];
+    }
+}
+
+__device__ __forceinline__ void load_pixel(const __nv_bfloat16* base, float* v, int n, int y,
+                                           int x, int H, int W)
+{
+  const uint4* src = reinterpret_cast<const uint4*>(base + padded_index(n, y + 1, x + 1, H, W)*64);
+#pragma unroll
+  for(int k = 0; k < 8; ++k) unpack8(src[k], v + 8*k);
+}
+
+template<int NOUT, int MODE>
+__global__ void __launch_bounds__(CONV_THREADS, 1)
+conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmW,
+               const ConvArgs a)
+{
+  using L = ConvSmem<NOUT>;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* sm = align1024(smem_raw);
+  uint8_t* Wsm = sm;
+  uint8_t* Asm = sm + L::A_OFF;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + L::BAR_OFF);
+  uint64_t* full = bars;
+  uint64_t* empty = bars + STAGES;
+  uint64_t* wbar = bars + 2*STAGES;
+  uint64_t* tfull = wbar + 1;
+  uint64_t* tempty = wbar + 3;
+  uint64_t* done = wbar + 5;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + L::MISC_OFF);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + L::MISC_OFF + 4);
+  float* bias_sm = reinterpret_cast<float*>(sm + L::BIAS_OFF);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int H = a.H, W = a.W, xt_n = W >> 7;
+  const int ntiles = a.B*H*xt_n;
+
+  if(threadIdx.x == 0)
+  {
+    for(int s = 0; s < STAGES; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+    mbar_init(wbar, 1);
+    mbar_init(&tfull[0], 1);
+    mbar_init(&tfull[1], 1);
+    mbar_init(&tempty[0], 4);
+    mbar_init(&tempty[1], 4);
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    fence_barrier_init();
+    fence_proxy_async();
+  }
+  if(warp == 1) tmem_alloc(tmem_slot, L::TMEM_COLS);
+  if(threadIdx.x >= 64 && threadIdx.x < 64 + NOUT)
+    bias_sm[threadIdx.x - 64] = (MODE <= CONV_FWD_OUT && a.bias) ? a.bias[threadIdx.x - 64] : 0.f;
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = *tmem_slot;
+
+  auto give_up = [&]() {
+    *abort_flag = 1;
+    atomicOr(a.err, 2);
+  };
+
+  if(warp == 0)
+  {
+    if(lane == 0)
+    {
+      prefetch_map(&tmX);
+      prefetch_map(&tmW);
+      mbar_expect_tx(wbar, L::W_BYTES);
+      for(int t = 0; t < 9; ++t) tma_load_3d(Wsm + t*NOUT*128, &tmW, 0, 0, t, wbar);
+      uint32_t it = 0;
+      for(int tile = blockIdx.x; tile < ntiles && !*abort_flag; tile += gridDim.x)
+      {
+        const int xt = tile % xt_n, row = tile / xt_n;
+        const int y = row % H, n = row / H, x0 = xt << 7;
+        for(int tap = 0; tap < 9; ++tap, ++it)
+        {
+          const uint32_t s = it % STAGES, ph = (it / STAGES) & 1u;
+          if(!mbar_wait(&empty[s], ph ^ 1u)) { give_up(); break; }
+          mbar_expect_tx(&full[s], TILE_BYTES);
+          tma_load_4d(Asm + s*TILE_BYTES, &tmX, 0, x0 + tap % 3, y + tap / 3, n, &full[s]);
+        }
+      }
+      // loads still in flight after an abort land before the CTA exits
+      if(*abort_flag)
+        for(uint32_t k = 0; k < STAGES && k < it; ++k)
+        {
+          const uint32_t j = it - 1 - k;
+          mbar_wait(&full[j % STAGES], (j / STAGES) & 1u);
+        }
+    }
+  }
+  else if(warp == 1)
+  {
+    if(lane == 0)
+    {
+      constexpr uint32_t IDESC = idesc_bf16_f32(128, NOUT, 0, 0);
+      bool ok = mbar_wait(wbar, 0);
+      if(!ok) give_up();
+      const uint32_t wbase = smem_u32(Wsm), abase = smem_u32(Asm);
+      uint32_t it = 0, tcount = 0;
+      for(int tile = blockIdx.x; ok && tile < ntiles && !*abort_flag; tile += gridDim.x, ++tcount)
+      {
+        const uint32_t acc = tcount & 1u, use = tcount >> 1;
+        if(!mbar_wait(&tempty[acc], (use & 1u) ^ 1u)) { give_up(); break; }
+        tc_fence_after();
+        const uint32_t d = tbase + acc*NOUT;
+        for(int tap = 0; tap < 9; ++tap, ++it)
+        {
+          const uint32_t s = it % STAGES, ph = (it / STAGES) & 1u;
+          if(!mbar_wait(&full[s], ph)) { give_up(); ok = false; break; }
+          tc_fence_after();
+          const uint32_t a0 = abase + s*TILE_BYTES, b0 = wbase + tap*NOUT*128;
+#pragma unroll
+          for(int k = 0; k < 4; ++k)
+            mma_bf16(d, sw128_desc(a0 + 32*k, 16, 1024), sw128_desc(b0 + 32*k, 16, 1024), IDESC,
+                     (tap | k) != 0);
+          mma_commit(&empty[s]);
+        }
+        if(!ok) break;
+        mma_commit(&tfull[acc]);
+      }
+      mma_commit(done);
+      if(!mbar_wait(done, 0)) give_up();
+    }
+  }
+  else
+  {
+    const int q = warp & 3;                       // TMEM lanes 32q..32q+31
+    uint32_t tcount = 0;
+    // decisions are warp-uniform: tcgen05.ld needs all 32 lanes
+    for(int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++tcount)
+    {
+      if(__any_sync(0xffffffffu, *abort_flag != 0)) break;
+      const uint32_t acc = tcount & 1u, use = tcount >> 1;
+      if(!__all_sync(0xffffffffu, mbar_wait(&tfull[acc], use & 1u)))
+      {
+        if(lane == 0) give_up();
+        break;
+      }
+      tc_fence_after();
+      const uint32_t taddr = tbase + (static_cast<uint32_t>(q*32) << 16) + acc*NOUT;
+      const int xt = tile % xt_n, row = tile / xt_n;
+      const int y = row % H, n = row / H;
+      const int x = (xt << 7) + q*32 + lane;
+      if constexpr(NOUT == 16)
+      {
+        float v[16];
+        tmem_ld16(taddr, v);
+        tc_fence_before();
+        __syncwarp();
+        if(lane == 0) mbar_arrive(&tempty[acc]);
+        const size_t p = (static_cast<size_t>(n)*H + y)*W + x;
+#pragma unroll
+        for(int c = 0; c < 5; ++c)
+          a.out_f[5*p + c] = v[c] + bias_sm[c] + (a.resid_f ? a.resid_f[5*p + c] : 0.f);
+      }
+      else
+      {
+        float v[64];
+        tmem_ld32(taddr, v);
+        tmem_ld32(taddr + 32, v + 32);
+        tc_fence_before();
+        __syncwarp();
+        if(lane == 0) mbar_arrive(&tempty[acc]);
+        if constexpr(MODE == CONV_FWD_BIAS || MODE == CONV_FWD_GELU || MODE == CONV_FWD_RESID)
+        {
+#pragma unroll
+          for(int c = 0; c < 64; ++c) v[c] += bias_sm[c];
+        }
+        if constexpr(MODE == CONV_FWD_GELU)
+        {
+          uint4* dst = reinterpret_cast<uint4*>(a.out2 + padded_index(n, y + 1, x + 1, H, W)*64);
+#pragma unroll
+          for(int k = 0; k < 8; ++k)
+            dst[k] = make_uint4(pack_bf16x2(v[8*k], v[8*k + 1]), pack_bf16x2(v[8*k + 2], v[8*k + 3]),
+                                pack_bf16x2(v[8*k + 4], v[8*k + 5]), pack_bf16x2(v[8*k + 6], v[8*k + 7]));
+#pragma unroll
+          for(int c = 0; c < 64; ++c) v[c] = gelu(v[c]);
+        }
+        if constexpr(MODE == CONV_FWD_RESID || MODE == CONV_BWD_RESID)
+        {
+          float r[64];
+          load_pixel(a.resid, r, n, y, x, H, W);
+#pragma unroll
+          for(int c = 0; c < 64; ++c) v[c] += r[c];
+        }
+        if constexpr(MODE == CONV_BWD_GELU)
+        {
+          float t[64];
+          load_pixel(a.aux, t, n, y, x, H, W);
+#pragma unroll
+          for(int c = 0; c < 64; ++c) v[c] *= gelu_grad(t[c]);
+        }
+        store_pixel(a.out, v, n, y, x, H, W);
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if(warp == 1)
+  {
+    tc_fence_after();
+    tmem_dealloc(tbase, L::TMEM_COLS);
+    tmem_relinquish();
+  }
+}
+
+// ---- weight gradient ---------------------------------------------------------
+
+constexpr int WG_STAGES = 4;
+constexpr uint32_t WG_STAGE = 3*TILE_BYTES;     // x tap a, x tap b, dy
+constexpr uint32_t WG_BAR_OFF = WG_STAGES*WG_STAGE;
+constexpr uint32_t WG_MISC_OFF = WG_BAR_OFF + (2*WG_STAGES + 1)*8;
+constexpr uint32_t WG_ALLOC = WG_MISC_OFF + 16 + 1024;
+constexpr int WG_GROUPS = 5;                     // tap pairs {0,1} {2,3} {4,5} {6,7} {8}
+
+struct WgradArgs
+{
+  int B, H, W, nchunks;
+  float* dW;
+  int* err;
+};
+
+__global__ void __launch_bounds__(CONV_THREADS, 1)
+conv3x3_wgrad_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmD,
+                     const WgradArgs a)
+{
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* sm = align1024(smem_raw);
+  uint64_t* full = reinterpret_cast<uint64_t*>(sm + WG_BAR_OFF);
+  uint64_t* empty = full + WG_STAGES;
+  uint64_t* done = full + 2*WG_STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + WG_MISC_OFF);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + WG_MISC_OFF + 4);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = blockIdx.x % WG_GROUPS, chunk = blockIdx.x / WG_GROUPS;
+  const int ta = 2*g, tb = 2*g + 1 < 9 ? 2*g + 1 : 8;
+  const int xt_n = a.W >> 7;
+  const long long nblocks = static_cast<long long>(a.B)*a.H*xt_n;
+  const int b0 = static_cast<int>(chunk*nblocks/a.nchunks);
+  const int b1 = static_cast<int>((chunk + 1)*nblocks/a.nchunks);
+
+  if(threadIdx.x == 0)
+  {
+    for(int s = 0; s < WG_STAGES; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    fence_barrier_init();
+    fence_proxy_async();
+  }
+  if(warp == 1) tmem_alloc(tmem_slot, 64);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = *tmem_slot;
+  auto give_up = [&]() {
+    *abort_flag = 1;
+    atomicOr(a.err, 2);
+  };
+
+  if(warp == 0)
+  {
+    if(lane == 0)
+    {
+      prefetch_map(&tmX);
+      prefetch_map(&tmD);
+      uint32_t it = 0;
+      for(int blk = b0; blk < b1 && !*abort_flag; ++blk, ++it)
+      {
+        const int xt = blk % xt_n, row = blk / xt_n;
+        const int y = row % a.H, n = row / a.H, x0 = xt << 7;
+        const uint32_t s = it % WG_STAGES, ph = (it / WG_STAGES) & 1u;
+        if(!mbar_wait(&empty[s], ph ^ 1u)) { give_up(); break; }
+        uint8_t* st = sm + s*WG_STAGE;
+        mbar_expect_tx(&full[s], WG_STAGE);
+        tma_load_4d(st, &tmX, 0, x0 + ta % 3, y + ta / 3, n, &full[s]);
+        tma_load_4d(st + TILE_BYTES, &tmX, 0, x0 + tb % 3, y + tb / 3, n, &full[s]);
+        tma_load_4d(st + 2*TILE_BYTES, &tmD, 0, x0 + 1, y + 1, n, &full[s]);
+      }
+      if(*abort_flag)
+        for(uint32_t k = 0; k < WG_STAGES && k < it; ++k)
+        {
+          const uint32_t j = it - 1 - k;
+          mbar_wait(&full[j % WG_STAGES], (j / WG_STAGES) & 1u);
+        }
+    }
+  }
+  else if(warp == 1)
+  {
+    if(lane == 0)
+    {
+      // A = the two x tiles (M = 2 x 64 input channels, MN groups one tile
+      // apart, K = pixels in 8-row groups 1024 B apart); B = the dy tile
+      // (N = 64 output channels, one MN group)
+      constexpr uint32_t IDESC = idesc_bf16_f32(128, 64, 1, 1);
+      const uint32_t base = smem_u32(sm);
+      uint32_t it = 0;
+      for(int blk = b0; blk < b1 && !*abort_flag; ++blk, ++it)
+      {
+        const uint32_t s = it % WG_STAGES, ph = (it / WG_STAGES) & 1u;
+        if(!mbar_wait(&full[s], ph)) { give_up(); break; }
+        tc_fence_after();
+        const uint32_t st = base + s*WG_STAGE;
+#pragma unroll
+        for(int kk = 0; kk < 8; ++kk)
+          mma_bf16(tbase, sw128_desc(st + kk*2048, TILE_BYTES, 1024),
+                   sw128_desc(st + 2*TILE_BYTES + kk*2048, 1024, 1024), IDESC,
+                   (blk != b0) || (kk != 0));
+        mma_commit(&empty[s]);
+      }
+      mma_commit(done);
+      if(!mbar_wait(done, 0)) give_up();
+    }
+  }
+  else if(b1 > b0)
+  {
+    const int q = warp & 3;
+    // warp-uniform: tcgen05.ld needs all 32 lanes
+    if(!__all_sync(0xffffffffu, mbar_wait(done, 0)))
+    {
+      if(lane == 0) give_up();
+    }
+    else
+    {
+      tc_fence_after();
+      const int m = q*32 + lane;
+      const int h = m >> 6, ci = m & 63;
+      const int tap = h ? tb : ta;
+      float v[64];
+      const uint32_t taddr = tbase + (static_cast<uint32_t>(q*32) << 16);
+      tmem_ld32(taddr, v);
+      tmem_ld32(taddr + 32, v + 32);
+      const bool aborted = __any_sync(0xffffffffu, *abort_flag != 0);
+      if(!(h == 1 && tb == ta) && !aborted)
+      {
+        float* dst = a.dW + (static_cast<size_t>(tap)*64 + ci)*64;
+#pragma unroll
+        for(int co = 0; co < 64; ++co) atomicAdd(dst + co, v[co]);
+      }
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if(warp == 1)
+  {
+    tc_fence_after();
+    tmem_dealloc(tbase, 64);
+    tmem_relinquish();
+  }
+}
+
+// ---- host side ------------------------------------------------------------------
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+       q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// padded NHWC64 bf16 [B][H+2][W+2][64], box 64 channels x 128 pixels
+bool map_activation(CUtensorMap* m, const void* base, int B, int H, int W)
+{
+  auto fn = encode_fn();
+  if(!fn) return false;
+  const cuuint64_t dims[4] = {64, static_cast<cuuint64_t>(W + 2), static_cast<cuuint64_t>(H + 2),
+                              static_cast<cuuint64_t>(B)};
+  const cuuint64_t strides[3] = {128, static_cast<cuuint64_t>(W + 2)*128,
+                                 static_cast<cuuint64_t>(H + 2)*(W + 2)*128};
+  const cuuint32_t box[4] = {64, 128, 1, 1};
+  const cuuint32_t es[4] = {1, 1, 1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// weights bf16 [9][nout][64], box 64 x nout
+bool map_weights(CUtensorMap* m, const void* base, int nout)
+{
+  auto fn = encode_fn();
+  if(!fn) return false;
+  const cuuint64_t dims[3] = {64, static_cast<cuuint64_t>(nout), 9};
+  const cuuint64_t strides[2] = {128, static_cast<cuuint64_t>(nout)*128};
+  const cuuint32_t box[3] = {64, static_cast<cuuint32_t>(nout), 1};
+  const cuuint32_t es[3] = {1, 1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<void*>(base), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+int sm_count()
+{
+  int dev = 0, n = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  return n;
+}
+
+// the dynamic shared-memory opt-in, once per kernel and device
+template<typename K>
+cudaError_t smem_attr(K kern, unsigned long long& set_mask, int bytes)
+{
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const unsigned long long bit = 1ull << (dev & 63);
+  if(set_mask & bit) return cudaSuccess;
+  const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if(e == cudaSuccess) set_mask |= bit;
+  return e;
+}
+
+template<int NOUT, int MODE>
+cudaError_t launch_mode(const CUtensorMap& tx, const CUtensorMap& tw, const ConvArgs& a,
+                        cudaStream_t st)
+{
+  static unsigned long long attr = 0;
+  auto kern = conv3x3_kernel<NOUT, MODE>;
+  const cudaError_t e = smem_attr(kern, attr, static_cast<int>(ConvSmem<NOUT>::ALLOC));
+  if(e != cudaSuccess) return e;
+  const int ntiles = a.B*a.H*(a.W >> 7);
+  const int grid = std::min(ntiles, sm_count());
+  kern<<<grid, CONV_THREADS, ConvSmem<NOUT>::ALLOC, st>>>(tx, tw, a);
+  return cudaGetLastError();
+}
+
+} // namespace
+
+cudaError_t conv3x3_launch(const __nv_bfloat16* in, const __nv_bfloat16* w, int nout, int mode,
+                           const ConvArgs& a, cudaStream_t st)
+{
+  if(a.B < 1 || a.H < 1 || a.W < 128 || (a.W & 127)) return cudaErrorInvalidValue;
+  if((nout == 16) != (mode == CONV_FWD_OUT) || (nout != 16 && nout != 64))
+    return cudaErrorInvalidValue;
+  CUtensorMap tx, tw;
+  if(!map_activation(&tx, in, a.B, a.H, a.W) || !map_weights(&tw, w, nout))
+    return cudaErrorInvalidValue;
+  switch(mode)
+  {
+    case CONV_FWD_BIAS: return launch_mode<64, CONV_FWD_BIAS>(tx, tw, a, st);
+    case CONV_FWD_GELU: return launch_mode<64, CONV_FWD_GELU>(tx, tw, a, st);
+    case CONV_FWD_RESID: return launch_mode<64, CONV_FWD_RESID>(tx, tw, a, st);
+    case CONV_FWD_OUT: return launch_mode<16, CONV_FWD_OUT>(tx, tw, a, st);
+    case CONV_BWD_GELU: return launch_mode<64, CONV_BWD_GELU>(tx, tw, a, st);
+    case CONV_BWD_RESID: return launch_mode<64, CONV_BWD_RESID>(tx, tw, a, st);
+    case CONV_BWD_PLAIN: return launch_mode<64, CONV_BWD_PLAIN>(tx, tw, a, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t conv3x3_wgrad_launch(const __nv_bfloat16* x, const __nv_bfloat16* dy, float* dW,
+                                 int B, int H, int W, int* err, cudaStream_t st)
+{
+  if(B < 1 || H < 1 || W < 128 || (W & 127)) return cudaErrorInvalidValue;
+  CUtensorMap tx, td;
+  if(!map_activation(&tx, x, B, H, W) || !map_activation(&td, dy, B, H, W))
+    return cudaErrorInvalidValue;
+  static unsigned long long attr = 0;
+  const cudaError_t e = smem_attr(conv3x3_wgrad_kernel, attr, static_cast<int>(WG_ALLOC));
+  if(e != cudaSuccess) return e;
+  const long long nblocks = static_cast<long long>(B)*H*(W >> 7);
+  // chunks per tap pair: about one wave of CTAs over all pairs
+  const int nchunks = static_cast<int>(std::max<long long>(1, std::min<long long>(
+    nblocks, (sm_count() + WG_GROUPS - 1)/WG_GROUPS)));
+  WgradArgs a{B, H, W, nchunks, dW, err};
+  conv3x3_wgrad_kernel<<<WG_GROUPS*nchunks, CONV_THREADS, WG_ALLOC, st>>>(tx, td, a);
+  return cudaGetLastError();
+}
+
+} // namespace mlb

@@ -19,7 +19,7 @@ def declared_functions():
             continue
         text = open(os.path.join(INCLUDE, f)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-        for m in re.finditer(r"^\s*[A-Za-z_][\w\s\*]*?\b(mass_lb_\w+)\s*\(", text, flags=re.M):
+        for m in re.finditer(r"^\s*[A-Za-z_][\w\s\*]*?\b(mass_(?:lb|sg)_\w+)\s*\(", text, flags=re.M):
             names.append(m.group(1))
     return sorted(set(names))
 
