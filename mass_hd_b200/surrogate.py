@@ -11,9 +11,9 @@ residual epilogues, FP32 master weights and moments. torch only allocates
 device buffers and provides the stream.
 
 Training data come from the GPU simulator itself (`generate_dataset`): an
-ensemble of 256^2 runs with zeta ~ U[0.005, 0.03], one snapshot every
-`jump` steps after a spin-up, consecutive snapshots forming (t, t+jump)
-pairs.
+ensemble of 256^2 runs with zeta ~ U[0.005, 0.03], from each run (t, t+jump)
+snapshot pairs at times spread evenly over the window the hybrid loop is
+run in.
 
 `hybrid()` advances lattices alternately with the plain method and the
 surrogate: every M jumps the plain method runs one jump from the current
@@ -304,25 +304,32 @@ def initial_state(L: int, rng: np.random.Generator) -> dict:
             "phi": 0.5 * (1 - np.tanh((r - L / 4) / 2))}
 
 
-def generate_dataset(ntraj=40, L=256, snapshots=51, jump=50, spinup=2000, seed=0,
+def generate_dataset(ntraj=40, L=256, pairs=50, jump=50, t_min=2000, t_max=22000, seed=0,
                      zeta_range=(0.005, 0.03)):
     """Simulate ntraj lattices together (one ensemble) and record the raw
-    fields every `jump` steps. Returns (fields [ntraj*snapshots, L, L, 5]
-    device fp32, zetas). Pair (k, k+1) within a trajectory is one sample."""
+    fields of `pairs` (t, t+jump) pairs per trajectory, t evenly spaced over
+    [t_min, t_max). Returns (fields [ntraj*2*pairs, L, L, 5] device fp32,
+    zetas); snapshots 2k and 2k+1 of a trajectory form pair k."""
     rng = np.random.default_rng(seed)
     zetas = rng.uniform(*zeta_range, ntraj)
     ens = lb.Ensemble(lb.LYOTROPIC, [training_params(z) for z in zetas], [(L, L)] * ntraj)
     for run in ens.runs:
         run.upload_state(initial_state(L, rng))
-    ens.step(spinup)
-    fields = torch.empty((ntraj * snapshots, L, L, NF), dtype=torch.float32, device="cuda")
+    per = 2 * pairs
+    fields = torch.empty((ntraj * per, L, L, NF), dtype=torch.float32, device="cuda")
     zero, one = np.zeros(NF), np.ones(NF)
-    for s in range(snapshots):
-        if s:
-            ens.step(jump)
-        for r, run in enumerate(ens.runs):
-            fields_from_lattice(run, fields[r * snapshots + s], zero, one)
-        torch.cuda.current_stream().synchronize()
+    gap = (t_max - t_min) // pairs
+    t = 0
+    for k in range(pairs):
+        t0 = t_min + k * gap
+        ens.step(t0 - t)
+        for half in (0, 1):
+            if half:
+                ens.step(jump)
+            for r, run in enumerate(ens.runs):
+                fields_from_lattice(run, fields[r * per + 2 * k + half], zero, one)
+            torch.cuda.current_stream().synchronize()
+        t = t0 + jump
     ens.close()
     return fields, zetas
 
@@ -335,9 +342,10 @@ def normalise(fields: torch.Tensor):
     return mean.cpu().numpy().astype(np.float32), scale.cpu().numpy().astype(np.float32)
 
 
-def pair_indices(ntraj, snapshots):
-    return np.array([(t * snapshots + k, t * snapshots + k + 1)
-                     for t in range(ntraj) for k in range(snapshots - 1)], dtype=np.int32)
+def pair_indices(ntraj, pairs):
+    """(input, target) snapshot indices of generate_dataset's layout."""
+    return np.array([(t * 2 * pairs + 2 * k, t * 2 * pairs + 2 * k + 1)
+                     for t in range(ntraj) for k in range(pairs)], dtype=np.int32)
 
 
 def train(params: Params, fields: torch.Tensor, pairs: np.ndarray, epochs=20, batch=32,

@@ -8,9 +8,9 @@ bench: CUDA-event time of each convolution kind at the training shape
 (batch x size^2 pixels, 64 channels) and of one whole training step,
 with the tensor-core rate against the measured bf16 peak.
 train: simulator-generated dataset (40 trajectories of 256^2, zeta ~
-U[0.005, 0.03], 51 snapshots 50 steps apart after a 2000-step spin-up, so
-2000 (t, t+50) pairs), AdamW with cosine learning rate, evaluation on 4
-held-out trajectories against persistence (prediction = input).
+U[0.005, 0.03], 50 (t, t+50) pairs each with t every 400 steps over
+[2000, 22000), so 2000 pairs), AdamW with cosine learning rate, evaluation
+on 4 held-out trajectories against persistence (prediction = input).
 hybrid: plain LB against the hybrid loop on held-out trajectories
 (`surrogate.hybrid`), simulated steps per second of each and the window
 means of defect density and enstrophy density of both.
@@ -96,14 +96,14 @@ def bench(batch=32, size=256) -> dict:
 
 def train_cmd(epochs, out_path, seed=0, ntraj=40, heldout=4) -> dict:
     t0 = time.time()
-    fields, zetas = G.generate_dataset(ntraj=ntraj + heldout, seed=seed)
+    npairs = 50
+    fields, zetas = G.generate_dataset(ntraj=ntraj + heldout, pairs=npairs, seed=seed)
     t_data = time.time() - t0
-    snaps = 51
-    n_train = ntraj * snaps
+    n_train = ntraj * 2 * npairs
     mean, scale = G.normalise(fields[:n_train])
     fields[n_train:].sub_(torch.tensor(mean, device="cuda")).div_(torch.tensor(scale, device="cuda"))
-    pairs = G.pair_indices(ntraj, snaps)
-    test_pairs = G.pair_indices(heldout, snaps) + n_train
+    pairs = G.pair_indices(ntraj, npairs)
+    test_pairs = G.pair_indices(heldout, npairs) + n_train
     P = G.Params(seed=seed)
     P.mean, P.scale = mean, scale
     t1 = time.time()
@@ -174,6 +174,7 @@ def hybrid_cmd(weights, steps, M, threshold, nruns=8, seed=123, stats_every=1000
            "surrogate_jumps": res_h["surrogate_jumps"],
            "plain_jumps_rejected": res_h["plain_jumps_rejected"], "checks": res_h["checks"],
            "check_error_median": float(np.median(errs)) if errs else None,
+           "check_errors": [round(e, 4) for e in errs],
            "window_from": win, "plain_means": mp, "hybrid_means": mh,
            "rel_diff": {k: abs(mh[k] - mp[k]) / abs(mp[k]) if mp[k] else None for k in mp}}
     plain.close()
