@@ -2,13 +2,18 @@
 //
 // Forward and input-gradient pass (conv3x3_kernel): D[128 pixels][NOUT] =
 // sum over 9 taps of A_tap[128 pixels][64 ci] * B_tap[NOUT][64 ci]^T. One
-// output tile is half a row of one image (128 consecutive x). A_tap is the
-// tile of the padded input shifted by the tap, fetched by one TMA tile load
-// (128-byte swizzle); all 9 weight taps stay in shared memory for the whole
-// persistent kernel. Warp roles: warp 0 issues TMA loads into a 6-stage
-// ring, warp 1 issues tcgen05.mma (4 x K=16 per tap) into one of two TMEM
-// accumulators, warps 2-5 drain the other accumulator (tcgen05.ld), apply
-// the fused epilogue and store bf16 pixels with their periodic ring copies.
+// output tile is half a row of one image (128 consecutive x). For each of
+// the three input rows a tile needs, one TMA load (128-byte swizzle) brings
+// a slab of 136 pixels; the three taps of that row are the slab read from
+// pixel 0, 1 and 2 (descriptor start 128 bytes apart), so the input is
+// fetched once per row instead of once per tap. All 9 weight taps stay in
+// shared memory for the whole persistent kernel. Warp roles: warp 0 issues
+// TMA loads into an 8-slab ring, warp 1 issues tcgen05.mma (4 x K=16 per
+// tap) into one of two TMEM
+// accumulators, warps 2-17 drain the other accumulator (tcgen05.ld; four
+// warps per 32-lane TMEM quarter, 16 channels each), apply the fused
+// epilogue and store bf16 pixels with their periodic ring copies. The
+// epilogue carries most of the instructions, so it gets most of the warps.
 //
 // Weight gradient (conv3x3_wgrad_kernel): dW_tap[ci][co] = sum over pixels of
 // x(p + tap)[ci] * dy(p)[co]. K runs over pixels, so both operands are read
@@ -34,16 +39,20 @@ using namespace tc;
 
 namespace {
 
-constexpr int CONV_THREADS = 192;     // 6 warps: TMA, MMA, 4 x epilogue
-constexpr int STAGES = 6;
-constexpr uint32_t TILE_BYTES = 128u*128u;   // 128 pixels x 64 bf16
+constexpr int EPI_WARPS = 16;         // epilogue warps of the forward / input-gradient kernel
+constexpr int CONV_THREADS = 64 + 32*EPI_WARPS;   // + TMA warp + MMA warp
+constexpr int WG_THREADS = 192;       // weight gradient: TMA, MMA, 4 x epilogue
+constexpr int STAGES = 8;                    // input slabs in flight
+constexpr int SLAB_PX = 136;                 // 128 outputs + 2 halo pixels, rounded to 8 rows
+constexpr uint32_t SLAB_BYTES = SLAB_PX*128u;   // multiple of 1024
+constexpr uint32_t TILE_BYTES = 128u*128u;   // 128 pixels x 64 bf16 (weight-gradient tiles)
 
 template<int NOUT>
 struct ConvSmem
 {
   static constexpr uint32_t W_BYTES = 9u*NOUT*128u;          // multiple of 1024
   static constexpr uint32_t A_OFF = W_BYTES;
-  static constexpr uint32_t BAR_OFF = A_OFF + STAGES*TILE_BYTES;
+  static constexpr uint32_t BAR_OFF = A_OFF + STAGES*SLAB_BYTES;
   static constexpr int NBAR = 2*STAGES + 6;                  // full, empty, w, tfull[2], tempty[2], done
   static constexpr uint32_t MISC_OFF = BAR_OFF + NBAR*8;
   static constexpr uint32_t BIAS_OFF = MISC_OFF + 16;
@@ -90,13 +99,13 @@ __device__ __forceinline__ void unpack8(const uint4& u, float* f)
   }
 }
 
-// 64 channels of pixel (n, y, x) -> padded tensor, with its periodic copies
-__device__ __forceinline__ void store_pixel(__nv_bfloat16* base, const float* v, int n, int y,
-                                            int x, int H, int W)
+// channels c0..c0+15 of pixel (n, y, x) -> padded tensor, with its periodic copies
+__device__ __forceinline__ void store_slice16(__nv_bfloat16* base, const float* v, int c0, int n,
+                                              int y, int x, int H, int W)
 {
-  uint4 pk[8];
+  uint4 pk[2];
 #pragma unroll
-  for(int k = 0; k < 8; ++k)
+  for(int k = 0; k < 2; ++k)
     pk[k] = make_uint4(pack_bf16x2(v[8*k], v[8*k + 1]), pack_bf16x2(v[8*k + 2], v[8*k + 3]),
                        pack_bf16x2(v[8*k + 4], v[8*k + 5]), pack_bf16x2(v[8*k + 6], v[8*k + 7]));
   int ys[3] = {y + 1, 0, 0}, xs[3] = {x + 1, 0, 0};
@@ -108,18 +117,19 @@ __device__ __forceinline__ void store_pixel(__nv_bfloat16* base, const float* v,
   for(int i = 0; i < ny; ++i)
     for(int j = 0; j < nx; ++j)
     {
-      uint4* dst = reinterpret_cast<uint4*>(base + padded_index(n, ys[i], xs[j], H, W)*64);
-#pragma unroll
-      for(int k = 0; k < 8; ++k) dst[k] = pk[k];
+      uint4* dst = reinterpret_cast<uint4*>(base + padded_index(n, ys[i], xs[j], H, W)*64 + c0);
+      dst[0] = pk[0];
+      dst[1] = pk[1];
     }
 }
 
-__device__ __forceinline__ void load_pixel(const __nv_bfloat16* base, float* v, int n, int y,
-                                           int x, int H, int W)
+__device__ __forceinline__ void load_slice16(const __nv_bfloat16* base, float* v, int c0, int n,
+                                             int y, int x, int H, int W)
 {
-  const uint4* src = reinterpret_cast<const uint4*>(base + padded_index(n, y + 1, x + 1, H, W)*64);
-#pragma unroll
-  for(int k = 0; k < 8; ++k) unpack8(src[k], v + 8*k);
+  const uint4* src =
+    reinterpret_cast<const uint4*>(base + padded_index(n, y + 1, x + 1, H, W)*64 + c0);
+  unpack8(src[0], v);
+  unpack8(src[1], v + 8);
 }
 
 template<int NOUT, int MODE>
@@ -153,8 +163,8 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
     mbar_init(wbar, 1);
     mbar_init(&tfull[0], 1);
     mbar_init(&tfull[1], 1);
-    mbar_init(&tempty[0], 4);
-    mbar_init(&tempty[1], 4);
+    mbar_init(&tempty[0], EPI_WARPS);
+    mbar_init(&tempty[1], EPI_WARPS);
     mbar_init(done, 1);
     *abort_flag = 0;
     fence_barrier_init();
@@ -186,12 +196,12 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
       {
         const int xt = tile % xt_n, row = tile / xt_n;
         const int y = row % H, n = row / H, x0 = xt << 7;
-        for(int tap = 0; tap < 9; ++tap, ++it)
+        for(int ky = 0; ky < 3; ++ky, ++it)
         {
           const uint32_t s = it % STAGES, ph = (it / STAGES) & 1u;
           if(!mbar_wait(&empty[s], ph ^ 1u)) { give_up(); break; }
-          mbar_expect_tx(&full[s], TILE_BYTES);
-          tma_load_4d(Asm + s*TILE_BYTES, &tmX, 0, x0 + tap % 3, y + tap / 3, n, &full[s]);
+          mbar_expect_tx(&full[s], SLAB_BYTES);
+          tma_load_4d(Asm + s*SLAB_BYTES, &tmX, 0, x0, y + ky, n, &full[s]);
         }
       }
       // loads still in flight after an abort land before the CTA exits
@@ -218,16 +228,21 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
         if(!mbar_wait(&tempty[acc], (use & 1u) ^ 1u)) { give_up(); break; }
         tc_fence_after();
         const uint32_t d = tbase + acc*NOUT;
-        for(int tap = 0; tap < 9; ++tap, ++it)
+        for(int ky = 0; ky < 3; ++ky, ++it)
         {
           const uint32_t s = it % STAGES, ph = (it / STAGES) & 1u;
           if(!mbar_wait(&full[s], ph)) { give_up(); ok = false; break; }
           tc_fence_after();
-          const uint32_t a0 = abase + s*TILE_BYTES, b0 = wbase + tap*NOUT*128;
 #pragma unroll
-          for(int k = 0; k < 4; ++k)
-            mma_bf16(d, sw128_desc(a0 + 32*k, 16, 1024), sw128_desc(b0 + 32*k, 16, 1024), IDESC,
-                     (tap | k) != 0);
+          for(int kx = 0; kx < 3; ++kx)
+          {
+            // tap (ky, kx): slab pixels kx .. kx+127
+            const uint32_t a0 = abase + s*SLAB_BYTES + kx*128, b0 = wbase + (3*ky + kx)*NOUT*128;
+#pragma unroll
+            for(int k = 0; k < 4; ++k)
+              mma_bf16(d, sw128_desc(a0 + 32*k, 16, 1024), sw128_desc(b0 + 32*k, 16, 1024), IDESC,
+                       (ky | kx | k) != 0);
+          }
           mma_commit(&empty[s]);
         }
         if(!ok) break;
@@ -240,72 +255,79 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
   else
   {
     const int q = warp & 3;                       // TMEM lanes 32q..32q+31
+    const int c0 = ((warp - 2) >> 2)*16;          // this warp's 16 channels
     uint32_t tcount = 0;
     // decisions are warp-uniform: tcgen05.ld needs all 32 lanes
     for(int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++tcount)
     {
       if(__any_sync(0xffffffffu, *abort_flag != 0)) break;
       const uint32_t acc = tcount & 1u, use = tcount >> 1;
+      const int xt = tile % xt_n, row = tile / xt_n;
+      const int y = row % H, n = row / H;
+      const int x = (xt << 7) + q*32 + lane;
+      // the second input of the epilogue is loaded before the accumulator
+      // is awaited, so its latency overlaps this tile's MMAs
+      float r[16];
+      if constexpr(MODE == CONV_FWD_RESID || MODE == CONV_BWD_RESID)
+        load_slice16(a.resid, r, c0, n, y, x, H, W);
+      if constexpr(MODE == CONV_BWD_GELU)
+        load_slice16(a.aux, r, c0, n, y, x, H, W);
       if(!__all_sync(0xffffffffu, mbar_wait(&tfull[acc], use & 1u)))
       {
         if(lane == 0) give_up();
         break;
       }
       tc_fence_after();
-      const uint32_t taddr = tbase + (static_cast<uint32_t>(q*32) << 16) + acc*NOUT;
-      const int xt = tile % xt_n, row = tile / xt_n;
-      const int y = row % H, n = row / H;
-      const int x = (xt << 7) + q*32 + lane;
       if constexpr(NOUT == 16)
       {
+        // one slice holds all 16 columns; the other warps only release
         float v[16];
-        tmem_ld16(taddr, v);
+        if(c0 == 0) tmem_ld16(tbase + (static_cast<uint32_t>(q*32) << 16) + acc*NOUT, v);
         tc_fence_before();
         __syncwarp();
         if(lane == 0) mbar_arrive(&tempty[acc]);
-        const size_t p = (static_cast<size_t>(n)*H + y)*W + x;
+        if(c0 == 0)
+        {
+          const size_t p = (static_cast<size_t>(n)*H + y)*W + x;
 #pragma unroll
-        for(int c = 0; c < 5; ++c)
-          a.out_f[5*p + c] = v[c] + bias_sm[c] + (a.resid_f ? a.resid_f[5*p + c] : 0.f);
+          for(int c = 0; c < 5; ++c)
+            a.out_f[5*p + c] = v[c] + bias_sm[c] + (a.resid_f ? a.resid_f[5*p + c] : 0.f);
+        }
       }
       else
       {
-        float v[64];
-        tmem_ld32(taddr, v);
-        tmem_ld32(taddr + 32, v + 32);
+        float v[16];
+        tmem_ld16(tbase + (static_cast<uint32_t>(q*32) << 16) + acc*NOUT + c0, v);
         tc_fence_before();
         __syncwarp();
         if(lane == 0) mbar_arrive(&tempty[acc]);
         if constexpr(MODE == CONV_FWD_BIAS || MODE == CONV_FWD_GELU || MODE == CONV_FWD_RESID)
         {
 #pragma unroll
-          for(int c = 0; c < 64; ++c) v[c] += bias_sm[c];
+          for(int c = 0; c < 16; ++c) v[c] += bias_sm[c0 + c];
         }
         if constexpr(MODE == CONV_FWD_GELU)
         {
-          uint4* dst = reinterpret_cast<uint4*>(a.out2 + padded_index(n, y + 1, x + 1, H, W)*64);
+          uint4* dst =
+            reinterpret_cast<uint4*>(a.out2 + padded_index(n, y + 1, x + 1, H, W)*64 + c0);
 #pragma unroll
-          for(int k = 0; k < 8; ++k)
+          for(int k = 0; k < 2; ++k)
             dst[k] = make_uint4(pack_bf16x2(v[8*k], v[8*k + 1]), pack_bf16x2(v[8*k + 2], v[8*k + 3]),
                                 pack_bf16x2(v[8*k + 4], v[8*k + 5]), pack_bf16x2(v[8*k + 6], v[8*k + 7]));
 #pragma unroll
-          for(int c = 0; c < 64; ++c) v[c] = gelu(v[c]);
+          for(int c = 0; c < 16; ++c) v[c] = gelu(v[c]);
         }
         if constexpr(MODE == CONV_FWD_RESID || MODE == CONV_BWD_RESID)
         {
-          float r[64];
-          load_pixel(a.resid, r, n, y, x, H, W);
 #pragma unroll
-          for(int c = 0; c < 64; ++c) v[c] += r[c];
+          for(int c = 0; c < 16; ++c) v[c] += r[c];
         }
         if constexpr(MODE == CONV_BWD_GELU)
         {
-          float t[64];
-          load_pixel(a.aux, t, n, y, x, H, W);
 #pragma unroll
-          for(int c = 0; c < 64; ++c) v[c] *= gelu_grad(t[c]);
+          for(int c = 0; c < 16; ++c) v[c] *= gelu_grad(r[c]);
         }
-        store_pixel(a.out, v, n, y, x, H, W);
+        store_slice16(a.out, v, c0, n, y, x, H, W);
       }
     }
   }
@@ -336,7 +358,7 @@ struct WgradArgs
   int* err;
 };
 
-__global__ void __launch_bounds__(CONV_THREADS, 1)
+__global__ void __launch_bounds__(WG_THREADS, 1)
 conv3x3_wgrad_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmD,
                      const WgradArgs a)
 {
@@ -482,8 +504,9 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
   return fn;
 }
 
-// padded NHWC64 bf16 [B][H+2][W+2][64], box 64 channels x 128 pixels
-bool map_activation(CUtensorMap* m, const void* base, int B, int H, int W)
+// padded NHWC64 bf16 [B][H+2][W+2][64], box 64 channels x box_px pixels
+// (a box reaching past the row's end is filled with zeros)
+bool map_activation(CUtensorMap* m, const void* base, int B, int H, int W, int box_px)
 {
   auto fn = encode_fn();
   if(!fn) return false;
@@ -491,7 +514,7 @@ bool map_activation(CUtensorMap* m, const void* base, int B, int H, int W)
                               static_cast<cuuint64_t>(B)};
   const cuuint64_t strides[3] = {128, static_cast<cuuint64_t>(W + 2)*128,
                                  static_cast<cuuint64_t>(H + 2)*(W + 2)*128};
-  const cuuint32_t box[4] = {64, 128, 1, 1};
+  const cuuint32_t box[4] = {64, static_cast<cuuint32_t>(box_px), 1, 1};
   const cuuint32_t es[4] = {1, 1, 1, 1};
   return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<void*>(base), dims, strides, box, es,
             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
@@ -556,7 +579,7 @@ cudaError_t conv3x3_launch(const __nv_bfloat16* in, const __nv_bfloat16* w, int 
   if((nout == 16) != (mode == CONV_FWD_OUT) || (nout != 16 && nout != 64))
     return cudaErrorInvalidValue;
   CUtensorMap tx, tw;
-  if(!map_activation(&tx, in, a.B, a.H, a.W) || !map_weights(&tw, w, nout))
+  if(!map_activation(&tx, in, a.B, a.H, a.W, SLAB_PX) || !map_weights(&tw, w, nout))
     return cudaErrorInvalidValue;
   switch(mode)
   {
@@ -576,17 +599,17 @@ cudaError_t conv3x3_wgrad_launch(const __nv_bfloat16* x, const __nv_bfloat16* dy
 {
   if(B < 1 || H < 1 || W < 128 || (W & 127)) return cudaErrorInvalidValue;
   CUtensorMap tx, td;
-  if(!map_activation(&tx, x, B, H, W) || !map_activation(&td, dy, B, H, W))
+  if(!map_activation(&tx, x, B, H, W, 128) || !map_activation(&td, dy, B, H, W, 128))
     return cudaErrorInvalidValue;
   static unsigned long long attr = 0;
   const cudaError_t e = smem_attr(conv3x3_wgrad_kernel, attr, static_cast<int>(WG_ALLOC));
   if(e != cudaSuccess) return e;
   const long long nblocks = static_cast<long long>(B)*H*(W >> 7);
-  // chunks per tap pair: about one wave of CTAs over all pairs
+  // chunks per tap pair: all CTAs in one wave (one CTA fits an SM)
   const int nchunks = static_cast<int>(std::max<long long>(1, std::min<long long>(
-    nblocks, (sm_count() + WG_GROUPS - 1)/WG_GROUPS)));
+    nblocks, std::max(1, sm_count()/WG_GROUPS))));
   WgradArgs a{B, H, W, nchunks, dW, err};
-  conv3x3_wgrad_kernel<<<WG_GROUPS*nchunks, CONV_THREADS, WG_ALLOC, st>>>(tx, td, a);
+  conv3x3_wgrad_kernel<<<WG_GROUPS*nchunks, WG_THREADS, WG_ALLOC, st>>>(tx, td, a);
   return cudaGetLastError();
 }
 

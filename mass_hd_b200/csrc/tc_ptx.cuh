@@ -5,8 +5,8 @@
 // Shared-memory matrix descriptors follow the PTX ISA "tcgen05 shared memory
 // descriptor" layout: start address >> 4 in bits 0-13, leading byte offset
 // >> 4 in bits 16-29, stride byte offset >> 4 in bits 32-45, the fixed value
-// 0b001 in bits 46-48, base offset 0, swizzle mode in bits 61-63 (2 = 128-byte
-// swizzle). Instruction descriptors for kind::f16: D format in bits 4-5
+// 0b001 in bits 46-48, base offset 0 in bits 49-51, swizzle mode in bits
+// 61-63 (2 = 128-byte swizzle). Instruction descriptors for kind::f16: D format in bits 4-5
 // (1 = f32), A/B formats in bits 7-9 / 10-12 (1 = bf16), A/B major in bits
 // 15 / 16 (0 = K-major, 1 = MN-major), N >> 3 in bits 17-22, M >> 4 in bits
 // 24-28.
@@ -173,7 +173,12 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v)
 // 128-byte-swizzled operand tile in shared memory. K-major: rows of 128 bytes
 // (64 bf16 along K), 8-row groups `sbo` bytes apart (lbo unused). MN-major:
 // rows are K indices holding 64 bf16 along M/N, 8-row K groups `sbo` apart,
-// 64-element M/N groups `lbo` apart.
+// 64-element M/N groups `lbo` apart. The 128-byte swizzle is a function of
+// the absolute shared-memory address (16-byte chunk bits 4-6 XOR row bits
+// 7-9), the same one TMA applies when it writes a tile to a 1024-aligned
+// address, so a matrix may start at any 128-byte row inside such a tile
+// with the base-offset field left 0 (the convolution kernels rely on this;
+// their GPU tests check it against the CPU oracle).
 __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
 {
   uint64_t d = 0;
