@@ -114,27 +114,45 @@ __global__ void k_mse(const float* __restrict__ pred, const float* __restrict__ 
   if(threadIdx.x == 0) atomicAdd(sse, red[0]);
 }
 
-// per-channel sums of a padded NHWC64 tensor: lane l owns channels 2l, 2l+1
+// Per-channel sums of a padded NHWC64 tensor. A warp takes whole image rows
+// (W pixels x 128 bytes, contiguous in the padded layout) with 16-byte
+// loads; lane l always holds channels 8(l%8)..8(l%8)+7 of pixel l/8 (mod 4)
+// and keeps 8 partial sums.
 __global__ void k_bias_grad(const __nv_bfloat16* __restrict__ dy, float* db, int B, int H, int W)
 {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const long long N = static_cast<long long>(H)*W, total = N*B;
-  const long long gw = blockIdx.x*8ll + warp, nw = gridDim.x*8ll;
-  float s0 = 0.f, s1 = 0.f;
-  for(long long i = gw; i < total; i += nw)
+  const int rows = B*H, per_row = W*8;        // 16-byte chunks per row
+  float acc[8];
+#pragma unroll
+  for(int c = 0; c < 8; ++c) acc[c] = 0.f;
+  for(int row = blockIdx.x*8 + warp; row < rows; row += gridDim.x*8)
   {
-    const int n = static_cast<int>(i / N);
-    const long long p = i % N;
-    const int y = static_cast<int>(p / W), x = static_cast<int>(p % W);
-    const __nv_bfloat162 v =
-      reinterpret_cast<const __nv_bfloat162*>(dy + pidx(n, y + 1, x + 1, H, W)*64)[lane];
-    const float2 f = __bfloat1622float2(v);
-    s0 += f.x;
-    s1 += f.y;
+    const int n = row / H, y = row % H;
+    const uint4* p = reinterpret_cast<const uint4*>(dy + pidx(n, y + 1, 1, H, W)*64);
+#pragma unroll 4
+    for(int k = lane; k < per_row; k += 32)
+    {
+      const uint4 u = __ldg(p + k);
+      const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+      for(int c = 0; c < 4; ++c)
+      {
+        const float2 f = __bfloat1622float2(h[c]);
+        acc[2*c] += f.x;
+        acc[2*c + 1] += f.y;
+      }
+    }
+  }
+#pragma unroll
+  for(int c = 0; c < 8; ++c)
+  {
+    acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], 8);
+    acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], 16);
   }
   __shared__ float red[8][64];
-  red[warp][2*lane] = s0;
-  red[warp][2*lane + 1] = s1;
+  if(lane < 8)
+#pragma unroll
+    for(int c = 0; c < 8; ++c) red[warp][8*lane + c] = acc[c];
   __syncthreads();
   if(threadIdx.x < 64)
   {
@@ -291,8 +309,10 @@ int mass_sg_bias_grad(const void* dy, float* db, int B, int H, int W, void* stre
   if(!dims_ok(B, H, W)) return sg_fail(MASS_LB_EINVAL, "need B, H >= 1 and W a multiple of 128");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if(int r = sg_cuda(cudaMemsetAsync(db, 0, 64*sizeof(float), st), "memset")) return r;
-  const long long total = static_cast<long long>(B)*H*W;
-  const int grid = static_cast<int>(std::max<long long>(1, std::min<long long>(total/64, 2048)));
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = std::max(1, std::min((B*H + 7)/8, 4*sms));
   k_bias_grad<<<grid, 256, 0, st>>>(static_cast<const __nv_bfloat16*>(dy), db, B, H, W);
   return sg_cuda(cudaGetLastError(), "bias grad");
 }
