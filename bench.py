@@ -148,26 +148,34 @@ def pinned_copy(a: np.ndarray):
     return out, t
 
 
-def dist_setup(n: int):
+def dist_setup(n: int, backend: str | None = None, timeout_s: float = 300.0):
+    """Join the process group of a torchrun launch (RANK, WORLD_SIZE,
+    LOCAL_RANK, MASTER_ADDR/PORT from the environment). NCCL on GPUs, gloo
+    where there are none (the CPU tests of the rank logic)."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
         import datetime
 
-        import torch.distributed as dist
         import torch
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        import torch.distributed as dist
+        if backend is None:
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
     return rank, world, local
 
 
 def max_over_ranks(x: float, world: int) -> float:
+    """The largest x over all ranks (every rank gets it)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -176,6 +184,13 @@ def barrier(world: int):
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
+
+
+def whole_job_rate(sites_per_rank: int, world: int, steps: int, ms_max: float) -> float:
+    """Site-updates per second of the whole job: every rank advances its own
+    lattice of sites_per_rank sites by `steps` steps; the job takes the
+    slowest rank's time ms_max."""
+    return sites_per_rank * world * steps / (ms_max / 1e3)
 
 
 def cpu_reference_run(model: str, L: int, steps: int, warmup: int, budget_s: float):
@@ -292,7 +307,7 @@ def run_ours(args):
     clocks = sampler.stop() if sampler else None
     ms = max_over_ranks(ms, world)
     ms_per_step = ms / args.steps
-    value = sites * world / (ms_per_step / 1e3)
+    value = whole_job_rate(sites, world, args.steps, ms)
     launches = args.steps * lat.launches_per_step
 
     # roofline of the dominant kernel (one fused launch per step)
@@ -335,7 +350,7 @@ def run_ours(args):
         e2e_step()
     dt = time.perf_counter() - t0
     dt = max_over_ranks(dt, world)
-    e2e = {"value": sites * NINFO * n_e2e * world / dt, "unit": UNIT,
+    e2e = {"value": whole_job_rate(sites, world, NINFO * n_e2e, dt * 1e3), "unit": UNIT,
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
            "steps_per_e2e_step": NINFO, "e2e_steps": n_e2e,
            "note": "per e2e step: upload state from pinned host memory, 100 Step() calls, "
