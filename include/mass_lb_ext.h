@@ -85,6 +85,32 @@ int mass_lb_state_sums_noalloc(const float* planes, long long plane_stride, int 
                                unsigned LX, unsigned LY, double rho, void* stream,
                                double* fsum, double* phisum, int* nonfinite);
 
+/* ---- division models ------------------------------------------------------
+ *
+ * Hooks for the reference's LyotropicWithDivision (src/models/
+ * lyotropic-with-division.cpp), lyotropic only.
+ *
+ * mass_lb_set_phi_source: per-site phi source rate r (LX*LY host doubles,
+ * site order k = y + LY*x). After every UpdateFields (predictor and
+ * corrector) phi_tmp += phi*r, which is LyotropicWithDivision::UpdateFields
+ * (:111-124) with r = alpha*division_mask - beta*death_mask. The masks
+ * themselves are drawn on the host by the caller (SetMasks, :35-106), which
+ * uploads the new r whenever they change. NULL removes the source. On FP32
+ * fused lattices the source runs in the warp-strip kernel (the tile is
+ * re-tuned among those). Ensembles reject runs that carry a source.
+ *
+ * mass_lb_set_phi_conservation: the conserve_phi correction the division
+ * models switch on when division and death are off (:29-30):
+ * Dp -= (sum phi - totalphi)/(LX*LY) (src/models/lyotropic.cpp:299), with
+ * sum phi taken before each UpdateFields in site order (serially, so FP64
+ * results match the serial reference bit for bit; this costs one pass over
+ * phi by a single thread per sub-step). totalphi is the sum of phi at
+ * Configure() (:152). FP64 and FP32-with-walls only: the fused FP32 kernel
+ * has no lattice-wide sum between the halves of a sub-step
+ * (MASS_LB_EUNSUPPORTED). */
+int mass_lb_set_phi_source(mass_lb_handle* h, const double* rate);
+int mass_lb_set_phi_conservation(mass_lb_handle* h, int on, double totalphi);
+
 /* ---- batched ensembles --------------------------------------------------
  *
  * Many independent FP32 periodic lattices, of uneven sizes and parameters,

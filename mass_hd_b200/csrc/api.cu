@@ -147,6 +147,13 @@ struct mass_lb_handle
 
   double ftot = 0, ptot = 0;
   unsigned long long steps = 0;
+
+  // division-model hooks (mass_lb_set_phi_source / _conservation)
+  float* src_fused = nullptr;   // FP32 fused: rate plane of LX*LY
+  double* src64 = nullptr;      // FP64: rate on the extended torus
+  float* src32 = nullptr;       // FP32 with walls: same
+  bool src_on = false;
+  double* phisum = nullptr;     // countphi scalar for conserve_phi
 };
 
 namespace {
@@ -245,6 +252,7 @@ FusedArgs fused_args(mass_lb_handle* h, const float* in, float* out, bool diag)
   a.LY = static_cast<int>(h->LY);
   a.plane = static_cast<long long>(h->LX)*h->LY;
   a.p = p32_of(h->P);
+  a.src = h->src_on ? h->src_fused : nullptr;
   return a;
 }
 
@@ -265,6 +273,7 @@ std::vector<FusedConfig> tile_candidates(const mass_lb_handle* h)
   for(int nt : {32, 64, 128, 256})
   {
     if(!fused_supported(static_cast<int>(h->LX), static_cast<int>(h->LY), nt)) continue;
+    if(h->src_on && nt != 32) continue;   // the phi source is in the warp-strip kernel only
     for(int rows : {32, 64, 128, 256, 512, 1024})
     {
       if(rows > static_cast<int>(h->LX) && rows != 32) continue;
@@ -883,6 +892,108 @@ int mass_lb_device_state(mass_lb_handle* h, void** planes, long long* plane_stri
   return 0;
 }
 
+// ---- division-model hooks --------------------------------------------------
+
+} // extern "C"
+
+namespace {
+
+// host doubles in site order (k = y + LY*x) -> a device plane with ghost
+// ring g and row stride EY
+template<typename T>
+int put_plane(mass_lb_handle* h, const double* src, T* dst, int g, int EY)
+{
+  const int LY = static_cast<int>(h->LY);
+  const long long rows_per = std::max<long long>(1, kStageSites/LY);
+  for(long long x0 = 0; x0 < h->LX; x0 += rows_per)
+  {
+    const int nrows = static_cast<int>(std::min<long long>(rows_per, h->LX - x0));
+    const long long n = static_cast<long long>(nrows)*LY;
+    CU(cudaMemcpyAsync(h->stage, src + x0*LY, n*sizeof(double), cudaMemcpyHostToDevice,
+                       h->stream), "upload copy");
+    k_put_scalar<T><<<blocks_for(n), 256, 0, h->stream>>>(h->stage, dst, x0, nrows, LY, g, EY);
+    CU(cudaGetLastError(), "upload kernel");
+  }
+  return 0;
+}
+
+} // namespace
+
+extern "C" {
+
+int mass_lb_set_phi_source(mass_lb_handle* h, const double* rate)
+{
+  if(!h) return fail(MASS_LB_EINVAL, "null handle");
+  if(h->model != LYO) return fail(MASS_LB_EUNSUPPORTED, "the nematic model has no phi");
+  DeviceGuard g(h->device);
+  CU(cudaStreamSynchronize(h->stream), "sync");
+  if(!rate)
+  {
+    h->src_on = false;
+    h->s64.src = nullptr;
+    h->s32.src = nullptr;
+    return 0;
+  }
+  if(h->fused)
+  {
+    if(!h->src_fused)
+      if(int r = dalloc(h, &h->src_fused, static_cast<size_t>(h->LX)*h->LY)) return r;
+    if(int r = put_plane<float>(h, rate, h->src_fused, 0, static_cast<int>(h->LY))) return r;
+    if(h->cfg.nt != 32) h->tuned = false;   // re-tune among warp-strip tiles
+  }
+  else if(h->precision == MASS_LB_FP64)
+  {
+    if(!h->src64)
+    {
+      if(int r = dalloc(h, &h->src64, h->d.NE)) return r;
+      CU(cudaMemsetAsync(h->src64, 0, h->d.NE*sizeof(double), h->stream), "memset");
+    }
+    if(int r = put_plane<double>(h, rate, h->src64, h->d.g, h->d.EY)) return r;
+    h->s64.src = h->src64;
+  }
+  else
+  {
+    if(!h->src32)
+    {
+      if(int r = dalloc(h, &h->src32, h->d.NE)) return r;
+      CU(cudaMemsetAsync(h->src32, 0, h->d.NE*sizeof(float), h->stream), "memset");
+    }
+    if(int r = put_plane<float>(h, rate, h->src32, h->d.g, h->d.EY)) return r;
+    h->s32.src = h->src32;
+  }
+  h->src_on = true;
+  CU(cudaStreamSynchronize(h->stream), "upload sync");
+  return 0;
+}
+
+int mass_lb_set_phi_conservation(mass_lb_handle* h, int on, double totalphi)
+{
+  if(!h) return fail(MASS_LB_EINVAL, "null handle");
+  if(h->model != LYO) return fail(MASS_LB_EUNSUPPORTED, "the nematic model has no phi");
+  if(on && h->fused)
+    return fail(MASS_LB_EUNSUPPORTED, "conserve_phi needs a lattice-wide sum between the two "
+                                      "halves of a sub-step; use precision FP64");
+  DeviceGuard g(h->device);
+  if(on && !h->phisum)
+    if(int r = dalloc(h, &h->phisum, 1)) return r;
+  for(int i = 0; i < 2; ++i)
+  {
+    if(i == 0)
+    {
+      h->s64.conserve_phi = on ? 1 : 0;
+      h->s64.totalphi = totalphi;
+      h->s64.phisum = h->phisum;
+    }
+    else
+    {
+      h->s32.conserve_phi = on ? 1 : 0;
+      h->s32.totalphi = totalphi;
+      h->s32.phisum = h->phisum;
+    }
+  }
+  return 0;
+}
+
 // ---- ensembles ------------------------------------------------------------
 
 } // extern "C"
@@ -1106,7 +1217,12 @@ int mass_lb_ensemble_step(mass_lb_ensemble* e, unsigned nsteps)
   if(nsteps == 0) return 0;
   DeviceGuard g(e->device);
   // the run handles may have been uploaded or stepped on their own streams
-  for(mass_lb_handle* h : e->runs) CU(cudaStreamSynchronize(h->stream), "run sync");
+  for(mass_lb_handle* h : e->runs)
+  {
+    if(h->src_on)
+      return fail(MASS_LB_EUNSUPPORTED, "ensemble runs cannot carry a phi source");
+    CU(cudaStreamSynchronize(h->stream), "run sync");
+  }
   if(e->rows == 0)
   {
     if(int r = ens_autotune(e)) return r;

@@ -42,6 +42,7 @@ struct FusedArgs
   int rows;            // rows per CTA chunk
   P32 p;
   PairParams pp;       // filled by the warp-strip launcher
+  const float* src;    // per-site phi source rate (LX*LY) or null; warp-strip kernel only
 };
 
 // Tile shapes the autotuner may pick.

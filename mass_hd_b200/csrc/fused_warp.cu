@@ -350,6 +350,7 @@ struct ItemView
   int LX, LY;
   long long plane;
   int rows;
+  const float* src;   // per-site phi source rate (SRC launches)
 };
 
 // Per-warp shared memory: input ring | delayed populations (3 rows) |
@@ -364,8 +365,10 @@ struct WarpSmem
 // Advance one strip chunk (strip `strip`, rows chunk*a.rows ..) of one
 // lattice by a full step. `rowbase` counts the input rows this warp has
 // copied through its ring so far (mbarrier phases continue across items).
-// Returns false if a bounded wait gave up.
-template<int MODEL, bool DIAG>
+// Returns false if a bounded wait gave up. SRC adds the division models'
+// phi source, phi_tmp += phi*r after each UpdateFields
+// (src/models/lyotropic-with-division.cpp:121), in C and E.
+template<int MODEL, bool DIAG, bool SRC>
 __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P, const int strip,
                                           const int chunk, float* ring, float* dpop, float* hrow,
                                           uint64_t* mbar, const int lane, unsigned& rowbase)
@@ -418,6 +421,12 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
   const bool lane_out = lane >= 2 && lane < 30;
   const bool colx_ok = lane_out && yg < LY;
   const bool coly_ok = lane_out && yg + 1 < LY;
+  // source-rate pair of this lane at lattice row x (any row of the window)
+  const int yw = yg < 0 ? yg + LY : (yg >= LY ? yg - LY : yg);
+  auto src_at = [&](int x) {
+    x = x < 0 ? x + LX : (x >= LX ? x - LX : x);
+    return f2{__ldg(reinterpret_cast<const float2*>(a.src + static_cast<long long>(x)*LY + yw))};
+  };
 
   UQ2o q1c{}, q2c{};
   UQx q1m{}, q2m{};
@@ -499,6 +508,7 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
         nQ[1] = Qyx + u.Dyx;
         nQN[2] = fma(W2(P.half), u.Dp, p);
         nQ[2] = p + u.Dp;
+        if constexpr (SRC) nQ[2] = fma(p, src_at(x0 - 4 + i), nQ[2]);
       }
       else
       {
@@ -605,7 +615,9 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
                       fma(hitau, u.fe[v], lds2(hrow + (((i + 1) & 1)*9 + v)*COLS + 2*lane)));
       const f2 Qo0 = fma(W2(P.half), u.Dxx, qn2[0]);
       const f2 Qo1 = fma(W2(P.half), u.Dyx, qn2[1]);
-      const f2 Qo2 = fma(W2(P.half), u.Dp, qn2[2]);
+      f2 Qo2 = fma(W2(P.half), u.Dp, qn2[2]);
+      // corrector source with the predicted phi of this row
+      if constexpr (SRC) Qo2 = fma(qa2[2], src_at(x0 - 6 + i), Qo2);
       if(i >= 6)
       {
         const long long pl = a.plane;
@@ -683,7 +695,7 @@ __device__ __forceinline__ void warp_smem(float*& ring, float*& dpop, float*& hr
 }
 
 // One lattice: work item = blockIdx.x*WPB + warp.
-template<int MODEL, bool DIAG>
+template<int MODEL, bool DIAG, bool SRC>
 __global__ void __launch_bounds__(32*WPB, 2)
 fused_warp_kernel(const __grid_constant__ FusedArgs a, const int nitems)
 {
@@ -693,9 +705,9 @@ fused_warp_kernel(const __grid_constant__ FusedArgs a, const int nitems)
   float *ring, *dpop, *hrow;
   uint64_t* mbar;
   warp_smem<MODEL>(ring, dpop, hrow, mbar, warp, lane);
-  const ItemView v{a.in, a.out, a.diag, a.err, a.LX, a.LY, a.plane, a.rows};
+  const ItemView v{a.in, a.out, a.diag, a.err, a.LX, a.LY, a.plane, a.rows, a.src};
   unsigned rowbase = 0;
-  warp_item<MODEL, DIAG>(v, a.pp, item % a.nstrips, item / a.nstrips, ring, dpop, hrow,
+  warp_item<MODEL, DIAG, SRC>(v, a.pp, item % a.nstrips, item / a.nstrips, ring, dpop, hrow,
                          mbar, lane, rowbase);
 }
 
@@ -724,8 +736,8 @@ fused_warp_ensemble_kernel(const EnsRun* __restrict__ runs, const int* __restric
     const EnsRun& R = runs[r];
     const int local = item - R.item0;
     const ItemView v{parity ? R.b : R.a, parity ? R.a : R.b, nullptr, err, R.LX, R.LY,
-                     R.plane, R.rows};
-    if(!warp_item<MODEL, false>(v, c_ens_pp[R.slot], local % R.nstrips, local / R.nstrips,
+                     R.plane, R.rows, nullptr};
+    if(!warp_item<MODEL, false, false>(v, c_ens_pp[R.slot], local % R.nstrips, local / R.nstrips,
                                 ring, dpop, hrow, mbar, lane, rowbase))
       break;
   }
@@ -738,10 +750,10 @@ constexpr size_t smem_bytes()
          static_cast<size_t>(WPB)*RING*sizeof(uint64_t);
 }
 
-template<int MODEL, bool DIAG>
+template<int MODEL, bool DIAG, bool SRC>
 cudaError_t launch_t(const FusedArgs& a, int rows, cudaStream_t st)
 {
-  auto kern = fused_warp_kernel<MODEL, DIAG>;
+  auto kern = fused_warp_kernel<MODEL, DIAG, SRC>;
   static unsigned long long attr_set = 0;
   int dev = 0;
   cudaGetDevice(&dev);
@@ -835,8 +847,12 @@ cudaError_t launch_fused_warp_step(const FusedArgs& a, int model, int rows, bool
                                    cudaStream_t st)
 {
   if(model == LYO)
-    return diag ? launch_t<LYO, true>(a, rows, st) : launch_t<LYO, false>(a, rows, st);
-  return diag ? launch_t<NEM, true>(a, rows, st) : launch_t<NEM, false>(a, rows, st);
+  {
+    if(a.src)
+      return diag ? launch_t<LYO, true, true>(a, rows, st) : launch_t<LYO, false, true>(a, rows, st);
+    return diag ? launch_t<LYO, true, false>(a, rows, st) : launch_t<LYO, false, false>(a, rows, st);
+  }
+  return diag ? launch_t<NEM, true, false>(a, rows, st) : launch_t<NEM, false, false>(a, rows, st);
 }
 
 } // namespace mlb

@@ -69,6 +69,14 @@ struct State
   T *sXX, *sYY, *sYX, *sXY;
   T *diag[7];  // sigma_bulk, elastic_xx, elastic_yx, phase_field_xx,
                // phase_field_yx, active_xx, active_yx
+  // division models (src/models/lyotropic-with-division.cpp:111-124): a
+  // per-site phi source rate r (phi_tmp += phi*r after each UpdateFields),
+  // and the conserve_phi correction Dp -= (sum phi - totalphi)/DomainSize
+  // (src/models/lyotropic.cpp:299) with the sum taken serially in site order
+  const T* src;        // null: no source
+  double* phisum;      // device scalar written before each UpdateFields
+  double totalphi;
+  int conserve_phi;
 };
 
 __host__ __device__ inline int wrapi(int a, int n)

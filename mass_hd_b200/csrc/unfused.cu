@@ -248,8 +248,12 @@ uf_kernel(Dims d, Params P, State<T> s)
     const T p = s.phi[e];
     const T del2mu = lap(s.MU, nb);
     const T pFlux = dX(s.uxp, nb) + dY(s.uyp, nb);
-    // conserve_phi is false in the reference (src/models/lyotropic.hpp:46)
-    const T Dp = T(P.GammaP)*del2mu - pFlux - T(0);
+    // conserve_phi is false for Lyotropic (src/models/lyotropic.hpp:46) and
+    // set by the division models when division and death are off
+    // (src/models/lyotropic-with-division.cpp:30)
+    const T corr = s.conserve_phi ? T((*s.phisum - s.totalphi)/static_cast<double>(d.LX*d.LY))
+                                  : T(0);
+    const T Dp = T(P.GammaP)*del2mu - pFlux - corr;
     const T tau = T(P.tauNem)*p + T(P.tauIso)*(T(1)-p);
     if constexpr (FIRST)
     {
@@ -258,7 +262,11 @@ uf_kernel(Dims d, Params P, State<T> s)
       s.phn[e]  = s.phi[e] + T(.5)*Dp;
       s.Qxx[e]  = s.Qxx[e] + Dxx;
       s.Qyx[e]  = s.Qyx[e] + Dyx;
-      s.phi_tmp[e] = s.phi[e] + Dp;
+      T pt = s.phi[e] + Dp;
+      // division source, added after the node update as the division model
+      // does (src/models/lyotropic-with-division.cpp:121)
+      if(s.src) pt = pt + s.phi[e]*s.src[e];
+      s.phi_tmp[e] = pt;
 #pragma unroll
       for(int v=0; v<9; ++v)
       {
@@ -272,7 +280,9 @@ uf_kernel(Dims d, Params P, State<T> s)
     {
       s.Qxx[e] = s.QNxx[e] + T(.5)*Dxx;
       s.Qyx[e] = s.QNyx[e] + T(.5)*Dyx;
-      s.phi_tmp[e] = s.phn[e] + T(.5)*Dp;
+      T pt = s.phn[e] + T(.5)*Dp;
+      if(s.src) pt = pt + s.phi[e]*s.src[e];
+      s.phi_tmp[e] = pt;
 #pragma unroll
       for(int v=0; v<9; ++v)
       {
@@ -560,6 +570,22 @@ inline dim3 site_grid(int nx, int ny, dim3 blk)
   return dim3((ny + blk.x - 1)/blk.x, (nx + blk.y - 1)/blk.y);
 }
 
+// countphi of UpdateQuantities (src/models/lyotropic.cpp:343-360) summed in
+// site order k = y + LY*x by one thread, so that the FP64 result is the
+// serial reference's bit for bit.
+template<typename T>
+__global__ void phi_sum_serial(Dims d, const T* __restrict__ phi, double* out)
+{
+  if(blockIdx.x != 0 || threadIdx.x != 0) return;
+  double sum = 0;
+  for(int x = 0; x < d.LX; ++x)
+  {
+    const T* row = phi + static_cast<long long>(d.EY)*(x + d.g) + d.g;
+    for(int y = 0; y < d.LY; ++y) sum = sum + static_cast<double>(row[y]);
+  }
+  *out = sum;
+}
+
 template<typename T, bool DEV, int MODEL>
 int step_impl(const Dims& d, const Params& P, State<T>& s, int bc,
               unsigned nsteps, bool diag_last, cudaStream_t st)
@@ -606,6 +632,7 @@ int step_impl(const Dims& d, const Params& P, State<T>& s, int bc,
     fields_bc();
     uq_kernel<T, DEV, MODEL, false><<<grd, blk, 0, st>>>(d, P, s);
     fields2_bc();
+    if(MODEL == LYO && s.conserve_phi) phi_sum_serial<T><<<1, 1, 0, st>>>(d, s.phi, s.phisum);
     uf_kernel<T, DEV, MODEL, true><<<grd, blk, 0, st>>>(d, P, s);
     if(MODEL == LYO) std::swap(s.phi, s.phi_tmp);
     if(bc) bc_lb_kernel<T><<<1, 1024, 0, st>>>(d, s.ff, s.fn, lbk);
@@ -619,6 +646,7 @@ int step_impl(const Dims& d, const Params& P, State<T>& s, int bc,
       if(diag) uq_kernel<T, DEV, MODEL, true><<<grd, blk, 0, st>>>(d, P, s);
       else uq_kernel<T, DEV, MODEL, false><<<grd, blk, 0, st>>>(d, P, s);
       fields2_bc();
+      if(MODEL == LYO && s.conserve_phi) phi_sum_serial<T><<<1, 1, 0, st>>>(d, s.phi, s.phisum);
       uf_kernel<T, DEV, MODEL, false><<<grd, blk, 0, st>>>(d, P, s);
       if(MODEL == LYO) std::swap(s.phi, s.phi_tmp);
     }

@@ -104,6 +104,8 @@ def load_library(build_if_missing: bool = False):
         "mass_lb_uses_fused": (C.c_int, [vp]),
         "mass_lb_device_state": (C.c_int, [vp, C.POINTER(vp), C.POINTER(C.c_longlong), ip]),
         "mass_lb_statistics": (C.c_int, [vp, C.POINTER(Stats)]),
+        "mass_lb_set_phi_source": (C.c_int, [vp, dp]),
+        "mass_lb_set_phi_conservation": (C.c_int, [vp, C.c_int, C.c_double]),
         "mass_lb_ensemble_create": (C.c_int, [C.c_int, C.POINTER(Params), C.POINTER(C.c_uint),
                                               C.POINTER(C.c_uint), C.POINTER(vp)]),
         "mass_lb_ensemble_destroy": (None, [vp]),
@@ -226,6 +228,22 @@ class Lattice:
 
     def step(self, n: int = 1):
         _check(load_library().mass_lb_step(self.h, n))
+
+    def set_phi_source(self, rate):
+        """Per-site phi source rate r (LX*LY values, site order; None
+        removes it): phi_tmp += phi*r after every UpdateFields, as the
+        division models do with r = alpha*division_mask - beta*death_mask."""
+        if rate is None:
+            _check(load_library().mass_lb_set_phi_source(self.h, None))
+            return
+        r = np.ascontiguousarray(rate, dtype=np.float64)
+        assert r.size == self.LX * self.LY
+        _check(load_library().mass_lb_set_phi_source(self.h, _dp(r)))
+
+    def set_phi_conservation(self, on: bool, totalphi: float = 0.0):
+        """The division models' conserve_phi correction
+        Dp -= (sum phi - totalphi)/(LX*LY) (FP64 / walls only)."""
+        _check(load_library().mass_lb_set_phi_conservation(self.h, int(bool(on)), float(totalphi)))
 
     def synchronize(self):
         _check(load_library().mass_lb_synchronize(self.h))

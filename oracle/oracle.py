@@ -29,6 +29,9 @@ LYO_OPTIONS = ("GammaQ", "GammaP", "xi", "tauNem", "tauIso", "rho", "friction",
                "level", "conc", "radius", "angle", "noise")
 NEM_OPTIONS = ("Gamma", "xi", "tau", "rho", "Q_kBT", "u_kBT", "friction", "CC",
                "LL", "zeta", "npc", "angle", "noise")
+# LyotropicWithDivision::GetOptions (src/models/lyotropic-with-division.cpp:126-142)
+DIV_OPTIONS = ("alpha", "beta", "division-rate", "division-time", "division-radius",
+               "death-rate", "death-time", "death-radius", "phi-critical")
 
 SCALAR_FIELDS_LYO = ("QQxx", "QQyx", "QNxx", "QNyx", "phi", "phn", "n", "ux",
                      "uy", "ux_phi", "uy_phi", "HHxx", "HHyx", "MU", "dxQQxx",
@@ -160,6 +163,8 @@ def _ref():
         lib.ref_configure.argtypes = [C.c_void_p, C.c_uint]
         lib.ref_set_field.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_double)]
         lib.ref_get_field.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_double)]
+        lib.ref_get_mask.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_ubyte)]
+        lib.ref_get_value.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(C.c_double)]
         lib.ref_reset_totals.argtypes = [C.c_void_p]
         lib.ref_step.argtypes = [C.c_void_p, C.c_uint, C.c_uint]
         lib.ref_time_steps.argtypes = [C.c_void_p, C.c_uint, C.c_uint]
@@ -175,15 +180,20 @@ def _ref():
 
 
 class RefOracle:
-    """The reference's own Lyotropic / Nematic model objects."""
+    """The reference's own Lyotropic / LyotropicWithDivision / Nematic model
+    objects (`division=True` selects "lyotropic-with-division")."""
 
-    def __init__(self, model: int, params: dict, LX: int, LY: int, bc: int = 0):
+    def __init__(self, model: int, params: dict, LX: int, LY: int, bc: int = 0,
+                 division: bool = False):
         self.model, self.LX, self.LY, self.bc = model, LX, LY, bc
-        name = b"lyotropic" if model == LYOTROPIC else b"nematic"
+        name = (b"lyotropic-with-division" if division else b"lyotropic") \
+            if model == LYOTROPIC else b"nematic"
         self.h = _ref().ref_new(name, LX, LY, bc)
         if not self.h:
             raise RuntimeError(_ref().ref_last_error().decode())
         names = LYO_OPTIONS if model == LYOTROPIC else NEM_OPTIONS
+        if division:
+            names = names + DIV_OPTIONS
         # every option gets a value: the reference leaves them uninitialised
         defaults = {"config": "circle", "level": 0.0, "conc": 1.0,
                     "radius": 0.0, "angle": 0.0, "noise": 0.0,
@@ -219,6 +229,20 @@ class RefOracle:
         if _ref().ref_get_field(self.h, name.encode(), _dp(out)) != 0:
             raise KeyError(name)
         return out.reshape(-1, 9) if name in ("ff", "fn") else out
+
+    def mask(self, name: str) -> np.ndarray:
+        """division_mask / death_mask of the division model (bool array)."""
+        out = np.empty(self.LX * self.LY, dtype=np.uint8)
+        if _ref().ref_get_mask(self.h, name.encode(), out.ctypes.data_as(C.POINTER(C.c_ubyte))) != 0:
+            raise KeyError(name)
+        return out.astype(bool)
+
+    def value(self, name: str) -> float:
+        """totalphi, countphi or conserve_phi of the lyotropic models."""
+        out = C.c_double()
+        if _ref().ref_get_value(self.h, name.encode(), C.byref(out)) != 0:
+            raise KeyError(name)
+        return out.value
 
     def step(self, n: int = 1, threads: int = 0) -> None:
         _ref().ref_step(self.h, n, threads)

@@ -2,7 +2,8 @@
 //
 // TEST INFRASTRUCTURE ONLY. This file is compiled together with the
 // reference sources (src/geometry.cpp, src/random.cpp, src/serialization.cpp,
-// src/models/lyotropic.cpp, src/models/nematic.cpp) by oracle/Makefile into
+// src/models/lyotropic.cpp, src/models/nematic.cpp,
+// src/models/lyotropic-with-division.cpp) by oracle/Makefile into
 // oracle/_ref/libmass_ref.so. Nothing in the product links it; the tests,
 // the golden-fixture generator and bench.py's reference arm load it through
 // ctypes as the checker / CPU baseline.
@@ -19,6 +20,7 @@
 #include "header.hpp"
 #include "models.hpp"
 #include "models/lyotropic.hpp"
+#include "models/lyotropic-with-division.hpp"
 #include "models/nematic.hpp"
 #include "random.hpp"
 #include "serialization.hpp"
@@ -53,6 +55,10 @@ struct RefModel
   virtual unsigned lx() = 0;
   virtual unsigned ly() = 0;
   virtual unsigned bc() = 0;
+  // boolean masks of the division models (null elsewhere)
+  virtual const std::vector<bool>* mask(const std::string&) { return nullptr; }
+  // scalar members (totalphi, countphi, conserve_phi); false if absent
+  virtual bool value(const std::string&, double*) { return false; }
   option_list opts;
 };
 
@@ -75,17 +81,26 @@ void write_params_common(Archive& ar, M& m, unsigned LX, unsigned LY,
   m.serialize_params(ar);
 }
 
-struct LyoAccess : Lyotropic, RefModel
+// Lyotropic and the models derived from it share fields and serialization.
+template<class Base>
+struct LyoAccessT : Base, RefModel
 {
-  LyoAccess(unsigned LX, unsigned LY, unsigned BC) : Lyotropic(LX, LY, BC) {}
+  LyoAccessT(unsigned LX, unsigned LY, unsigned BC) : Base(LX, LY, BC) {}
   Model& model() override { return *this; }
-  option_list options() override { return Lyotropic::GetOptions(); }
-  unsigned lx() override { return LX; }
-  unsigned ly() override { return LY; }
-  unsigned bc() override { return BC; }
+  option_list options() override { return Base::GetOptions(); }
+  unsigned lx() override { return this->LX; }
+  unsigned ly() override { return this->LY; }
+  unsigned bc() override { return this->BC; }
+  bool value(const std::string& name, double* out) override
+  {
+    if(name=="totalphi") { *out = this->totalphi; return true; }
+    if(name=="countphi") { *out = this->countphi; return true; }
+    if(name=="conserve_phi") { *out = this->conserve_phi ? 1. : 0.; return true; }
+    return false;
+  }
   ScalarField* scalar(const std::string& name) override
   {
-#define F(x) if(name==#x) return &x;
+#define F(x) if(name==#x) return &this->x;
     F(QQxx) F(QQyx) F(QNxx) F(QNyx) F(phi) F(phn) F(phi_tmp) F(n) F(ux) F(uy)
     F(ux_phi) F(uy_phi) F(HHxx) F(HHyx) F(MU) F(dxQQxx) F(dyQQxx) F(dxQQyx)
     F(dyQQyx) F(sigmaXX) F(sigmaYY) F(sigmaYX) F(sigmaXY) F(sigma_bulk)
@@ -96,31 +111,46 @@ struct LyoAccess : Lyotropic, RefModel
   }
   LBField* lb(const std::string& name) override
   {
-    if(name=="ff") return &ff;
-    if(name=="fn") return &fn;
+    if(name=="ff") return &this->ff;
+    if(name=="fn") return &this->fn;
     return nullptr;
   }
   void reset_totals() override
   {
-    ftot = 0; ptot = 0;
-    for(unsigned k=0; k<DomainSize; ++k)
+    this->ftot = 0; this->ptot = 0;
+    for(unsigned k=0; k<this->DomainSize; ++k)
     {
-      for(unsigned v=0; v<lbq; ++v) ftot += ff[k][v];
-      ptot += phi[k];
+      for(unsigned v=0; v<lbq; ++v) this->ftot += this->ff[k][v];
+      this->ptot += this->phi[k];
     }
   }
   void write_params(std::ostream& os, unsigned nsteps, unsigned ninfo,
                     unsigned nstart, const std::string& name) override
   {
     oarchive ar(os, "parameters", 1);
-    write_params_common(ar, *this, LX, LY, BC, nsteps, ninfo, nstart, name);
+    write_params_common(ar, *this, this->LX, this->LY, this->BC, nsteps, ninfo, nstart, name);
     if(ar.bad_value()) throw error_msg("nan found while writing file.");
   }
   void write_frame(std::ostream& os) override
   {
     oarchive ar(os, "frame", 1);
-    serialize_frame(ar);
+    this->serialize_frame(ar);
     if(ar.bad_value()) throw error_msg("nan found while writing file.");
+  }
+};
+
+using LyoAccess = LyoAccessT<Lyotropic>;
+
+// LyotropicWithDivision (src/models/lyotropic-with-division.cpp) with its
+// division / death masks readable
+struct DivAccess : LyoAccessT<LyotropicWithDivision>
+{
+  DivAccess(unsigned LX, unsigned LY, unsigned BC) : LyoAccessT(LX, LY, BC) {}
+  const std::vector<bool>* mask(const std::string& name) override
+  {
+    if(name=="division_mask") return &division_mask;
+    if(name=="death_mask") return &death_mask;
+    return nullptr;
   }
 };
 
@@ -177,13 +207,15 @@ extern "C" {
 /** Last error message of this thread (empty if none). */
 const char* ref_last_error() { return last_error.c_str(); }
 
-/** Construct "lyotropic" or "nematic" with the factory arguments of
+/** Construct "lyotropic", "lyotropic-with-division" or "nematic" with the
+ * factory arguments of
  * declare_model (src/models.hpp:197-205): (LX, LY, BC). */
 void* ref_new(const char* model, unsigned LX, unsigned LY, unsigned BC)
 {
   try {
     RefModel* m = nullptr;
     if(std::strcmp(model, "lyotropic")==0) m = new LyoAccess(LX, LY, BC);
+    else if(std::strcmp(model, "lyotropic-with-division")==0) m = new DivAccess(LX, LY, BC);
     else if(std::strcmp(model, "nematic")==0) m = new NemAccess(LX, LY, BC);
     else { last_error = "unknown model"; return nullptr; }
     m->opts = m->options();
@@ -265,6 +297,26 @@ int ref_get_field(void* h, const char* name, double* dst)
   }
   last_error = std::string("unknown field ") + name;
   return -1;
+}
+
+/** Copy a boolean mask of the division models (division_mask,
+ * death_mask) out as 0/1 bytes in site order. */
+int ref_get_mask(void* h, const char* name, unsigned char* dst)
+{
+  auto* m = static_cast<RefModel*>(h);
+  const std::vector<bool>* v = m->mask(name);
+  if(!v) { last_error = std::string("unknown mask ") + name; return -1; }
+  for(size_t k=0; k<v->size(); ++k) dst[k] = (*v)[k] ? 1 : 0;
+  return 0;
+}
+
+/** A scalar member of the lyotropic models: totalphi, countphi,
+ * conserve_phi (1 or 0). */
+int ref_get_value(void* h, const char* name, double* out)
+{
+  auto* m = static_cast<RefModel*>(h);
+  if(!m->value(name, out)) { last_error = std::string("unknown value ") + name; return -1; }
+  return 0;
 }
 
 /** Recompute the conservation totals (ftot, ptot) from the current state,

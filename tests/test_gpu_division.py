@@ -1,0 +1,136 @@
+"""LyotropicWithDivision on the GPU against the reference's own division model.
+
+The reference (oracle/_ref, src/models/lyotropic-with-division.cpp) draws
+its division and death masks with its RNG at the start of every Step(); the
+GPU lattice gets the same masks through mass_lb_set_phi_source as the rate
+r = alpha*division_mask - beta*death_mask, and the conserve_phi correction
+through mass_lb_set_phi_conservation when the model switches it on.
+FP64: bit-identical fields after every run (periodic, walls, conservation).
+FP32 fused: within the FP32 tolerances of tests/test_gpu_fp32.py against the
+FP64 path with the same masks.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.helpers import LYO_C1, ff_dev, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+import mass_hd_b200 as M  # noqa: E402
+
+DIV = {"alpha": 0.05, "beta": 0.03, "division-rate": 0.05, "division-time": 3,
+       "division-radius": 4, "death-rate": 0.02, "death-time": 4, "death-radius": 3,
+       "phi-critical": 1.2}
+STATE = ("ff", "QQxx", "QQyx", "phi")
+
+
+def params(**over):
+    p = dict(LYO_C1)
+    p.update(DIV)
+    p.update({"config": "circle", "radius": 10, "conc": 1.0, "noise": 0.5})
+    p.update(over)
+    return p
+
+
+def run_pair(p, LX, LY, bc, steps, precision=M.FP64, seed=11):
+    ref = O.RefOracle(O.LYOTROPIC, p, LX, LY, bc, division=True)
+    ref.configure(seed)
+    lat = M.Lattice(M.LYOTROPIC, p, LX, LY, bc, precision)
+    lat.upload_state({n: ref.get(n) for n in STATE})
+    if ref.value("conserve_phi"):
+        lat.set_phi_conservation(True, ref.value("totalphi"))
+    prev = None
+    masked = 0
+    for _ in range(steps):
+        ref.step(1)
+        dm = ref.mask("division_mask").astype(np.float64)
+        dd = ref.mask("death_mask").astype(np.float64)
+        masked += int(dm.sum() + dd.sum())
+        rate = p["alpha"] * dm - p["beta"] * dd
+        if prev is None or not np.array_equal(rate, prev):
+            lat.set_phi_source(rate)
+            prev = rate
+        lat.step(1)
+    return ref, lat, masked
+
+
+@pytest.mark.parametrize("LX,LY,bc", [(40, 36, 0), (64, 64, 0), (36, 40, 3), (40, 36, 2)])
+def test_fp64_division_bit_identical(LX, LY, bc):
+    ref, lat, masked = run_pair(params(), LX, LY, bc, 24)
+    assert masked > 0, "the masks never switched on"
+    assert ref.value("conserve_phi") == 0.0
+    for n in STATE:
+        assert np.array_equal(lat.get(n), ref.get(n)), n
+    lat.close()
+
+
+@pytest.mark.parametrize("bc", [0, 1])
+def test_fp64_conserve_phi_bit_identical(bc):
+    p = params(alpha=0.0, beta=0.0)
+    ref, lat, _ = run_pair(p, 40, 36, bc, 20)
+    assert ref.value("conserve_phi") == 1.0
+    for n in STATE:
+        assert np.array_equal(lat.get(n), ref.get(n)), n
+    # the correction keeps the total at its configured value
+    assert abs(lat.get("phi").sum() - ref.value("totalphi")) < 1e-9 * ref.value("totalphi")
+    lat.close()
+
+
+def test_fp32_fused_division_within_tolerance():
+    p = params()
+    LX = LY = 64
+    ref = O.RefOracle(O.LYOTROPIC, p, LX, LY, 0, division=True)
+    ref.configure(5)
+    st = {n: ref.get(n) for n in STATE}
+    a = M.Lattice(M.LYOTROPIC, p, LX, LY, 0, M.FP32)
+    b = M.Lattice(M.LYOTROPIC, p, LX, LY, 0, M.FP64)
+    assert a.uses_fused
+    a.upload_state(st)
+    b.upload_state(st)
+    masked = 0
+    for _ in range(10):
+        ref.step(1)
+        dm = ref.mask("division_mask").astype(np.float64)
+        dd = ref.mask("death_mask").astype(np.float64)
+        masked += int(dm.sum() + dd.sum())
+        rate = p["alpha"] * dm - p["beta"] * dd
+        a.set_phi_source(rate)
+        b.set_phi_source(rate)
+        a.step(1)
+        b.step(1)
+    assert masked > 0
+    assert a.tile()[0] == 32                  # the source runs in the warp-strip kernel
+    for n in STATE:
+        x, y = a.get(n), b.get(n)
+        if n == "ff":
+            x, y = ff_dev(x, 40.0), ff_dev(y, 40.0)
+        assert rel_l2(x, y) < 1e-4, n
+    # the source changed phi compared with no source at all
+    c = M.Lattice(M.LYOTROPIC, p, LX, LY, 0, M.FP32)
+    c.upload_state(st)
+    c.step(10)
+    assert rel_l2(c.get("phi"), a.get("phi")) > 1e-4
+    for lat in (a, b, c):
+        lat.close()
+
+
+def test_unsupported_combinations_are_rejected():
+    p = params()
+    a = M.Lattice(M.LYOTROPIC, p, 64, 64, 0, M.FP32)
+    with pytest.raises(M.MassLBError):
+        a.set_phi_conservation(True, 1.0)
+    n = M.Lattice(M.NEMATIC, {"Gamma": 0.3, "xi": 0.7, "tau": 1.5, "CC": 0.1, "LL": 0.05},
+                  64, 64, 0, M.FP64)
+    with pytest.raises(M.MassLBError):
+        n.set_phi_source(np.zeros(64 * 64))
+    ens = M.Ensemble(M.LYOTROPIC, [LYO_C1], [(64, 64)])
+    ens.runs[0].upload_state({"ff": np.tile(O.W_EQ * 40.0, (64 * 64, 1)), "QQxx": np.zeros(4096),
+                              "QQyx": np.zeros(4096), "phi": np.full(4096, 0.5)})
+    ens.runs[0].set_phi_source(np.full(64 * 64, 0.01))
+    with pytest.raises(M.MassLBError):
+        ens.step(1)
+    ens.runs[0].set_phi_source(None)
+    ens.step(1)
+    for x in (a, n, ens):
+        x.close()
