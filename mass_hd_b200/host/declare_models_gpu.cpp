@@ -4,6 +4,7 @@
 // registered as well, so unchanged reference runcards run on the GPU.
 #include "models.hpp"
 #include "lyotropic_gpu.hpp"
+#include "lyotropic_with_division_gpu.hpp"
 #include "nematic_gpu.hpp"
 
 void DeclareModels()
@@ -16,6 +17,10 @@ void DeclareModels()
   const char* nem = "Active nematic model with its time step on a B200 GPU.";
   declare_model<LyotropicGPU>("lyotropic-gpu", lyo);
   declare_model<NematicGPU>("nematic-gpu", nem);
+  const char* div = "Lyotropic model with cell division and death, with its time step on a "
+                    "B200 GPU.";
+  declare_model<LyotropicWithDivisionGPU>("lyotropic-with-division-gpu", div);
   declare_model<LyotropicGPU>("lyotropic", lyo);
+  declare_model<LyotropicWithDivisionGPU>("lyotropic-with-division", div);
   declare_model<NematicGPU>("nematic", nem);
 }

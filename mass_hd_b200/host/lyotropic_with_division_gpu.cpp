@@ -1,0 +1,148 @@
+#include "header.hpp"
+#include "lyotropic_with_division_gpu.hpp"
+#include "error_msg.hpp"
+#include "random.hpp"
+#include "mass_lb_ext.h"
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+
+using namespace std;
+namespace opt = boost::program_options;
+
+namespace {
+
+// unsigned distance on a periodic axis of length L, as the reference's
+// wrap(diff(a, b), L) (src/tools.hpp:30-63)
+unsigned periodic_distance(unsigned a, unsigned b, unsigned L)
+{
+  const unsigned d = a > b ? a - b : b - a;
+  return std::min(d % L, L - d % L);
+}
+
+} // namespace
+
+LyotropicWithDivisionGPU::LyotropicWithDivisionGPU(unsigned LX_, unsigned LY_, unsigned BC_)
+  : LyotropicGPU(LX_, LY_, BC_)
+{}
+
+void LyotropicWithDivisionGPU::Initialize()
+{
+  LyotropicGPU::Initialize();
+  division_mask.assign(DomainSize, false);
+  death_mask.assign(DomainSize, false);
+  rate.assign(DomainSize, 0.);
+  division_count = death_count = 0u;
+  // as src/models/lyotropic-with-division.cpp:29-30
+  conserve_phi = ((alpha == 0 || division_rate == 0) && (beta == 0 || death_rate == 0));
+}
+
+void LyotropicWithDivisionGPU::Configure()
+{
+  LyotropicGPU::Configure();
+  if(conserve_phi)
+  {
+    const int r = mass_lb_set_phi_conservation(lattice, 1, totalphi);
+    if(r != MASS_LB_OK)
+      throw error_msg(mass_gpu::abi_error("mass_lb_set_phi_conservation", r),
+                      " (division and death are off, so phi is conserved by a lattice-wide "
+                      "correction; run with precision=fp64)");
+  }
+}
+
+void LyotropicWithDivisionGPU::SetMasks()
+{
+  bool have_phi = false, changed = false;
+  auto draw = [&](std::vector<bool>& mask, double rate_coef, bool division, double radius) {
+    if(!have_phi)
+    {
+      const int r = mass_lb_download(lattice, MASS_LB_PHI, phi.data());
+      if(r != MASS_LB_OK) throw error_msg(mass_gpu::abi_error("mass_lb_download", r));
+      have_phi = true;
+    }
+    mask.assign(DomainSize, false);
+    // centres: one random_real() per site with phi >= .5, in site order
+    std::vector<std::array<unsigned, 2>> centers;
+    for(unsigned k = 0; k < DomainSize; ++k)
+    {
+      if(phi[k] >= .5)
+      {
+        const double p = division ? rate_coef*phi[k]*(1 - phi[k]/phi_critical)
+                                  : rate_coef*phi[k];
+        if(random_real() < p)
+          centers.push_back({GetXPosition(k), GetYPosition(k)});
+      }
+    }
+    const double r2 = ceil(radius*radius);
+    for(unsigned k = 0; k < DomainSize; ++k)
+    {
+      const unsigned yk = GetYPosition(k), xk = GetXPosition(k);
+      for(const auto& c : centers)
+        if(pow(periodic_distance(yk, c[1], LY), 2) + pow(periodic_distance(xk, c[0], LX), 2) <= r2)
+        {
+          mask[k] = true;
+          break;
+        }
+    }
+    changed = true;
+  };
+  if(not division_count--)
+  {
+    draw(division_mask, division_rate, true, division_radius);
+    division_count = division_time;
+  }
+  if(not death_count--)
+  {
+    draw(death_mask, death_rate, false, death_radius);
+    death_count = death_time;
+  }
+  if(changed)
+  {
+    for(unsigned k = 0; k < DomainSize; ++k)
+      rate[k] = alpha*(division_mask[k] ? 1. : 0.) - beta*(death_mask[k] ? 1. : 0.);
+    const int r = mass_lb_set_phi_source(lattice, rate.data());
+    if(r != MASS_LB_OK) throw error_msg(mass_gpu::abi_error("mass_lb_set_phi_source", r));
+  }
+}
+
+void LyotropicWithDivisionGPU::Step()
+{
+  // Step() must not throw (src/models.hpp:81-86): a failure is kept and
+  // reported by the next RuntimeChecks().
+  if(!step_error.empty()) return;
+  try { SetMasks(); }
+  catch(const error_msg& e) { step_error = e.what(); return; }
+  LyotropicGPU::Step();
+}
+
+void LyotropicWithDivisionGPU::RuntimeChecks()
+{
+  LyotropicGPU::RuntimeChecks();
+  // phi is checked only when it is conserved (src/models/lyotropic.cpp:538-548)
+  if(conserve_phi)
+  {
+    double fcheck = 0, pcheck = 0;
+    int bad = 0;
+    const int r = mass_lb_checks(lattice, &fcheck, &pcheck, &bad);
+    if(r != MASS_LB_OK) throw error_msg(mass_gpu::abi_error("mass_lb_checks", r));
+    if(abs(ptot - pcheck) > 1)
+      throw error_msg("phi is not conserved (", ptot, "/", pcheck, ")");
+  }
+}
+
+option_list LyotropicWithDivisionGPU::GetOptions()
+{
+  auto options = LyotropicGPU::GetOptions();
+  options[0].add_options()
+    ("alpha", opt::value<double>(&alpha), "division strength")
+    ("beta", opt::value<double>(&beta), "death strength")
+    ("division-rate", opt::value<double>(&division_rate), "division rate")
+    ("division-time", opt::value<double>(&division_time), "division life time")
+    ("division-radius", opt::value<double>(&division_radius), "division radius")
+    ("death-rate", opt::value<double>(&death_rate), "death rate")
+    ("death-time", opt::value<double>(&death_time), "death life time")
+    ("death-radius", opt::value<double>(&death_radius), "death radius")
+    ("phi-critical", opt::value<double>(&phi_critical), "phi critical");
+  return options;
+}

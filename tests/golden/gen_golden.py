@@ -132,9 +132,39 @@ def gen_json():
         print("wrote json", tag)
 
 
+DIV_JSON = {"alpha": 0.05, "beta": 0.03, "division-rate": 0.6, "division-time": 1,
+            "division-radius": 1.5, "death-rate": 0.3, "death-time": 2, "death-radius": 1.0,
+            "phi-critical": 1.5}
+
+
+def gen_json_division():
+    """Reference output of LyotropicWithDivision (masks included in the
+    frame) for an 8x6 lattice after 5 steps with division and death on."""
+    params = dict(LYO, config="circle", radius=2.5, level=0.0, conc=1.0, angle=0.0, noise=1.0)
+    params.update(DIV_JSON)
+    r = O.RefOracle(O.LYOTROPIC, params, 8, 6, 0, division=True)
+    r.configure(7)
+    r.step(5)
+    with tempfile.TemporaryDirectory() as d:
+        pth = os.path.join(d, "p.json")
+        fr = os.path.join(d, "f.json")
+        r.write_params(pth, 5, 5, 0, "lyotropic-with-division")
+        r.write_frame(fr)
+        for src, dst in ((pth, "div_parameters.json"), (fr, "div_frame5.json")):
+            with open(src) as fi, open(os.path.join(HERE, dst), "w") as fo:
+                fo.write(fi.read())
+    print("wrote json div")
+
+
 if __name__ == "__main__":
     if not O.ref_available():
         O.build(ref=True)
-    gen_cases()
-    gen_configure()
-    gen_json()
+    which = sys.argv[1:] or ["cases", "configure", "json", "division"]
+    if "cases" in which:
+        gen_cases()
+    if "configure" in which:
+        gen_configure()
+    if "json" in which:
+        gen_json()
+    if "division" in which:
+        gen_json_division()

@@ -66,6 +66,26 @@ def test_fp64_output_files_identical_to_reference(tmp_path, tag):
         assert got == want, name
 
 
+def test_fp64_division_output_identical_to_reference(tmp_path):
+    """LyotropicWithDivision through the plugin: masks drawn on the host from
+    the reference's random stream, source rate and steps on the device;
+    parameters.json and frame5.json (masks included) text-identical to the
+    reference's (tests/golden/gen_golden.py division)."""
+    opts = dict(LYO, config="circle", radius=2.5, level=0.0, conc=1.0, angle=0.0, noise=1.0)
+    opts.update({"alpha": 0.05, "beta": 0.03, "division-rate": 0.6, "division-time": 1,
+                 "division-radius": 1.5, "death-rate": 0.3, "death-time": 2,
+                 "death-radius": 1.0, "phi-critical": 1.5})
+    opts.update(LX=8, LY=6, nsteps=5, ninfo=5, seed=7, precision="fp64")
+    card = tmp_path / "run.dat"
+    runcard(card, "lyotropic-with-division", opts)
+    run(card, tmp_path / "out")
+    for name, gold in (("parameters.json", "div_parameters.json"),
+                       ("frame5.json", "div_frame5.json")):
+        got = (tmp_path / "out" / name).read_text()
+        want = open(os.path.join(GOLDEN, gold)).read()
+        assert got == want, name
+
+
 def load_frame(path):
     d = json.load(open(path))["data"]
     return {k: np.asarray(v["value"], dtype=float) for k, v in d.items()}
