@@ -85,6 +85,24 @@ int mass_lb_state_sums_noalloc(const float* planes, long long plane_stride, int 
                                unsigned LX, unsigned LY, double rho, void* stream,
                                double* fsum, double* phisum, int* nonfinite);
 
+/* ---- checkpoints ------------------------------------------------------------
+ *
+ * Full-precision binary checkpoint of a lattice, filling the role of the
+ * reference's unimplemented input archive (src/serialization.hpp:276-286).
+ * The file holds a header (model, precision, LX, LY, bc, npc, step count,
+ * the conservation totals of the runtime checks, the parameters) and the
+ * primary state - ff, QQxx, QQyx, phi - as IEEE doubles in the reference's
+ * site order, guarded by an FNV-1a checksum. Everything else a step uses is
+ * recomputed from these, so a loaded lattice continues bit for bit as if it
+ * had never stopped (FP32 values are stored exactly as doubles). A
+ * checkpoint loads into a handle of the same model and lattice size; the
+ * precision and boundary may differ. Errors (MASS_LB_EINVAL): unreadable
+ * file, wrong magic or version, other model or size, short or corrupted
+ * payload. Division-model masks, counters and the RNG state belong to the
+ * host model and are not part of the file. */
+int mass_lb_save(mass_lb_handle* h, const char* path);
+int mass_lb_load(mass_lb_handle* h, const char* path);
+
 /* ---- division models ------------------------------------------------------
  *
  * Hooks for the reference's LyotropicWithDivision (src/models/

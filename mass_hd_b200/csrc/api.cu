@@ -11,6 +11,7 @@
 #include "stats.cuh"
 
 #include <algorithm>
+#include <cstdint>
 #include <mutex>
 #include <cstdio>
 #include <cstdlib>
@@ -889,6 +890,112 @@ int mass_lb_device_state(mass_lb_handle* h, void** planes, long long* plane_stri
   *planes = h->cur;
   if(plane_stride) *plane_stride = static_cast<long long>(h->LX)*h->LY;
   if(nplanes_out) *nplanes_out = nplanes(h);
+  return 0;
+}
+
+// ---- checkpoints -------------------------------------------------------------
+
+} // extern "C"
+
+namespace {
+
+// Checkpoint file: a fixed header, then ff (LX*LY*9 doubles, site-major
+// [k][v]), QQxx, QQyx and, for lyotropic, phi (LX*LY doubles each), all in
+// the reference's site order k = y + LY*x, little-endian IEEE doubles.
+struct CkptHeader
+{
+  char magic[8];             // "MASSLBCK"
+  int32_t version;           // 1
+  int32_t model, precision;  // of the handle that wrote it
+  uint32_t LX, LY, bc, npc;
+  uint64_t steps;
+  double ftot, ptot;
+  double params[14];         // GammaQ .. conc of mass_lb_params
+  uint64_t payload_doubles;
+  uint64_t checksum;         // FNV-1a 64 over the payload bytes
+};
+
+uint64_t fnv1a(const void* data, size_t n, uint64_t h)
+{
+  const unsigned char* p = static_cast<const unsigned char*>(data);
+  for(size_t i = 0; i < n; ++i) { h ^= p[i]; h *= 1099511628211ull; }
+  return h;
+}
+
+constexpr uint64_t kFnvOffset = 14695981039346656037ull;
+
+void params_out(const Params& P, double* v)
+{
+  const double a[14] = {P.GammaQ, P.GammaP, P.xi, P.tauNem, P.tauIso, P.rho, P.friction,
+                        P.AA, P.CC, P.LL, P.KK, P.zeta, P.zetaI, P.conc};
+  for(int i = 0; i < 14; ++i) v[i] = a[i];
+}
+
+} // namespace
+
+extern "C" {
+
+int mass_lb_save(mass_lb_handle* h, const char* path)
+{
+  if(!h || !path) return fail(MASS_LB_EINVAL, "null argument");
+  const size_t N = static_cast<size_t>(h->LX)*h->LY;
+  const int nf = h->model == LYO ? 3 : 2;
+  std::vector<double> buf(N*9 + nf*N);
+  if(int r = mass_lb_download(h, MASS_LB_FF, buf.data())) return r;
+  const int fields[3] = {MASS_LB_QQXX, MASS_LB_QQYX, MASS_LB_PHI};
+  for(int i = 0; i < nf; ++i)
+    if(int r = mass_lb_download(h, fields[i], buf.data() + N*9 + i*N)) return r;
+  CkptHeader hd{};
+  std::memcpy(hd.magic, "MASSLBCK", 8);
+  hd.version = 1;
+  hd.model = h->model;
+  hd.precision = h->precision;
+  hd.LX = h->LX; hd.LY = h->LY; hd.bc = h->bc; hd.npc = h->P.npc;
+  hd.steps = h->steps;
+  hd.ftot = h->ftot; hd.ptot = h->ptot;
+  params_out(h->P, hd.params);
+  hd.payload_doubles = buf.size();
+  hd.checksum = fnv1a(buf.data(), buf.size()*sizeof(double), kFnvOffset);
+  FILE* f = std::fopen(path, "wb");
+  if(!f) return fail(MASS_LB_EINVAL, std::string("cannot open ") + path + " for writing");
+  const bool ok = std::fwrite(&hd, sizeof(hd), 1, f) == 1 &&
+                  std::fwrite(buf.data(), sizeof(double), buf.size(), f) == buf.size();
+  const bool closed = std::fclose(f) == 0;
+  if(!ok || !closed) return fail(MASS_LB_EINVAL, std::string("write failed: ") + path);
+  return 0;
+}
+
+int mass_lb_load(mass_lb_handle* h, const char* path)
+{
+  if(!h || !path) return fail(MASS_LB_EINVAL, "null argument");
+  FILE* f = std::fopen(path, "rb");
+  if(!f) return fail(MASS_LB_EINVAL, std::string("cannot open ") + path);
+  CkptHeader hd{};
+  auto bad = [&](const std::string& why) {
+    std::fclose(f);
+    return fail(MASS_LB_EINVAL, std::string(path) + ": " + why);
+  };
+  if(std::fread(&hd, sizeof(hd), 1, f) != 1) return bad("short header");
+  if(std::memcmp(hd.magic, "MASSLBCK", 8) != 0) return bad("not a mass_lb checkpoint");
+  if(hd.version != 1) return bad("unknown checkpoint version");
+  if(hd.model != h->model) return bad("checkpoint of another model");
+  if(hd.LX != h->LX || hd.LY != h->LY) return bad("checkpoint of another lattice size");
+  const size_t N = static_cast<size_t>(h->LX)*h->LY;
+  const int nf = h->model == LYO ? 3 : 2;
+  if(hd.payload_doubles != N*9 + nf*N) return bad("payload size does not match the lattice");
+  std::vector<double> buf(hd.payload_doubles);
+  if(std::fread(buf.data(), sizeof(double), buf.size(), f) != buf.size()) return bad("short payload");
+  std::fclose(f);
+  if(fnv1a(buf.data(), buf.size()*sizeof(double), kFnvOffset) != hd.checksum)
+    return fail(MASS_LB_EINVAL, std::string(path) + ": checksum mismatch (corrupted file)");
+  const double* ff = buf.data();
+  const double* q = buf.data() + N*9;
+  if(int r = mass_lb_upload(h, ff, q, q + N, h->model == LYO ? q + 2*N : nullptr)) return r;
+  // continue the run the checkpoint came from: step count and the totals
+  // the runtime checks compare against
+  h->steps = hd.steps;
+  h->ftot = hd.ftot;
+  h->ptot = hd.ptot;
   return 0;
 }
 

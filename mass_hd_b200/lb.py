@@ -104,6 +104,8 @@ def load_library(build_if_missing: bool = False):
         "mass_lb_uses_fused": (C.c_int, [vp]),
         "mass_lb_device_state": (C.c_int, [vp, C.POINTER(vp), C.POINTER(C.c_longlong), ip]),
         "mass_lb_statistics": (C.c_int, [vp, C.POINTER(Stats)]),
+        "mass_lb_save": (C.c_int, [vp, C.c_char_p]),
+        "mass_lb_load": (C.c_int, [vp, C.c_char_p]),
         "mass_lb_set_phi_source": (C.c_int, [vp, dp]),
         "mass_lb_set_phi_conservation": (C.c_int, [vp, C.c_int, C.c_double]),
         "mass_lb_ensemble_create": (C.c_int, [C.c_int, C.POINTER(Params), C.POINTER(C.c_uint),
@@ -228,6 +230,14 @@ class Lattice:
 
     def step(self, n: int = 1):
         _check(load_library().mass_lb_step(self.h, n))
+
+    def save(self, path: str):
+        """Full-precision binary checkpoint of the state (mass_lb_save)."""
+        _check(load_library().mass_lb_save(self.h, os.fsencode(path)))
+
+    def load(self, path: str):
+        """Restore a checkpoint written by save() (same model and size)."""
+        _check(load_library().mass_lb_load(self.h, os.fsencode(path)))
 
     def set_phi_source(self, rate):
         """Per-site phi source rate r (LX*LY values, site order; None
