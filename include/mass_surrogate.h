@@ -31,7 +31,7 @@ extern "C" {
 
 enum mass_sg_conv_mode {
   MASS_SG_FWD_BIAS = 0,   /* out = conv + bias */
-  MASS_SG_FWD_GELU = 1,   /* out2 = conv + bias; out = gelu(out2) (erf form) */
+  MASS_SG_FWD_GELU = 1,   /* out2 = conv + bias; out = gelu(out2) (tanh form) */
   MASS_SG_FWD_RESID = 2,  /* out = conv + bias + resid */
   MASS_SG_FWD_OUT = 3,    /* out_f[c < 5] = conv + bias + resid_f (nout = 16) */
   MASS_SG_BWD_GELU = 4,   /* out = conv * gelu'(aux) */

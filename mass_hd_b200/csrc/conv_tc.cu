@@ -42,7 +42,6 @@ namespace {
 constexpr int EPI_WARPS = 16;         // epilogue warps of the forward / input-gradient kernel
 constexpr int CONV_THREADS = 64 + 32*EPI_WARPS;   // + TMA warp + MMA warp
 constexpr int WG_THREADS = 192;       // weight gradient: TMA, MMA, 4 x epilogue
-constexpr int STAGES = 8;                    // input slabs in flight
 constexpr int SLAB_PX = 136;                 // 128 outputs + 2 halo pixels, rounded to 8 rows
 constexpr uint32_t SLAB_BYTES = SLAB_PX*128u;   // multiple of 1024
 constexpr uint32_t TILE_BYTES = 128u*128u;   // 128 pixels x 64 bf16 (weight-gradient tiles)
@@ -50,15 +49,22 @@ constexpr uint32_t TILE_BYTES = 128u*128u;   // 128 pixels x 64 bf16 (weight-gra
 template<int NOUT>
 struct ConvSmem
 {
+  // 64-channel outputs go out through a staging tile and a TMA store; an
+  // epilogue input (residual, pre-activation) comes in as a TMA tile, or the
+  // second staging tile holds the pre-activation output of FWD_GELU.
+  static constexpr int NSTAGE = NOUT == 64 ? 7 : 8;
   static constexpr uint32_t W_BYTES = 9u*NOUT*128u;          // multiple of 1024
   static constexpr uint32_t A_OFF = W_BYTES;
-  static constexpr uint32_t BAR_OFF = A_OFF + STAGES*SLAB_BYTES;
-  static constexpr int NBAR = 2*STAGES + 6;                  // full, empty, w, tfull[2], tempty[2], done
+  static constexpr uint32_t OUT_OFF = A_OFF + NSTAGE*SLAB_BYTES;
+  static constexpr uint32_t AUX_OFF = OUT_OFF + (NOUT == 64 ? TILE_BYTES : 0u);
+  static constexpr uint32_t BAR_OFF = AUX_OFF + (NOUT == 64 ? TILE_BYTES : 0u);
+  static constexpr int NBAR = 2*NSTAGE + 7;  // full, empty, w, tfull[2], tempty[2], done, aux
   static constexpr uint32_t MISC_OFF = BAR_OFF + NBAR*8;
   static constexpr uint32_t BIAS_OFF = MISC_OFF + 16;
   static constexpr uint32_t BYTES = BIAS_OFF + 64*4;
   static constexpr uint32_t ALLOC = BYTES + 1024;            // room to align the base
   static constexpr uint32_t TMEM_COLS = NOUT == 64 ? 128 : 32;
+  static_assert(ALLOC <= 232448, "shared memory per CTA");
 };
 
 __device__ __forceinline__ uint8_t* align1024(uint8_t* p)
@@ -72,13 +78,47 @@ __device__ __forceinline__ size_t padded_index(int n, int yy, int xx, int H, int
   return (static_cast<size_t>(n)*(H + 2) + yy)*static_cast<size_t>(W + 2) + xx;
 }
 
-__device__ __forceinline__ float gelu(float x)
+// GELU in its tanh form (Hendrycks & Gimpel, "Gaussian Error Linear Units",
+// 2016): gelu(x) = x/2 (1 + tanh(u)), u = sqrt(2/pi) (x + 0.044715 x^3),
+// with the hardware tanh estimate (tanh.approx.f32). Pairs of channels go
+// through the packed FP32x2 pipe.
+constexpr float GELU_C = 0.7978845608028654f;    // sqrt(2/pi)
+constexpr float GELU_A = 0.044715f;
+
+__device__ __forceinline__ float tanh_approx(float x)
 {
-  return 0.5f*x*(1.f + erff(x*0.70710678118654752f));
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
 }
-__device__ __forceinline__ float gelu_grad(float x)
+__device__ __forceinline__ float2 f2add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 f2mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 f2fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 f2s(float s) { return make_float2(s, s); }
+
+// tanh(u) of a pair, with u = C x (1 + A x^2)
+__device__ __forceinline__ float2 gelu_t(float2 x, float2& x2)
 {
-  return 0.5f*(1.f + erff(x*0.70710678118654752f)) + x*0.39894228040143268f*expf(-0.5f*x*x);
+  x2 = f2mul(x, x);
+  const float2 u = f2mul(f2mul(f2s(GELU_C), x), f2fma(f2s(GELU_A), x2, f2s(1.f)));
+  return make_float2(tanh_approx(u.x), tanh_approx(u.y));
+}
+__device__ __forceinline__ float2 gelu2(float2 x)
+{
+  float2 x2;
+  const float2 t = gelu_t(x, x2);
+  const float2 hx = f2mul(f2s(0.5f), x);
+  return f2fma(hx, t, hx);                                   // x/2 (1 + t)
+}
+// d gelu / dx = (1 + t)/2 + x/2 (1 - t^2) C (1 + 3 A x^2)
+__device__ __forceinline__ float2 gelu_grad2(float2 x)
+{
+  float2 x2;
+  const float2 t = gelu_t(x, x2);
+  const float2 sech2 = f2fma(make_float2(-t.x, -t.y), t, f2s(1.f));          // 1 - t^2
+  const float2 du = f2mul(f2s(GELU_C), f2fma(f2s(3.f*GELU_A), x2, f2s(1.f))); // du/dx
+  const float2 a = f2fma(f2s(0.5f), t, f2s(0.5f));                          // (1 + t)/2
+  return f2fma(f2mul(f2mul(f2s(0.5f), x), sech2), du, a);
 }
 
 __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b)
@@ -135,13 +175,18 @@ __device__ __forceinline__ void load_slice16(const __nv_bfloat16* base, float* v
 template<int NOUT, int MODE>
 __global__ void __launch_bounds__(CONV_THREADS, 1)
 conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmW,
-               const ConvArgs a)
+               const __grid_constant__ CUtensorMap tmO, const __grid_constant__ CUtensorMap tmO2,
+               const __grid_constant__ CUtensorMap tmR, const ConvArgs a)
 {
   using L = ConvSmem<NOUT>;
+  constexpr int STAGES = L::NSTAGE;
+  constexpr bool HAS_AUX = MODE == CONV_FWD_RESID || MODE == CONV_BWD_RESID || MODE == CONV_BWD_GELU;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* sm = align1024(smem_raw);
   uint8_t* Wsm = sm;
   uint8_t* Asm = sm + L::A_OFF;
+  uint8_t* outS = sm + L::OUT_OFF;
+  uint8_t* auxS = sm + L::AUX_OFF;
   uint64_t* bars = reinterpret_cast<uint64_t*>(sm + L::BAR_OFF);
   uint64_t* full = bars;
   uint64_t* empty = bars + STAGES;
@@ -149,6 +194,7 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
   uint64_t* tfull = wbar + 1;
   uint64_t* tempty = wbar + 3;
   uint64_t* done = wbar + 5;
+  uint64_t* abar = wbar + 6;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + L::MISC_OFF);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + L::MISC_OFF + 4);
   float* bias_sm = reinterpret_cast<float*>(sm + L::BIAS_OFF);
@@ -166,6 +212,7 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
     mbar_init(&tempty[0], EPI_WARPS);
     mbar_init(&tempty[1], EPI_WARPS);
     mbar_init(done, 1);
+    mbar_init(abar, 1);
     *abort_flag = 0;
     fence_barrier_init();
     fence_proxy_async();
@@ -252,12 +299,13 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
       if(!mbar_wait(done, 0)) give_up();
     }
   }
-  else
+  else if constexpr(NOUT == 16)
   {
-    const int q = warp & 3;                       // TMEM lanes 32q..32q+31
-    const int c0 = ((warp - 2) >> 2)*16;          // this warp's 16 channels
+    // output layer: 5 fp32 channels per pixel, stored directly; the warps of
+    // the first 16-column slice hold all 16 columns, the others only release
+    const int q = warp & 3;
+    const int c0 = ((warp - 2) >> 2)*16;
     uint32_t tcount = 0;
-    // decisions are warp-uniform: tcgen05.ld needs all 32 lanes
     for(int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++tcount)
     {
       if(__any_sync(0xffffffffu, *abort_flag != 0)) break;
@@ -265,70 +313,168 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
       const int xt = tile % xt_n, row = tile / xt_n;
       const int y = row % H, n = row / H;
       const int x = (xt << 7) + q*32 + lane;
-      // the second input of the epilogue is loaded before the accumulator
-      // is awaited, so its latency overlaps this tile's MMAs
-      float r[16];
-      if constexpr(MODE == CONV_FWD_RESID || MODE == CONV_BWD_RESID)
-        load_slice16(a.resid, r, c0, n, y, x, H, W);
-      if constexpr(MODE == CONV_BWD_GELU)
-        load_slice16(a.aux, r, c0, n, y, x, H, W);
       if(!__all_sync(0xffffffffu, mbar_wait(&tfull[acc], use & 1u)))
       {
         if(lane == 0) give_up();
         break;
       }
       tc_fence_after();
-      if constexpr(NOUT == 16)
+      float v[16];
+      if(c0 == 0) tmem_ld16(tbase + (static_cast<uint32_t>(q*32) << 16) + acc*NOUT, v);
+      tc_fence_before();
+      __syncwarp();
+      if(lane == 0) mbar_arrive(&tempty[acc]);
+      if(c0 == 0)
       {
-        // one slice holds all 16 columns; the other warps only release
-        float v[16];
-        if(c0 == 0) tmem_ld16(tbase + (static_cast<uint32_t>(q*32) << 16) + acc*NOUT, v);
-        tc_fence_before();
-        __syncwarp();
-        if(lane == 0) mbar_arrive(&tempty[acc]);
-        if(c0 == 0)
-        {
-          const size_t p = (static_cast<size_t>(n)*H + y)*W + x;
+        const size_t p = (static_cast<size_t>(n)*H + y)*W + x;
 #pragma unroll
-          for(int c = 0; c < 5; ++c)
-            a.out_f[5*p + c] = v[c] + bias_sm[c] + (a.resid_f ? a.resid_f[5*p + c] : 0.f);
+        for(int c = 0; c < 5; ++c)
+          a.out_f[5*p + c] = v[c] + bias_sm[c] + (a.resid_f ? a.resid_f[5*p + c] : 0.f);
+      }
+    }
+  }
+  else
+  {
+    // 16 epilogue warps, 512 threads. Thread = pixel p = 32q + lane of the
+    // tile, channels c0..c0+15. The output tile is staged in shared memory in
+    // the 128-byte-swizzled layout and written by TMA stores (row y and, on
+    // the first / last image row, the periodic ring row); the two ring
+    // columns are written directly by the threads of pixels 0 and W-1.
+    // Every branch that leaves the loop is agreed by all 512 threads
+    // (named_and), so the named barriers below are always met by all.
+    constexpr int EPI_BAR = 1, EPI_N = 32*EPI_WARPS;
+    const int q = warp & 3;
+    const int c0 = ((warp - 2) >> 2)*16;
+    const int p = q*32 + lane;
+    const bool leader = warp == 2 && lane == 0;
+    // 16-byte chunks c0/8 and c0/8 + 1 of this pixel's 128-byte row, swizzled
+    const uint32_t off0 = p*128u + (((c0 >> 3) ^ (p & 7)) << 4);
+    const uint32_t off1 = p*128u + ((((c0 >> 3) + 1) ^ (p & 7)) << 4);
+    bool aux_pending = false;
+    if constexpr(HAS_AUX)
+    {
+      if(leader && static_cast<int>(blockIdx.x) < ntiles)
+      {
+        const int t0 = blockIdx.x, xt = t0 % xt_n, row = t0 / xt_n;
+        mbar_expect_tx(abar, TILE_BYTES);
+        tma_load_4d(auxS, &tmR, 0, (xt << 7) + 1, row % H + 1, row / H, abar);
+        aux_pending = true;
+      }
+    }
+    uint32_t tcount = 0;
+    for(int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++tcount)
+    {
+      const uint32_t acc = tcount & 1u, use = tcount >> 1;
+      const int xt = tile % xt_n, row = tile / xt_n;
+      const int y = row % H, n = row / H, x0 = xt << 7;
+      const int x = x0 + p;
+      bool ok = *abort_flag == 0 && mbar_wait(&tfull[acc], use & 1u);
+      if constexpr(HAS_AUX) ok = ok && mbar_wait(abar, tcount & 1u);
+      if(!named_and(EPI_BAR, EPI_N, ok))
+      {
+        if(leader) give_up();
+        break;
+      }
+      if constexpr(HAS_AUX) if(leader) aux_pending = false;
+      tc_fence_after();
+      float v[16];
+      tmem_ld16(tbase + (static_cast<uint32_t>(q*32) << 16) + acc*NOUT + c0, v);
+      tc_fence_before();
+      __syncwarp();
+      if(lane == 0) mbar_arrive(&tempty[acc]);
+      float r[16];
+      if constexpr(HAS_AUX)
+      {
+        unpack8(*reinterpret_cast<const uint4*>(auxS + off0), r);
+        unpack8(*reinterpret_cast<const uint4*>(auxS + off1), r + 8);
+      }
+      float2* v2 = reinterpret_cast<float2*>(v);
+      const float2* r2 = reinterpret_cast<const float2*>(r);
+      if constexpr(MODE == CONV_FWD_BIAS || MODE == CONV_FWD_GELU || MODE == CONV_FWD_RESID)
+      {
+        const float2* b2 = reinterpret_cast<const float2*>(bias_sm + c0);
+#pragma unroll
+        for(int c = 0; c < 8; ++c) v2[c] = f2add(v2[c], b2[c]);
+      }
+      uint4 pre[2];
+      if constexpr(MODE == CONV_FWD_GELU)
+      {
+#pragma unroll
+        for(int k = 0; k < 2; ++k)
+          pre[k] = make_uint4(pack_bf16x2(v[8*k], v[8*k + 1]), pack_bf16x2(v[8*k + 2], v[8*k + 3]),
+                              pack_bf16x2(v[8*k + 4], v[8*k + 5]), pack_bf16x2(v[8*k + 6], v[8*k + 7]));
+#pragma unroll
+        for(int c = 0; c < 8; ++c) v2[c] = gelu2(v2[c]);
+      }
+      if constexpr(MODE == CONV_FWD_RESID || MODE == CONV_BWD_RESID)
+      {
+#pragma unroll
+        for(int c = 0; c < 8; ++c) v2[c] = f2add(v2[c], r2[c]);
+      }
+      if constexpr(MODE == CONV_BWD_GELU)
+      {
+#pragma unroll
+        for(int c = 0; c < 8; ++c) v2[c] = f2mul(v2[c], gelu_grad2(r2[c]));
+      }
+      uint4 pk[2];
+#pragma unroll
+      for(int k = 0; k < 2; ++k)
+        pk[k] = make_uint4(pack_bf16x2(v[8*k], v[8*k + 1]), pack_bf16x2(v[8*k + 2], v[8*k + 3]),
+                           pack_bf16x2(v[8*k + 4], v[8*k + 5]), pack_bf16x2(v[8*k + 6], v[8*k + 7]));
+      // (A) every thread has read this tile's aux tile, and the previous
+      // tile's stores have finished reading the staging tiles
+      named_sync(EPI_BAR, EPI_N);
+      if constexpr(HAS_AUX)
+      {
+        const int nt = tile + static_cast<int>(gridDim.x);
+        if(leader && nt < ntiles)
+        {
+          const int nxt = nt % xt_n, nrow = nt / xt_n;
+          mbar_expect_tx(abar, TILE_BYTES);
+          tma_load_4d(auxS, &tmR, 0, (nxt << 7) + 1, nrow % H + 1, nrow / H, abar);
+          aux_pending = true;
         }
       }
-      else
+      *reinterpret_cast<uint4*>(outS + off0) = pk[0];
+      *reinterpret_cast<uint4*>(outS + off1) = pk[1];
+      if constexpr(MODE == CONV_FWD_GELU)
       {
-        float v[16];
-        tmem_ld16(tbase + (static_cast<uint32_t>(q*32) << 16) + acc*NOUT + c0, v);
-        tc_fence_before();
-        __syncwarp();
-        if(lane == 0) mbar_arrive(&tempty[acc]);
-        if constexpr(MODE == CONV_FWD_BIAS || MODE == CONV_FWD_GELU || MODE == CONV_FWD_RESID)
-        {
-#pragma unroll
-          for(int c = 0; c < 16; ++c) v[c] += bias_sm[c0 + c];
-        }
-        if constexpr(MODE == CONV_FWD_GELU)
-        {
-          uint4* dst =
-            reinterpret_cast<uint4*>(a.out2 + padded_index(n, y + 1, x + 1, H, W)*64 + c0);
-#pragma unroll
-          for(int k = 0; k < 2; ++k)
-            dst[k] = make_uint4(pack_bf16x2(v[8*k], v[8*k + 1]), pack_bf16x2(v[8*k + 2], v[8*k + 3]),
-                                pack_bf16x2(v[8*k + 4], v[8*k + 5]), pack_bf16x2(v[8*k + 6], v[8*k + 7]));
-#pragma unroll
-          for(int c = 0; c < 16; ++c) v[c] = gelu(v[c]);
-        }
-        if constexpr(MODE == CONV_FWD_RESID || MODE == CONV_BWD_RESID)
-        {
-#pragma unroll
-          for(int c = 0; c < 16; ++c) v[c] += r[c];
-        }
-        if constexpr(MODE == CONV_BWD_GELU)
-        {
-#pragma unroll
-          for(int c = 0; c < 16; ++c) v[c] *= gelu_grad(r[c]);
-        }
-        store_slice16(a.out, v, c0, n, y, x, H, W);
+        *reinterpret_cast<uint4*>(auxS + off0) = pre[0];
+        *reinterpret_cast<uint4*>(auxS + off1) = pre[1];
       }
+      // the two periodic ring columns (and the four corners) directly
+      if(x == 0 || x == W - 1)
+      {
+        const int xs = x == 0 ? W + 1 : 0;
+        int ys[3] = {y + 1, 0, 0}, ny = 1;
+        if(y == 0) ys[ny++] = H + 1;
+        if(y == H - 1) ys[ny++] = 0;
+        for(int i2 = 0; i2 < ny; ++i2)
+        {
+          uint4* dst = reinterpret_cast<uint4*>(a.out + padded_index(n, ys[i2], xs, H, W)*64 + c0);
+          dst[0] = pk[0];
+          dst[1] = pk[1];
+        }
+      }
+      fence_proxy_async();
+      // (B) the staging tiles are complete
+      named_sync(EPI_BAR, EPI_N);
+      if(leader)
+      {
+        tma_store_4d(&tmO, 0, x0 + 1, y + 1, n, outS);
+        if(y == 0) tma_store_4d(&tmO, 0, x0 + 1, H + 1, n, outS);
+        if(y == H - 1) tma_store_4d(&tmO, 0, x0 + 1, 0, n, outS);
+        if constexpr(MODE == CONV_FWD_GELU) tma_store_4d(&tmO2, 0, x0 + 1, y + 1, n, auxS);
+        bulk_commit();
+        bulk_wait_read_all();
+      }
+    }
+    if(leader)
+    {
+      bulk_wait_all();
+      // an aux tile requested for a tile that was never processed lands
+      // before the CTA exits
+      if(aux_pending) mbar_wait(abar, tcount & 1u);
     }
   }
 
@@ -557,7 +703,8 @@ cudaError_t smem_attr(K kern, unsigned long long& set_mask, int bytes)
 }
 
 template<int NOUT, int MODE>
-cudaError_t launch_mode(const CUtensorMap& tx, const CUtensorMap& tw, const ConvArgs& a,
+cudaError_t launch_mode(const CUtensorMap& tx, const CUtensorMap& tw, const CUtensorMap& to,
+                        const CUtensorMap& to2, const CUtensorMap& tr, const ConvArgs& a,
                         cudaStream_t st)
 {
   static unsigned long long attr = 0;
@@ -566,7 +713,7 @@ cudaError_t launch_mode(const CUtensorMap& tx, const CUtensorMap& tw, const Conv
   if(e != cudaSuccess) return e;
   const int ntiles = a.B*a.H*(a.W >> 7);
   const int grid = std::min(ntiles, sm_count());
-  kern<<<grid, CONV_THREADS, ConvSmem<NOUT>::ALLOC, st>>>(tx, tw, a);
+  kern<<<grid, CONV_THREADS, ConvSmem<NOUT>::ALLOC, st>>>(tx, tw, to, to2, tr, a);
   return cudaGetLastError();
 }
 
@@ -578,18 +725,27 @@ cudaError_t conv3x3_launch(const __nv_bfloat16* in, const __nv_bfloat16* w, int 
   if(a.B < 1 || a.H < 1 || a.W < 128 || (a.W & 127)) return cudaErrorInvalidValue;
   if((nout == 16) != (mode == CONV_FWD_OUT) || (nout != 16 && nout != 64))
     return cudaErrorInvalidValue;
-  CUtensorMap tx, tw;
+  CUtensorMap tx, tw, to, to2, tr;
   if(!map_activation(&tx, in, a.B, a.H, a.W, SLAB_PX) || !map_weights(&tw, w, nout))
+    return cudaErrorInvalidValue;
+  // output, pre-activation output and epilogue input tiles (128 pixels);
+  // maps a mode does not use repeat one it does
+  const void* out = mode == CONV_FWD_OUT ? static_cast<const void*>(in) : a.out;
+  const void* out2 = mode == CONV_FWD_GELU ? static_cast<const void*>(a.out2) : out;
+  const void* res = (mode == CONV_FWD_RESID || mode == CONV_BWD_RESID) ? static_cast<const void*>(a.resid)
+                  : mode == CONV_BWD_GELU ? static_cast<const void*>(a.aux) : out;
+  if(!map_activation(&to, out, a.B, a.H, a.W, 128) || !map_activation(&to2, out2, a.B, a.H, a.W, 128) ||
+     !map_activation(&tr, res, a.B, a.H, a.W, 128))
     return cudaErrorInvalidValue;
   switch(mode)
   {
-    case CONV_FWD_BIAS: return launch_mode<64, CONV_FWD_BIAS>(tx, tw, a, st);
-    case CONV_FWD_GELU: return launch_mode<64, CONV_FWD_GELU>(tx, tw, a, st);
-    case CONV_FWD_RESID: return launch_mode<64, CONV_FWD_RESID>(tx, tw, a, st);
-    case CONV_FWD_OUT: return launch_mode<16, CONV_FWD_OUT>(tx, tw, a, st);
-    case CONV_BWD_GELU: return launch_mode<64, CONV_BWD_GELU>(tx, tw, a, st);
-    case CONV_BWD_RESID: return launch_mode<64, CONV_BWD_RESID>(tx, tw, a, st);
-    case CONV_BWD_PLAIN: return launch_mode<64, CONV_BWD_PLAIN>(tx, tw, a, st);
+    case CONV_FWD_BIAS: return launch_mode<64, CONV_FWD_BIAS>(tx, tw, to, to2, tr, a, st);
+    case CONV_FWD_GELU: return launch_mode<64, CONV_FWD_GELU>(tx, tw, to, to2, tr, a, st);
+    case CONV_FWD_RESID: return launch_mode<64, CONV_FWD_RESID>(tx, tw, to, to2, tr, a, st);
+    case CONV_FWD_OUT: return launch_mode<16, CONV_FWD_OUT>(tx, tw, to, to2, tr, a, st);
+    case CONV_BWD_GELU: return launch_mode<64, CONV_BWD_GELU>(tx, tw, to, to2, tr, a, st);
+    case CONV_BWD_RESID: return launch_mode<64, CONV_BWD_RESID>(tx, tw, to, to2, tr, a, st);
+    case CONV_BWD_PLAIN: return launch_mode<64, CONV_BWD_PLAIN>(tx, tw, to, to2, tr, a, st);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -87,6 +87,49 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, i
     :: "r"(smem_u32(dst)), "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(bar))
     : "memory");
 }
+// shared memory -> global tile store (this GPU's memory); completes through
+// the bulk async-group of the issuing thread
+__device__ __forceinline__ void tma_store_4d(const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                             const void* src)
+{
+  asm volatile(
+    "cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4}], [%5];"
+    :: "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_u32(src)) : "memory");
+}
+__device__ __forceinline__ void bulk_commit()
+{
+  asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+}
+// the issuing thread's committed stores have finished reading shared memory
+__device__ __forceinline__ void bulk_wait_read_all()
+{
+  asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+// ... and have completed their global writes
+__device__ __forceinline__ void bulk_wait_all()
+{
+  asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+}
+
+// named barrier `id` over `n` threads (a multiple of 32)
+__device__ __forceinline__ void named_sync(int id, int n)
+{
+  asm volatile("bar.sync %0, %1;" :: "r"(id), "r"(n) : "memory");
+}
+// named barrier that also returns the AND of `v` over its `n` threads, so
+// every participant takes the same branch afterwards
+__device__ __forceinline__ bool named_and(int id, int n, bool v)
+{
+  uint32_t r;
+  asm volatile(
+    "{\n\t.reg .pred pi, po;\n\t"
+    "setp.ne.u32 pi, %1, 0;\n\t"
+    "bar.red.and.pred po, %2, %3, pi;\n\t"
+    "selp.u32 %0, 1, 0, po;\n\t}"
+    : "=r"(r) : "r"(static_cast<uint32_t>(v)), "r"(id), "r"(n) : "memory");
+  return r != 0;
+}
+
 __device__ __forceinline__ void prefetch_map(const CUtensorMap* map)
 {
   asm volatile("prefetch.tensormap [%0];" :: "l"(map) : "memory");

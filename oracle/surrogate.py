@@ -4,14 +4,14 @@ numpy float64 forward and backward of the residual CNN that
 mass_hd_b200/surrogate.py trains on the GPU, used to check the GPU
 convolutions, epilogues and gradients. The reference has no surrogate: the
 network follows the stated design (6 residual blocks of two 3x3
-circular-padded convolutions, 64 channels, erf-GELU, a linear 5->64 input
+circular-padded convolutions, 64 channels, GELU (tanh form), a linear 5->64 input
 convolution and a 64->5 output convolution added to the input fields), and
 this restatement is pinned by finite differences (tests/test_surrogate_oracle.py).
 
 With `bf=True` the values the GPU stores in bfloat16 (weights, the padded
 activations, the loss gradient and the gradients between layers) are rounded
 the same way, so GPU and oracle differ only by FP32 accumulation order and
-the erf/exp implementations.
+the hardware tanh estimate.
 
 Layouts: images [B, H, W, C]; weights [cout, 9, cin] with tap = 3*ky + kx
 multiplying input pixel (y+ky-1, x+kx-1) (periodic).
@@ -19,7 +19,6 @@ multiplying input pixel (y+ky-1, x+kx-1) (periodic).
 from __future__ import annotations
 
 import numpy as np
-from scipy.special import erf
 
 NBLOCKS = 6
 CH = 64
@@ -69,12 +68,19 @@ def conv_weight_grad(x: np.ndarray, dy: np.ndarray) -> np.ndarray:
     return g
 
 
+GELU_C = np.sqrt(2.0 / np.pi)
+GELU_A = 0.044715
+
+
 def gelu(x):
-    return 0.5 * x * (1.0 + erf(x / np.sqrt(2.0)))
+    """GELU in its tanh form (Hendrycks & Gimpel 2016), the form the GPU
+    epilogues compute: x/2 (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3)))."""
+    return 0.5 * x * (1.0 + np.tanh(GELU_C * (x + GELU_A * x ** 3)))
 
 
 def gelu_grad(x):
-    return 0.5 * (1.0 + erf(x / np.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / np.sqrt(2 * np.pi)
+    t = np.tanh(GELU_C * (x + GELU_A * x ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * x * (1.0 - t * t) * GELU_C * (1.0 + 3.0 * GELU_A * x * x)
 
 
 def layer_shapes():
