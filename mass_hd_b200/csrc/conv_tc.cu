@@ -8,12 +8,13 @@
 // pixel 0, 1 and 2 (descriptor start 128 bytes apart), so the input is
 // fetched once per row instead of once per tap. All 9 weight taps stay in
 // shared memory for the whole persistent kernel. Warp roles: warp 0 issues
-// TMA loads into an 8-slab ring, warp 1 issues tcgen05.mma (4 x K=16 per
-// tap) into one of two TMEM
-// accumulators, warps 2-17 drain the other accumulator (tcgen05.ld; four
-// warps per 32-lane TMEM quarter, 16 channels each), apply the fused
-// epilogue and store bf16 pixels with their periodic ring copies. The
-// epilogue carries most of the instructions, so it gets most of the warps.
+// TMA loads into a 5-slab ring, warp 1 issues tcgen05.mma (4 x K=16 per
+// tap) into two TMEM accumulators (alternate tiles), and warps 2-17 form
+// two epilogue groups, one per accumulator, so two tiles' epilogues run at
+// once. An epilogue drains its accumulator (tcgen05.ld), applies the fused
+// bias / GELU / residual / GELU' epilogue in packed FP32x2, stages the bf16
+// tile in swizzled shared memory and writes it (and its periodic ring row)
+// with TMA stores; residual and pre-activation inputs arrive as TMA tiles.
 //
 // Weight gradient (conv3x3_wgrad_kernel): dW_tap[ci][co] = sum over pixels of
 // x(p + tap)[ci] * dy(p)[co]. K runs over pixels, so both operands are read
@@ -52,13 +53,15 @@ struct ConvSmem
   // 64-channel outputs go out through a staging tile and a TMA store; an
   // epilogue input (residual, pre-activation) comes in as a TMA tile, or the
   // second staging tile holds the pre-activation output of FWD_GELU.
-  static constexpr int NSTAGE = NOUT == 64 ? 7 : 8;
+  // Two epilogue groups (one per TMEM accumulator) each own an output
+  // staging tile and an aux tile.
+  static constexpr int NSTAGE = NOUT == 64 ? 5 : 8;
   static constexpr uint32_t W_BYTES = 9u*NOUT*128u;          // multiple of 1024
   static constexpr uint32_t A_OFF = W_BYTES;
-  static constexpr uint32_t OUT_OFF = A_OFF + NSTAGE*SLAB_BYTES;
-  static constexpr uint32_t AUX_OFF = OUT_OFF + (NOUT == 64 ? TILE_BYTES : 0u);
-  static constexpr uint32_t BAR_OFF = AUX_OFF + (NOUT == 64 ? TILE_BYTES : 0u);
-  static constexpr int NBAR = 2*NSTAGE + 7;  // full, empty, w, tfull[2], tempty[2], done, aux
+  static constexpr uint32_t OUT_OFF = A_OFF + NSTAGE*SLAB_BYTES;          // [group]
+  static constexpr uint32_t AUX_OFF = OUT_OFF + (NOUT == 64 ? 2*TILE_BYTES : 0u);  // [group]
+  static constexpr uint32_t BAR_OFF = AUX_OFF + (NOUT == 64 ? 2*TILE_BYTES : 0u);
+  static constexpr int NBAR = 2*NSTAGE + 8;  // full, empty, w, tfull[2], tempty[2], done, aux[2]
   static constexpr uint32_t MISC_OFF = BAR_OFF + NBAR*8;
   static constexpr uint32_t BIAS_OFF = MISC_OFF + 16;
   static constexpr uint32_t BYTES = BIAS_OFF + 64*4;
@@ -185,8 +188,8 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
   uint8_t* sm = align1024(smem_raw);
   uint8_t* Wsm = sm;
   uint8_t* Asm = sm + L::A_OFF;
-  uint8_t* outS = sm + L::OUT_OFF;
-  uint8_t* auxS = sm + L::AUX_OFF;
+  uint8_t* outS0 = sm + L::OUT_OFF;
+  uint8_t* auxS0 = sm + L::AUX_OFF;
   uint64_t* bars = reinterpret_cast<uint64_t*>(sm + L::BAR_OFF);
   uint64_t* full = bars;
   uint64_t* empty = bars + STAGES;
@@ -194,7 +197,7 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
   uint64_t* tfull = wbar + 1;
   uint64_t* tempty = wbar + 3;
   uint64_t* done = wbar + 5;
-  uint64_t* abar = wbar + 6;
+  uint64_t* abar0 = wbar + 6;       // [group]
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + L::MISC_OFF);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + L::MISC_OFF + 4);
   float* bias_sm = reinterpret_cast<float*>(sm + L::BIAS_OFF);
@@ -209,10 +212,14 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
     mbar_init(wbar, 1);
     mbar_init(&tfull[0], 1);
     mbar_init(&tfull[1], 1);
-    mbar_init(&tempty[0], EPI_WARPS);
-    mbar_init(&tempty[1], EPI_WARPS);
+    // 64-channel kernels: one epilogue group of EPI_WARPS/2 warps releases
+    // each accumulator; the output layer: every epilogue warp
+    const uint32_t releases = NOUT == 64 ? EPI_WARPS/2 : EPI_WARPS;
+    mbar_init(&tempty[0], releases);
+    mbar_init(&tempty[1], releases);
     mbar_init(done, 1);
-    mbar_init(abar, 1);
+    mbar_init(&abar0[0], 1);
+    mbar_init(&abar0[1], 1);
     *abort_flag = 0;
     fence_barrier_init();
     fence_proxy_async();
@@ -280,14 +287,17 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
           const uint32_t s = it % STAGES, ph = (it / STAGES) & 1u;
           if(!mbar_wait(&full[s], ph)) { give_up(); ok = false; break; }
           tc_fence_after();
+          // descriptors of this slab and weight row, advanced by plain adds
+          // (the start address sits in the low bits, in 16-byte units)
+          const uint64_t da = sw128_desc(abase + s*SLAB_BYTES, 16, 1024);
+          const uint64_t db = sw128_desc(wbase + 3*ky*NOUT*128, 16, 1024);
 #pragma unroll
           for(int kx = 0; kx < 3; ++kx)
           {
             // tap (ky, kx): slab pixels kx .. kx+127
-            const uint32_t a0 = abase + s*SLAB_BYTES + kx*128, b0 = wbase + (3*ky + kx)*NOUT*128;
 #pragma unroll
             for(int k = 0; k < 4; ++k)
-              mma_bf16(d, sw128_desc(a0 + 32*k, 16, 1024), sw128_desc(b0 + 32*k, 16, 1024), IDESC,
+              mma_bf16(d, da + ((kx*128 + 32*k) >> 4), db + ((kx*NOUT*128 + 32*k) >> 4), IDESC,
                        (ky | kx | k) != 0);
           }
           mma_commit(&empty[s]);
@@ -335,58 +345,70 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
   }
   else
   {
-    // 16 epilogue warps, 512 threads. Thread = pixel p = 32q + lane of the
-    // tile, channels c0..c0+15. The output tile is staged in shared memory in
-    // the 128-byte-swizzled layout and written by TMA stores (row y and, on
-    // the first / last image row, the periodic ring row); the two ring
-    // columns are written directly by the threads of pixels 0 and W-1.
-    // Every branch that leaves the loop is agreed by all 512 threads
-    // (named_and), so the named barriers below are always met by all.
-    constexpr int EPI_BAR = 1, EPI_N = 32*EPI_WARPS;
+    // Two groups of 8 epilogue warps; group g drains accumulator g, i.e.
+    // every other tile, so two tiles' epilogues run at once. Within a group
+    // thread = pixel p = 32q + lane of the tile, channels c0..c0+31 (two
+    // warps per TMEM lane quarter). The output tile is staged in shared
+    // memory in the 128-byte-swizzled layout and written by TMA stores (row
+    // y and, on the first / last image row, the periodic ring row); the two
+    // ring columns are written directly by the threads of pixels 0 and W-1.
+    // Every branch that leaves the loop is agreed by all 256 threads of the
+    // group (named_and), so the group's named barrier is always met by all.
+    constexpr int GROUP_N = 32*EPI_WARPS/2;
+    const int e = warp - 2;
+    const int g = e / (EPI_WARPS/2);
+    const int bar_id = 1 + g;
     const int q = warp & 3;
-    const int c0 = ((warp - 2) >> 2)*16;
+    const int c0 = ((e % (EPI_WARPS/2)) >> 2)*32;
     const int p = q*32 + lane;
-    const bool leader = warp == 2 && lane == 0;
-    // 16-byte chunks c0/8 and c0/8 + 1 of this pixel's 128-byte row, swizzled
-    const uint32_t off0 = p*128u + (((c0 >> 3) ^ (p & 7)) << 4);
-    const uint32_t off1 = p*128u + ((((c0 >> 3) + 1) ^ (p & 7)) << 4);
+    const bool leader = (e % (EPI_WARPS/2)) == 0 && lane == 0;
+    uint8_t* outS = outS0 + g*TILE_BYTES;
+    uint8_t* auxS = auxS0 + g*TILE_BYTES;
+    uint64_t* abar = &abar0[g];
+    // the four 16-byte chunks of channels c0..c0+31 in this pixel's swizzled row
+    uint32_t off[4];
+#pragma unroll
+    for(int k = 0; k < 4; ++k) off[k] = p*128u + ((((c0 >> 3) + k) ^ (p & 7)) << 4);
+    const int stride = 2*static_cast<int>(gridDim.x);
+    const int first = static_cast<int>(blockIdx.x) + g*static_cast<int>(gridDim.x);
     bool aux_pending = false;
     if constexpr(HAS_AUX)
     {
-      if(leader && static_cast<int>(blockIdx.x) < ntiles)
+      if(leader && first < ntiles)
       {
-        const int t0 = blockIdx.x, xt = t0 % xt_n, row = t0 / xt_n;
+        const int xt = first % xt_n, row = first / xt_n;
         mbar_expect_tx(abar, TILE_BYTES);
         tma_load_4d(auxS, &tmR, 0, (xt << 7) + 1, row % H + 1, row / H, abar);
         aux_pending = true;
       }
     }
-    uint32_t tcount = 0;
-    for(int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++tcount)
+    uint32_t k = 0;
+    for(int tile = first; tile < ntiles; tile += stride, ++k)
     {
-      const uint32_t acc = tcount & 1u, use = tcount >> 1;
       const int xt = tile % xt_n, row = tile / xt_n;
       const int y = row % H, n = row / H, x0 = xt << 7;
       const int x = x0 + p;
-      bool ok = *abort_flag == 0 && mbar_wait(&tfull[acc], use & 1u);
-      if constexpr(HAS_AUX) ok = ok && mbar_wait(abar, tcount & 1u);
-      if(!named_and(EPI_BAR, EPI_N, ok))
+      bool ok = *abort_flag == 0 && mbar_wait(&tfull[g], k & 1u);
+      if constexpr(HAS_AUX) ok = ok && mbar_wait(abar, k & 1u);
+      if(!named_and(bar_id, GROUP_N, ok))
       {
         if(leader) give_up();
         break;
       }
       if constexpr(HAS_AUX) if(leader) aux_pending = false;
       tc_fence_after();
-      float v[16];
-      tmem_ld16(tbase + (static_cast<uint32_t>(q*32) << 16) + acc*NOUT + c0, v);
+      float v[32];
+      const uint32_t taddr = tbase + (static_cast<uint32_t>(q*32) << 16) + g*NOUT + c0;
+      tmem_ld16(taddr, v);
+      tmem_ld16(taddr + 16, v + 16);
       tc_fence_before();
       __syncwarp();
-      if(lane == 0) mbar_arrive(&tempty[acc]);
-      float r[16];
+      if(lane == 0) mbar_arrive(&tempty[g]);
+      float r[32];
       if constexpr(HAS_AUX)
       {
-        unpack8(*reinterpret_cast<const uint4*>(auxS + off0), r);
-        unpack8(*reinterpret_cast<const uint4*>(auxS + off1), r + 8);
+#pragma unroll
+        for(int c = 0; c < 4; ++c) unpack8(*reinterpret_cast<const uint4*>(auxS + off[c]), r + 8*c);
       }
       float2* v2 = reinterpret_cast<float2*>(v);
       const float2* r2 = reinterpret_cast<const float2*>(r);
@@ -394,39 +416,42 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
       {
         const float2* b2 = reinterpret_cast<const float2*>(bias_sm + c0);
 #pragma unroll
-        for(int c = 0; c < 8; ++c) v2[c] = f2add(v2[c], b2[c]);
+        for(int c = 0; c < 16; ++c) v2[c] = f2add(v2[c], b2[c]);
       }
-      uint4 pre[2];
+      uint4 pre[4];
       if constexpr(MODE == CONV_FWD_GELU)
       {
 #pragma unroll
-        for(int k = 0; k < 2; ++k)
-          pre[k] = make_uint4(pack_bf16x2(v[8*k], v[8*k + 1]), pack_bf16x2(v[8*k + 2], v[8*k + 3]),
-                              pack_bf16x2(v[8*k + 4], v[8*k + 5]), pack_bf16x2(v[8*k + 6], v[8*k + 7]));
+        for(int c = 0; c < 4; ++c)
+          pre[c] = make_uint4(pack_bf16x2(v[8*c], v[8*c + 1]), pack_bf16x2(v[8*c + 2], v[8*c + 3]),
+                              pack_bf16x2(v[8*c + 4], v[8*c + 5]), pack_bf16x2(v[8*c + 6], v[8*c + 7]));
 #pragma unroll
-        for(int c = 0; c < 8; ++c) v2[c] = gelu2(v2[c]);
+        for(int c = 0; c < 16; ++c) v2[c] = gelu2(v2[c]);
       }
       if constexpr(MODE == CONV_FWD_RESID || MODE == CONV_BWD_RESID)
       {
 #pragma unroll
-        for(int c = 0; c < 8; ++c) v2[c] = f2add(v2[c], r2[c]);
+        for(int c = 0; c < 16; ++c) v2[c] = f2add(v2[c], r2[c]);
       }
       if constexpr(MODE == CONV_BWD_GELU)
       {
 #pragma unroll
-        for(int c = 0; c < 8; ++c) v2[c] = f2mul(v2[c], gelu_grad2(r2[c]));
+        for(int c = 0; c < 16; ++c) v2[c] = f2mul(v2[c], gelu_grad2(r2[c]));
       }
-      uint4 pk[2];
+      uint4 pk[4];
 #pragma unroll
-      for(int k = 0; k < 2; ++k)
-        pk[k] = make_uint4(pack_bf16x2(v[8*k], v[8*k + 1]), pack_bf16x2(v[8*k + 2], v[8*k + 3]),
-                           pack_bf16x2(v[8*k + 4], v[8*k + 5]), pack_bf16x2(v[8*k + 6], v[8*k + 7]));
-      // (A) every thread has read this tile's aux tile, and the previous
-      // tile's stores have finished reading the staging tiles
-      named_sync(EPI_BAR, EPI_N);
+      for(int c = 0; c < 4; ++c)
+        pk[c] = make_uint4(pack_bf16x2(v[8*c], v[8*c + 1]), pack_bf16x2(v[8*c + 2], v[8*c + 3]),
+                           pack_bf16x2(v[8*c + 4], v[8*c + 5]), pack_bf16x2(v[8*c + 6], v[8*c + 7]));
+      // the group's previous stores must have read its staging tiles before
+      // they are rewritten
+      if(leader) bulk_wait_read_all();
+      // (A) every thread of the group has read this tile's aux tile, and the
+      // staging tiles are free
+      named_sync(bar_id, GROUP_N);
       if constexpr(HAS_AUX)
       {
-        const int nt = tile + static_cast<int>(gridDim.x);
+        const int nt = tile + stride;
         if(leader && nt < ntiles)
         {
           const int nxt = nt % xt_n, nrow = nt / xt_n;
@@ -435,12 +460,12 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
           aux_pending = true;
         }
       }
-      *reinterpret_cast<uint4*>(outS + off0) = pk[0];
-      *reinterpret_cast<uint4*>(outS + off1) = pk[1];
+#pragma unroll
+      for(int c = 0; c < 4; ++c) *reinterpret_cast<uint4*>(outS + off[c]) = pk[c];
       if constexpr(MODE == CONV_FWD_GELU)
       {
-        *reinterpret_cast<uint4*>(auxS + off0) = pre[0];
-        *reinterpret_cast<uint4*>(auxS + off1) = pre[1];
+#pragma unroll
+        for(int c = 0; c < 4; ++c) *reinterpret_cast<uint4*>(auxS + off[c]) = pre[c];
       }
       // the two periodic ring columns (and the four corners) directly
       if(x == 0 || x == W - 1)
@@ -452,13 +477,13 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
         for(int i2 = 0; i2 < ny; ++i2)
         {
           uint4* dst = reinterpret_cast<uint4*>(a.out + padded_index(n, ys[i2], xs, H, W)*64 + c0);
-          dst[0] = pk[0];
-          dst[1] = pk[1];
+#pragma unroll
+          for(int c = 0; c < 4; ++c) dst[c] = pk[c];
         }
       }
       fence_proxy_async();
       // (B) the staging tiles are complete
-      named_sync(EPI_BAR, EPI_N);
+      named_sync(bar_id, GROUP_N);
       if(leader)
       {
         tma_store_4d(&tmO, 0, x0 + 1, y + 1, n, outS);
@@ -466,7 +491,6 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
         if(y == H - 1) tma_store_4d(&tmO, 0, x0 + 1, 0, n, outS);
         if constexpr(MODE == CONV_FWD_GELU) tma_store_4d(&tmO2, 0, x0 + 1, y + 1, n, auxS);
         bulk_commit();
-        bulk_wait_read_all();
       }
     }
     if(leader)
@@ -474,7 +498,7 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
       bulk_wait_all();
       // an aux tile requested for a tile that was never processed lands
       // before the CTA exits
-      if(aux_pending) mbar_wait(abar, tcount & 1u);
+      if(aux_pending) mbar_wait(abar, k & 1u);
     }
   }
 
@@ -585,10 +609,11 @@ conv3x3_wgrad_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_const
         if(!mbar_wait(&full[s], ph)) { give_up(); break; }
         tc_fence_after();
         const uint32_t st = base + s*WG_STAGE;
+        const uint64_t da = sw128_desc(st, TILE_BYTES, 1024);
+        const uint64_t db = sw128_desc(st + 2*TILE_BYTES, 1024, 1024);
 #pragma unroll
         for(int kk = 0; kk < 8; ++kk)
-          mma_bf16(tbase, sw128_desc(st + kk*2048, TILE_BYTES, 1024),
-                   sw128_desc(st + 2*TILE_BYTES + kk*2048, 1024, 1024), IDESC,
+          mma_bf16(tbase, da + ((kk*2048) >> 4), db + ((kk*2048) >> 4), IDESC,
                    (blk != b0) || (kk != 0));
         mma_commit(&empty[s]);
       }

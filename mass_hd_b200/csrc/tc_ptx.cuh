@@ -161,7 +161,10 @@ __device__ __forceinline__ void tc_fence_after()
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
 
-// D[tmem] (+)= A[smem] * B[smem]^T, one thread issues
+// D[tmem] (+)= A[smem] * B[smem]^T, one thread issues. No memory clobber:
+// the operands are ordered by the mbarrier waits before and the commits
+// after (both volatile with clobbers), and a memory clobber here costs
+// issue slots on every MMA.
 __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc,
                                          uint32_t idesc, uint32_t accumulate)
 {
@@ -169,7 +172,7 @@ __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a_desc, uint6
     "{\n\t.reg .pred p;\n\t"
     "setp.ne.b32 p, %4, 0;\n\t"
     "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-    :: "r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate) : "memory");
+    :: "r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate));
 }
 // arrive on `bar` once every tcgen05.mma issued so far by this thread is done
 __device__ __forceinline__ void mma_commit(uint64_t* bar)
