@@ -20,7 +20,8 @@ surrogate: every M jumps the plain method runs one jump from the current
 state and the surrogate predicts the same jump; if their difference is
 below the threshold the surrogate takes the next M-1 jumps (the lattice is
 re-initialised from the predicted fields with equilibrium populations),
-otherwise the plain method does.
+otherwise - or if the surrogate's rollout left the finite range - the
+plain method does.
 
 Buffers passed to the kernels must stay referenced for the duration of
 each call: a temporary tensor's memory goes back to torch's caching
@@ -417,7 +418,7 @@ def hybrid(params: Params, ens: lb.Ensemble, steps: int, jump=50, M=10, threshol
     x = torch.zeros_like(cur)
     idx = np.arange(B)
     t = 0
-    taken = rejected = checks = 0
+    taken = rejected = checks = nonfinite = 0
     errors = []
     samples = []
     torch.cuda.synchronize()
@@ -435,16 +436,22 @@ def hybrid(params: Params, ens: lb.Ensemble, steps: int, jump=50, M=10, threshol
                      torch.linalg.vector_norm(after - cur).clamp_min(1e-12)).item())
         errors.append(err)
         checks += 1
+        accepted = False
         if err < threshold:
             x.copy_(after)
             for _ in range(M - 1):
                 net.pack(x, idx)
                 x.copy_(net.forward())
-            for r, run in enumerate(runs):
-                lattice_from_fields(run, x[r], params.mean, params.scale)
-            torch.cuda.current_stream().synchronize()
-            taken += M - 1
-        else:
+            # a rollout that left the finite range never reaches the lattice
+            if bool(torch.isfinite(x).all().item()):
+                for r, run in enumerate(runs):
+                    lattice_from_fields(run, x[r], params.mean, params.scale)
+                torch.cuda.current_stream().synchronize()
+                taken += M - 1
+                accepted = True
+            else:
+                nonfinite += 1
+        if not accepted:
             ens.step(jump * (M - 1))
             rejected += M - 1
         t += jump * M
@@ -454,4 +461,5 @@ def hybrid(params: Params, ens: lb.Ensemble, steps: int, jump=50, M=10, threshol
     wall = time.perf_counter() - t0
     net.check_error_flag()
     return {"steps": t, "wall_s": wall, "surrogate_jumps": taken, "plain_jumps_rejected": rejected,
-            "checks": checks, "check_errors": errors, "samples": samples}
+            "checks": checks, "nonfinite_rollouts": nonfinite, "check_errors": errors,
+            "samples": samples}

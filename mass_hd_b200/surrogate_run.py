@@ -173,6 +173,7 @@ def hybrid_cmd(weights, steps, M, threshold, nruns=8, seed=123, stats_every=1000
            "speedup": t_plain / res_h["wall_s"],
            "surrogate_jumps": res_h["surrogate_jumps"],
            "plain_jumps_rejected": res_h["plain_jumps_rejected"], "checks": res_h["checks"],
+           "nonfinite_rollouts": res_h["nonfinite_rollouts"],
            "check_error_median": float(np.median(errs)) if errs else None,
            "check_errors": [round(e, 4) for e in errs],
            "window_from": win, "plain_means": mp, "hybrid_means": mh,
