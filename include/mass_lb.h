@@ -37,7 +37,11 @@ extern "C" {
 
 typedef struct mass_lb_handle mass_lb_handle;
 
-enum mass_lb_model { MASS_LB_LYOTROPIC = 0, MASS_LB_NEMATIC = 1 };
+/* MASS_LB_GO_OR_GROW: the reference's GoOrGrow (src/models/go-or-grow.cpp),
+ * the lyotropic model with a crowding penalty, a preferred nematic order and
+ * a phenotype density m = phi*chi (chi = 1 grow, 0 go). Its extra parameters
+ * are set by mass_lb_set_go_or_grow_params (mass_lb_ext.h). */
+enum mass_lb_model { MASS_LB_LYOTROPIC = 0, MASS_LB_NEMATIC = 1, MASS_LB_GO_OR_GROW = 2 };
 
 /* MASS_LB_FP64: the oracle mode. Unfused sweeps in the reference's own
  *   evaluation order, no FMA contraction, IEEE division: agrees with the
@@ -91,7 +95,10 @@ enum mass_lb_field {
   /* step-internal predictor values (FP64 mode only) */
   MASS_LB_FN = 27,       /* LX*LY*9 */
   MASS_LB_QNXX = 28, MASS_LB_QNYX = 29, MASS_LB_PHN = 30,
-  MASS_LB_NUM_FIELDS = 31
+  /* go-or-grow only: the phenotype density m (primary state, uploadable),
+   * chi = m/phi (derived from m and phi), and m's predictor (FP64 only) */
+  MASS_LB_M = 31, MASS_LB_CHI = 32, MASS_LB_MN = 33,
+  MASS_LB_NUM_FIELDS = 34
 };
 
 /* ABI version compiled into the library (== MASS_LB_ABI_VERSION). */
@@ -116,10 +123,12 @@ int mass_lb_create(const mass_lb_params* params, unsigned LX, unsigned LY,
 void mass_lb_destroy(mass_lb_handle* h);
 
 /* Upload the primary state from host memory: ff (LX*LY*9, site-major),
- * QQxx, QQyx (LX*LY) and, for lyotropic, phi (LX*LY; may be NULL for the
- * nematic model). Replaces the state written by Model::Configure()
- * (src/models/lyotropic.cpp:149-156). Synchronous. Also records the
- * reference totals used by mass_lb_checks (ftot, ptot). */
+ * QQxx, QQyx (LX*LY) and, for lyotropic and go-or-grow, phi (LX*LY; may be
+ * NULL for the nematic model). Replaces the state written by
+ * Model::Configure() (src/models/lyotropic.cpp:149-156). Synchronous. Also
+ * records the reference totals used by mass_lb_checks (ftot, ptot). A
+ * go-or-grow lattice keeps its m (zero until uploaded with
+ * mass_lb_upload_field) and recomputes chi = m/phi. */
 int mass_lb_upload(mass_lb_handle* h, const double* ff, const double* QQxx,
                    const double* QQyx, const double* phi);
 
@@ -131,9 +140,9 @@ int mass_lb_step(mass_lb_handle* h, unsigned nsteps);
  * Synchronous. In FP32 mode the derived fields (N .. SIGMA_ACTIVE_YX) are
  * produced by re-running the last step from the retained previous state
  * with the diagnostic outputs enabled (the state itself is unchanged).
- * Returns MASS_LB_EUNSUPPORTED for FN, QNXX, QNYX, PHN in FP32 mode, for PHI and the
- * phase-field fields in the nematic model, or when no step has run yet for
- * a derived field in FP32 mode. */
+ * Returns MASS_LB_EUNSUPPORTED for FN, QNXX, QNYX, PHN, MN in FP32 mode, for PHI and the
+ * phase-field fields in the nematic model, for M, CHI, MN outside go-or-grow,
+ * or when no step has run yet for a derived field in FP32 mode. */
 int mass_lb_download(mass_lb_handle* h, int field, double* out);
 
 /* FP64 sums used by Model::RuntimeChecks() (src/models/lyotropic.cpp:527-549):

@@ -12,8 +12,11 @@
 extern "C" {
 #endif
 
-/* Upload one primary field (MASS_LB_FF, QQXX, QQYX or PHI) from host memory,
- * same layout as mass_lb_upload. Does not reset the recorded totals. */
+/* Upload one primary field (MASS_LB_FF, QQXX, QQYX, PHI or, for go-or-grow,
+ * M) from host memory, same layout as mass_lb_upload. Does not reset the
+ * recorded totals. On a go-or-grow lattice an upload of PHI or M recomputes
+ * chi = m/phi (0 where phi <= 1e-12), as UpdatePhenotypeQuantities does
+ * (src/models/go-or-grow.cpp:208-216). */
 int mass_lb_upload_field(mass_lb_handle* h, int field, const double* src);
 
 /* Tile of the fused FP32 kernel: `threads` lattice columns per CTA strip
@@ -91,7 +94,8 @@ int mass_lb_state_sums_noalloc(const float* planes, long long plane_stride, int 
  * reference's unimplemented input archive (src/serialization.hpp:276-286).
  * The file holds a header (model, precision, LX, LY, bc, npc, step count,
  * the conservation totals of the runtime checks, the parameters) and the
- * primary state - ff, QQxx, QQyx, phi - as IEEE doubles in the reference's
+ * primary state - ff, QQxx, QQyx, phi and, for go-or-grow, m - as IEEE
+ * doubles in the reference's
  * site order, guarded by an FNV-1a checksum. Everything else a step uses is
  * recomputed from these, so a loaded lattice continues bit for bit as if it
  * had never stopped (FP32 values are stored exactly as doubles). A
@@ -106,7 +110,8 @@ int mass_lb_load(mass_lb_handle* h, const char* path);
 /* ---- division models ------------------------------------------------------
  *
  * Hooks for the reference's LyotropicWithDivision (src/models/
- * lyotropic-with-division.cpp), lyotropic only.
+ * lyotropic-with-division.cpp), lyotropic and go-or-grow (whose source is
+ * chi*phi*r, see below).
  *
  * mass_lb_set_phi_source: per-site phi source rate r (LX*LY host doubles,
  * site order k = y + LY*x). After every UpdateFields (predictor and
@@ -128,6 +133,35 @@ int mass_lb_load(mass_lb_handle* h, const char* path);
  * (MASS_LB_EUNSUPPORTED). */
 int mass_lb_set_phi_source(mass_lb_handle* h, const double* rate);
 int mass_lb_set_phi_conservation(mass_lb_handle* h, int on, double totalphi);
+
+/* ---- go-or-grow -----------------------------------------------------------
+ *
+ * Parameters of the reference's GoOrGrow (src/models/go-or-grow.hpp:9-20,
+ * runcard names B, Snem, Dchi, Achi, Ochi, phiswitch, growTogether) and the
+ * phi-critical of LyotropicWithDivision. A go-or-grow handle starts with
+ * B = Dchi = Achi = Ochi = phiswitch = growTogether = 0, Snem = 1,
+ * phi_critical = 1. The growth rate alpha*division_mask - beta*death_mask
+ * is mass_lb_set_phi_source's rate r: after every UpdateFields
+ * phi += chi*phi*r and m grows by chi*phi*r (times chi when growTogether),
+ * src/models/go-or-grow.cpp:329-391. EUNSUPPORTED on other models. */
+typedef struct {
+  double B, Snem, Dchi, Achi, Ochi, phiswitch, phi_critical;
+  int growTogether;
+} mass_lb_go_or_grow_params;
+
+int mass_lb_set_go_or_grow_params(mass_lb_handle* h, const mass_lb_go_or_grow_params* p);
+
+/* GoOrGrow::RelaxFreeEnergy (src/models/go-or-grow.cpp:42-119) on the
+ * device: `steps` explicit descent steps of phi (relax_phi != 0) and Q
+ * (relax_Q != 0) with time step dt, walls as the reference applies them;
+ * then *phisum (may be NULL) receives the relaxed total of phi summed in
+ * site order, which the reference stores as totalphi, countphi and ptot.
+ * Also resets the recorded ptot to that sum. Populations are untouched
+ * (the reference's ResetHydrodynamics, :121-141, is an upload of the rest
+ * equilibrium). FP64 results equal the reference's bit for bit.
+ * Synchronous. EUNSUPPORTED on other models. */
+int mass_lb_relax_free_energy(mass_lb_handle* h, unsigned steps, double dt, int relax_phi,
+                              int relax_Q, double* phisum);
 
 /* ---- batched ensembles --------------------------------------------------
  *

@@ -44,7 +44,7 @@ const char* kFieldNames[MASS_LB_NUM_FIELDS] = {
   "HHyx", "MU", "dxQQxx", "dyQQxx", "dxQQyx", "dyQQyx", "sigmaXX", "sigmaYY",
   "sigmaYX", "sigmaXY", "sigma_bulk", "sigma_elastic_xx", "sigma_elastic_yx",
   "sigma_phase_field_xx", "sigma_phase_field_yx", "sigma_active_xx",
-  "sigma_active_yx", "fn", "QNxx", "QNyx", "phn"};
+  "sigma_active_yx", "fn", "QNxx", "QNyx", "phn", "m", "chi", "mN"};
 
 constexpr long long kStageSites = 1ll << 22;   // sites per transfer chunk
 
@@ -76,9 +76,12 @@ __global__ void k_get_ff(double* __restrict__ st, const T* ff, long long plane,
   {
     const int x = x0 + static_cast<int>(k / LY), y = static_cast<int>(k % LY);
     const long long e = (y + g) + static_cast<long long>(EY)*(x + g);
+    // rest = 0 (FP64 planes hold the populations themselves): no add, so
+    // that a -0 stays -0
 #pragma unroll
     for(int v = 0; v < 9; ++v)
-      st[9*k + v] = static_cast<double>(ff[v*plane + e]) + Tv(v)*rest;
+      st[9*k + v] = rest != 0.0 ? static_cast<double>(ff[v*plane + e]) + Tv(v)*rest
+                                : static_cast<double>(ff[v*plane + e]);
   }
 }
 
@@ -102,7 +105,8 @@ __global__ void k_get_scalar(double* __restrict__ st, const T* a, int x0, int nr
   for(long long k = blockIdx.x*256ll + threadIdx.x; k < n; k += 256ll*gridDim.x)
   {
     const int x = x0 + static_cast<int>(k / LY), y = static_cast<int>(k % LY);
-    st[k] = static_cast<double>(a[(y + g) + static_cast<long long>(EY)*(x + g)]) + add;
+    const double v = static_cast<double>(a[(y + g) + static_cast<long long>(EY)*(x + g)]);
+    st[k] = add != 0.0 ? v + add : v;   // keeps the sign of a zero
   }
 }
 
@@ -155,6 +159,7 @@ struct mass_lb_handle
   float* src32 = nullptr;       // FP32 with walls: same
   bool src_on = false;
   double* phisum = nullptr;     // countphi scalar for conserve_phi
+  double* relaxsum = nullptr;   // relaxed phi total (go-or-grow)
 };
 
 namespace {
@@ -201,11 +206,16 @@ int alloc_state(mass_lb_handle* h, State<T>& s)
   std::vector<T**> sc = {&s.Qxx, &s.Qyx, &s.QNxx, &s.QNyx, &s.n, &s.ux, &s.uy,
                          &s.Hxx, &s.Hyx, &s.dxQxx, &s.dyQxx, &s.dxQyx, &s.dyQyx,
                          &s.sXX, &s.sYY, &s.sYX, &s.sXY};
-  if(h->model == LYO)
+  if(h->model != NEM)
   {
     T** extra[6] = {&s.phi, &s.phn, &s.phi_tmp, &s.uxp, &s.uyp, &s.MU};
     for(int i = 0; i < 6; ++i) sc.push_back(extra[i]);
     for(int i = 0; i < 7; ++i) sc.push_back(&s.diag[i]);
+  }
+  if(h->model == GOG)
+  {
+    T** extra[5] = {&s.m, &s.mN, &s.m_tmp, &s.chi, &s.chi_tmp};
+    for(int i = 0; i < 5; ++i) sc.push_back(extra[i]);
   }
   for(auto p : sc) if(int r = dalloc(h, p, NE)) return r;
   return 0;
@@ -219,11 +229,16 @@ int zero_state(mass_lb_handle* h, State<T>& s)
   for(T* p : lb) CU(cudaMemsetAsync(p, 0, 9*NE*sizeof(T), h->stream), "memset");
   std::vector<T*> sc = {s.Qxx, s.Qyx, s.QNxx, s.QNyx, s.n, s.ux, s.uy, s.Hxx, s.Hyx,
                         s.dxQxx, s.dyQxx, s.dxQyx, s.dyQyx, s.sXX, s.sYY, s.sYX, s.sXY};
-  if(h->model == LYO)
+  if(h->model != NEM)
   {
     T* extra[6] = {s.phi, s.phn, s.phi_tmp, s.uxp, s.uyp, s.MU};
     for(int i = 0; i < 6; ++i) sc.push_back(extra[i]);
     for(int i = 0; i < 7; ++i) sc.push_back(s.diag[i]);
+  }
+  if(h->model == GOG)
+  {
+    T* extra[5] = {s.m, s.mN, s.m_tmp, s.chi, s.chi_tmp};
+    for(int i = 0; i < 5; ++i) sc.push_back(extra[i]);
   }
   for(T* p : sc) CU(cudaMemsetAsync(p, 0, NE*sizeof(T), h->stream), "memset");
   return 0;
@@ -349,7 +364,8 @@ int mass_lb_create(const mass_lb_params* params, unsigned LX, unsigned LY,
   if(!params || !out) return fail(MASS_LB_EINVAL, "null argument");
   *out = nullptr;
   if(LX == 0 || LY == 0) return fail(MASS_LB_EINVAL, "empty lattice");
-  if(params->model != MASS_LB_LYOTROPIC && params->model != MASS_LB_NEMATIC)
+  if(params->model != MASS_LB_LYOTROPIC && params->model != MASS_LB_NEMATIC &&
+     params->model != MASS_LB_GO_OR_GROW)
     return fail(MASS_LB_EINVAL, "unknown model");
   if(precision != MASS_LB_FP64 && precision != MASS_LB_FP32)
     return fail(MASS_LB_EINVAL, "unknown precision");
@@ -373,10 +389,11 @@ int mass_lb_create(const mass_lb_params* params, unsigned LX, unsigned LY,
   h->model = params->model;
   h->LX = LX; h->LY = LY;
   h->bc = bc;
-  // Which bc values carry walls: lyotropic 1..4 (src/models/lyotropic.cpp:388-498),
+  // Which bc values carry walls: lyotropic and go-or-grow 1..4
+  // (src/models/lyotropic.cpp:388-498, src/models/go-or-grow.cpp:393-418),
   // nematic 1 (src/models/nematic.cpp:259-368). Every other non-zero value is
   // the periodic ghost layer, which computes exactly what bc = 0 computes.
-  h->wall = (h->model == LYO) ? (bc >= 1 && bc <= 4) : (bc == 1);
+  h->wall = (h->model != NEM) ? (bc >= 1 && bc <= 4) : (bc == 1);
   if(h->wall && (LX < 2 || LY < 2))
   {
     delete h;
@@ -399,6 +416,11 @@ int mass_lb_create(const mass_lb_params* params, unsigned LX, unsigned LY,
   const long long stage_sites = std::min<long long>(kStageSites, static_cast<long long>(LX)*LY);
   if(int r = dalloc(h, &h->stage, 9*stage_sites)) return bail(r);
 
+  // go-or-grow defaults: the reference's initialisers (src/models/go-or-grow.hpp:11-13)
+  // and phi_critical = 1
+  const Pheno ph0{0., 1., 0., 0., 0., 0., 1., 0};
+  h->s64.ph = ph0;
+  h->s32.ph = ph0;
   if(precision == MASS_LB_FP64)
   {
     if(int r = alloc_state(h, h->s64)) return bail(r);
@@ -406,7 +428,9 @@ int mass_lb_create(const mass_lb_params* params, unsigned LX, unsigned LY,
   }
   else
   {
-    h->fused = !h->wall && h->P.npc == 1 &&
+    // the fused kernel covers lyotropic and nematic; go-or-grow runs the
+    // unfused sweeps in FP32
+    h->fused = !h->wall && h->P.npc == 1 && h->model != GOG &&
                fused_supported(static_cast<int>(LX), static_cast<int>(LY), 64);
     if(h->fused)
     {
@@ -486,18 +510,26 @@ static int put_field(mass_lb_handle* h, int field, const double* src)
     else if(f64)
     {
       State<double>& s = h->s64;
-      double* a = field == MASS_LB_QQXX ? s.Qxx : field == MASS_LB_QQYX ? s.Qyx : s.phi;
+      double* a = field == MASS_LB_QQXX ? s.Qxx : field == MASS_LB_QQYX ? s.Qyx
+                : field == MASS_LB_M ? s.m : s.phi;
       if(isff) k_put_ff<double><<<nb, 256, 0, h->stream>>>(h->stage, s.ff, h->d.NE, x0, nrows, LY, h->d.g, h->d.EY, 0.0);
       else k_put_scalar<double><<<nb, 256, 0, h->stream>>>(h->stage, a, x0, nrows, LY, h->d.g, h->d.EY);
     }
     else
     {
       State<float>& s = h->s32;
-      float* a = field == MASS_LB_QQXX ? s.Qxx : field == MASS_LB_QQYX ? s.Qyx : s.phi;
+      float* a = field == MASS_LB_QQXX ? s.Qxx : field == MASS_LB_QQYX ? s.Qyx
+               : field == MASS_LB_M ? s.m : s.phi;
       if(isff) k_put_ff<float><<<nb, 256, 0, h->stream>>>(h->stage, s.ff, h->d.NE, x0, nrows, LY, h->d.g, h->d.EY, rest);
       else k_put_scalar<float><<<nb, 256, 0, h->stream>>>(h->stage, a, x0, nrows, LY, h->d.g, h->d.EY);
     }
     CU(cudaGetLastError(), "upload kernel");
+  }
+  if(h->model == GOG && (field == MASS_LB_PHI || field == MASS_LB_M))
+  {
+    const int r = h->precision == MASS_LB_FP64 ? update_chi_f64(h->d, h->s64, h->stream)
+                                               : update_chi_f32(h->d, h->s32, h->stream);
+    if(r) return cuda_fail(cudaGetLastError(), "chi update");
   }
   return 0;
 }
@@ -505,10 +537,13 @@ static int put_field(mass_lb_handle* h, int field, const double* src)
 int mass_lb_upload_field(mass_lb_handle* h, int field, const double* src)
 {
   if(!h || !src) return fail(MASS_LB_EINVAL, "null argument");
-  if(field != MASS_LB_FF && field != MASS_LB_QQXX && field != MASS_LB_QQYX && field != MASS_LB_PHI)
-    return fail(MASS_LB_EINVAL, "only ff, QQxx, QQyx, phi can be uploaded");
-  if(field == MASS_LB_PHI && h->model != LYO)
+  if(field != MASS_LB_FF && field != MASS_LB_QQXX && field != MASS_LB_QQYX &&
+     field != MASS_LB_PHI && field != MASS_LB_M)
+    return fail(MASS_LB_EINVAL, "only ff, QQxx, QQyx, phi and m can be uploaded");
+  if(field == MASS_LB_PHI && h->model == NEM)
     return fail(MASS_LB_EUNSUPPORTED, "the nematic model has no phi");
+  if(field == MASS_LB_M && h->model != GOG)
+    return fail(MASS_LB_EUNSUPPORTED, "m exists in the go-or-grow model only");
   DeviceGuard g(h->device);
   if(int r = put_field(h, field, src)) return r;
   h->has_prev = false;
@@ -520,12 +555,12 @@ int mass_lb_upload(mass_lb_handle* h, const double* ff, const double* QQxx,
                    const double* QQyx, const double* phi)
 {
   if(!h || !ff || !QQxx || !QQyx) return fail(MASS_LB_EINVAL, "null argument");
-  if(h->model == LYO && !phi) return fail(MASS_LB_EINVAL, "lyotropic needs phi");
+  if(h->model != NEM && !phi) return fail(MASS_LB_EINVAL, "lyotropic models need phi");
   DeviceGuard g(h->device);
   if(int r = put_field(h, MASS_LB_FF, ff)) return r;
   if(int r = put_field(h, MASS_LB_QQXX, QQxx)) return r;
   if(int r = put_field(h, MASS_LB_QQYX, QQyx)) return r;
-  if(h->model == LYO)
+  if(h->model != NEM)
     if(int r = put_field(h, MASS_LB_PHI, phi)) return r;
   h->has_prev = false;
   h->steps = 0;
@@ -620,6 +655,8 @@ static int get_primary(mass_lb_handle* h, int field, double* out)
         case MASS_LB_SIGMAYX: a = s.sYX; break; case MASS_LB_SIGMAXY: a = s.sXY; break;
         case MASS_LB_QNXX: a = s.QNxx; break; case MASS_LB_QNYX: a = s.QNyx; break;
         case MASS_LB_PHN: a = s.phn; break;
+        case MASS_LB_M: a = s.m; break;       case MASS_LB_CHI: a = s.chi; break;
+        case MASS_LB_MN: a = s.mN; break;
         default:
           if(field >= MASS_LB_SIGMA_BULK && field <= MASS_LB_SIGMA_ACTIVE_YX)
             a = s.diag[field - MASS_LB_SIGMA_BULK];
@@ -646,6 +683,7 @@ static int get_primary(mass_lb_handle* h, int field, double* out)
         case MASS_LB_DXQQYX: a = s.dxQyx; break; case MASS_LB_DYQQYX: a = s.dyQyx; break;
         case MASS_LB_SIGMAXX: a = s.sXX; break; case MASS_LB_SIGMAYY: a = s.sYY; break;
         case MASS_LB_SIGMAYX: a = s.sYX; break; case MASS_LB_SIGMAXY: a = s.sXY; break;
+        case MASS_LB_M: a = s.m; break;       case MASS_LB_CHI: a = s.chi; break;
         default:
           if(field >= MASS_LB_SIGMA_BULK && field <= MASS_LB_SIGMA_ACTIVE_YX)
             a = s.diag[field - MASS_LB_SIGMA_BULK];
@@ -668,9 +706,12 @@ int mass_lb_download(mass_lb_handle* h, int field, double* out)
   const bool phase_field = field == MASS_LB_PHI || field == MASS_LB_UX_PHI ||
     field == MASS_LB_UY_PHI || field == MASS_LB_MU || field == MASS_LB_PHN ||
     (field >= MASS_LB_SIGMA_BULK && field <= MASS_LB_SIGMA_ACTIVE_YX);
-  if(h->model != LYO && phase_field)
+  if(h->model == NEM && phase_field)
     return fail(MASS_LB_EUNSUPPORTED, "field does not exist in the nematic model");
-  if(h->precision == MASS_LB_FP32 && field >= MASS_LB_FN)
+  if(h->model != GOG && (field == MASS_LB_M || field == MASS_LB_CHI || field == MASS_LB_MN))
+    return fail(MASS_LB_EUNSUPPORTED, "m and chi exist in the go-or-grow model only");
+  const bool predictor = (field >= MASS_LB_FN && field <= MASS_LB_PHN) || field == MASS_LB_MN;
+  if(h->precision == MASS_LB_FP32 && predictor)
     return fail(MASS_LB_EUNSUPPORTED, "step-internal predictor fields are FP64-mode only");
   DeviceGuard g(h->device);
   if(h->fused && field >= MASS_LB_N && field <= MASS_LB_SIGMA_ACTIVE_YX)
@@ -704,14 +745,14 @@ int mass_lb_checks(mass_lb_handle* h, double* fsum, double* phisum, int* nonfini
   else if(h->precision == MASS_LB_FP64)
   {
     const State<double>& s = h->s64;
-    SumView<double> v{s.ff, s.Qxx, s.Qyx, h->model == LYO ? s.phi : nullptr, h->d.NE,
+    SumView<double> v{s.ff, s.Qxx, s.Qyx, h->model != NEM ? s.phi : nullptr, h->d.NE,
                       h->d.LX, h->d.LY, h->d.g, h->d.EY, 0.0};
     e = launch_sums_f64(v, h->red_scratch, h->red_out, h->stream);
   }
   else
   {
     const State<float>& s = h->s32;
-    SumView<float> v{s.ff, s.Qxx, s.Qyx, h->model == LYO ? s.phi : nullptr, h->d.NE,
+    SumView<float> v{s.ff, s.Qxx, s.Qyx, h->model != NEM ? s.phi : nullptr, h->d.NE,
                      h->d.LX, h->d.LY, h->d.g, h->d.EY, h->P.rho};
     e = launch_sums_f32(v, h->red_scratch, h->red_out, h->stream);
   }
@@ -815,14 +856,14 @@ int mass_lb_statistics(mass_lb_handle* h, mass_lb_stats* out)
   else if(h->precision == MASS_LB_FP64)
   {
     const State<double>& s = h->s64;
-    StatView<double> v{s.ff, h->d.NE, s.Qxx, s.Qyx, h->model == LYO ? s.phi : nullptr,
+    StatView<double> v{s.ff, h->d.NE, s.Qxx, s.Qyx, h->model != NEM ? s.phi : nullptr,
                        h->d.LX, h->d.LY, h->d.g, h->d.EY, 0.0};
     e = launch_stats_f64(v, h->stats, 0.4, h->stream);
   }
   else
   {
     const State<float>& s = h->s32;
-    StatView<float> v{s.ff, h->d.NE, s.Qxx, s.Qyx, h->model == LYO ? s.phi : nullptr,
+    StatView<float> v{s.ff, h->d.NE, s.Qxx, s.Qyx, h->model != NEM ? s.phi : nullptr,
                       h->d.LX, h->d.LY, h->d.g, h->d.EY, h->P.rho};
     e = launch_stats_f32(v, h->stats, 0.4, h->stream);
   }
@@ -900,8 +941,9 @@ int mass_lb_device_state(mass_lb_handle* h, void** planes, long long* plane_stri
 namespace {
 
 // Checkpoint file: a fixed header, then ff (LX*LY*9 doubles, site-major
-// [k][v]), QQxx, QQyx and, for lyotropic, phi (LX*LY doubles each), all in
-// the reference's site order k = y + LY*x, little-endian IEEE doubles.
+// [k][v]), QQxx, QQyx and, for lyotropic and go-or-grow, phi and, for
+// go-or-grow, m (LX*LY doubles each), all in the reference's site order
+// k = y + LY*x, little-endian IEEE doubles.
 struct CkptHeader
 {
   char magic[8];             // "MASSLBCK"
@@ -924,6 +966,9 @@ uint64_t fnv1a(const void* data, size_t n, uint64_t h)
 
 constexpr uint64_t kFnvOffset = 14695981039346656037ull;
 
+// scalar planes after ff: Q (2), phi, m
+int ckpt_scalars(int model) { return model == NEM ? 2 : model == LYO ? 3 : 4; }
+
 void params_out(const Params& P, double* v)
 {
   const double a[14] = {P.GammaQ, P.GammaP, P.xi, P.tauNem, P.tauIso, P.rho, P.friction,
@@ -939,10 +984,10 @@ int mass_lb_save(mass_lb_handle* h, const char* path)
 {
   if(!h || !path) return fail(MASS_LB_EINVAL, "null argument");
   const size_t N = static_cast<size_t>(h->LX)*h->LY;
-  const int nf = h->model == LYO ? 3 : 2;
+  const int nf = ckpt_scalars(h->model);
   std::vector<double> buf(N*9 + nf*N);
   if(int r = mass_lb_download(h, MASS_LB_FF, buf.data())) return r;
-  const int fields[3] = {MASS_LB_QQXX, MASS_LB_QQYX, MASS_LB_PHI};
+  const int fields[4] = {MASS_LB_QQXX, MASS_LB_QQYX, MASS_LB_PHI, MASS_LB_M};
   for(int i = 0; i < nf; ++i)
     if(int r = mass_lb_download(h, fields[i], buf.data() + N*9 + i*N)) return r;
   CkptHeader hd{};
@@ -981,7 +1026,7 @@ int mass_lb_load(mass_lb_handle* h, const char* path)
   if(hd.model != h->model) return bad("checkpoint of another model");
   if(hd.LX != h->LX || hd.LY != h->LY) return bad("checkpoint of another lattice size");
   const size_t N = static_cast<size_t>(h->LX)*h->LY;
-  const int nf = h->model == LYO ? 3 : 2;
+  const int nf = ckpt_scalars(h->model);
   if(hd.payload_doubles != N*9 + nf*N) return bad("payload size does not match the lattice");
   std::vector<double> buf(hd.payload_doubles);
   if(std::fread(buf.data(), sizeof(double), buf.size(), f) != buf.size()) return bad("short payload");
@@ -990,7 +1035,9 @@ int mass_lb_load(mass_lb_handle* h, const char* path)
     return fail(MASS_LB_EINVAL, std::string(path) + ": checksum mismatch (corrupted file)");
   const double* ff = buf.data();
   const double* q = buf.data() + N*9;
-  if(int r = mass_lb_upload(h, ff, q, q + N, h->model == LYO ? q + 2*N : nullptr)) return r;
+  if(h->model == GOG)
+    if(int r = mass_lb_upload_field(h, MASS_LB_M, q + 3*N)) return r;
+  if(int r = mass_lb_upload(h, ff, q, q + N, h->model != NEM ? q + 2*N : nullptr)) return r;
   // continue the run the checkpoint came from: step count and the totals
   // the runtime checks compare against
   h->steps = hd.steps;
@@ -1031,7 +1078,7 @@ extern "C" {
 int mass_lb_set_phi_source(mass_lb_handle* h, const double* rate)
 {
   if(!h) return fail(MASS_LB_EINVAL, "null handle");
-  if(h->model != LYO) return fail(MASS_LB_EUNSUPPORTED, "the nematic model has no phi");
+  if(h->model == NEM) return fail(MASS_LB_EUNSUPPORTED, "the nematic model has no phi");
   DeviceGuard g(h->device);
   CU(cudaStreamSynchronize(h->stream), "sync");
   if(!rate)
@@ -1076,7 +1123,7 @@ int mass_lb_set_phi_source(mass_lb_handle* h, const double* rate)
 int mass_lb_set_phi_conservation(mass_lb_handle* h, int on, double totalphi)
 {
   if(!h) return fail(MASS_LB_EINVAL, "null handle");
-  if(h->model != LYO) return fail(MASS_LB_EUNSUPPORTED, "the nematic model has no phi");
+  if(h->model == NEM) return fail(MASS_LB_EUNSUPPORTED, "the nematic model has no phi");
   if(on && h->fused)
     return fail(MASS_LB_EUNSUPPORTED, "conserve_phi needs a lattice-wide sum between the two "
                                       "halves of a sub-step; use precision FP64");
@@ -1098,6 +1145,46 @@ int mass_lb_set_phi_conservation(mass_lb_handle* h, int on, double totalphi)
       h->s32.phisum = h->phisum;
     }
   }
+  return 0;
+}
+
+// ---- go-or-grow ------------------------------------------------------------
+
+int mass_lb_set_go_or_grow_params(mass_lb_handle* h, const mass_lb_go_or_grow_params* p)
+{
+  if(!h || !p) return fail(MASS_LB_EINVAL, "null argument");
+  if(h->model != GOG) return fail(MASS_LB_EUNSUPPORTED, "not a go-or-grow lattice");
+  const Pheno ph{p->B, p->Snem, p->Dchi, p->Achi, p->Ochi, p->phiswitch, p->phi_critical,
+                 p->growTogether ? 1 : 0};
+  h->s64.ph = ph;
+  h->s32.ph = ph;
+  return 0;
+}
+
+int mass_lb_relax_free_energy(mass_lb_handle* h, unsigned steps, double dt, int relax_phi,
+                              int relax_Q, double* phisum)
+{
+  if(!h) return fail(MASS_LB_EINVAL, "null handle");
+  if(h->model != GOG) return fail(MASS_LB_EUNSUPPORTED, "not a go-or-grow lattice");
+  DeviceGuard g(h->device);
+  if(!h->relaxsum)
+    if(int r = dalloc(h, &h->relaxsum, 1)) return r;
+  const int bc = h->wall ? static_cast<int>(h->bc) : 0;
+  const int r = h->precision == MASS_LB_FP64
+    ? relax_unfused_f64(h->d, h->P, h->s64, bc, steps, dt, relax_phi, relax_Q, h->relaxsum, h->stream)
+    : relax_unfused_f32(h->d, h->P, h->s32, bc, steps, dt, relax_phi, relax_Q, h->relaxsum, h->stream);
+  if(r) return cuda_fail(cudaGetLastError(), "relaxation");
+  // chi follows the relaxed phi
+  const int rc = h->precision == MASS_LB_FP64 ? update_chi_f64(h->d, h->s64, h->stream)
+                                              : update_chi_f32(h->d, h->s32, h->stream);
+  if(rc) return cuda_fail(cudaGetLastError(), "chi update");
+  double sum = 0;
+  CU(cudaMemcpyAsync(&sum, h->relaxsum, sizeof(double), cudaMemcpyDeviceToHost, h->stream),
+     "relaxation sum");
+  CU(cudaStreamSynchronize(h->stream), "relaxation sync");
+  h->ptot = sum;
+  h->has_prev = false;
+  if(phisum) *phisum = sum;
   return 0;
 }
 
@@ -1240,6 +1327,8 @@ int mass_lb_ensemble_create(int nruns, const mass_lb_params* params, const unsig
   if(nruns < 1) return fail(MASS_LB_EINVAL, "an ensemble needs at least one run");
   if(nruns > ENS_MAX_RUNS) return fail(MASS_LB_EINVAL, "too many runs for one ensemble");
   const int model = params[0].model;
+  if(model != MASS_LB_LYOTROPIC && model != MASS_LB_NEMATIC)
+    return fail(MASS_LB_EUNSUPPORTED, "ensembles run the lyotropic or nematic model");
   for(int i = 0; i < nruns; ++i)
   {
     if(params[i].model != model) return fail(MASS_LB_EINVAL, "all runs must use one model");

@@ -16,7 +16,7 @@
 
 namespace mlb {
 
-enum { LYO = 0, NEM = 1 };
+enum { LYO = 0, NEM = 1, GOG = 2 };   // GOG: go-or-grow (lyotropic + phenotype)
 
 // D2Q9 velocity set, src/geometry.hpp:17-27
 __host__ __device__ constexpr int CXv(int v)
@@ -58,6 +58,14 @@ struct Params
   unsigned npc;
 };
 
+// Go-or-grow parameters (runcard names, src/models/go-or-grow.hpp:9-20;
+// phi_critical is LyotropicWithDivision's, src/models/lyotropic-with-division.hpp:34)
+struct Pheno
+{
+  double B, Snem, Dchi, Achi, Ochi, phiswitch, phi_critical;
+  int growTogether;
+};
+
 // Every device array of one lattice (unfused kernels).
 template<typename T>
 struct State
@@ -77,6 +85,10 @@ struct State
   double* phisum;      // device scalar written before each UpdateFields
   double totalphi;
   int conserve_phi;
+  // go-or-grow (src/models/go-or-grow.cpp): the phenotype density m, its
+  // predictor mN, the next m, and chi = m/phi (plus the next chi)
+  T *m, *mN, *m_tmp, *chi, *chi_tmp;
+  Pheno ph;
 };
 
 __host__ __device__ inline int wrapi(int a, int n)

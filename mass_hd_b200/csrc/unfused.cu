@@ -168,6 +168,56 @@ uq_kernel(Dims d, Params P, State<T> s)
       s.diag[6][e] = -zeta*Qyx*(T(1)-p);
     }
   }
+  else if constexpr (MODEL == GOG)
+  {
+    // GoOrGrow::UpdateQuantitiesAtNode (src/models/go-or-grow.cpp:230-308):
+    // preferred order Snem, crowding penalty B above phi_critical, and an
+    // active stress weighted by the go fraction 1 - chi
+    const T AA = T(P.AA), KK = T(P.KK), zetaI = T(P.zetaI), conc = T(P.conc);
+    const T B = T(s.ph.B), Snem = T(s.ph.Snem), phic = T(s.ph.phi_critical);
+    const T p = s.phi[e];
+    const T del2p = lap(s.phi, nb);
+    const T dxPhi = dX(s.phi, nb);
+    const T dyPhi = dY(s.phi, nb);
+    const T q2 = Qxx*Qxx + Qyx*Qyx;
+    const T term = Snem - q2;
+    const T Hxx = T(2)*CC*term*Qxx + LL*del2Qxx;
+    const T Hyx = T(2)*CC*term*Qyx + LL*del2Qyx;
+    const T dpc = p - phic;
+    const T f_compress = dpc > T(0) ? T(.5)*B*dpc*dpc : T(0);
+    const T mu_compress = dpc > T(0) ? B*dpc : T(0);
+    const T mu = AA*p*(T(1)-p)*(T(1)-T(2)*p) + mu_compress - KK*del2p;
+    const T sigmaB = T(.5)*AA*p*p*(T(1)-p)*(T(1)-p)
+      + f_compress + T(.5)*CC*term*term - mu*p;
+    const T ap = zeta*p*(T(1)-s.chi[e]);
+    const T sigmaF = T(2)*xi*( (Qxx*Qxx-T(1))*Hxx + Qxx*Qyx*Hyx )
+      - ap*Qxx + T(.5)*KK*(dyPhi*dyPhi-dxPhi*dxPhi)
+      + LL*(dyQxx*dyQxx+dyQyx*dyQyx-dxQxx*dxQxx-dxQyx*dxQyx);
+    const T sigmaS = T(2)*xi*(Qyx*Qxx*Hxx + (Qyx*Qyx-T(1))*Hyx)
+      - ap*Qyx - KK*dxPhi*dyPhi
+      - T(2)*LL*(dxQxx*dyQxx+dxQyx*dyQyx);
+    const T sigmaA = T(2)*(Qxx*Hyx - Qyx*Hxx);
+
+    s.uxp[e] = vx*p;
+    s.uyp[e] = vy*p;
+    s.Hxx[e] = Hxx;
+    s.Hyx[e] = Hyx;
+    s.MU[e] = mu;
+    s.sXX[e] = sigmaF + sigmaB + zetaI*(conc-p);
+    s.sYY[e] = -sigmaF + sigmaB + zetaI*(conc-p);
+    s.sXY[e] = sigmaS + sigmaA;
+    s.sYX[e] = sigmaS - sigmaA;
+    if constexpr (DIAG)
+    {
+      s.diag[0][e] = sigmaB + zetaI*(conc-p);
+      s.diag[1][e] = sigmaF - T(.5)*KK*(dyPhi*dyPhi-dxPhi*dxPhi) + ap*Qxx;
+      s.diag[2][e] = sigmaS + KK*dxPhi*dyPhi + ap*Qyx;
+      s.diag[3][e] = T(.5)*KK*(dyPhi*dyPhi-dxPhi*dxPhi);
+      s.diag[4][e] = -KK*dxPhi*dyPhi;
+      s.diag[5][e] = -ap*Qxx;
+      s.diag[6][e] = -ap*Qyx;
+    }
+  }
   else
   {
     const T term = T(1.) - Qxx*Qxx - Qyx*Qyx;
@@ -243,9 +293,49 @@ uf_kernel(Dims d, Params P, State<T> s)
   T* __restrict__ FF = s.ff;
   T* __restrict__ FN = s.fn;
 
-  if constexpr (MODEL == LYO)
+  if constexpr (MODEL != NEM)
   {
     const T p = s.phi[e];
+    // go-or-grow phenotype update (src/models/go-or-grow.cpp:331-362): the
+    // growth R = chi*phi*(alpha*division_mask - beta*death_mask) and the
+    // rate of change Dm of m = phi*chi
+    T R = T(0), Dm = T(0);
+    if constexpr (MODEL == GOG)
+    {
+      const T rate = s.src ? s.src[e] : T(0);
+      const T chi_eff = s.chi[e];
+      R = chi_eff*p*rate;
+      const T mFlux = T(.5)*(s.ux[nb.e1]*s.m[nb.e1] - s.ux[nb.e2]*s.m[nb.e2])
+                    + T(.5)*(s.uy[nb.e3]*s.m[nb.e3] - s.uy[nb.e4]*s.m[nb.e4]);
+      const T chi_px = s.chi[nb.e1], chi_mx = s.chi[nb.e2];
+      const T chi_py = s.chi[nb.e3], chi_my = s.chi[nb.e4];
+      const T MUe = s.MU[e];
+      const T diffusiveMFlux =
+        T(.5)*(chi_px + chi_eff)*(s.MU[nb.e1] - MUe)
+      - T(.5)*(chi_eff + chi_mx)*(MUe - s.MU[nb.e2])
+      + T(.5)*(chi_py + chi_eff)*(s.MU[nb.e3] - MUe)
+      - T(.5)*(chi_eff + chi_my)*(MUe - s.MU[nb.e4]);
+      const T phenotypeDiffusion =
+        T(.5)*(s.phi[nb.e1] + p)*(chi_px - chi_eff)
+      - T(.5)*(p + s.phi[nb.e2])*(chi_eff - chi_mx)
+      + T(.5)*(s.phi[nb.e3] + p)*(chi_py - chi_eff)
+      - T(.5)*(p + s.phi[nb.e4])*(chi_eff - chi_my);
+      const T Achi = T(s.ph.Achi);
+      const T dVdChi = T(2)*Achi*chi_eff*(T(1)-chi_eff)*(T(1)-T(2)*chi_eff)
+                     + T(s.ph.Ochi)*(p-T(s.ph.phiswitch));
+      const T Sswitch = -p*dVdChi;
+      const T mGrowth = s.ph.growTogether ? chi_eff*R : R;
+      Dm = T(P.GammaP)*diffusiveMFlux + T(s.ph.Dchi)*phenotypeDiffusion - mFlux + Sswitch + mGrowth;
+    }
+    // m after the sub-step, clamped to [0, max(phi, 0)], and chi = m/phi
+    // (src/models/go-or-grow.cpp:364-384, :208-216)
+    auto phenotype_out = [&](T pt, T mt) {
+      const T upper = pt > T(0) ? pt : T(0);
+      if(mt < T(0)) mt = T(0);
+      else if(mt > upper) mt = upper;
+      s.m_tmp[e] = mt;
+      s.chi_tmp[e] = pt > T(1e-12) ? mt/pt : T(0);
+    };
     const T del2mu = lap(s.MU, nb);
     const T pFlux = dX(s.uxp, nb) + dY(s.uyp, nb);
     // conserve_phi is false for Lyotropic (src/models/lyotropic.hpp:46) and
@@ -263,9 +353,15 @@ uf_kernel(Dims d, Params P, State<T> s)
       s.Qxx[e]  = s.Qxx[e] + Dxx;
       s.Qyx[e]  = s.Qyx[e] + Dyx;
       T pt = s.phi[e] + Dp;
+      if constexpr (MODEL == GOG)
+      {
+        pt = pt + R;
+        s.mN[e] = s.m[e] + T(.5)*Dm;
+        phenotype_out(pt, s.m[e] + Dm);
+      }
       // division source, added after the node update as the division model
       // does (src/models/lyotropic-with-division.cpp:121)
-      if(s.src) pt = pt + s.phi[e]*s.src[e];
+      else if(s.src) pt = pt + s.phi[e]*s.src[e];
       s.phi_tmp[e] = pt;
 #pragma unroll
       for(int v=0; v<9; ++v)
@@ -281,7 +377,12 @@ uf_kernel(Dims d, Params P, State<T> s)
       s.Qxx[e] = s.QNxx[e] + T(.5)*Dxx;
       s.Qyx[e] = s.QNyx[e] + T(.5)*Dyx;
       T pt = s.phn[e] + T(.5)*Dp;
-      if(s.src) pt = pt + s.phi[e]*s.src[e];
+      if constexpr (MODEL == GOG)
+      {
+        pt = pt + R;
+        phenotype_out(pt, s.mN[e] + T(.5)*Dm);
+      }
+      else if(s.src) pt = pt + s.phi[e]*s.src[e];
       s.phi_tmp[e] = pt;
 #pragma unroll
       for(int v=0; v<9; ++v)
@@ -586,6 +687,107 @@ __global__ void phi_sum_serial(Dims d, const T* __restrict__ phi, double* out)
   *out = sum;
 }
 
+// GoOrGrow::RelaxFreeEnergy (src/models/go-or-grow.cpp:42-119): dry
+// free-energy descent of phi (Cahn-Hilliard) and Q (molecular field) before
+// the dynamics. First sweep: H and mu at every site.
+template<typename T>
+__global__ void __launch_bounds__(256)
+relax_mu_kernel(Dims d, Params P, State<T> s)
+{
+  const int y = blockIdx.x*blockDim.x + threadIdx.x;
+  const int x = blockIdx.y*blockDim.y + threadIdx.y;
+  if(x >= d.LX || y >= d.LY) return;
+  const Nbr<T> nb = neighbours<T>(d, x + d.g, y + d.g);
+  const long long e = nb.e;
+  const T CC = T(P.CC), LL = T(P.LL), AA = T(P.AA), KK = T(P.KK);
+  const T B = T(s.ph.B), Snem = T(s.ph.Snem), phic = T(s.ph.phi_critical);
+  const T Qxx = s.Qxx[e];
+  const T Qyx = s.Qyx[e];
+  const T p = s.phi[e];
+  const T q2 = Qxx*Qxx + Qyx*Qyx;
+  const T term = Snem - q2;
+  const T dpc = p - phic;
+  const T mu_compress = dpc > T(0) ? B*dpc : T(0);
+  s.Hxx[e] = T(2)*CC*term*Qxx + LL*lap(s.Qxx, nb);
+  s.Hyx[e] = T(2)*CC*term*Qyx + LL*lap(s.Qyx, nb);
+  s.MU[e] = AA*p*(T(1)-p)*(T(1)-T(2)*p) + mu_compress - KK*lap(s.phi, nb);
+}
+
+// Second sweep: explicit descent step into phi_tmp and QN (swapped in after).
+template<typename T>
+__global__ void __launch_bounds__(256)
+relax_update_kernel(Dims d, Params P, State<T> s, double dt, int relax_phi, int relax_Q)
+{
+  const int y = blockIdx.x*blockDim.x + threadIdx.x;
+  const int x = blockIdx.y*blockDim.y + threadIdx.y;
+  if(x >= d.LX || y >= d.LY) return;
+  const Nbr<T> nb = neighbours<T>(d, x + d.g, y + d.g);
+  const long long e = nb.e;
+  const T rdt = T(dt);
+  if(relax_phi) s.phi_tmp[e] = s.phi[e] + rdt*T(P.GammaP)*lap(s.MU, nb);
+  else s.phi_tmp[e] = s.phi[e];
+  if(relax_Q)
+  {
+    s.QNxx[e] = s.Qxx[e] + rdt*T(P.GammaQ)*s.Hxx[e];
+    s.QNyx[e] = s.Qyx[e] + rdt*T(P.GammaQ)*s.Hyx[e];
+  }
+  else
+  {
+    s.QNxx[e] = s.Qxx[e];
+    s.QNyx[e] = s.Qyx[e];
+  }
+}
+
+// chi = m/phi where phi > 1e-12, else 0, at every domain site
+// (GoOrGrow::UpdatePhenotypeQuantities, src/models/go-or-grow.cpp:208-216)
+template<typename T>
+__global__ void __launch_bounds__(256)
+chi_kernel(Dims d, State<T> s)
+{
+  const int y = blockIdx.x*blockDim.x + threadIdx.x;
+  const int x = blockIdx.y*blockDim.y + threadIdx.y;
+  if(x >= d.LX || y >= d.LY) return;
+  const long long e = (y + d.g) + static_cast<long long>(d.EY)*(x + d.g);
+  const T p = s.phi[e];
+  s.chi[e] = p > T(1e-12) ? s.m[e]/p : T(0);
+}
+
+template<typename T>
+int relax_impl(const Dims& d, const Params& P, State<T>& s, int bc, unsigned nsteps,
+               double dt, int relax_phi, int relax_Q, double* sum_out, cudaStream_t st)
+{
+  const dim3 blk(64, 4);
+  const dim3 grd = site_grid(d.LX, d.LY, blk);
+  const int bcm = bc_mode(GOG, bc);
+  // Lyotropic::BoundaryConditionsFields (Q, phi) and the mu walls of :70-83
+  auto scalar_bc = [&](T* a, T* b, T* c) {
+    if(!bc) return;
+    ScalarBC<T> j{};
+    j.mode = bcm;
+    j.f[0] = a; j.f[1] = b; j.f[2] = c;
+    j.nf = c ? 3 : 1;
+    for(int i = 0; i < j.nf; ++i) j.kind[i] = BC_NEUMANN;
+    bc_scalar_kernel<T><<<1, 1024, 0, st>>>(d, j);
+  };
+  if(nsteps > 0 && (relax_phi || relax_Q))
+  {
+    for(unsigned it = 0; it < nsteps; ++it)
+    {
+      scalar_bc(s.Qxx, s.Qyx, s.phi);
+      relax_mu_kernel<T><<<grd, blk, 0, st>>>(d, P, s);
+      scalar_bc(s.MU, nullptr, nullptr);
+      relax_update_kernel<T><<<grd, blk, 0, st>>>(d, P, s, dt, relax_phi, relax_Q);
+      std::swap(s.phi, s.phi_tmp);
+      std::swap(s.Qxx, s.QNxx);
+      std::swap(s.Qyx, s.QNyx);
+    }
+    scalar_bc(s.Qxx, s.Qyx, s.phi);
+  }
+  // the relaxed total of phi, summed in site order (:114-118)
+  phi_sum_serial<T><<<1, 1, 0, st>>>(d, s.phi, sum_out);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
 template<typename T, bool DEV, int MODEL>
 int step_impl(const Dims& d, const Params& P, State<T>& s, int bc,
               unsigned nsteps, bool diag_last, cudaStream_t st)
@@ -601,7 +803,9 @@ int step_impl(const Dims& d, const Params& P, State<T>& s, int bc,
     ScalarBC<T> j{};
     j.mode = bcm_fields;
     j.f[0] = s.Qxx; j.f[1] = s.Qyx; j.nf = 2;
-    if(MODEL == LYO) { j.f[2] = s.phi; j.nf = 3; }
+    if(MODEL != NEM) { j.f[2] = s.phi; j.nf = 3; }
+    // go-or-grow walls treat m and chi as phi (src/models/go-or-grow.cpp:393-418)
+    if(MODEL == GOG) { j.f[3] = s.m; j.f[4] = s.chi; j.nf = 5; }
     for(int i = 0; i < j.nf; ++i) j.kind[i] = BC_NEUMANN;
     bc_scalar_kernel<T><<<1, 1024, 0, st>>>(d, j);
   };
@@ -609,7 +813,7 @@ int step_impl(const Dims& d, const Params& P, State<T>& s, int bc,
     if(!bc) return;
     ScalarBC<T> j{};
     j.mode = bcm_fields;
-    if(MODEL == LYO)
+    if(MODEL != NEM)
     {
       T* fs[9] = {s.uy, s.ux, s.uyp, s.uxp, s.MU, s.sXX, s.sYY, s.sYX, s.sXY};
       const int ks[9] = {BC_COPYDERIV, BC_COPYDERIV, BC_DIRICHLET0, BC_DIRICHLET0,
@@ -627,14 +831,21 @@ int step_impl(const Dims& d, const Params& P, State<T>& s, int bc,
     bc_scalar_kernel<T><<<1, 1024, 0, st>>>(d, j);
   };
 
+  // after UpdateFields: the new phi (and, for go-or-grow, m and chi =
+  // m/phi, UpdatePhenotypeQuantities of src/models/go-or-grow.cpp:208-216)
+  auto swap_fields = [&]() {
+    if(MODEL != NEM) std::swap(s.phi, s.phi_tmp);
+    if(MODEL == GOG) { std::swap(s.m, s.m_tmp); std::swap(s.chi, s.chi_tmp); }
+  };
+
   for(unsigned it = 0; it < nsteps; ++it)
   {
     fields_bc();
     uq_kernel<T, DEV, MODEL, false><<<grd, blk, 0, st>>>(d, P, s);
     fields2_bc();
-    if(MODEL == LYO && s.conserve_phi) phi_sum_serial<T><<<1, 1, 0, st>>>(d, s.phi, s.phisum);
+    if(MODEL != NEM && s.conserve_phi) phi_sum_serial<T><<<1, 1, 0, st>>>(d, s.phi, s.phisum);
     uf_kernel<T, DEV, MODEL, true><<<grd, blk, 0, st>>>(d, P, s);
-    if(MODEL == LYO) std::swap(s.phi, s.phi_tmp);
+    swap_fields();
     if(bc) bc_lb_kernel<T><<<1, 1024, 0, st>>>(d, s.ff, s.fn, lbk);
     move_kernel<T><<<egrd, blk, 0, st>>>(d, s.ff, s.fn, s.ff_tmp, s.fn_tmp);
     std::swap(s.ff, s.ff_tmp);
@@ -646,9 +857,9 @@ int step_impl(const Dims& d, const Params& P, State<T>& s, int bc,
       if(diag) uq_kernel<T, DEV, MODEL, true><<<grd, blk, 0, st>>>(d, P, s);
       else uq_kernel<T, DEV, MODEL, false><<<grd, blk, 0, st>>>(d, P, s);
       fields2_bc();
-      if(MODEL == LYO && s.conserve_phi) phi_sum_serial<T><<<1, 1, 0, st>>>(d, s.phi, s.phisum);
+      if(MODEL != NEM && s.conserve_phi) phi_sum_serial<T><<<1, 1, 0, st>>>(d, s.phi, s.phisum);
       uf_kernel<T, DEV, MODEL, false><<<grd, blk, 0, st>>>(d, P, s);
-      if(MODEL == LYO) std::swap(s.phi, s.phi_tmp);
+      swap_fields();
     }
   }
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
@@ -658,7 +869,7 @@ int step_impl(const Dims& d, const Params& P, State<T>& s, int bc,
 
 int lb_kind(int model, int bc)
 {
-  if(model == LYO)
+  if(model != NEM)
   {
     switch(bc)
     {
@@ -674,7 +885,7 @@ int lb_kind(int model, int bc)
 
 int bc_mode(int model, int bc)
 {
-  if(model == LYO)
+  if(model != NEM)
     return (bc == 1 || bc == 2) ? BCM_CHANNEL : (bc == 3 || bc == 4) ? BCM_BOX : BCM_PBC;
   return bc == 1 ? BCM_CHANNEL : BCM_PBC;
 }
@@ -690,15 +901,51 @@ int launches_unfused(int model, int bc, unsigned npc)
 int step_unfused_f64(const Dims& d, const Params& P, State<double>& s, int bc,
                      unsigned nsteps, bool diag_last, cudaStream_t st)
 {
-  return P.model == LYO ? step_impl<double, false, LYO>(d, P, s, bc, nsteps, diag_last, st)
-                        : step_impl<double, false, NEM>(d, P, s, bc, nsteps, diag_last, st);
+  switch(P.model)
+  {
+    case LYO: return step_impl<double, false, LYO>(d, P, s, bc, nsteps, diag_last, st);
+    case GOG: return step_impl<double, false, GOG>(d, P, s, bc, nsteps, diag_last, st);
+    default: return step_impl<double, false, NEM>(d, P, s, bc, nsteps, diag_last, st);
+  }
 }
 
 int step_unfused_f32(const Dims& d, const Params& P, State<float>& s, int bc,
                      unsigned nsteps, bool diag_last, cudaStream_t st)
 {
-  return P.model == LYO ? step_impl<float, true, LYO>(d, P, s, bc, nsteps, diag_last, st)
-                        : step_impl<float, true, NEM>(d, P, s, bc, nsteps, diag_last, st);
+  switch(P.model)
+  {
+    case LYO: return step_impl<float, true, LYO>(d, P, s, bc, nsteps, diag_last, st);
+    case GOG: return step_impl<float, true, GOG>(d, P, s, bc, nsteps, diag_last, st);
+    default: return step_impl<float, true, NEM>(d, P, s, bc, nsteps, diag_last, st);
+  }
+}
+
+int relax_unfused_f64(const Dims& d, const Params& P, State<double>& s, int bc,
+                      unsigned nsteps, double dt, int relax_phi, int relax_Q,
+                      double* sum_out, cudaStream_t st)
+{
+  return relax_impl<double>(d, P, s, bc, nsteps, dt, relax_phi, relax_Q, sum_out, st);
+}
+
+int relax_unfused_f32(const Dims& d, const Params& P, State<float>& s, int bc,
+                      unsigned nsteps, double dt, int relax_phi, int relax_Q,
+                      double* sum_out, cudaStream_t st)
+{
+  return relax_impl<float>(d, P, s, bc, nsteps, dt, relax_phi, relax_Q, sum_out, st);
+}
+
+int update_chi_f64(const Dims& d, State<double>& s, cudaStream_t st)
+{
+  const dim3 blk(64, 4);
+  chi_kernel<double><<<site_grid(d.LX, d.LY, blk), blk, 0, st>>>(d, s);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int update_chi_f32(const Dims& d, State<float>& s, cudaStream_t st)
+{
+  const dim3 blk(64, 4);
+  chi_kernel<float><<<site_grid(d.LX, d.LY, blk), blk, 0, st>>>(d, s);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 } // namespace mlb

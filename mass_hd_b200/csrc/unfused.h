@@ -34,4 +34,17 @@ int step_unfused_f64(const Dims& d, const Params& P, State<double>& s, int bc,
 int step_unfused_f32(const Dims& d, const Params& P, State<float>& s, int bc,
                      unsigned nsteps, bool diag_last, cudaStream_t st);
 
+// Go-or-grow dry relaxation: `nsteps` descent steps of phi and/or Q, then
+// the site-order sum of the relaxed phi into the device scalar sum_out.
+int relax_unfused_f64(const Dims& d, const Params& P, State<double>& s, int bc,
+                      unsigned nsteps, double dt, int relax_phi, int relax_Q,
+                      double* sum_out, cudaStream_t st);
+int relax_unfused_f32(const Dims& d, const Params& P, State<float>& s, int bc,
+                      unsigned nsteps, double dt, int relax_phi, int relax_Q,
+                      double* sum_out, cudaStream_t st);
+
+// chi = m/phi over the domain (after an upload of m or phi)
+int update_chi_f64(const Dims& d, State<double>& s, cudaStream_t st);
+int update_chi_f32(const Dims& d, State<float>& s, cudaStream_t st);
+
 } // namespace mlb

@@ -1,10 +1,12 @@
 // Model registrations of the standalone GPU build. Inside the reference tree
-// the same two declare_model calls go into src/declare_models.cpp (see
-// INTEGRATION.md); here the reference's names "lyotropic" and "nematic" are
-// registered as well, so unchanged reference runcards run on the GPU.
+// the same declare_model calls go into src/declare_models.cpp; here the
+// reference's names ("lyotropic", "lyotropic-with-division", "go-or-grow",
+// "nematic") are registered as well, so unchanged reference runcards run on
+// the GPU.
 #include "models.hpp"
 #include "lyotropic_gpu.hpp"
 #include "lyotropic_with_division_gpu.hpp"
+#include "go_or_grow_gpu.hpp"
 #include "nematic_gpu.hpp"
 
 void DeclareModels()
@@ -20,7 +22,11 @@ void DeclareModels()
   const char* div = "Lyotropic model with cell division and death, with its time step on a "
                     "B200 GPU.";
   declare_model<LyotropicWithDivisionGPU>("lyotropic-with-division-gpu", div);
+  const char* gog = "Go-or-grow lyotropic model with a passive phenotype field chi, with its "
+                    "time step on a B200 GPU.";
+  declare_model<GoOrGrowGPU>("go-or-grow-gpu", gog);
   declare_model<LyotropicGPU>("lyotropic", lyo);
   declare_model<LyotropicWithDivisionGPU>("lyotropic-with-division", div);
+  declare_model<GoOrGrowGPU>("go-or-grow", gog);
   declare_model<NematicGPU>("nematic", nem);
 }

@@ -47,7 +47,7 @@ void LyotropicGPU::Initialize()
     f->assign(N, 0.);
 
   mass_lb_params p{};
-  p.model = MASS_LB_LYOTROPIC;
+  p.model = DeviceModel();
   p.GammaQ = GammaQ; p.GammaP = GammaP; p.xi = xi; p.tauNem = tauNem;
   p.tauIso = tauIso; p.rho = rho; p.friction = friction; p.AA = AA; p.CC = CC;
   p.LL = LL; p.KK = KK; p.zeta = zeta; p.zetaI = zetaI; p.conc = conc;

@@ -41,6 +41,8 @@ protected:
 
   /** Refresh the host frame fields from the device. */
   void SyncFrame();
+  /** mass_lb_model of the device lattice this class creates */
+  virtual int DeviceModel() const { return MASS_LB_LYOTROPIC; }
 
 public:
   LyotropicGPU(unsigned LX, unsigned LY, unsigned BC);

@@ -12,11 +12,16 @@
 // JSON layout, so massPy's loadarchive reads them.
 //
 // The reference's `-t` (OpenMP threads) is accepted and ignored; zip
-// compression is not provided.
+// compression is not provided. --save-state=<file> writes the device state
+// at the end of the run as a full-precision checkpoint (mass_lb_save), which
+// a lattice of the same model and size loads with mass_lb_load.
 #include "header.hpp"
 #include "models.hpp"
 #include "error_msg.hpp"
 #include "random.hpp"
+#include "lyotropic_gpu.hpp"
+#include "nematic_gpu.hpp"
+#include "mass_lb_ext.h"
 
 #include <chrono>
 #include <fstream>
@@ -30,7 +35,7 @@ namespace {
 
 struct Program
 {
-  string runname = "./", model_name, inputname;
+  string runname = "./", model_name, inputname, save_state;
   unsigned LX = 0, LY = 0, nsteps = 0, ninfo = 1, nstart = 0, BC = 0, seed = 0;
   bool has_seed = false, no_write = false, no_warning = false, stop_at_warning = false;
   bool force_delete = false;
@@ -91,6 +96,7 @@ bool set_program_option(Program& p, const string& k, const string& v)
   else if(k == "force-delete" || k == "f") p.force_delete = true;
   else if(k == "verbose" || k == "v") to(v.empty() ? string("2") : v, p.verbose, k);
   else if(k == "threads" || k == "t") {}
+  else if(k == "save-state") p.save_state = v;
   else return false;
   return true;
 }
@@ -218,6 +224,15 @@ int run(int argc, char** argv)
   if(!p.no_write && p.nsteps >= p.nstart) write_frame(p.nsteps);
   const auto dt = chrono::duration<double>(chrono::steady_clock::now() - start).count();
   model->Post();
+  if(!p.save_state.empty())
+  {
+    mass_lb_handle* h = nullptr;
+    if(auto* l = dynamic_cast<LyotropicGPU*>(model.operator->())) h = l->device_lattice();
+    else if(auto* n = dynamic_cast<NematicGPU*>(model.operator->())) h = n->device_lattice();
+    if(!h) throw error_msg("model '", p.model_name, "' has no device lattice to save");
+    if(mass_lb_save(h, p.save_state.c_str()) != MASS_LB_OK)
+      throw error_msg("mass_lb_save: ", mass_lb_last_error());
+  }
   if(p.verbose) cout << "Total run time :                    " << dt << " s" << endl;
   return 0;
 }

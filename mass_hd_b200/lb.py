@@ -20,7 +20,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "lib", "libmass_lb.so")
 
-LYOTROPIC, NEMATIC = 0, 1
+LYOTROPIC, NEMATIC, GO_OR_GROW = 0, 1, 2
 FP64, FP32 = 0, 1
 
 FIELDS = ("ff", "QQxx", "QQyx", "phi", "n", "ux", "uy", "ux_phi", "uy_phi",
@@ -28,7 +28,7 @@ FIELDS = ("ff", "QQxx", "QQyx", "phi", "n", "ux", "uy", "ux_phi", "uy_phi",
           "sigmaXX", "sigmaYY", "sigmaYX", "sigmaXY", "sigma_bulk",
           "sigma_elastic_xx", "sigma_elastic_yx", "sigma_phase_field_xx",
           "sigma_phase_field_yx", "sigma_active_xx", "sigma_active_yx", "fn",
-          "QNxx", "QNyx", "phn")
+          "QNxx", "QNyx", "phn", "m", "chi", "mN")
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
 
 STATUS = {0: "OK", -1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "EUNSUPPORTED",
@@ -47,6 +47,27 @@ class Params(C.Structure):
                                   "rho", "friction", "AA", "CC", "LL", "KK",
                                   "zeta", "zetaI", "conc")
     ] + [("npc", C.c_uint)]
+
+
+class GogParams(C.Structure):
+    """mass_lb_go_or_grow_params (include/mass_lb_ext.h)."""
+    _fields_ = [(n, C.c_double) for n in ("B", "Snem", "Dchi", "Achi", "Ochi", "phiswitch",
+                                          "phi_critical")] + [("growTogether", C.c_int)]
+
+
+# GoOrGrow runcard names -> mass_lb_go_or_grow_params fields, with the
+# reference's initialisers (src/models/go-or-grow.hpp:9-13) as defaults
+GOG_PARAMS = (("B", "B", 0.0), ("Snem", "Snem", 1.0), ("Dchi", "Dchi", 0.0),
+              ("Achi", "Achi", 0.0), ("Ochi", "Ochi", 0.0), ("phiswitch", "phiswitch", 0.0),
+              ("phi-critical", "phi_critical", 1.0))
+
+
+def make_gog_params(params: dict) -> GogParams:
+    g = GogParams()
+    for key, field, default in GOG_PARAMS:
+        setattr(g, field, float(params.get(key, default)))
+    g.growTogether = int(params.get("growTogether", 0))
+    return g
 
 
 class Stats(C.Structure):
@@ -108,6 +129,8 @@ def load_library(build_if_missing: bool = False):
         "mass_lb_load": (C.c_int, [vp, C.c_char_p]),
         "mass_lb_set_phi_source": (C.c_int, [vp, dp]),
         "mass_lb_set_phi_conservation": (C.c_int, [vp, C.c_int, C.c_double]),
+        "mass_lb_set_go_or_grow_params": (C.c_int, [vp, C.POINTER(GogParams)]),
+        "mass_lb_relax_free_energy": (C.c_int, [vp, C.c_uint, C.c_double, C.c_int, C.c_int, dp]),
         "mass_lb_ensemble_create": (C.c_int, [C.c_int, C.POINTER(Params), C.POINTER(C.c_uint),
                                               C.POINTER(C.c_uint), C.POINTER(vp)]),
         "mass_lb_ensemble_destroy": (None, [vp]),
@@ -130,14 +153,14 @@ def _check(code: int):
 
 
 def make_params(model: int, params: dict) -> Params:
-    """Runcard names -> mass_lb_params. Lyotropic: GammaQ, GammaP, xi,
-    tauNem, tauIso, rho, friction, AA, CC, LL, KK, zeta, zetaI, conc, npc.
-    Nematic: Gamma, xi, tau, rho, friction, CC, LL, zeta, npc (Q_kBT and
-    u_kBT must be 0)."""
+    """Runcard names -> mass_lb_params. Lyotropic and go-or-grow: GammaQ,
+    GammaP, xi, tauNem, tauIso, rho, friction, AA, CC, LL, KK, zeta, zetaI,
+    conc, npc. Nematic: Gamma, xi, tau, rho, friction, CC, LL, zeta, npc
+    (Q_kBT and u_kBT must be 0)."""
     p = Params()
     p.model = model
     g = lambda k, d=0.0: float(params.get(k, d))
-    if model == LYOTROPIC:
+    if model in (LYOTROPIC, GO_OR_GROW):
         for k in ("GammaQ", "GammaP", "xi", "tauNem", "tauIso", "friction",
                   "AA", "CC", "LL", "KK", "zeta", "zetaI", "conc"):
             setattr(p, k, g(k))
@@ -172,6 +195,8 @@ class Lattice:
         h = C.c_void_p()
         _check(lib.mass_lb_create(C.byref(self._params), LX, LY, bc, precision, C.byref(h)))
         self.h = h
+        if model == GO_OR_GROW:
+            self.set_go_or_grow_params(params)
 
     @classmethod
     def _borrowed(cls, h, model: int, LX: int, LY: int, params: Params) -> "Lattice":
@@ -211,6 +236,9 @@ class Lattice:
                                              _dp(ph) if ph is not None else None))
 
     def upload_state(self, state: dict):
+        """ff, QQxx, QQyx, phi and (go-or-grow) m from a dict of arrays."""
+        if self.model == GO_OR_GROW and "m" in state:
+            self.upload_field("m", state["m"])
         self.upload(state["ff"], state["QQxx"], state["QQyx"], state.get("phi"))
 
     def upload_field(self, name: str, arr):
@@ -254,6 +282,23 @@ class Lattice:
         """The division models' conserve_phi correction
         Dp -= (sum phi - totalphi)/(LX*LY) (FP64 / walls only)."""
         _check(load_library().mass_lb_set_phi_conservation(self.h, int(bool(on)), float(totalphi)))
+
+    def set_go_or_grow_params(self, params: dict):
+        """Go-or-grow runcard values (B, Snem, Dchi, Achi, Ochi, phiswitch,
+        phi-critical, growTogether); missing keys take the reference's
+        defaults. Called by the constructor for GO_OR_GROW lattices."""
+        self._gog = make_gog_params(params)
+        _check(load_library().mass_lb_set_go_or_grow_params(self.h, C.byref(self._gog)))
+
+    def relax_free_energy(self, steps: int, dt: float = 1.0, relax_phi: bool = True,
+                          relax_Q: bool = True) -> float:
+        """GoOrGrow::RelaxFreeEnergy on the device; returns the relaxed
+        total of phi (the reference's totalphi)."""
+        out = C.c_double()
+        _check(load_library().mass_lb_relax_free_energy(self.h, int(steps), float(dt),
+                                                        int(bool(relax_phi)), int(bool(relax_Q)),
+                                                        C.byref(out)))
+        return out.value
 
     def synchronize(self):
         _check(load_library().mass_lb_synchronize(self.h))

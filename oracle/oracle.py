@@ -20,7 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_SO = os.path.join(HERE, "_build", "libmass_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libmass_ref.so")
 
-LYOTROPIC, NEMATIC = 0, 1
+LYOTROPIC, NEMATIC, GO_OR_GROW = 0, 1, 2
 
 # Runcard option names per model (src/models/lyotropic.cpp:556-599,
 # src/models/nematic.cpp:414-442).
@@ -32,6 +32,10 @@ NEM_OPTIONS = ("Gamma", "xi", "tau", "rho", "Q_kBT", "u_kBT", "friction", "CC",
 # LyotropicWithDivision::GetOptions (src/models/lyotropic-with-division.cpp:126-142)
 DIV_OPTIONS = ("alpha", "beta", "division-rate", "division-time", "division-radius",
                "death-rate", "death-time", "death-radius", "phi-critical")
+# GoOrGrow::GetOptions (src/models/go-or-grow.cpp:420-470)
+GOG_OPTIONS = ("B", "Snem", "Dchi", "Achi", "Ochi", "phiswitch", "growTogether",
+               "chi-config", "chi0", "chi-noise", "chi-length", "relax-steps",
+               "relax-dt", "relax-phi", "relax-Q")
 
 SCALAR_FIELDS_LYO = ("QQxx", "QQyx", "QNxx", "QNyx", "phi", "phn", "n", "ux",
                      "uy", "ux_phi", "uy_phi", "HHxx", "HHyx", "MU", "dxQQxx",
@@ -180,24 +184,34 @@ def _ref():
 
 
 class RefOracle:
-    """The reference's own Lyotropic / LyotropicWithDivision / Nematic model
-    objects (`division=True` selects "lyotropic-with-division")."""
+    """The reference's own Lyotropic / LyotropicWithDivision / GoOrGrow /
+    Nematic model objects (`division=True` selects "lyotropic-with-division";
+    model GO_OR_GROW selects "go-or-grow", which carries the division
+    options too)."""
 
     def __init__(self, model: int, params: dict, LX: int, LY: int, bc: int = 0,
                  division: bool = False):
         self.model, self.LX, self.LY, self.bc = model, LX, LY, bc
-        name = (b"lyotropic-with-division" if division else b"lyotropic") \
-            if model == LYOTROPIC else b"nematic"
+        if model == GO_OR_GROW:
+            name = b"go-or-grow"
+        elif model == LYOTROPIC:
+            name = b"lyotropic-with-division" if division else b"lyotropic"
+        else:
+            name = b"nematic"
         self.h = _ref().ref_new(name, LX, LY, bc)
         if not self.h:
             raise RuntimeError(_ref().ref_last_error().decode())
-        names = LYO_OPTIONS if model == LYOTROPIC else NEM_OPTIONS
-        if division:
+        names = NEM_OPTIONS if model == NEMATIC else LYO_OPTIONS
+        if division or model == GO_OR_GROW:
             names = names + DIV_OPTIONS
+        if model == GO_OR_GROW:
+            names = names + GOG_OPTIONS
         # every option gets a value: the reference leaves them uninitialised
         defaults = {"config": "circle", "level": 0.0, "conc": 1.0,
                     "radius": 0.0, "angle": 0.0, "noise": 0.0,
-                    "Q_kBT": 0.0, "u_kBT": 0.0, "npc": 1, "rho": 40.0}
+                    "Q_kBT": 0.0, "u_kBT": 0.0, "npc": 1, "rho": 40.0,
+                    "Snem": 1.0, "relax-dt": 1.0, "chi-config": "noise",
+                    "phi-critical": 1.0}
         for k in names:
             v = params.get(k, defaults.get(k, 0.0))
             r = _ref().ref_set_option(self.h, k.encode(), str(v).encode())

@@ -3,7 +3,8 @@
 // TEST INFRASTRUCTURE ONLY. This file is compiled together with the
 // reference sources (src/geometry.cpp, src/random.cpp, src/serialization.cpp,
 // src/models/lyotropic.cpp, src/models/nematic.cpp,
-// src/models/lyotropic-with-division.cpp) by oracle/Makefile into
+// src/models/lyotropic-with-division.cpp, src/models/go-or-grow.cpp) by
+// oracle/Makefile into
 // oracle/_ref/libmass_ref.so. Nothing in the product links it; the tests,
 // the golden-fixture generator and bench.py's reference arm load it through
 // ctypes as the checker / CPU baseline.
@@ -21,6 +22,7 @@
 #include "models.hpp"
 #include "models/lyotropic.hpp"
 #include "models/lyotropic-with-division.hpp"
+#include "models/go-or-grow.hpp"
 #include "models/nematic.hpp"
 #include "random.hpp"
 #include "serialization.hpp"
@@ -154,6 +156,27 @@ struct DivAccess : LyoAccessT<LyotropicWithDivision>
   }
 };
 
+// GoOrGrow (src/models/go-or-grow.cpp): the division masks plus the
+// phenotype fields m, mN, m_tmp, chi
+struct GogAccess : LyoAccessT<GoOrGrow>
+{
+  GogAccess(unsigned LX, unsigned LY, unsigned BC) : LyoAccessT(LX, LY, BC) {}
+  const std::vector<bool>* mask(const std::string& name) override
+  {
+    if(name=="division_mask") return &division_mask;
+    if(name=="death_mask") return &death_mask;
+    return nullptr;
+  }
+  ScalarField* scalar(const std::string& name) override
+  {
+    if(name=="m") return &m;
+    if(name=="mN") return &mN;
+    if(name=="m_tmp") return &m_tmp;
+    if(name=="chi") return &chi;
+    return LyoAccessT::scalar(name);
+  }
+};
+
 struct NemAccess : Nematic, RefModel
 {
   NemAccess(unsigned LX, unsigned LY, unsigned BC) : Nematic(LX, LY, BC) {}
@@ -207,7 +230,8 @@ extern "C" {
 /** Last error message of this thread (empty if none). */
 const char* ref_last_error() { return last_error.c_str(); }
 
-/** Construct "lyotropic", "lyotropic-with-division" or "nematic" with the
+/** Construct "lyotropic", "lyotropic-with-division", "go-or-grow" or
+ * "nematic" with the
  * factory arguments of
  * declare_model (src/models.hpp:197-205): (LX, LY, BC). */
 void* ref_new(const char* model, unsigned LX, unsigned LY, unsigned BC)
@@ -216,6 +240,7 @@ void* ref_new(const char* model, unsigned LX, unsigned LY, unsigned BC)
     RefModel* m = nullptr;
     if(std::strcmp(model, "lyotropic")==0) m = new LyoAccess(LX, LY, BC);
     else if(std::strcmp(model, "lyotropic-with-division")==0) m = new DivAccess(LX, LY, BC);
+    else if(std::strcmp(model, "go-or-grow")==0) m = new GogAccess(LX, LY, BC);
     else if(std::strcmp(model, "nematic")==0) m = new NemAccess(LX, LY, BC);
     else { last_error = "unknown model"; return nullptr; }
     m->opts = m->options();

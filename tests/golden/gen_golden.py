@@ -156,10 +156,45 @@ def gen_json_division():
     print("wrote json div")
 
 
+# go-or-grow: every phenotype term on, crowding active (phi-critical below
+# the circle's plateau), relaxation, division and death
+GOG_JSON = {"B": 0.1, "Snem": 1.0, "Dchi": 0.01, "Achi": 0.1, "Ochi": 0.05, "phiswitch": 0.5,
+            "growTogether": 1, "chi0": 0.6, "chi-noise": 0.05, "chi-length": 1.5,
+            "relax-steps": 10, "relax-dt": 1.0, "relax-phi": 1, "relax-Q": 1,
+            "alpha": 0.01, "beta": 0.005, "division-rate": 0.6, "division-time": 1,
+            "division-radius": 1.5, "death-rate": 0.3, "death-time": 2, "death-radius": 1.0,
+            "phi-critical": 0.9}
+# (fixture prefix, bc, chi-config, LX, LY)
+GOG_CASES = (("gog", 0, "noise", 16, 12), ("gog_box", 3, "front", 12, 10))
+
+
+def gen_json_gog(outdir: str = HERE):
+    """Reference output of GoOrGrow (masks, m and chi included in the frame)
+    after 5 steps: a periodic lattice with smoothed phenotype noise, and a
+    box with the phenotype front. Written to `outdir`."""
+    for prefix, bc, cfg, LX, LY in GOG_CASES:
+        params = dict(LYO, config="circle", radius=3.5, level=0.0, conc=1.0, angle=0.0,
+                      noise=1.0, zeta=0.02)
+        params.update(GOG_JSON)
+        params["chi-config"] = cfg
+        r = O.RefOracle(O.GO_OR_GROW, params, LX, LY, bc)
+        r.configure(7)
+        r.step(5)
+        with tempfile.TemporaryDirectory() as d:
+            pth = os.path.join(d, "p.json")
+            fr = os.path.join(d, "f.json")
+            r.write_params(pth, 5, 5, 0, "go-or-grow")
+            r.write_frame(fr)
+            for src, dst in ((pth, f"{prefix}_parameters.json"), (fr, f"{prefix}_frame5.json")):
+                with open(src) as fi, open(os.path.join(outdir, dst), "w") as fo:
+                    fo.write(fi.read())
+    print("wrote json go-or-grow")
+
+
 if __name__ == "__main__":
     if not O.ref_available():
         O.build(ref=True)
-    which = sys.argv[1:] or ["cases", "configure", "json", "division"]
+    which = sys.argv[1:] or ["cases", "configure", "json", "division", "go-or-grow"]
     if "cases" in which:
         gen_cases()
     if "configure" in which:
@@ -168,3 +203,5 @@ if __name__ == "__main__":
         gen_json()
     if "division" in which:
         gen_json_division()
+    if "go-or-grow" in which:
+        gen_json_gog()

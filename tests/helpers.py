@@ -46,3 +46,11 @@ def rel_l2(a, b):
 def ff_dev(ff, rho=40.0):
     """Populations minus their rest-state part t_v*rho."""
     return np.asarray(ff).reshape(-1, 9) - W_EQ[None, :] * rho
+
+
+def bits_equal(a, b):
+    """Bit-for-bit equality of two float64 arrays (distinguishes -0 from +0,
+    which np.array_equal does not)."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    return a.shape == b.shape and np.array_equal(a.view(np.uint64), b.view(np.uint64))

@@ -42,7 +42,9 @@ def test_abi_version_and_names():
     assert lib.mass_lb_field_name(0) == b"ff"
     assert lib.mass_lb_field_name(26) == b"sigma_active_yx"
     assert lib.mass_lb_field_name(99) is None
-    assert [lib.mass_lb_field_name(i).decode() for i in range(31)] == list(M.FIELDS)
+    assert [lib.mass_lb_field_name(i).decode() for i in range(len(M.FIELDS))] == list(M.FIELDS)
+    assert lib.mass_lb_field_name(len(M.FIELDS)) is None
+    assert lib.mass_lb_field_name(31) == b"m" and lib.mass_lb_field_name(32) == b"chi"
 
 
 def test_create_rejects_bad_arguments_without_device():

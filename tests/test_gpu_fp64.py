@@ -11,7 +11,8 @@ import numpy as np
 import pytest
 
 from oracle import oracle as O
-from tests.helpers import LYO_ALL, LYO_C1, NEM_ALL, NEM_C2, golden_cases, load_golden, rel_l2
+from tests.helpers import (LYO_ALL, LYO_C1, NEM_ALL, NEM_C2, bits_equal, golden_cases, load_golden,
+                           rel_l2)
 
 pytestmark = pytest.mark.gpu
 
@@ -30,7 +31,7 @@ def test_fp64_matches_reference_golden(path):
         name = k[4:]
         got = L.get(name)
         want = z[k]
-        assert np.array_equal(got, want), (name, float(np.max(np.abs(got - want))))
+        assert bits_equal(got, want), (name, float(np.max(np.abs(got - want))))
 
 
 CASES = [
@@ -63,7 +64,7 @@ def test_fp64_matches_oracle_100_steps(model, params, LX, LY, bc):
     for n in names:
         got, want = L.get(n), P.get(n)
         assert rel_l2(got, want) <= 1e-10, n
-        assert np.array_equal(got, want), n
+        assert bits_equal(got, want), n
 
 
 def test_fp64_steps_split_equal_single_call():
@@ -90,7 +91,7 @@ def test_fp64_npc3_matches_oracle():
     L.upload_state(st)
     L.step(9)
     for n in ("ff", "fn", "QQxx", "QNxx", "phi", "phn"):
-        assert np.array_equal(L.get(n), P.get(n)), n
+        assert bits_equal(L.get(n), P.get(n)), n
 
 
 def test_fp64_odd_tiny_lattices():
@@ -103,8 +104,8 @@ def test_fp64_odd_tiny_lattices():
         L = M.Lattice(O.LYOTROPIC, LYO_ALL, LX, LY, 0, M.FP64)
         L.upload_state(st)
         L.step(5)
-        assert np.array_equal(L.get("ff"), P.get("ff")), (LX, LY)
-        assert np.array_equal(L.get("phi"), P.get("phi")), (LX, LY)
+        assert bits_equal(L.get("ff"), P.get("ff")), (LX, LY)
+        assert bits_equal(L.get("phi"), P.get("phi")), (LX, LY)
 
 
 def test_runtime_checks_conservation_and_nan():

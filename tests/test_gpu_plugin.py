@@ -86,6 +86,72 @@ def test_fp64_division_output_identical_to_reference(tmp_path):
         assert got == want, name
 
 
+@pytest.mark.parametrize("prefix,bc,cfg,LX,LY", [("gog", 0, "noise", 16, 12),
+                                                  ("gog_box", 3, "front", 12, 10)])
+def test_fp64_go_or_grow_output_identical_to_reference(tmp_path, prefix, bc, cfg, LX, LY):
+    """GoOrGrow through the plugin: lyotropic configuration, device
+    relaxation, phenotype noise (smoothed on the host) or front, masks from
+    the reference's random stream; parameters.json and frame5.json (m and
+    chi included) text-identical to the reference's (tests/golden/gen_golden.py
+    go-or-grow)."""
+    opts = dict(LYO, config="circle", radius=3.5, level=0.0, conc=1.0, angle=0.0, noise=1.0,
+                zeta=0.02)
+    opts.update({"B": 0.1, "Snem": 1.0, "Dchi": 0.01, "Achi": 0.1, "Ochi": 0.05,
+                 "phiswitch": 0.5, "growTogether": 1, "chi0": 0.6, "chi-noise": 0.05,
+                 "chi-length": 1.5, "relax-steps": 10, "relax-dt": 1.0, "relax-phi": 1,
+                 "relax-Q": 1, "alpha": 0.01, "beta": 0.005, "division-rate": 0.6,
+                 "division-time": 1, "division-radius": 1.5, "death-rate": 0.3,
+                 "death-time": 2, "death-radius": 1.0, "phi-critical": 0.9,
+                 "chi-config": cfg})
+    opts.update(LX=LX, LY=LY, bc=bc, nsteps=5, ninfo=5, seed=7, precision="fp64")
+    card = tmp_path / "run.dat"
+    runcard(card, "go-or-grow", opts)
+    run(card, tmp_path / "out")
+    for name, gold in (("parameters.json", f"{prefix}_parameters.json"),
+                       ("frame5.json", f"{prefix}_frame5.json")):
+        got = (tmp_path / "out" / name).read_text()
+        want = open(os.path.join(GOLDEN, gold)).read()
+        assert got == want, name
+
+
+@pytest.mark.parametrize("nsteps", [0, 5])
+def test_fp64_go_or_grow_state_bit_identical_to_reference(tmp_path, nsteps):
+    """The plugin's configured state (nsteps = 0: lyotropic set-up, device
+    relaxation, host phenotype noise and smoothing) and its state after 5
+    steps, saved at full precision by --save-state, against the reference's
+    in-memory fields bit for bit (signs of zero included)."""
+    import sys
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    from tests.helpers import bits_equal
+    import mass_hd_b200 as M
+    gog = {"B": 0.1, "Snem": 1.0, "Dchi": 0.01, "Achi": 0.1, "Ochi": 0.05,
+           "phiswitch": 0.5, "growTogether": 1, "chi0": 0.6, "chi-noise": 0.05,
+           "chi-length": 1.5, "relax-steps": 10, "relax-dt": 1.0, "relax-phi": 1,
+           "relax-Q": 1, "alpha": 0.01, "beta": 0.005, "division-rate": 0.6,
+           "division-time": 1, "division-radius": 1.5, "death-rate": 0.3,
+           "death-time": 2, "death-radius": 1.0, "phi-critical": 0.9, "chi-config": "noise"}
+    opts = dict(LYO, config="circle", radius=3.5, level=0.0, conc=1.0, angle=0.0, noise=1.0,
+                zeta=0.02)
+    opts.update(gog)
+    LX, LY = 16, 12
+    opts.update(LX=LX, LY=LY, nsteps=nsteps, ninfo=5, seed=7, precision="fp64")
+    card = tmp_path / "run.dat"
+    runcard(card, "go-or-grow", opts)
+    state = tmp_path / "state.ckpt"
+    run(card, tmp_path / "out", "--no-write", f"--save-state={state}")
+    ref = O.RefOracle(O.GO_OR_GROW, {k: v for k, v in opts.items()
+                                     if k not in ("LX", "LY", "nsteps", "ninfo", "seed",
+                                                  "precision")}, LX, LY, 0)
+    ref.configure(7)
+    ref.step(nsteps)
+    lat = M.Lattice(M.GO_OR_GROW, opts, LX, LY, 0, M.FP64)
+    lat.load(str(state))
+    for n in ("ff", "QQxx", "QQyx", "phi", "m", "chi"):
+        assert bits_equal(lat.get(n), ref.get(n)), n
+    lat.close()
+
+
 def load_frame(path):
     d = json.load(open(path))["data"]
     return {k: np.asarray(v["value"], dtype=float) for k, v in d.items()}

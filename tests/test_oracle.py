@@ -83,3 +83,25 @@ def test_port_conserves_mass():
     f1, p1 = P.totals()
     assert abs(f1 - f0) < 1e-8 * f0
     assert abs(p1 - p0) < 1e-9 * LX * LY
+
+
+@needs_ref
+def test_reference_go_or_grow_reproduces_golden_json(tmp_path):
+    """The reference build's GoOrGrow (configure with relaxation and
+    phenotype set-up, 5 steps with division and death) writes exactly the
+    committed fixtures, which the GPU plugin test compares against."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "gen_golden", os.path.join(os.path.dirname(__file__), "golden", "gen_golden.py"))
+    gen = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gen)
+    gen.gen_json_gog(str(tmp_path))
+    for prefix, *_ in gen.GOG_CASES:
+        for part in ("parameters", "frame5"):
+            name = f"{prefix}_{part}.json"
+            got = (tmp_path / name).read_text()
+            want = open(os.path.join(os.path.dirname(__file__), "golden", name)).read()
+            assert got == want, name
+    frame = json.loads(open(os.path.join(os.path.dirname(__file__), "golden",
+                                         "gog_frame5.json")).read())["data"]
+    assert {"m", "chi", "division_mask", "death_mask"} <= set(frame)
