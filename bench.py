@@ -1,7 +1,8 @@
 """Benchmark of the FP32 lyotropic Model::Step() on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--size L] [--model lyotropic|nematic] [--precision fp32|fp64]
+                    [--size L] [--model lyotropic|nematic|go-or-grow]
+                    [--precision fp32|fp64]
 
 Workload (default): the lyotropic model on a periodic 4096 x 4096 lattice in
 FP32 - the throughput target named for this path - with the physics of the
@@ -24,6 +25,16 @@ is the max over ranks.
 --impl reference times the reference's own OpenMP build of the same step
 (oracle/_ref, compiled from the reference sources) on the host cores, on a
 bounded sample of the same workload.
+
+--model go-or-grow measures the model every shipped runcard uses, with the
+physics and division settings of the reference's cases/test/test.dat on an
+L x L periodic lattice (default 500, the runcards' size). `value` times
+the device step alone (a fixed growth-rate plane, CUDA events); `e2e` runs
+the mass-gpu driver on the runcard (Configure with the device relaxation,
+then the time loop with the division masks drawn on the host every step
+they are due, as Model::Step() does) and divides by the driver's own
+time-loop clock. The CPU baseline and the reference arm time the
+reference's GoOrGrow::Step(), masks included, on all host cores.
 """
 from __future__ import annotations
 
@@ -52,10 +63,33 @@ NEM_C2 = dict(Gamma=0.3, xi=0.7, tau=1.5, rho=40.0, friction=0.0, CC=0.1,
               LL=0.05, zeta=0.02, npc=1)
 
 
+# go-or-grow: the physics and division settings of the reference's
+# cases/test/test.dat (its lattice is 100^2; the study runcards use 500^2)
+GOG_RUNCARD = dict(GammaQ=0.3, GammaP=5e-2, zeta=0.0, zetaI=0.0, friction=0.0, tauNem=1.0,
+                   tauIso=1.0, AA=0.03, CC=0.1, LL=0.002, KK=0.06, rho=40.0, xi=0.3, B=0.1,
+                   Snem=1.0, config="circle", level=50, conc=1.0, noise=1.0, angle=0,
+                   npc=1, **{"relax-steps": 2000, "relax-dt": 1.0, "relax-phi": 1,
+                             "relax-Q": 1, "chi-config": "noise", "chi0": 1.0,
+                             "chi-noise": 0.0, "chi-length": 0.0, "Dchi": 0.0,
+                             "Achi": 0.0, "Ochi": 0.0, "phiswitch": 0.0,
+                             "growTogether": 0, "beta": 0.0, "death-rate": 0.0,
+                             "death-time": 1, "death-radius": 0.0,
+                             "division-rate": 0.1, "division-time": 2, "alpha": 0.001,
+                             "phi-critical": 1.2, "division-radius": 3})
+
+
+def gog_runcard(L: int) -> dict:
+    """The runcard at lattice L: the circle's radius scales with L (20 at
+    the runcard's 100^2)."""
+    p = dict(GOG_RUNCARD)
+    p["radius"] = 0.2 * L
+    return p
+
+
 def algorithmic_bytes(model: str, precision: str) -> int:
     """Primary state read once and written once per site-update:
-    (9 populations + Qxx + Qyx [+ phi]) x 2 x element size."""
-    planes = 12 if model == "lyotropic" else 11
+    (9 populations + Qxx + Qyx [+ phi [+ m]]) x 2 x element size."""
+    planes = {"lyotropic": 12, "nematic": 11, "go-or-grow": 13}[model]
     return planes * 2 * (4 if precision == "fp32" else 8)
 
 
@@ -243,18 +277,53 @@ def cpu_reference_run(model: str, L: int, steps: int, warmup: int, budget_s: flo
     return rate, kind, threads, sample
 
 
+def cpu_reference_gog(L: int, steps: int, warmup: int, budget_s: float):
+    """The reference's GoOrGrow::Step() (division masks included) on all host
+    cores, on the runcard at lattice L. Configure() runs without the dry
+    relaxation (it is not part of Step()). Returns (site-updates/s, kind,
+    cores, sample description)."""
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    p = gog_runcard(L)
+    p["relax-steps"] = 0
+    m = O.RefOracle(O.GO_OR_GROW, p, L, L, 0)
+    m.configure(1001)
+    # blocks of 6 steps hold the masks' schedule (division every 3rd step,
+    # death every 2nd) in its true proportion
+    for _ in range(warmup):
+        m.time_steps(6, cores)
+    times = []
+    t_start = time.perf_counter()
+    for _ in range(max(1, steps)):
+        times.append(m.time_steps(6, cores) / 6)
+        if time.perf_counter() - t_start > budget_s:
+            break
+    per_step = statistics.median(times)
+    sample = (f"go-or-grow {L}x{L} periodic FP64 (cases/test/test.dat physics, division masks "
+              f"every 3rd step, death masks every 2nd), {len(times)} timed blocks of 6 Step() "
+              f"calls after {warmup} warm-up block(s), median {per_step:.4f} s per step")
+    return L * L / per_step, "reference", cores, sample
+
+
 def run_reference(args):
     rank, world, _ = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), 0
     if rank != 0:
         return 0
-    rate, kind, cores, sample = cpu_reference_run(args.model, args.size, args.steps,
-                                                  max(1, min(args.warmup, 2)), 240.0)
+    if args.model == "go-or-grow":
+        rate, kind, cores, sample = cpu_reference_gog(args.size, args.steps,
+                                                      max(1, min(args.warmup, 2)), 120.0)
+    else:
+        rate, kind, cores, sample = cpu_reference_run(args.model, args.size, args.steps,
+                                                      max(1, min(args.warmup, 2)), 240.0)
     line = {
         "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": f"{args.model} {args.size}x{args.size} periodic", "model": args.model,
+        "config": {"workload": (f"go-or-grow {args.size}x{args.size} periodic, cases/test/test.dat "
+                                f"physics and division settings" if args.model == "go-or-grow"
+                                else f"{args.model} {args.size}x{args.size} periodic"),
+                   "model": args.model,
                    "LX": args.size, "LY": args.size, "precision": "fp64 (reference build)"},
         "cpu_baseline": {"value": rate, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -263,11 +332,160 @@ def run_reference(args):
     return 0
 
 
+def driver_path() -> str:
+    host = os.path.join(ROOT, "mass_hd_b200", "host")
+    exe = os.path.join(host, "_build", "mass-gpu")
+    if not os.path.exists(exe):
+        subprocess.run(["make", "-s", "-C", host], check=True)
+    return exe
+
+
+def run_driver_gog(L: int, nsteps: int, precision: str, workdir: str) -> float:
+    """mass-gpu on the go-or-grow runcard at lattice L; returns the driver's
+    own clock around its time loop (seconds)."""
+    card = os.path.join(workdir, f"gog_{L}.dat")
+    opts = gog_runcard(L)
+    opts.update(LX=L, LY=L, nsteps=nsteps, ninfo=max(nsteps, 1), seed=1001, precision=precision)
+    with open(card, "w") as fh:
+        fh.write("model = go-or-grow\n")
+        for k, v in opts.items():
+            fh.write(f"{k} = {v}\n")
+    r = subprocess.run([driver_path(), card, "--no-write", "-o", workdir], capture_output=True,
+                       text=True, timeout=900)
+    if r.returncode != 0:
+        raise RuntimeError(f"mass-gpu failed: {r.stderr.strip()[-400:]}")
+    for line in r.stdout.splitlines():
+        if line.startswith("Total run time"):
+            return float(line.split(":")[1].split()[0])
+    raise RuntimeError("mass-gpu printed no run time")
+
+
+def gog_state(L: int, seed: int):
+    """Runcard-like go-or-grow state: random director (S=1), tanh phi disk of
+    radius L/5, m = phi (chi0 = 1, no phenotype noise), rest populations."""
+    st = synthetic_state("lyotropic", L, seed)
+    x = np.arange(L)[:, None] - L / 2
+    y = np.arange(L)[None, :] - L / 2
+    r = np.sqrt(x * x + y * y).reshape(-1)
+    st["phi"] = 0.5 * (1 - np.tanh((r - 0.2 * L) / 2))
+    st["m"] = np.maximum(st["phi"], 0.0)
+    return st
+
+
+def run_ours_gog(args):
+    """--model go-or-grow (see the module docstring)."""
+    import tempfile
+
+    import torch
+
+    import mass_hd_b200 as M
+
+    rank, world, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    prec = M.FP32 if args.precision == "fp32" else M.FP64
+    L = args.size
+    sites = L * L
+    p = gog_runcard(L)
+    st = gog_state(L, seed=1 + rank)
+    lat = M.Lattice(M.GO_OR_GROW, p, L, L, 0, prec)
+    lat.upload_state(st)
+    # the dry relaxation of Configure(), timed on its own
+    t0 = time.perf_counter()
+    lat.relax_free_energy(int(p["relax-steps"]), p["relax-dt"], True, True)
+    relax_s = time.perf_counter() - t0
+    # a fixed growth-rate plane: alpha on every 7th site with phi >= 0.5
+    phi = lat.get("phi")
+    rate = np.where((phi >= 0.5) & (np.arange(sites) % 7 == 0), p["alpha"], 0.0)
+    lat.set_phi_source(rate)
+    stream = torch.cuda.ExternalStream(lat.stream)
+    for _ in range(max(args.warmup, 3)):
+        lat.step(1)
+    lat.synchronize()
+    sampler = ClockSampler(local) if rank == 0 else None
+    barrier(world)
+    torch.cuda.synchronize()
+    if sampler:
+        sampler.start()
+        time.sleep(0.3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    # L2: the FP32 state of a 500^2 lattice (~60 MB with all sweep fields)
+    # stays in the 126 MB L2 between steps, as it does in a real run
+    e0.record(stream)
+    for _ in range(args.steps):
+        lat.step(1)
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    barrier(world)
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    clocks = sampler.stop() if sampler else None
+    ms_per_step = ms / args.steps
+    value = whole_job_rate(sites, world, args.steps, ms)
+    launches = args.steps * lat.launches_per_step
+    bps = algorithmic_bytes("go-or-grow", args.precision)
+    peak, peak_kind = measured_hbm_peak()
+    achieved = sites * bps / (ms_per_step / 1e3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind, "bytes_per_site": bps,
+                "traffic": None,
+                "note": "whole step (unfused sweeps, ~5 launches) against the primary state's "
+                        "bytes; small lattices are launch-bound"}
+    lat.close()
+
+    # end to end: the driver on the runcard (host masks, Configure excluded)
+    n_e2e = max(args.steps, 30)
+    with tempfile.TemporaryDirectory() as d:
+        run_driver_gog(L, 3, args.precision, d)          # warm-up (build, first launch)
+        t_loop = run_driver_gog(L, n_e2e, args.precision, d)
+    t_loop = max_over_ranks(t_loop, world)
+    # per step: phi (8 B/site) down and the rate plane (8 B/site) up on the
+    # steps that redraw a mask: division every 3rd, death every 2nd step
+    redraw = sum(1 for t in range(n_e2e) if t % 3 == 0 or t % 2 == 0) / n_e2e
+    e2e = {"value": whole_job_rate(sites, world, n_e2e, t_loop * 1e3), "unit": UNIT,
+           "h2d_bytes_per_step": int(8 * sites * redraw),
+           "d2h_bytes_per_step": int(8 * sites * redraw),
+           "e2e_steps": n_e2e,
+           "note": "mass-gpu driver on the runcard: Step() = host mask draw when due "
+                   "(reference RNG stream, stamped circles) + device step; driver clock "
+                   "around the time loop"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate_c, kind, cores, sample = cpu_reference_gog(L, 5, 1, 30.0)
+        cpu = {"value": rate_c, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if args.precision == "fp32" else "f64",
+            "data": "synthetic (seeded random director S=1, tanh phi disk R=L/5, m = phi)",
+            "config": {"workload": f"go-or-grow {args.precision.upper()} {L}x{L} periodic, "
+                                   f"cases/test/test.dat physics and division settings",
+                       "model": "go-or-grow", "LX": L, "LY": L, "precision": args.precision,
+                       "lattices": world, "relax_2000_steps_s": relax_s,
+                       "l2": "state fits in L2 (as in a real run), no flush"},
+            "gpu_launches": launches,
+            "roofline": roofline,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
 def run_ours(args):
     import torch
 
     import mass_hd_b200 as M
 
+    if args.model == "go-or-grow":
+        return run_ours_gog(args)
     rank, world, local = dist_setup(args.gpus)
     torch.cuda.set_device(local)
     model = args.model
@@ -398,11 +616,14 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--size", type=int, default=4096)
-    ap.add_argument("--model", default="lyotropic", choices=["lyotropic", "nematic"])
+    ap.add_argument("--size", type=int, default=None,
+                    help="lattice side (default 4096; 500 for go-or-grow)")
+    ap.add_argument("--model", default="lyotropic", choices=["lyotropic", "nematic", "go-or-grow"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    if args.size is None:
+        args.size = 500 if args.model == "go-or-grow" else 4096
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -3,6 +3,7 @@
 #include "error_msg.hpp"
 #include "random.hpp"
 #include "mass_lb_ext.h"
+#include "mask_draw.hpp"
 
 #include <algorithm>
 #include <array>
@@ -10,18 +11,6 @@
 
 using namespace std;
 namespace opt = boost::program_options;
-
-namespace {
-
-// unsigned distance on a periodic axis of length L, as the reference's
-// wrap(diff(a, b), L) (src/tools.hpp:30-63)
-unsigned periodic_distance(unsigned a, unsigned b, unsigned L)
-{
-  const unsigned d = a > b ? a - b : b - a;
-  return std::min(d % L, L - d % L);
-}
-
-} // namespace
 
 LyotropicWithDivisionGPU::LyotropicWithDivisionGPU(unsigned LX_, unsigned LY_, unsigned BC_)
   : LyotropicGPU(LX_, LY_, BC_)
@@ -61,7 +50,6 @@ void LyotropicWithDivisionGPU::SetMasks()
       if(r != MASS_LB_OK) throw error_msg(mass_gpu::abi_error("mass_lb_download", r));
       have_phi = true;
     }
-    mask.assign(DomainSize, false);
     // centres: one random_real() per site with phi >= .5, in site order
     std::vector<std::array<unsigned, 2>> centers;
     for(unsigned k = 0; k < DomainSize; ++k)
@@ -74,17 +62,9 @@ void LyotropicWithDivisionGPU::SetMasks()
           centers.push_back({GetXPosition(k), GetYPosition(k)});
       }
     }
-    const double r2 = ceil(radius*radius);
-    for(unsigned k = 0; k < DomainSize; ++k)
-    {
-      const unsigned yk = GetYPosition(k), xk = GetXPosition(k);
-      for(const auto& c : centers)
-        if(pow(periodic_distance(yk, c[1], LY), 2) + pow(periodic_distance(xk, c[0], LX), 2) <= r2)
-        {
-          mask[k] = true;
-          break;
-        }
-    }
+    // the circles around the centres, stamped (the same set as the
+    // reference's per-site test over all centres)
+    mass_gpu::stamp_circles(mask, centers, radius, LX, LY);
     changed = true;
   };
   if(not division_count--)

@@ -46,6 +46,14 @@ def test_plugin_compiles_against_reference_headers():
     subprocess.run(["make", "-s", "-C", HOST, "refcheck"], check=True)
 
 
+def test_mask_stamping_equals_reference_circle_test(tmp_path):
+    """The division masks are stamped around their centres; the set equals
+    the reference's test of every site against every centre."""
+    exe = compile_native(tmp_path, "mask_stamp.cpp", ["-I", HOST])
+    out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout
+    assert int(out.split()[-1]) == 7 * 10 * 4
+
+
 def test_compat_random_matches_reference_stream(tmp_path):
     exe = compile_native(tmp_path, "print_random.cpp", [os.path.join(COMPAT, "random.cpp")])
     out = subprocess.run([exe, "42", "64"], check=True, capture_output=True, text=True).stdout
