@@ -3,19 +3,32 @@
 //   { "id" : ..., "version" : ..., "data" : { "name" : { "type" : ...,
 //   "value" : ... }, ... } }
 // two-space indentation, iterables as "[ a, b ]" and typed "array(...)",
-// scalars through a default std::stringstream (6 significant digits),
-// NaN detection. `auto_name(x)` pairs a member with its source name, which
-// becomes the JSON key. Standalone build of the GPU plugin only.
+// scalars as a default std::stringstream prints them (6 significant
+// digits), NaN detection. `auto_name(x)` pairs a member with its source
+// name, which becomes the JSON key. Standalone build of the GPU plugin only.
+//
+// Frames are large (a 500^2 go-or-grow frame is 74 MB of text), so the
+// field arrays are not printed value by value through a stringstream as the
+// reference does: doubles go through std::to_chars with the general format
+// at precision 6, which yields the same characters as `stringstream << v`
+// (printf's %.6g), and long arrays are formatted in chunks on all host
+// threads, then joined in order. The text is identical.
 #ifndef MASS_GPU_COMPAT_SERIALIZATION_HPP_
 #define MASS_GPU_COMPAT_SERIALIZATION_HPP_
 
+#include <algorithm>
 #include <array>
+#include <cstdio>
 #include <ostream>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <type_traits>
 #include <utility>
 #include <vector>
+#if __cplusplus >= 201703L
+#include <charconv>
+#endif
 
 #define auto_name(obj) std::pair<decltype(obj)&, std::string> {obj, #obj}
 
@@ -39,6 +52,87 @@ template<class T, class A> struct tname<std::vector<T, A>>
 { static std::string get() { return "array(" + tname<T>::get() + ")"; } };
 template<class T, std::size_t N> struct tname<std::array<T, N>>
 { static std::string get() { return "array(" + tname<T>::get() + ")"; } };
+
+// one value as `std::stringstream() << v` prints it; returns the end
+inline char* put_value(char* p, double v)
+{
+#if __cplusplus >= 201703L
+  return std::to_chars(p, p + 32, v, std::chars_format::general, 6).ptr;
+#else
+  return p + std::snprintf(p, 32, "%.6g", v);
+#endif
+}
+inline char* put_value(char* p, bool b) { *p++ = b ? '1' : '0'; return p; }
+
+// element types formatted in bulk, and the most characters one takes
+template<class T> struct flat : std::false_type {};
+template<> struct flat<double> : std::true_type { static constexpr std::size_t chars = 34; };
+template<> struct flat<bool> : std::true_type { static constexpr std::size_t chars = 3; };
+template<std::size_t N> struct flat<std::array<double, N>> : std::true_type
+{ static constexpr std::size_t chars = 4 + 34*N; };
+
+inline char* put_elem(char* p, double v, bool& bad) { if(v != v) bad = true; return put_value(p, v); }
+inline char* put_elem(char* p, bool b, bool&) { return put_value(p, b); }
+template<std::size_t N>
+inline char* put_elem(char* p, const std::array<double, N>& a, bool& bad)
+{
+  *p++ = '['; *p++ = ' ';
+  for(std::size_t i = 0; i < N; ++i)
+  {
+    if(i) { *p++ = ','; *p++ = ' '; }
+    p = put_elem(p, a[i], bad);
+  }
+  *p++ = ' '; *p++ = ']';
+  return p;
+}
+// "[ a, b, ... ]" of a whole array, in parallel chunks joined in order
+template<class V>
+std::string format_array(const V& c, bool& bad)
+{
+  using T = typename V::value_type;
+  const std::size_t n = c.size();
+  const std::size_t per = flat<T>::chars;
+  const std::size_t chunk = 1 << 15;
+  const std::size_t nchunks = (n + chunk - 1)/chunk;
+  std::vector<std::string> parts(nchunks);
+  std::vector<char> badv(nchunks, 0);
+  auto work = [&](std::size_t first, std::size_t stride) {
+    std::vector<char> buf((chunk + 1)*per);
+    for(std::size_t j = first; j < nchunks; j += stride)
+    {
+      char* p = buf.data();
+      bool b = false;
+      const std::size_t lo = j*chunk, hi = std::min(n, lo + chunk);
+      typename V::const_iterator it = c.begin();
+      std::advance(it, lo);
+      for(std::size_t i = lo; i < hi; ++i, ++it)
+      {
+        if(i) { *p++ = ','; *p++ = ' '; }
+        p = put_elem(p, *it, b);
+      }
+      parts[j].assign(buf.data(), p);
+      badv[j] = b;
+    }
+  };
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const std::size_t nthr = std::min<std::size_t>(hw, nchunks);
+  if(nthr <= 1) work(0, 1);
+  else
+  {
+    std::vector<std::thread> th;
+    for(std::size_t t = 0; t < nthr; ++t) th.emplace_back(work, t, nthr);
+    for(auto& t : th) t.join();
+  }
+  std::size_t total = 4;
+  for(const auto& s : parts) total += s.size();
+  std::string out;
+  out.reserve(total);
+  out += "[ ";
+  for(const auto& s : parts) out += s;
+  out += " ]";
+  for(char b : badv) if(b) bad = true;
+  return out;
+}
 
 } // namespace mass_json
 
@@ -92,7 +186,11 @@ class oarchive
     stream << " ]";
   }
   template<class T> void value(const T& v) { element(v); }
-  template<class T, class A> void value(const std::vector<T, A>& v) { iterable(v); }
+  template<class T, class A>
+  void value(const std::vector<T, A>& v) { vector_value(v, mass_json::flat<T>()); }
+  template<class V> void vector_value(const V& v, std::true_type)
+  { stream << mass_json::format_array(v, f_bad_value); }
+  template<class V> void vector_value(const V& v, std::false_type) { iterable(v); }
   template<class T, std::size_t N> void value(const std::array<T, N>& v) { iterable(v); }
 
 public:

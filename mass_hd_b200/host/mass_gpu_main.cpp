@@ -25,6 +25,7 @@
 
 #include <chrono>
 #include <fstream>
+#include <thread>
 #include <sys/stat.h>
 
 using namespace std;
@@ -112,8 +113,39 @@ void set_model_option(const option_list& opts, const string& k, const string& v)
   throw error_msg("unknown option '", k, "'");
 }
 
+// Files are written by a background thread while the time loop goes on;
+// the next write (and the end of the run) waits for the previous one and
+// reports its failure.
+class AsyncFileWriter
+{
+  thread worker;
+  string failure;
+
+public:
+  void wait()
+  {
+    if(worker.joinable()) worker.join();
+    if(!failure.empty())
+    {
+      const string f = failure;
+      failure.clear();
+      throw error_msg(f);
+    }
+  }
+  void write(const string& path, string&& text)
+  {
+    wait();
+    worker = thread([this, path](string t) {
+      ofstream ofs(path.c_str(), ios::out);
+      ofs << t;
+      if(!ofs.good()) failure = "can not write " + path;
+    }, std::move(text));
+  }
+  ~AsyncFileWriter() { if(worker.joinable()) worker.join(); }
+};
+
 template<class Writer>
-void write_json(const string& path, const string& id, Writer&& w)
+void write_json(AsyncFileWriter& out, const string& path, const string& id, Writer&& w)
 {
   stringstream buffer;
   {
@@ -121,9 +153,7 @@ void write_json(const string& path, const string& id, Writer&& w)
     w(ar);
     if(ar.bad_value()) throw error_msg("nan found while writing file.");
   }
-  ofstream ofs(path.c_str(), ios::out);
-  ofs << buffer.rdbuf();
-  if(!ofs.good()) throw error_msg("can not write ", path);
+  out.write(path, buffer.str());
 }
 
 int run(int argc, char** argv)
@@ -175,11 +205,12 @@ int run(int argc, char** argv)
   model->Configure();
 
   string output_dir = p.runname + (p.runname.back() == '/' ? "" : "/");
+  AsyncFileWriter files;
   if(!p.no_write)
   {
     if(system(("mkdir -p '" + output_dir + "'").c_str()) != 0)
       throw error_msg("can not create output directory ", output_dir);
-    write_json(output_dir + "parameters.json", "parameters", [&](oarchive& ar) {
+    write_json(files, output_dir + "parameters.json", "parameters", [&](oarchive& ar) {
       unsigned LX = p.LX, LY = p.LY, BC = p.BC, nsteps = p.nsteps, ninfo = p.ninfo,
                nstart = p.nstart, nsubsteps_ = nsubsteps;
       unsigned& nsubsteps = nsubsteps_;
@@ -192,7 +223,7 @@ int run(int argc, char** argv)
   }
 
   auto write_frame = [&](unsigned t) {
-    write_json(output_dir + "frame" + to_string(t) + ".json", "frame",
+    write_json(files, output_dir + "frame" + to_string(t) + ".json", "frame",
                [&](oarchive& ar) { model.ptr->serialize_frame(ar); });
   };
 
@@ -222,6 +253,7 @@ int run(int argc, char** argv)
     }
   }
   if(!p.no_write && p.nsteps >= p.nstart) write_frame(p.nsteps);
+  files.wait();
   const auto dt = chrono::duration<double>(chrono::steady_clock::now() - start).count();
   model->Post();
   if(!p.save_state.empty())

@@ -31,7 +31,7 @@ def gxx():
 
 def compile_native(tmp_path, src, extra=()):
     exe = os.path.join(str(tmp_path), os.path.basename(src).replace(".cpp", ""))
-    subprocess.run([gxx(), "-std=c++14", "-O1", "-I", COMPAT, os.path.join(NATIVE, src),
+    subprocess.run([gxx(), "-std=c++17", "-O1", "-pthread", "-I", COMPAT, os.path.join(NATIVE, src),
                     *extra, "-o", exe], check=True)
     return exe
 
@@ -44,6 +44,14 @@ def test_standalone_driver_builds():
 @pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "src")), reason="reference tree absent")
 def test_plugin_compiles_against_reference_headers():
     subprocess.run(["make", "-s", "-C", HOST, "refcheck"], check=True)
+
+
+def test_bulk_number_format_equals_stringstream(tmp_path):
+    """Frame arrays are formatted in parallel chunks with std::to_chars; every
+    value must print exactly as the reference's `stringstream << v`."""
+    exe = compile_native(tmp_path, "format_check.cpp")
+    out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout
+    assert out.split()[-1] == "0", out
 
 
 def test_mask_stamping_equals_reference_circle_test(tmp_path):
