@@ -134,6 +134,32 @@ int mass_lb_load(mass_lb_handle* h, const char* path);
 int mass_lb_set_phi_source(mass_lb_handle* h, const double* rate);
 int mass_lb_set_phi_conservation(mass_lb_handle* h, int on, double totalphi);
 
+/* The masks themselves on the device, with the caller's random numbers
+ * (SetMasks, :35-106), so that the reference's generator stream stays with
+ * the caller while the per-site work and the transfers of phi and of the
+ * rate plane disappear.
+ *
+ * mass_lb_mask_candidates: *count = the number of domain sites with
+ * phi >= 0.5. These are the sites that draw one random_real() each, in
+ * site order k = y + LY*x. Synchronous.
+ *
+ * mass_lb_draw_mask: kind 0 (division) or 1 (death). `draws` holds one
+ * uniform per candidate site in site order (ndraws must equal the count of
+ * the last mass_lb_mask_candidates). A candidate becomes a centre when its
+ * draw is below coef*phi*(1 - phi/phi_critical) (division) or coef*phi
+ * (death). The mask of that kind becomes the set of sites whose periodic
+ * distance (dx, dy) to some centre has dx^2 + dy^2 <= ceil(radius^2).
+ * Then the phi source becomes alpha*division_mask - beta*death_mask, as
+ * mass_lb_set_phi_source(alpha*dm - beta*de) would set it. Both masks start
+ * empty. Synchronous.
+ *
+ * mass_lb_get_mask: the current mask of a kind as LX*LY bytes (0/1), site
+ * order. */
+int mass_lb_mask_candidates(mass_lb_handle* h, long long* count);
+int mass_lb_draw_mask(mass_lb_handle* h, int kind, const double* draws, long long ndraws,
+                      double coef, double phi_critical, double radius, double alpha, double beta);
+int mass_lb_get_mask(mass_lb_handle* h, int kind, unsigned char* out);
+
 /* ---- go-or-grow -----------------------------------------------------------
  *
  * Parameters of the reference's GoOrGrow (src/models/go-or-grow.hpp:9-20,

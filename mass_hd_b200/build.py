@@ -29,6 +29,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
           "-I", INCLUDE, "-I", CSRC]
 UNITS = {
     "unfused.cu": ["--fmad=false"],
+    "masks.cu": ["--fmad=false"],
     "fused32.cu": [],
     "fused_warp.cu": [],
     "reduce.cu": [],

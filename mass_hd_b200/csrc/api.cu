@@ -9,6 +9,7 @@
 #include "fused32.cuh"
 #include "reduce.cuh"
 #include "stats.cuh"
+#include "masks.cuh"
 
 #include <algorithm>
 #include <cstdint>
@@ -160,6 +161,10 @@ struct mass_lb_handle
   bool src_on = false;
   double* phisum = nullptr;     // countphi scalar for conserve_phi
   double* relaxsum = nullptr;   // relaxed phi total (go-or-grow)
+
+  // device-side division / death masks (mass_lb_mask_candidates, _draw_mask)
+  MaskScratch mk{};
+  long long mk_count = -1;      // candidates of the last count, -1: none
 };
 
 namespace {
@@ -1129,7 +1134,7 @@ int mass_lb_set_phi_conservation(mass_lb_handle* h, int on, double totalphi)
                                       "halves of a sub-step; use precision FP64");
   DeviceGuard g(h->device);
   if(on && !h->phisum)
-    if(int r = dalloc(h, &h->phisum, 1)) return r;
+    if(int r = dalloc(h, &h->phisum, 1 + PHI_PARTS)) return r;
   for(int i = 0; i < 2; ++i)
   {
     if(i == 0)
@@ -1145,6 +1150,155 @@ int mass_lb_set_phi_conservation(mass_lb_handle* h, int on, double totalphi)
       h->s32.phisum = h->phisum;
     }
   }
+  return 0;
+}
+
+// ---- device-side masks -------------------------------------------------------
+
+} // extern "C"
+
+namespace {
+
+int ensure_masks(mass_lb_handle* h)
+{
+  MaskScratch& m = h->mk;
+  if(m.center) return 0;
+  const long long N = static_cast<long long>(h->LX)*h->LY;
+  const int nb = mask_blocks(N);
+  if(int r = dalloc(h, &m.block_cnt, nb)) return r;
+  if(int r = dalloc(h, &m.block_off, nb)) return r;
+  if(int r = dalloc(h, &m.total, 1)) return r;
+  if(int r = dalloc(h, &m.center, N)) return r;
+  for(int i = 0; i < 2; ++i)
+  {
+    if(int r = dalloc(h, &m.mask[i], N)) return r;
+    CU(cudaMemsetAsync(m.mask[i], 0, N, h->stream), "memset");
+  }
+  return 0;
+}
+
+// phi as the step kernels of this handle hold it
+template<typename F>
+cudaError_t with_phi(mass_lb_handle* h, F&& f)
+{
+  if(h->fused)
+  {
+    const long long plane = static_cast<long long>(h->LX)*h->LY;
+    return f(MaskView<float>{h->cur + 11*plane, static_cast<int>(h->LX), static_cast<int>(h->LY),
+                             0, static_cast<int>(h->LY)});
+  }
+  if(h->precision == MASS_LB_FP64)
+    return f(MaskView<double>{h->s64.phi, h->d.LX, h->d.LY, h->d.g, h->d.EY});
+  return f(MaskView<float>{h->s32.phi, h->d.LX, h->d.LY, h->d.g, h->d.EY});
+}
+
+// the source plane of this handle's step kernels, allocated on first use
+int source_plane(mass_lb_handle* h, void** plane, int* is_double, int* g, int* EY)
+{
+  if(h->fused)
+  {
+    if(!h->src_fused)
+      if(int r = dalloc(h, &h->src_fused, static_cast<size_t>(h->LX)*h->LY)) return r;
+    *plane = h->src_fused; *is_double = 0; *g = 0; *EY = static_cast<int>(h->LY);
+  }
+  else if(h->precision == MASS_LB_FP64)
+  {
+    if(!h->src64)
+    {
+      if(int r = dalloc(h, &h->src64, h->d.NE)) return r;
+      CU(cudaMemsetAsync(h->src64, 0, h->d.NE*sizeof(double), h->stream), "memset");
+    }
+    *plane = h->src64; *is_double = 1; *g = h->d.g; *EY = h->d.EY;
+  }
+  else
+  {
+    if(!h->src32)
+    {
+      if(int r = dalloc(h, &h->src32, h->d.NE)) return r;
+      CU(cudaMemsetAsync(h->src32, 0, h->d.NE*sizeof(float), h->stream), "memset");
+    }
+    *plane = h->src32; *is_double = 0; *g = h->d.g; *EY = h->d.EY;
+  }
+  return 0;
+}
+
+} // namespace
+
+extern "C" {
+
+int mass_lb_mask_candidates(mass_lb_handle* h, long long* count)
+{
+  if(!h || !count) return fail(MASS_LB_EINVAL, "null argument");
+  if(h->model == NEM) return fail(MASS_LB_EUNSUPPORTED, "the nematic model has no phi");
+  DeviceGuard g(h->device);
+  if(int r = ensure_masks(h)) return r;
+  const cudaError_t e = with_phi(h, [&](const auto& v) { return mask_count(v, h->mk, h->stream); });
+  if(e != cudaSuccess) return cuda_fail(e, "mask candidates");
+  long long n = 0;
+  CU(cudaMemcpyAsync(&n, h->mk.total, sizeof(n), cudaMemcpyDeviceToHost, h->stream), "count copy");
+  CU(cudaStreamSynchronize(h->stream), "count sync");
+  h->mk_count = n;
+  *count = n;
+  return 0;
+}
+
+int mass_lb_draw_mask(mass_lb_handle* h, int kind, const double* draws, long long ndraws,
+                      double coef, double phi_critical, double radius, double alpha, double beta)
+{
+  if(!h) return fail(MASS_LB_EINVAL, "null handle");
+  if(h->model == NEM) return fail(MASS_LB_EUNSUPPORTED, "the nematic model has no phi");
+  if(kind != 0 && kind != 1) return fail(MASS_LB_EINVAL, "kind must be 0 (division) or 1 (death)");
+  if(h->mk_count < 0) return fail(MASS_LB_EINVAL, "call mass_lb_mask_candidates first");
+  if(ndraws != h->mk_count)
+    return fail(MASS_LB_EINVAL, "one draw per candidate site is needed (ndraws != candidates)");
+  if(ndraws > 0 && !draws) return fail(MASS_LB_EINVAL, "null draws");
+  DeviceGuard g(h->device);
+  MaskScratch& m = h->mk;
+  if(ndraws > m.draws_cap)
+  {
+    double* p = nullptr;
+    if(int r = dalloc(h, &p, static_cast<size_t>(ndraws))) return r;
+    m.draws = p;
+    m.draws_cap = ndraws;
+  }
+  if(ndraws > 0)
+    CU(cudaMemcpyAsync(m.draws, draws, ndraws*sizeof(double), cudaMemcpyHostToDevice, h->stream),
+       "draws copy");
+  cudaError_t e = with_phi(h, [&](const auto& v) {
+    return mask_draw(v, m, kind, ndraws, coef, phi_critical, radius, h->stream);
+  });
+  if(e != cudaSuccess) return cuda_fail(e, "mask draw");
+  void* plane = nullptr;
+  int dbl = 0, gg = 0, EY = 0;
+  if(int r = source_plane(h, &plane, &dbl, &gg, &EY)) return r;
+  e = dbl ? mask_rate<double>(static_cast<int>(h->LX), static_cast<int>(h->LY), gg, EY, m, alpha,
+                              beta, static_cast<double*>(plane), h->stream)
+          : mask_rate<float>(static_cast<int>(h->LX), static_cast<int>(h->LY), gg, EY, m, alpha,
+                             beta, static_cast<float*>(plane), h->stream);
+  if(e != cudaSuccess) return cuda_fail(e, "mask rate");
+  if(h->fused && h->cfg.nt != 32) h->tuned = false;   // the source runs in the warp-strip kernel
+  h->s64.src = h->src64;
+  h->s32.src = h->src32;
+  h->src_on = true;
+  // the draws buffer is read by the kernels above: wait before the caller
+  // may reuse its array
+  CU(cudaStreamSynchronize(h->stream), "mask sync");
+  return 0;
+}
+
+int mass_lb_get_mask(mass_lb_handle* h, int kind, unsigned char* out)
+{
+  if(!h || !out) return fail(MASS_LB_EINVAL, "null argument");
+  if(kind != 0 && kind != 1) return fail(MASS_LB_EINVAL, "kind must be 0 (division) or 1 (death)");
+  DeviceGuard g(h->device);
+  const size_t N = static_cast<size_t>(h->LX)*h->LY;
+  if(!h->mk.center)
+  {
+    std::memset(out, 0, N);
+    return 0;
+  }
+  CU(cudaMemcpyAsync(out, h->mk.mask[kind], N, cudaMemcpyDeviceToHost, h->stream), "mask copy");
+  CU(cudaStreamSynchronize(h->stream), "mask sync");
   return 0;
 }
 

@@ -1,0 +1,39 @@
+// Device-side division / death masks (masks.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace mlb {
+
+// phi of a lattice as the step kernels hold it: plane with ghost ring g and
+// row stride EY (FP64 / FP32 unfused), or g = 0, EY = LY (FP32 fused)
+template<typename T>
+struct MaskView
+{
+  const T* phi;
+  int LX, LY, g, EY;
+};
+
+struct MaskScratch
+{
+  int* block_cnt = nullptr;        // candidates per block of 1024 sites
+  long long* block_off = nullptr;  // exclusive offsets
+  long long* total = nullptr;      // number of candidates
+  unsigned char* center = nullptr; // LX*LY, site order
+  unsigned char* mask[2] = {nullptr, nullptr};   // division, death (LX*LY)
+  double* draws = nullptr;         // the caller's uniforms
+  long long draws_cap = 0;
+};
+
+int mask_blocks(long long nsites);
+
+template<typename T>
+cudaError_t mask_count(const MaskView<T>& v, const MaskScratch& s, cudaStream_t st);
+template<typename T>
+cudaError_t mask_draw(const MaskView<T>& v, const MaskScratch& s, int kind, long long ndraws,
+                      double coef, double phi_critical, double radius, cudaStream_t st);
+template<typename T>
+cudaError_t mask_rate(int LX, int LY, int g, int EY, const MaskScratch& s, double alpha,
+                      double beta, T* src, cudaStream_t st);
+
+} // namespace mlb

@@ -22,6 +22,7 @@
 #include "lb_common.cuh"
 #include "unfused.h"
 
+#include <type_traits>
 #include <utility>
 
 namespace mlb {
@@ -687,6 +688,60 @@ __global__ void phi_sum_serial(Dims d, const T* __restrict__ phi, double* out)
   *out = sum;
 }
 
+// countphi for the FP32 sweeps, which do not reproduce the reference's
+// rounding anyway: per-block FP64 partial sums (PHI_PARTS blocks), then one
+// block adds the partials. Writes out[0]; out[1 .. PHI_PARTS] is scratch.
+__global__ void __launch_bounds__(256)
+phi_sum_partial(Dims d, const float* __restrict__ phi, double* __restrict__ out)
+{
+  __shared__ double red[256];
+  const long long N = static_cast<long long>(d.LX)*d.LY;
+  double s = 0;
+  for(long long k = static_cast<long long>(blockIdx.x)*256 + threadIdx.x; k < N;
+      k += static_cast<long long>(gridDim.x)*256)
+  {
+    const int x = static_cast<int>(k / d.LY), y = static_cast<int>(k % d.LY);
+    s += static_cast<double>(phi[(y + d.g) + static_cast<long long>(d.EY)*(x + d.g)]);
+  }
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for(int w = 128; w > 0; w >>= 1)
+  {
+    if(threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if(threadIdx.x == 0) out[1 + blockIdx.x] = red[0];
+}
+
+__global__ void __launch_bounds__(256)
+phi_sum_final(int nparts, double* __restrict__ out)
+{
+  __shared__ double red[256];
+  double s = 0;
+  for(int i = threadIdx.x; i < nparts; i += 256) s += out[1 + i];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for(int w = 128; w > 0; w >>= 1)
+  {
+    if(threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+    __syncthreads();
+  }
+  if(threadIdx.x == 0) out[0] = red[0];
+}
+
+// countphi before an UpdateFields: the serial site-order sum in FP64 (the
+// reference's rounding), a parallel sum in FP32
+template<typename T>
+void phi_sum(const Dims& d, const T* phi, double* out, cudaStream_t st)
+{
+  if constexpr (std::is_same<T, float>::value)
+  {
+    phi_sum_partial<<<PHI_PARTS, 256, 0, st>>>(d, phi, out);
+    phi_sum_final<<<1, 256, 0, st>>>(PHI_PARTS, out);
+  }
+  else phi_sum_serial<T><<<1, 1, 0, st>>>(d, phi, out);
+}
+
 // GoOrGrow::RelaxFreeEnergy (src/models/go-or-grow.cpp:42-119): dry
 // free-energy descent of phi (Cahn-Hilliard) and Q (molecular field) before
 // the dynamics. First sweep: H and mu at every site.
@@ -843,7 +898,7 @@ int step_impl(const Dims& d, const Params& P, State<T>& s, int bc,
     fields_bc();
     uq_kernel<T, DEV, MODEL, false><<<grd, blk, 0, st>>>(d, P, s);
     fields2_bc();
-    if(MODEL != NEM && s.conserve_phi) phi_sum_serial<T><<<1, 1, 0, st>>>(d, s.phi, s.phisum);
+    if(MODEL != NEM && s.conserve_phi) phi_sum<T>(d, s.phi, s.phisum, st);
     uf_kernel<T, DEV, MODEL, true><<<grd, blk, 0, st>>>(d, P, s);
     swap_fields();
     if(bc) bc_lb_kernel<T><<<1, 1024, 0, st>>>(d, s.ff, s.fn, lbk);
@@ -857,7 +912,7 @@ int step_impl(const Dims& d, const Params& P, State<T>& s, int bc,
       if(diag) uq_kernel<T, DEV, MODEL, true><<<grd, blk, 0, st>>>(d, P, s);
       else uq_kernel<T, DEV, MODEL, false><<<grd, blk, 0, st>>>(d, P, s);
       fields2_bc();
-      if(MODEL != NEM && s.conserve_phi) phi_sum_serial<T><<<1, 1, 0, st>>>(d, s.phi, s.phisum);
+      if(MODEL != NEM && s.conserve_phi) phi_sum<T>(d, s.phi, s.phisum, st);
       uf_kernel<T, DEV, MODEL, false><<<grd, blk, 0, st>>>(d, P, s);
       swap_fields();
     }

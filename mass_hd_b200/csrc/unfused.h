@@ -9,6 +9,9 @@ namespace mlb {
 enum { BC_NEUMANN = 0, BC_DIRICHLET0 = 1, BC_COPYDERIV = 2 };
 // scalar ghost layouts: channel (pbc left/right), box, full pbc
 enum { BCM_CHANNEL = 0, BCM_BOX = 1, BCM_PBC = 2 };
+// blocks of the FP32 countphi sum; the conservation scalar needs
+// 1 + PHI_PARTS doubles
+constexpr int PHI_PARTS = 512;
 // population ghost layouts (src/fields.hpp:792-930)
 enum { LBK_PBC = 0, LBK_FREESLIP_CHANNEL = 1, LBK_NOSLIP_CHANNEL = 2,
        LBK_FREESLIP_BOX = 3, LBK_NOSLIP_BOX = 4 };

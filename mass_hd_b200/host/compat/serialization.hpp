@@ -18,7 +18,12 @@
 
 #include <algorithm>
 #include <array>
+#include <cmath>
+#include <cstdint>
 #include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
 #include <ostream>
 #include <sstream>
 #include <string>
@@ -53,8 +58,9 @@ template<class T, class A> struct tname<std::vector<T, A>>
 template<class T, std::size_t N> struct tname<std::array<T, N>>
 { static std::string get() { return "array(" + tname<T>::get() + ")"; } };
 
-// one value as `std::stringstream() << v` prints it; returns the end
-inline char* put_value(char* p, double v)
+// one value as `std::stringstream() << v` prints it (printf's %.6g), with
+// the general-purpose conversion
+inline char* put_value_exact(char* p, double v)
 {
 #if __cplusplus >= 201703L
   return std::to_chars(p, p + 32, v, std::chars_format::general, 6).ptr;
@@ -62,6 +68,98 @@ inline char* put_value(char* p, double v)
   return p + std::snprintf(p, 32, "%.6g", v);
 #endif
 }
+
+// 10^i as the nearest double, i in [-330, 330] (index i + 330)
+inline const double* pow10_table()
+{
+  static const double* t = [] {
+    static double a[661];
+    for(int i = -330; i <= 330; ++i)
+    {
+      char b[16];
+      std::snprintf(b, sizeof b, "1e%d", i);
+      a[i + 330] = std::strtod(b, nullptr);
+    }
+    return a;
+  }();
+  return t;
+}
+
+// %.6g written from its definition (C11 7.21.6.1): the value rounded to 6
+// significant digits d0.d1..d5 x 10^X; fixed notation with 5 - X decimals
+// when -4 <= X < 6, else d0.d1..d5e+-XX; trailing zeros and a bare decimal
+// point removed. The 6-digit rounding is decided from |v| scaled into
+// [1e5, 1e6) by a tabulated power of ten, in double arithmetic, whose error
+// (a few ulp, below 1e-9 in absolute terms) only matters when the scaled
+// value lies within 1e-9 of a rounding tie; those values, zeros,
+// non-finite and extreme magnitudes go to put_value_exact. Same characters
+// as put_value_exact for every value.
+inline char* put_value(char* p, double v, const double* t)
+{
+  const double a = v < 0 ? -v : v;
+  if(!(a >= 1e-290 && a <= 1e290)) return put_value_exact(p, v);
+  uint64_t bits;
+  std::memcpy(&bits, &a, sizeof bits);
+  const int k = static_cast<int>(bits >> 52) - 1023;     // a in [2^k, 2^(k+1))
+  int e = (k*78913) >> 18;                                 // floor(k*log10(2)), within 1 of floor(log10 a)
+  double sc = 0;
+  for(int it = 0; it < 3; ++it)
+  {
+    sc = a*t[330 + 5 - e];
+    if(sc < 99999.9999) --e;
+    else if(sc >= 999999.4999) ++e;
+    else break;
+  }
+  if(!(sc >= 99999.9999 && sc < 999999.4999)) return put_value_exact(p, v);
+  const long r = static_cast<long>(sc);                   // floor: sc > 0
+  const double frac = sc - static_cast<double>(r);
+  if(frac > 0.5 - 1e-9 && frac < 0.5 + 1e-9) return put_value_exact(p, v);
+  long m = r + (frac > 0.5 ? 1 : 0);
+  int X = e;
+  if(m >= 1000000) { m /= 10; ++X; }
+  char d[6];
+  for(int i = 5; i >= 0; --i) { d[i] = static_cast<char>('0' + m % 10); m /= 10; }
+  int nd = 6;                       // significant digits after trailing-zero removal
+  while(nd > 1 && d[nd - 1] == '0') --nd;
+  if(v < 0) *p++ = '-';
+  if(X >= -4 && X < 6)
+  {
+    if(X >= 0)
+    {
+      for(int i = 0; i <= X; ++i) *p++ = d[i];
+      if(nd > X + 1)
+      {
+        *p++ = '.';
+        for(int i = X + 1; i < nd; ++i) *p++ = d[i];
+      }
+    }
+    else
+    {
+      *p++ = '0';
+      *p++ = '.';
+      for(int i = 0; i < -X - 1; ++i) *p++ = '0';
+      for(int i = 0; i < nd; ++i) *p++ = d[i];
+    }
+  }
+  else
+  {
+    *p++ = d[0];
+    if(nd > 1)
+    {
+      *p++ = '.';
+      for(int i = 1; i < nd; ++i) *p++ = d[i];
+    }
+    *p++ = 'e';
+    int ex = X;
+    if(ex < 0) { *p++ = '-'; ex = -ex; }
+    else *p++ = '+';
+    if(ex >= 100) { *p++ = static_cast<char>('0' + ex/100); ex %= 100; }
+    *p++ = static_cast<char>('0' + ex/10);
+    *p++ = static_cast<char>('0' + ex%10);
+  }
+  return p;
+}
+inline char* put_value(char* p, double v) { return put_value(p, v, pow10_table()); }
 inline char* put_value(char* p, bool b) { *p++ = b ? '1' : '0'; return p; }
 
 // element types formatted in bulk, and the most characters one takes
@@ -71,7 +169,12 @@ template<> struct flat<bool> : std::true_type { static constexpr std::size_t cha
 template<std::size_t N> struct flat<std::array<double, N>> : std::true_type
 { static constexpr std::size_t chars = 4 + 34*N; };
 
-inline char* put_elem(char* p, double v, bool& bad) { if(v != v) bad = true; return put_value(p, v); }
+inline char* put_elem(char* p, double v, bool& bad)
+{
+  static const double* const t = pow10_table();
+  if(v != v) bad = true;
+  return put_value(p, v, t);
+}
 inline char* put_elem(char* p, bool b, bool&) { return put_value(p, b); }
 template<std::size_t N>
 inline char* put_elem(char* p, const std::array<double, N>& a, bool& bad)
@@ -97,10 +200,10 @@ std::string format_array(const V& c, bool& bad)
   std::vector<std::string> parts(nchunks);
   std::vector<char> badv(nchunks, 0);
   auto work = [&](std::size_t first, std::size_t stride) {
-    std::vector<char> buf((chunk + 1)*per);
+    std::unique_ptr<char[]> buf(new char[(chunk + 1)*per]);   // not zeroed
     for(std::size_t j = first; j < nchunks; j += stride)
     {
-      char* p = buf.data();
+      char* p = buf.get();
       bool b = false;
       const std::size_t lo = j*chunk, hi = std::min(n, lo + chunk);
       typename V::const_iterator it = c.begin();
@@ -110,7 +213,7 @@ std::string format_array(const V& c, bool& bad)
         if(i) { *p++ = ','; *p++ = ' '; }
         p = put_elem(p, *it, b);
       }
-      parts[j].assign(buf.data(), p);
+      parts[j].assign(buf.get(), p);
       badv[j] = b;
     }
   };

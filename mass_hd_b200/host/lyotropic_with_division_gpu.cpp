@@ -3,7 +3,6 @@
 #include "error_msg.hpp"
 #include "random.hpp"
 #include "mass_lb_ext.h"
-#include "mask_draw.hpp"
 
 #include <algorithm>
 #include <array>
@@ -21,7 +20,6 @@ void LyotropicWithDivisionGPU::Initialize()
   LyotropicGPU::Initialize();
   division_mask.assign(DomainSize, false);
   death_mask.assign(DomainSize, false);
-  rate.assign(DomainSize, 0.);
   division_count = death_count = 0u;
   // as src/models/lyotropic-with-division.cpp:29-30
   conserve_phi = ((alpha == 0 || division_rate == 0) && (beta == 0 || death_rate == 0));
@@ -42,47 +40,42 @@ void LyotropicWithDivisionGPU::Configure()
 
 void LyotropicWithDivisionGPU::SetMasks()
 {
-  bool have_phi = false, changed = false;
-  auto draw = [&](std::vector<bool>& mask, double rate_coef, bool division, double radius) {
-    if(!have_phi)
+  long long candidates = -1;
+  auto draw = [&](int kind, double rate_coef, double radius) {
+    if(candidates < 0)
     {
-      const int r = mass_lb_download(lattice, MASS_LB_PHI, phi.data());
-      if(r != MASS_LB_OK) throw error_msg(mass_gpu::abi_error("mass_lb_download", r));
-      have_phi = true;
+      const int r = mass_lb_mask_candidates(lattice, &candidates);
+      if(r != MASS_LB_OK) throw error_msg(mass_gpu::abi_error("mass_lb_mask_candidates", r));
     }
-    // centres: one random_real() per site with phi >= .5, in site order
-    std::vector<std::array<unsigned, 2>> centers;
-    for(unsigned k = 0; k < DomainSize; ++k)
-    {
-      if(phi[k] >= .5)
-      {
-        const double p = division ? rate_coef*phi[k]*(1 - phi[k]/phi_critical)
-                                  : rate_coef*phi[k];
-        if(random_real() < p)
-          centers.push_back({GetXPosition(k), GetYPosition(k)});
-      }
-    }
-    // the circles around the centres, stamped (the same set as the
-    // reference's per-site test over all centres)
-    mass_gpu::stamp_circles(mask, centers, radius, LX, LY);
-    changed = true;
+    // one random_real() per site with phi >= .5, in site order, from the
+    // reference's generator; the centres and circles are drawn on the device
+    draws.resize(static_cast<size_t>(candidates));
+    for(auto& u : draws) u = random_real();
+    const int r = mass_lb_draw_mask(lattice, kind, draws.data(), candidates, rate_coef,
+                                    phi_critical, radius, alpha, beta);
+    if(r != MASS_LB_OK) throw error_msg(mass_gpu::abi_error("mass_lb_draw_mask", r));
   };
   if(not division_count--)
   {
-    draw(division_mask, division_rate, true, division_radius);
+    draw(0, division_rate, division_radius);
     division_count = division_time;
   }
   if(not death_count--)
   {
-    draw(death_mask, death_rate, false, death_radius);
+    draw(1, death_rate, death_radius);
     death_count = death_time;
   }
-  if(changed)
+}
+
+void LyotropicWithDivisionGPU::SyncMasks()
+{
+  std::vector<unsigned char> bytes(DomainSize);
+  std::vector<bool>* masks[2] = {&division_mask, &death_mask};
+  for(int kind = 0; kind < 2; ++kind)
   {
-    for(unsigned k = 0; k < DomainSize; ++k)
-      rate[k] = alpha*(division_mask[k] ? 1. : 0.) - beta*(death_mask[k] ? 1. : 0.);
-    const int r = mass_lb_set_phi_source(lattice, rate.data());
-    if(r != MASS_LB_OK) throw error_msg(mass_gpu::abi_error("mass_lb_set_phi_source", r));
+    const int r = mass_lb_get_mask(lattice, kind, bytes.data());
+    if(r != MASS_LB_OK) throw error_msg(mass_gpu::abi_error("mass_lb_get_mask", r));
+    for(unsigned k = 0; k < DomainSize; ++k) (*masks[kind])[k] = bytes[k] != 0;
   }
 }
 

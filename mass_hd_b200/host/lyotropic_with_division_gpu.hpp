@@ -3,12 +3,13 @@
 // on a B200 through include/mass_lb.h and include/mass_lb_ext.h.
 //
 // Same options, members and serialization order as the reference model.
-// The division and death masks are drawn on the host exactly as the
-// reference's SetMasks() draws them (same random_real() stream, same site
-// order, same circle test), from phi read back from the device whenever a
-// mask is due; the device gets the source rate alpha*division_mask -
-// beta*death_mask (mass_lb_set_phi_source) and, when division and death
-// are off, the conserve_phi correction (mass_lb_set_phi_conservation).
+// The division and death masks follow the reference's SetMasks(): the host
+// draws one random_real() per site with phi >= .5 in site order from the
+// reference's generator (mass_lb_mask_candidates gives their number), and
+// the device picks the centres, draws the circles and sets the source rate
+// alpha*division_mask - beta*death_mask (mass_lb_draw_mask). When division
+// and death are off the device applies the conserve_phi correction
+// (mass_lb_set_phi_conservation).
 #ifndef MODELS_LYOTROPIC_WITH_DIVISION_GPU_HPP_
 #define MODELS_LYOTROPIC_WITH_DIVISION_GPU_HPP_
 
@@ -24,10 +25,12 @@ protected:
   double phi_critical = 1;
   unsigned division_count = 0, death_count = 0;
   bool conserve_phi = false;
-  std::vector<double> rate;     // alpha*division_mask - beta*death_mask
+  std::vector<double> draws;    // random_real() draws of one mask
 
   /** Redraw the masks that are due (src/models/lyotropic-with-division.cpp:35-106). */
   void SetMasks();
+  /** Refresh the host copies of the masks from the device. */
+  void SyncMasks();
 
 public:
   LyotropicWithDivisionGPU(unsigned LX, unsigned LY, unsigned BC);
@@ -59,6 +62,7 @@ public:
   void serialize_frame(Archive& ar)
   {
     LyotropicGPU::serialize_frame(ar);
+    SyncMasks();
     ar & auto_name(division_mask)
        & auto_name(death_mask);
   }

@@ -130,6 +130,10 @@ def load_library(build_if_missing: bool = False):
         "mass_lb_set_phi_source": (C.c_int, [vp, dp]),
         "mass_lb_set_phi_conservation": (C.c_int, [vp, C.c_int, C.c_double]),
         "mass_lb_set_go_or_grow_params": (C.c_int, [vp, C.POINTER(GogParams)]),
+        "mass_lb_mask_candidates": (C.c_int, [vp, C.POINTER(C.c_longlong)]),
+        "mass_lb_draw_mask": (C.c_int, [vp, C.c_int, dp, C.c_longlong, C.c_double, C.c_double,
+                                        C.c_double, C.c_double, C.c_double]),
+        "mass_lb_get_mask": (C.c_int, [vp, C.c_int, C.POINTER(C.c_ubyte)]),
         "mass_lb_relax_free_energy": (C.c_int, [vp, C.c_uint, C.c_double, C.c_int, C.c_int, dp]),
         "mass_lb_ensemble_create": (C.c_int, [C.c_int, C.POINTER(Params), C.POINTER(C.c_uint),
                                               C.POINTER(C.c_uint), C.POINTER(vp)]),
@@ -282,6 +286,28 @@ class Lattice:
         """The division models' conserve_phi correction
         Dp -= (sum phi - totalphi)/(LX*LY) (FP64 / walls only)."""
         _check(load_library().mass_lb_set_phi_conservation(self.h, int(bool(on)), float(totalphi)))
+
+    def mask_candidates(self) -> int:
+        """Number of sites with phi >= 0.5 (one random draw each)."""
+        n = C.c_longlong()
+        _check(load_library().mass_lb_mask_candidates(self.h, C.byref(n)))
+        return n.value
+
+    def draw_mask(self, kind: int, draws, coef: float, phi_critical: float, radius: float,
+                  alpha: float, beta: float):
+        """Division (kind 0) or death (kind 1) mask from one uniform draw per
+        candidate site (site order), then the phi source
+        alpha*division_mask - beta*death_mask."""
+        d = np.ascontiguousarray(draws, dtype=np.float64)
+        _check(load_library().mass_lb_draw_mask(self.h, int(kind), _dp(d), d.size, float(coef),
+                                                float(phi_critical), float(radius),
+                                                float(alpha), float(beta)))
+
+    def get_mask(self, kind: int) -> np.ndarray:
+        out = np.empty(self.LX * self.LY, dtype=np.uint8)
+        _check(load_library().mass_lb_get_mask(self.h, int(kind),
+                                               out.ctypes.data_as(C.POINTER(C.c_ubyte))))
+        return out.astype(bool)
 
     def set_go_or_grow_params(self, params: dict):
         """Go-or-grow runcard values (B, Snem, Dchi, Achi, Ochi, phiswitch,

@@ -1,6 +1,7 @@
 // The bulk array formatting of the standalone JSON archive
-// (mass_hd_b200/host/compat/serialization.hpp: std::to_chars, chunks on all
-// threads) against the reference's per-value `std::stringstream << v`:
+// (mass_hd_b200/host/compat/serialization.hpp: a %.6g conversion written
+// from its definition with std::to_chars for the cases it defers, chunks on
+// all threads) against the reference's per-value `std::stringstream << v`:
 // arrays of doubles (random bit patterns, values at 6-digit rounding
 // boundaries, signed zeros, subnormals, infinities), of 9-double nodes and
 // of bools, written both ways and compared as text. Prints the number of
@@ -76,6 +77,30 @@ int main()
     if(mass_json::format_array(mask, badflag) != slow(mask)) ++bad;
     if(badflag) ++bad;
   }
+  // the fast %.6g path against the general-purpose conversion, value by
+  // value: random bit patterns, wide magnitudes, values at and next to
+  // 6-digit rounding ties, integers
+  long single = 0;
+  for(int i = 0; i < 400000; ++i)
+  {
+    double vals[5];
+    uint64_t b = g();
+    std::memcpy(&vals[0], &b, 8);
+    if(vals[0] != vals[0]) vals[0] = 1.0;
+    vals[1] = u(g)*std::pow(10.0, static_cast<int>(g() % 80) - 40);
+    const double tie = (std::floor(u(g)*1e6) + 0.5)*std::pow(10.0, static_cast<int>(g() % 30) - 15);
+    vals[2] = tie;
+    vals[3] = std::nextafter(tie, (i & 1) ? 1e300 : -1e300);
+    vals[4] = static_cast<double>(static_cast<long>(u(g)*1e9));
+    for(double x : vals)
+    {
+      char a[64], c[64];
+      *mass_json::put_value(a, x) = 0;
+      *mass_json::put_value_exact(c, x) = 0;
+      if(std::strcmp(a, c) != 0) ++single;
+    }
+  }
+  if(single) ++bad;
   std::vector<double> withnan = {1.0, std::nan(""), 2.0};
   bool nanflag = false;
   mass_json::format_array(withnan, nanflag);

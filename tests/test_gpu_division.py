@@ -134,3 +134,65 @@ def test_unsupported_combinations_are_rejected():
     ens.step(1)
     for x in (a, n, ens):
         x.close()
+
+
+def masks_rule(phi, LX, LY, draws, coef, phi_critical, radius, division):
+    """The reference's SetMasks rule (src/models/lyotropic-with-division.cpp:
+    35-106) restated for tests: candidates phi >= .5 in site order, one draw
+    each, centre when draw < threshold, every site within the periodic
+    circle test of a centre masked."""
+    cand = np.flatnonzero(phi >= 0.5)
+    p = phi[cand]
+    thr = coef * p * (1 - p / phi_critical) if division else coef * p
+    centers = cand[draws < thr]
+    r2 = np.ceil(radius * radius)
+    x = np.arange(LX)[:, None]
+    y = np.arange(LY)[None, :]
+    mask = np.zeros((LX, LY), dtype=bool)
+    for c in centers:
+        cx, cy = divmod(int(c), LY)
+        dx = np.abs(x - cx)
+        dx = np.minimum(dx % LX, LX - dx % LX)
+        dy = np.abs(y - cy)
+        dy = np.minimum(dy % LY, LY - dy % LY)
+        mask |= (dx.astype(float) ** 2 + dy.astype(float) ** 2) <= r2
+    return mask.reshape(-1), len(centers)
+
+
+@pytest.mark.parametrize("LX,LY,bc,prec", [(40, 36, 0, M.FP64), (36, 40, 3, M.FP64),
+                                           (64, 64, 0, M.FP32), (40, 36, 2, M.FP32)])
+def test_device_masks_follow_reference_rule(LX, LY, bc, prec):
+    """mass_lb_mask_candidates / mass_lb_draw_mask against the reference's
+    rule on a phi with many candidates: masks, and the source they set
+    (a lattice stepped with the device masks equals one stepped with
+    mass_lb_set_phi_source(alpha*dm - beta*dd) bit for bit)."""
+    rng = np.random.default_rng(LX + bc)
+    st = O.synthetic_state(O.LYOTROPIC, LX, LY, seed=3, flow=0.01, phi_kind="disk",
+                           radius=LX / 3)
+    a = M.Lattice(M.LYOTROPIC, params(), LX, LY, bc, prec)
+    b = M.Lattice(M.LYOTROPIC, params(), LX, LY, bc, prec)
+    a.upload_state(st)
+    b.upload_state(st)
+    phi = a.get("phi")
+    n = a.mask_candidates()
+    assert n == int((phi >= 0.5).sum()) and n > 50
+    expect = {}
+    for kind, coef, radius in ((0, 0.3, 2.2), (1, 0.2, 0.0), (0, 0.05, 7.5), (1, 0.4, 1.0)):
+        draws = rng.uniform(0, 1, n)
+        a.draw_mask(kind, draws, coef, 1.3, radius, 0.05, 0.03)
+        want, ncent = masks_rule(phi, LX, LY, draws, coef, 1.3, radius, kind == 0)
+        assert ncent > 0
+        assert np.array_equal(a.get_mask(kind), want), (kind, radius)
+        expect[kind] = want
+    rate = 0.05 * expect[0].astype(float) - 0.03 * expect[1].astype(float)
+    b.set_phi_source(rate)
+    a.step(3)
+    b.step(3)
+    for n_ in STATE:
+        assert bits_equal(a.get(n_), b.get(n_)), n_
+    with pytest.raises(M.MassLBError):
+        a.draw_mask(0, np.zeros(n + 1), 0.1, 1.3, 1.0, 0.05, 0.03)
+    with pytest.raises(M.MassLBError):
+        a.draw_mask(2, np.zeros(n), 0.1, 1.3, 1.0, 0.05, 0.03)
+    a.close()
+    b.close()

@@ -163,6 +163,30 @@ def test_fp32_go_or_grow_within_tolerance():
     b.close()
 
 
+def test_fp32_conserve_phi_parallel_sum():
+    """FP32 sweeps take countphi from a parallel FP64 sum (FP64 keeps the
+    serial site order): with division and death off, phi stays at its
+    configured total and the fields track the FP64 run."""
+    p = params(alpha=0.0, beta=0.0)
+    LX, LY = 96, 80
+    ref = O.RefOracle(O.GO_OR_GROW, p, LX, LY, 0)
+    ref.configure(4)
+    assert ref.value("conserve_phi") == 1.0
+    st = {n: ref.get(n) for n in STATE}
+    total = ref.value("totalphi")
+    a = M.Lattice(M.GO_OR_GROW, p, LX, LY, 0, M.FP32)
+    b = M.Lattice(M.GO_OR_GROW, p, LX, LY, 0, M.FP64)
+    for lat in (a, b):
+        lat.upload_state(st)
+        lat.set_phi_conservation(True, total)
+        lat.step(40)
+    assert abs(a.get("phi").sum() - total) < 1e-4 * total
+    for n in ("phi", "m", "QQxx"):
+        assert rel_l2(a.get(n), b.get(n)) < 1e-4, n
+    a.close()
+    b.close()
+
+
 def test_go_or_grow_checkpoint_resumes_bit_identical(tmp_path):
     p = params()
     ref = O.RefOracle(O.GO_OR_GROW, p, 36, 36, 2)

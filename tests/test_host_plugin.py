@@ -47,19 +47,12 @@ def test_plugin_compiles_against_reference_headers():
 
 
 def test_bulk_number_format_equals_stringstream(tmp_path):
-    """Frame arrays are formatted in parallel chunks with std::to_chars; every
-    value must print exactly as the reference's `stringstream << v`."""
+    """Frame arrays are formatted in parallel chunks by a %.6g conversion of
+    our own (std::to_chars near rounding ties); every value must print
+    exactly as the reference's `stringstream << v`."""
     exe = compile_native(tmp_path, "format_check.cpp")
     out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout
     assert out.split()[-1] == "0", out
-
-
-def test_mask_stamping_equals_reference_circle_test(tmp_path):
-    """The division masks are stamped around their centres; the set equals
-    the reference's test of every site against every centre."""
-    exe = compile_native(tmp_path, "mask_stamp.cpp", ["-I", HOST])
-    out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout
-    assert int(out.split()[-1]) == 7 * 10 * 4
 
 
 def test_compat_random_matches_reference_stream(tmp_path):
