@@ -142,39 +142,6 @@ __device__ __forceinline__ void unpack8(const uint4& u, float* f)
   }
 }
 
-// channels c0..c0+15 of pixel (n, y, x) -> padded tensor, with its periodic copies
-__device__ __forceinline__ void store_slice16(__nv_bfloat16* base, const float* v, int c0, int n,
-                                              int y, int x, int H, int W)
-{
-  uint4 pk[2];
-#pragma unroll
-  for(int k = 0; k < 2; ++k)
-    pk[k] = make_uint4(pack_bf16x2(v[8*k], v[8*k + 1]), pack_bf16x2(v[8*k + 2], v[8*k + 3]),
-                       pack_bf16x2(v[8*k + 4], v[8*k + 5]), pack_bf16x2(v[8*k + 6], v[8*k + 7]));
-  int ys[3] = {y + 1, 0, 0}, xs[3] = {x + 1, 0, 0};
-  int ny = 1, nx = 1;
-  if(y == 0) ys[ny++] = H + 1;
-  if(y == H - 1) ys[ny++] = 0;
-  if(x == 0) xs[nx++] = W + 1;
-  if(x == W - 1) xs[nx++] = 0;
-  for(int i = 0; i < ny; ++i)
-    for(int j = 0; j < nx; ++j)
-    {
-      uint4* dst = reinterpret_cast<uint4*>(base + padded_index(n, ys[i], xs[j], H, W)*64 + c0);
-      dst[0] = pk[0];
-      dst[1] = pk[1];
-    }
-}
-
-__device__ __forceinline__ void load_slice16(const __nv_bfloat16* base, float* v, int c0, int n,
-                                             int y, int x, int H, int W)
-{
-  const uint4* src =
-    reinterpret_cast<const uint4*>(base + padded_index(n, y + 1, x + 1, H, W)*64 + c0);
-  unpack8(src[0], v);
-  unpack8(src[1], v + 8);
-}
-
 template<int NOUT, int MODE>
 __global__ void __launch_bounds__(CONV_THREADS, 1)
 conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmW,
