@@ -151,7 +151,8 @@ int mass_lb_set_phi_conservation(mass_lb_handle* h, int on, double totalphi);
  * distance (dx, dy) to some centre has dx^2 + dy^2 <= ceil(radius^2).
  * Then the phi source becomes alpha*division_mask - beta*death_mask, as
  * mass_lb_set_phi_source(alpha*dm - beta*de) would set it. Both masks start
- * empty. Synchronous.
+ * empty. Asynchronous on the handle's stream; `draws` may be reused as
+ * soon as the call returns (it is copied to an internal pinned buffer).
  *
  * mass_lb_get_mask: the current mask of a kind as LX*LY bytes (0/1), site
  * order. */

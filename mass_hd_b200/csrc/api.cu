@@ -165,6 +165,9 @@ struct mass_lb_handle
   // device-side division / death masks (mass_lb_mask_candidates, _draw_mask)
   MaskScratch mk{};
   long long mk_count = -1;      // candidates of the last count, -1: none
+  double* mk_pinned = nullptr;  // pinned host staging of the draws
+  long long mk_pinned_cap = 0;
+  cudaEvent_t mk_copied = nullptr;   // the last staging copy has been read
 };
 
 namespace {
@@ -481,6 +484,8 @@ void mass_lb_destroy(mass_lb_handle* h)
   DeviceGuard g(h->device);
   if(h->stream) cudaStreamSynchronize(h->stream);
   for(void* p : h->allocs) cudaFree(p);
+  if(h->mk_pinned) cudaFreeHost(h->mk_pinned);
+  if(h->mk_copied) cudaEventDestroy(h->mk_copied);
   if(h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
@@ -1254,16 +1259,40 @@ int mass_lb_draw_mask(mass_lb_handle* h, int kind, const double* draws, long lon
   if(ndraws > 0 && !draws) return fail(MASS_LB_EINVAL, "null draws");
   DeviceGuard g(h->device);
   MaskScratch& m = h->mk;
+  // the candidate count drifts from draw to draw: buffers grow
+  // geometrically, up to one draw per site
+  const long long N = static_cast<long long>(h->LX)*h->LY;
+  const long long cap = std::min(N, std::max(2*ndraws, 1ll << 16));
   if(ndraws > m.draws_cap)
   {
     double* p = nullptr;
-    if(int r = dalloc(h, &p, static_cast<size_t>(ndraws))) return r;
+    if(int r = dalloc(h, &p, static_cast<size_t>(cap))) return r;
     m.draws = p;
-    m.draws_cap = ndraws;
+    m.draws_cap = cap;
   }
   if(ndraws > 0)
-    CU(cudaMemcpyAsync(m.draws, draws, ndraws*sizeof(double), cudaMemcpyHostToDevice, h->stream),
-       "draws copy");
+  {
+    // through a pinned staging buffer, so that neither this copy nor the
+    // caller waits for the stream; the buffer is refilled only after the
+    // previous copy out of it has run
+    if(!h->mk_copied)
+      CU(cudaEventCreateWithFlags(&h->mk_copied, cudaEventDisableTiming), "event");
+    else
+      CU(cudaEventSynchronize(h->mk_copied), "staging wait");
+    if(ndraws > h->mk_pinned_cap)
+    {
+      if(h->mk_pinned) cudaFreeHost(h->mk_pinned);
+      h->mk_pinned = nullptr;
+      h->mk_pinned_cap = 0;
+      CU(cudaMallocHost(reinterpret_cast<void**>(&h->mk_pinned), cap*sizeof(double)),
+         "pinned staging");
+      h->mk_pinned_cap = cap;
+    }
+    std::memcpy(h->mk_pinned, draws, ndraws*sizeof(double));
+    CU(cudaMemcpyAsync(m.draws, h->mk_pinned, ndraws*sizeof(double), cudaMemcpyHostToDevice,
+                       h->stream), "draws copy");
+    CU(cudaEventRecord(h->mk_copied, h->stream), "event");
+  }
   cudaError_t e = with_phi(h, [&](const auto& v) {
     return mask_draw(v, m, kind, ndraws, coef, phi_critical, radius, h->stream);
   });
@@ -1280,9 +1309,6 @@ int mass_lb_draw_mask(mass_lb_handle* h, int kind, const double* draws, long lon
   h->s64.src = h->src64;
   h->s32.src = h->src32;
   h->src_on = true;
-  // the draws buffer is read by the kernels above: wait before the caller
-  // may reuse its array
-  CU(cudaStreamSynchronize(h->stream), "mask sync");
   return 0;
 }
 

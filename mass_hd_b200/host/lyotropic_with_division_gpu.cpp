@@ -50,7 +50,11 @@ void LyotropicWithDivisionGPU::SetMasks()
     // one random_real() per site with phi >= .5, in site order, from the
     // reference's generator; the centres and circles are drawn on the device
     draws.resize(static_cast<size_t>(candidates));
+#ifdef MASS_GPU_STANDALONE
+    random_reals(draws.data(), draws.size());   // the same draws, in bulk
+#else
     for(auto& u : draws) u = random_real();
+#endif
     const int r = mass_lb_draw_mask(lattice, kind, draws.data(), candidates, rate_coef,
                                     phi_critical, radius, alpha, beta);
     if(r != MASS_LB_OK) throw error_msg(mass_gpu::abi_error("mass_lb_draw_mask", r));

@@ -55,6 +55,15 @@ def test_bulk_number_format_equals_stringstream(tmp_path):
     assert out.split()[-1] == "0", out
 
 
+def test_compat_generator_equals_std_mt19937(tmp_path):
+    """The standalone build's own Mersenne Twister (block-wise, vectorised)
+    and its bulk random_reals give exactly the standard library's
+    std::mt19937 / uniform_real_distribution / normal_distribution values."""
+    exe = compile_native(tmp_path, "random_check.cpp", [os.path.join(COMPAT, "random.cpp")])
+    out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout
+    assert out.split()[0] == "0", out
+
+
 def test_compat_random_matches_reference_stream(tmp_path):
     exe = compile_native(tmp_path, "print_random.cpp", [os.path.join(COMPAT, "random.cpp")])
     out = subprocess.run([exe, "42", "64"], check=True, capture_output=True, text=True).stdout
