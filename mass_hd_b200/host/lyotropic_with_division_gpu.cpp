@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <cstddef>
 
 using namespace std;
 namespace opt = boost::program_options;
@@ -49,13 +50,9 @@ void LyotropicWithDivisionGPU::SetMasks()
     }
     // one random_real() per site with phi >= .5, in site order, from the
     // reference's generator; the centres and circles are drawn on the device
-    draws.resize(static_cast<size_t>(candidates));
-#ifdef MASS_GPU_STANDALONE
-    random_reals(draws.data(), draws.size());   // the same draws, in bulk
-#else
-    for(auto& u : draws) u = random_real();
-#endif
-    const int r = mass_lb_draw_mask(lattice, kind, draws.data(), candidates, rate_coef,
+    last_candidates = candidates;
+    const double* draws = TakeDraws(static_cast<size_t>(candidates));
+    const int r = mass_lb_draw_mask(lattice, kind, draws, candidates, rate_coef,
                                     phi_critical, radius, alpha, beta);
     if(r != MASS_LB_OK) throw error_msg(mass_gpu::abi_error("mass_lb_draw_mask", r));
   };
@@ -83,6 +80,31 @@ void LyotropicWithDivisionGPU::SyncMasks()
   }
 }
 
+void LyotropicWithDivisionGPU::DrawAhead(size_t n)
+{
+  if(fifo.size() - fifo_head >= n) return;
+  if(fifo_head > 0)
+  {
+    fifo.erase(fifo.begin(), fifo.begin() + static_cast<std::ptrdiff_t>(fifo_head));
+    fifo_head = 0;
+  }
+  const size_t have = fifo.size();
+  fifo.resize(n);
+#ifdef MASS_GPU_STANDALONE
+  random_reals(fifo.data() + have, n - have);   // the same values, in bulk
+#else
+  for(size_t i = have; i < n; ++i) fifo[i] = random_real();
+#endif
+}
+
+const double* LyotropicWithDivisionGPU::TakeDraws(size_t n)
+{
+  DrawAhead(n);
+  const double* p = fifo.data() + fifo_head;
+  fifo_head += n;
+  return p;
+}
+
 void LyotropicWithDivisionGPU::Step()
 {
   // Step() must not throw (src/models.hpp:81-86): a failure is kept and
@@ -91,6 +113,10 @@ void LyotropicWithDivisionGPU::Step()
   try { SetMasks(); }
   catch(const error_msg& e) { step_error = e.what(); return; }
   LyotropicGPU::Step();
+  // while the device steps, draw the values of the next masks (two masks
+  // of about the last candidate count); only masks consume the generator
+  // after Configure(), so drawing early leaves every value in its place
+  DrawAhead(2*static_cast<size_t>(last_candidates));
 }
 
 void LyotropicWithDivisionGPU::RuntimeChecks()

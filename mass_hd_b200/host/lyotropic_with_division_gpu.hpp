@@ -25,7 +25,17 @@ protected:
   double phi_critical = 1;
   unsigned division_count = 0, death_count = 0;
   bool conserve_phi = false;
-  std::vector<double> draws;    // random_real() draws of one mask
+  /** random_real() values drawn ahead of need, in stream order:
+   * fifo[fifo_head..] are the next values a mask takes. They are drawn
+   * while the device runs a step, so the host's share of a mask draw is
+   * only the candidate count and the copy. */
+  std::vector<double> fifo;
+  size_t fifo_head = 0;
+  long long last_candidates = 0;
+  /** Make at least `n` values available in the fifo. */
+  void DrawAhead(size_t n);
+  /** The next `n` values of the stream (valid until the next DrawAhead). */
+  const double* TakeDraws(size_t n);
 
   /** Redraw the masks that are due (src/models/lyotropic-with-division.cpp:35-106). */
   void SetMasks();
