@@ -439,16 +439,19 @@ def run_ours_gog(args):
         run_driver_gog(L, 3, args.precision, d)          # warm-up (build, first launch)
         t_loop = run_driver_gog(L, n_e2e, args.precision, d)
     t_loop = max_over_ranks(t_loop, world)
-    # per step: phi (8 B/site) down and the rate plane (8 B/site) up on the
-    # steps that redraw a mask: division every 3rd, death every 2nd step
+    # per step: one uniform (8 B) per phi >= 0.5 site up for every mask
+    # drawn (division every 3rd step, death every 2nd), and the 8-byte
+    # candidate count down on the steps that draw
+    masks = sum((t % 3 == 0) + (t % 2 == 0) for t in range(n_e2e)) / n_e2e
     redraw = sum(1 for t in range(n_e2e) if t % 3 == 0 or t % 2 == 0) / n_e2e
+    cand = int((st["phi"] >= 0.5).sum())
     e2e = {"value": whole_job_rate(sites, world, n_e2e, t_loop * 1e3), "unit": UNIT,
-           "h2d_bytes_per_step": int(8 * sites * redraw),
-           "d2h_bytes_per_step": int(8 * sites * redraw),
+           "h2d_bytes_per_step": int(8 * cand * masks),
+           "d2h_bytes_per_step": int(8 * redraw),
            "e2e_steps": n_e2e,
-           "note": "mass-gpu driver on the runcard: Step() = host mask draw when due "
-                   "(reference RNG stream, stamped circles) + device step; driver clock "
-                   "around the time loop"}
+           "note": "mass-gpu driver on the runcard: Step() = host draws of the reference's "
+                   "random stream for the masks when due, masks and step on the device; "
+                   "driver clock around the time loop"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
