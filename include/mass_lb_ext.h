@@ -161,6 +161,31 @@ int mass_lb_draw_mask(mass_lb_handle* h, int kind, const double* draws, long lon
                       double coef, double phi_critical, double radius, double alpha, double beta);
 int mass_lb_get_mask(mass_lb_handle* h, int kind, unsigned char* out);
 
+/* The same masks without a round trip to the host: the caller supplies
+ * uniforms ahead of need, in stream order, and the device takes exactly one
+ * per candidate site and mask drawn.
+ *
+ * mass_lb_mask_supply: append n uniforms to the lattice's queue (a ring of
+ * 3*LX*LY + 65536 draws; MASS_LB_EINVAL if the unconsumed draws would not
+ * fit). Asynchronous; `u` may be reused on return.
+ *
+ * mass_lb_draw_masks_queued: `kinds` bit 0 draws the division mask, bit 1
+ * the death mask. The candidates are counted on the device. The division
+ * mask takes the next `count` queued draws, then the death mask the `count`
+ * after those, as the reference draws them. Then the source becomes
+ * alpha*division_mask - beta*death_mask, as mass_lb_draw_mask sets it.
+ * Asynchronous. A caller that keeps at least 2*LX*LY draws unconsumed never
+ * runs the queue dry. When it does run dry, the next
+ * mass_lb_mask_consumed fails with MASS_LB_EINVAL.
+ *
+ * mass_lb_mask_consumed: the number of queued draws taken so far, up to and
+ * including the last mass_lb_draw_masks_queued (waits for that draw only). */
+int mass_lb_mask_supply(mass_lb_handle* h, const double* u, long long n);
+int mass_lb_draw_masks_queued(mass_lb_handle* h, int kinds, double division_coef,
+                              double division_radius, double death_coef, double death_radius,
+                              double phi_critical, double alpha, double beta);
+int mass_lb_mask_consumed(mass_lb_handle* h, long long* consumed);
+
 /* ---- go-or-grow -----------------------------------------------------------
  *
  * Parameters of the reference's GoOrGrow (src/models/go-or-grow.hpp:9-20,

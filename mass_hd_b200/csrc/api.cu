@@ -168,6 +168,17 @@ struct mass_lb_handle
   double* mk_pinned = nullptr;  // pinned host staging of the draws
   long long mk_pinned_cap = 0;
   cudaEvent_t mk_copied = nullptr;   // the last staging copy has been read
+
+  // queued uniforms (mass_lb_mask_supply / mass_lb_draw_masks_queued)
+  MaskQueue mq{};
+  double* mq_pinned = nullptr;        // staging of supplied draws
+  long long mq_pinned_cap = 0;
+  cudaEvent_t mq_copied = nullptr;    // the last supply copy has been read
+  long long* mq_host = nullptr;       // pinned: [0] draws consumed, [1] error flag
+  int* mq_err = nullptr;              // device: a mask needed more draws than supplied
+  cudaEvent_t mq_counted = nullptr;   // mq_host of the last queued draw has landed
+  long long mq_consumed = 0;          // last value read from mq_host[0]
+  bool mq_drawn = false;
 };
 
 namespace {
@@ -486,6 +497,10 @@ void mass_lb_destroy(mass_lb_handle* h)
   for(void* p : h->allocs) cudaFree(p);
   if(h->mk_pinned) cudaFreeHost(h->mk_pinned);
   if(h->mk_copied) cudaEventDestroy(h->mk_copied);
+  if(h->mq_pinned) cudaFreeHost(h->mq_pinned);
+  if(h->mq_host) cudaFreeHost(h->mq_host);
+  if(h->mq_copied) cudaEventDestroy(h->mq_copied);
+  if(h->mq_counted) cudaEventDestroy(h->mq_counted);
   if(h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
@@ -1325,6 +1340,152 @@ int mass_lb_get_mask(mass_lb_handle* h, int kind, unsigned char* out)
   }
   CU(cudaMemcpyAsync(out, h->mk.mask[kind], N, cudaMemcpyDeviceToHost, h->stream), "mask copy");
   CU(cudaStreamSynchronize(h->stream), "mask sync");
+  return 0;
+}
+
+} // extern "C"
+
+namespace {
+
+int ensure_queue(mass_lb_handle* h)
+{
+  if(h->mq.buf) return 0;
+  const long long N = static_cast<long long>(h->LX)*h->LY;
+  const long long cap = 3*N + (1ll << 16);
+  if(int r = dalloc(h, &h->mq.buf, static_cast<size_t>(cap))) return r;
+  if(int r = dalloc(h, &h->mq.head, 1)) return r;
+  if(int r = dalloc(h, &h->mq_err, 1)) return r;
+  CU(cudaMemsetAsync(h->mq.head, 0, sizeof(long long), h->stream), "memset");
+  CU(cudaMemsetAsync(h->mq_err, 0, sizeof(int), h->stream), "memset");
+  CU(cudaMallocHost(reinterpret_cast<void**>(&h->mq_host), 2*sizeof(long long)), "pinned");
+  h->mq_host[0] = h->mq_host[1] = 0;
+  CU(cudaEventCreateWithFlags(&h->mq_copied, cudaEventDisableTiming), "event");
+  CU(cudaEventCreateWithFlags(&h->mq_counted, cudaEventDisableTiming), "event");
+  CU(cudaEventRecord(h->mq_copied, h->stream), "event");
+  h->mq.cap = cap;
+  h->mq.supplied = 0;
+  h->mq_consumed = 0;
+  return 0;
+}
+
+// the consumed count and error flag of the last queued draw
+int queue_refresh(mass_lb_handle* h)
+{
+  if(!h->mq_drawn) return 0;
+  CU(cudaEventSynchronize(h->mq_counted), "queue count");
+  h->mq_consumed = h->mq_host[0];
+  if(h->mq_host[1])
+    return fail(MASS_LB_EINVAL, "a queued mask needed more draws than were supplied");
+  return 0;
+}
+
+} // namespace
+
+extern "C" {
+
+int mass_lb_mask_supply(mass_lb_handle* h, const double* u, long long n)
+{
+  if(!h) return fail(MASS_LB_EINVAL, "null handle");
+  if(h->model == NEM) return fail(MASS_LB_EUNSUPPORTED, "the nematic model has no phi");
+  if(n < 0 || (n > 0 && !u)) return fail(MASS_LB_EINVAL, "bad draws");
+  if(n == 0) return 0;
+  DeviceGuard g(h->device);
+  if(int r = ensure_queue(h)) return r;
+  MaskQueue& q = h->mq;
+  if(q.supplied + n - h->mq_consumed > q.cap)
+  {
+    if(int r = queue_refresh(h)) return r;
+    if(q.supplied + n - h->mq_consumed > q.cap)
+      return fail(MASS_LB_EINVAL, "mask queue full (more than 3*LX*LY + 65536 unconsumed draws)");
+  }
+  // the staging buffer is refilled once its previous copy has been read
+  CU(cudaEventSynchronize(h->mq_copied), "staging wait");
+  if(n > h->mq_pinned_cap)
+  {
+    if(h->mq_pinned) cudaFreeHost(h->mq_pinned);
+    h->mq_pinned = nullptr;
+    h->mq_pinned_cap = 0;
+    const long long cap = std::max(2*n, 1ll << 16);
+    CU(cudaMallocHost(reinterpret_cast<void**>(&h->mq_pinned), cap*sizeof(double)), "pinned");
+    h->mq_pinned_cap = cap;
+  }
+  std::memcpy(h->mq_pinned, u, n*sizeof(double));
+  const long long p = q.supplied % q.cap;
+  const long long n1 = std::min(n, q.cap - p);
+  CU(cudaMemcpyAsync(q.buf + p, h->mq_pinned, n1*sizeof(double), cudaMemcpyHostToDevice,
+                     h->stream), "supply copy");
+  if(n1 < n)
+    CU(cudaMemcpyAsync(q.buf, h->mq_pinned + n1, (n - n1)*sizeof(double),
+                       cudaMemcpyHostToDevice, h->stream), "supply copy");
+  CU(cudaEventRecord(h->mq_copied, h->stream), "event");
+  q.supplied += n;
+  return 0;
+}
+
+int mass_lb_draw_masks_queued(mass_lb_handle* h, int kinds, double division_coef,
+                              double division_radius, double death_coef, double death_radius,
+                              double phi_critical, double alpha, double beta)
+{
+  if(!h) return fail(MASS_LB_EINVAL, "null handle");
+  if(h->model == NEM) return fail(MASS_LB_EUNSUPPORTED, "the nematic model has no phi");
+  if(kinds < 1 || kinds > 3) return fail(MASS_LB_EINVAL, "kinds: bit 0 division, bit 1 death");
+  DeviceGuard g(h->device);
+  if(int r = ensure_masks(h)) return r;
+  if(int r = ensure_queue(h)) return r;
+  MaskScratch& m = h->mk;
+  const MaskQueue& q = h->mq;
+  cudaError_t e = with_phi(h, [&](const auto& v) { return mask_count(v, m, h->stream); });
+  if(e != cudaSuccess) return cuda_fail(e, "mask candidates");
+  int slot = 0;
+  if(kinds & 1)
+  {
+    e = with_phi(h, [&](const auto& v) {
+      return mask_draw_queued(v, m, q, 0, slot, division_coef, phi_critical, division_radius,
+                              h->mq_err, h->stream);
+    });
+    if(e != cudaSuccess) return cuda_fail(e, "division mask");
+    ++slot;
+  }
+  if(kinds & 2)
+  {
+    e = with_phi(h, [&](const auto& v) {
+      return mask_draw_queued(v, m, q, 1, slot, death_coef, phi_critical, death_radius,
+                              h->mq_err, h->stream);
+    });
+    if(e != cudaSuccess) return cuda_fail(e, "death mask");
+    ++slot;
+  }
+  e = mask_queue_advance(m, q, slot, h->stream);
+  if(e != cudaSuccess) return cuda_fail(e, "queue advance");
+  // the consumed count and error flag travel to pinned memory behind the
+  // kernels; the caller reads them later without stalling this call
+  CU(cudaMemcpyAsync(h->mq_host, q.head, sizeof(long long), cudaMemcpyDeviceToHost, h->stream),
+     "queue count");
+  CU(cudaMemcpyAsync(h->mq_host + 1, h->mq_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream),
+     "queue flag");
+  CU(cudaEventRecord(h->mq_counted, h->stream), "event");
+  h->mq_drawn = true;
+  void* plane = nullptr;
+  int dbl = 0, gg = 0, EY = 0;
+  if(int r = source_plane(h, &plane, &dbl, &gg, &EY)) return r;
+  e = dbl ? mask_rate<double>(static_cast<int>(h->LX), static_cast<int>(h->LY), gg, EY, m, alpha,
+                              beta, static_cast<double*>(plane), h->stream)
+          : mask_rate<float>(static_cast<int>(h->LX), static_cast<int>(h->LY), gg, EY, m, alpha,
+                             beta, static_cast<float*>(plane), h->stream);
+  if(e != cudaSuccess) return cuda_fail(e, "mask rate");
+  if(h->fused && h->cfg.nt != 32) h->tuned = false;   // the source runs in the warp-strip kernel
+  h->s64.src = h->src64;
+  h->s32.src = h->src32;
+  h->src_on = true;
+  return 0;
+}
+
+int mass_lb_mask_consumed(mass_lb_handle* h, long long* consumed)
+{
+  if(!h || !consumed) return fail(MASS_LB_EINVAL, "null argument");
+  DeviceGuard g(h->device);
+  if(int r = queue_refresh(h)) return r;
+  *consumed = h->mq_consumed;
   return 0;
 }
 

@@ -25,6 +25,17 @@ struct MaskScratch
   long long draws_cap = 0;
 };
 
+// Uniforms supplied ahead by the caller, consumed on the device: a ring of
+// `cap` doubles, `head` (device) = draws taken so far, `supplied` = draws
+// written so far (host-side count, passed to the kernels by value).
+struct MaskQueue
+{
+  double* buf = nullptr;
+  long long cap = 0;
+  long long* head = nullptr;
+  long long supplied = 0;
+};
+
 int mask_blocks(long long nsites);
 
 template<typename T>
@@ -32,6 +43,15 @@ cudaError_t mask_count(const MaskView<T>& v, const MaskScratch& s, cudaStream_t 
 template<typename T>
 cudaError_t mask_draw(const MaskView<T>& v, const MaskScratch& s, int kind, long long ndraws,
                       double coef, double phi_critical, double radius, cudaStream_t st);
+// centre test and circles of one mask (kind 0 division, 1 death) from the
+// queue, its draws starting kslot candidate counts past the head
+template<typename T>
+cudaError_t mask_draw_queued(const MaskView<T>& v, const MaskScratch& s, const MaskQueue& q,
+                             int kind, int kslot, double coef, double phi_critical, double radius,
+                             int* err, cudaStream_t st);
+// head += nkinds * candidates, after the masks of one draw
+cudaError_t mask_queue_advance(const MaskScratch& s, const MaskQueue& q, int nkinds,
+                               cudaStream_t st);
 template<typename T>
 cudaError_t mask_rate(int LX, int LY, int g, int EY, const MaskScratch& s, double alpha,
                       double beta, T* src, cudaStream_t st);

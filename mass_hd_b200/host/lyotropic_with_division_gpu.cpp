@@ -41,31 +41,45 @@ void LyotropicWithDivisionGPU::Configure()
 
 void LyotropicWithDivisionGPU::SetMasks()
 {
-  long long candidates = -1;
-  auto draw = [&](int kind, double rate_coef, double radius) {
-    if(candidates < 0)
-    {
-      const int r = mass_lb_mask_candidates(lattice, &candidates);
-      if(r != MASS_LB_OK) throw error_msg(mass_gpu::abi_error("mass_lb_mask_candidates", r));
-    }
-    // one random_real() per site with phi >= .5, in site order, from the
-    // reference's generator; the centres and circles are drawn on the device
-    last_candidates = candidates;
-    const double* draws = TakeDraws(static_cast<size_t>(candidates));
-    const int r = mass_lb_draw_mask(lattice, kind, draws, candidates, rate_coef,
-                                    phi_critical, radius, alpha, beta);
-    if(r != MASS_LB_OK) throw error_msg(mass_gpu::abi_error("mass_lb_draw_mask", r));
-  };
+  // the reference's schedule (:37, :73): a mask is redrawn when its counter
+  // runs out, then the counter restarts from its life time
+  int kinds = 0;
   if(not division_count--)
   {
-    draw(0, division_rate, division_radius);
+    kinds |= 1;
     division_count = division_time;
   }
   if(not death_count--)
   {
-    draw(1, death_rate, death_radius);
+    kinds |= 2;
     death_count = death_time;
   }
+  if(!kinds) return;
+  // The device takes one uniform per site with phi >= .5 and mask, in site
+  // order, from a queue of the reference generator's values. Keeping
+  // 2*LX*LY of them unconsumed covers two masks of any count, so the host
+  // never waits for the candidate count; it only learns, from the previous
+  // draw, how many values to add.
+  long long consumed = 0;
+  int r = mass_lb_mask_consumed(lattice, &consumed);
+  if(r != MASS_LB_OK) throw error_msg(mass_gpu::abi_error("mass_lb_mask_consumed", r));
+  const long long want = consumed + 2*static_cast<long long>(DomainSize);
+  if(supplied < want)
+  {
+    const size_t n = static_cast<size_t>(want - supplied);
+    draws.resize(n);
+#ifdef MASS_GPU_STANDALONE
+    random_reals(draws.data(), n);   // the same values as n random_real() calls
+#else
+    for(auto& u : draws) u = random_real();
+#endif
+    r = mass_lb_mask_supply(lattice, draws.data(), static_cast<long long>(n));
+    if(r != MASS_LB_OK) throw error_msg(mass_gpu::abi_error("mass_lb_mask_supply", r));
+    supplied = want;
+  }
+  r = mass_lb_draw_masks_queued(lattice, kinds, division_rate, division_radius, death_rate,
+                                death_radius, phi_critical, alpha, beta);
+  if(r != MASS_LB_OK) throw error_msg(mass_gpu::abi_error("mass_lb_draw_masks_queued", r));
 }
 
 void LyotropicWithDivisionGPU::SyncMasks()
@@ -80,31 +94,6 @@ void LyotropicWithDivisionGPU::SyncMasks()
   }
 }
 
-void LyotropicWithDivisionGPU::DrawAhead(size_t n)
-{
-  if(fifo.size() - fifo_head >= n) return;
-  if(fifo_head > 0)
-  {
-    fifo.erase(fifo.begin(), fifo.begin() + static_cast<std::ptrdiff_t>(fifo_head));
-    fifo_head = 0;
-  }
-  const size_t have = fifo.size();
-  fifo.resize(n);
-#ifdef MASS_GPU_STANDALONE
-  random_reals(fifo.data() + have, n - have);   // the same values, in bulk
-#else
-  for(size_t i = have; i < n; ++i) fifo[i] = random_real();
-#endif
-}
-
-const double* LyotropicWithDivisionGPU::TakeDraws(size_t n)
-{
-  DrawAhead(n);
-  const double* p = fifo.data() + fifo_head;
-  fifo_head += n;
-  return p;
-}
-
 void LyotropicWithDivisionGPU::Step()
 {
   // Step() must not throw (src/models.hpp:81-86): a failure is kept and
@@ -113,10 +102,6 @@ void LyotropicWithDivisionGPU::Step()
   try { SetMasks(); }
   catch(const error_msg& e) { step_error = e.what(); return; }
   LyotropicGPU::Step();
-  // while the device steps, draw the values of the next masks (two masks
-  // of about the last candidate count); only masks consume the generator
-  // after Configure(), so drawing early leaves every value in its place
-  DrawAhead(2*static_cast<size_t>(last_candidates));
 }
 
 void LyotropicWithDivisionGPU::RuntimeChecks()

@@ -3,11 +3,12 @@
 // on a B200 through include/mass_lb.h and include/mass_lb_ext.h.
 //
 // Same options, members and serialization order as the reference model.
-// The division and death masks follow the reference's SetMasks(): the host
-// draws one random_real() per site with phi >= .5 in site order from the
-// reference's generator (mass_lb_mask_candidates gives their number), and
-// the device picks the centres, draws the circles and sets the source rate
-// alpha*division_mask - beta*death_mask (mass_lb_draw_mask). When division
+// The division and death masks follow the reference's SetMasks(): one
+// random_real() per site with phi >= .5 in site order from the reference's
+// generator. The host queues the generator's values on the device ahead of
+// need (mass_lb_mask_supply), and the device counts the candidates, takes
+// their draws, picks the centres, draws the circles and sets the source
+// rate alpha*division_mask - beta*death_mask (mass_lb_draw_masks_queued). When division
 // and death are off the device applies the conserve_phi correction
 // (mass_lb_set_phi_conservation).
 #ifndef MODELS_LYOTROPIC_WITH_DIVISION_GPU_HPP_
@@ -25,17 +26,12 @@ protected:
   double phi_critical = 1;
   unsigned division_count = 0, death_count = 0;
   bool conserve_phi = false;
-  /** random_real() values drawn ahead of need, in stream order:
-   * fifo[fifo_head..] are the next values a mask takes. They are drawn
-   * while the device runs a step, so the host's share of a mask draw is
-   * only the candidate count and the copy. */
-  std::vector<double> fifo;
-  size_t fifo_head = 0;
-  long long last_candidates = 0;
-  /** Make at least `n` values available in the fifo. */
-  void DrawAhead(size_t n);
-  /** The next `n` values of the stream (valid until the next DrawAhead). */
-  const double* TakeDraws(size_t n);
+  /** random_real() values handed to the device's draw queue so far, and
+   * the buffer they pass through. Values are drawn ahead of need, in
+   * stream order; only the masks consume the generator after Configure(),
+   * so every value keeps its place in the reference's stream. */
+  long long supplied = 0;
+  std::vector<double> draws;
 
   /** Redraw the masks that are due (src/models/lyotropic-with-division.cpp:35-106). */
   void SetMasks();

@@ -134,6 +134,9 @@ def load_library(build_if_missing: bool = False):
         "mass_lb_draw_mask": (C.c_int, [vp, C.c_int, dp, C.c_longlong, C.c_double, C.c_double,
                                         C.c_double, C.c_double, C.c_double]),
         "mass_lb_get_mask": (C.c_int, [vp, C.c_int, C.POINTER(C.c_ubyte)]),
+        "mass_lb_mask_supply": (C.c_int, [vp, dp, C.c_longlong]),
+        "mass_lb_draw_masks_queued": (C.c_int, [vp, C.c_int] + [C.c_double] * 7),
+        "mass_lb_mask_consumed": (C.c_int, [vp, C.POINTER(C.c_longlong)]),
         "mass_lb_relax_free_energy": (C.c_int, [vp, C.c_uint, C.c_double, C.c_int, C.c_int, dp]),
         "mass_lb_ensemble_create": (C.c_int, [C.c_int, C.POINTER(Params), C.POINTER(C.c_uint),
                                               C.POINTER(C.c_uint), C.POINTER(vp)]),
@@ -302,6 +305,24 @@ class Lattice:
         _check(load_library().mass_lb_draw_mask(self.h, int(kind), _dp(d), d.size, float(coef),
                                                 float(phi_critical), float(radius),
                                                 float(alpha), float(beta)))
+
+    def mask_supply(self, draws):
+        """Queue uniforms (stream order) for draw_masks_queued."""
+        d = np.ascontiguousarray(draws, dtype=np.float64)
+        _check(load_library().mass_lb_mask_supply(self.h, _dp(d), d.size))
+
+    def draw_masks_queued(self, kinds: int, division_coef: float, division_radius: float,
+                          death_coef: float, death_radius: float, phi_critical: float,
+                          alpha: float, beta: float):
+        """Division (bit 0) and/or death (bit 1) masks from queued draws."""
+        _check(load_library().mass_lb_draw_masks_queued(
+            self.h, int(kinds), float(division_coef), float(division_radius), float(death_coef),
+            float(death_radius), float(phi_critical), float(alpha), float(beta)))
+
+    def mask_consumed(self) -> int:
+        n = C.c_longlong()
+        _check(load_library().mass_lb_mask_consumed(self.h, C.byref(n)))
+        return n.value
 
     def get_mask(self, kind: int) -> np.ndarray:
         out = np.empty(self.LX * self.LY, dtype=np.uint8)

@@ -196,3 +196,60 @@ def test_device_masks_follow_reference_rule(LX, LY, bc, prec):
         a.draw_mask(2, np.zeros(n), 0.1, 1.3, 1.0, 0.05, 0.03)
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("prec", [M.FP64, M.FP32])
+def test_queued_masks_equal_direct_masks(prec):
+    """mass_lb_draw_masks_queued takes the same uniforms in the same order as
+    mass_lb_draw_mask: over a run whose masks are redrawn on a schedule
+    (division alone, death alone, both in one step), two lattices, one fed
+    through the queue and one draw by draw, keep bit-identical masks and
+    states, and the queue reports every draw it consumed."""
+    LX, LY = 64, 64
+    st = O.synthetic_state(O.LYOTROPIC, LX, LY, seed=12, flow=0.01, phi_kind="disk",
+                           radius=LX / 3)
+    p = params()
+    a = M.Lattice(M.LYOTROPIC, p, LX, LY, 0, prec)
+    b = M.Lattice(M.LYOTROPIC, p, LX, LY, 0, prec)
+    a.upload_state(st)
+    b.upload_state(st)
+    rng = np.random.default_rng(3)
+    stream = rng.uniform(0, 1, 200000)
+    pos_b = 0
+    a.mask_supply(stream[:2 * LX * LY])
+    supplied = 2 * LX * LY
+    args = dict(division_coef=0.3, division_radius=2.5, death_coef=0.2, death_radius=1.5,
+                phi_critical=1.3, alpha=0.05, beta=0.03)
+    for t in range(12):
+        kinds = (1 if t % 3 == 0 else 0) | (2 if t % 2 == 0 else 0)
+        if kinds:
+            consumed = a.mask_consumed()
+            assert consumed == pos_b
+            if supplied - consumed < 2 * LX * LY:
+                n = consumed + 2 * LX * LY - supplied
+                a.mask_supply(stream[supplied:supplied + n])
+                supplied += n
+            a.draw_masks_queued(kinds, **args)
+            n = b.mask_candidates()
+            if kinds & 1:
+                b.draw_mask(0, stream[pos_b:pos_b + n], 0.3, 1.3, 2.5, 0.05, 0.03)
+                pos_b += n
+            if kinds & 2:
+                b.draw_mask(1, stream[pos_b:pos_b + n], 0.2, 1.3, 1.5, 0.05, 0.03)
+                pos_b += n
+        a.step(1)
+        b.step(1)
+    assert a.mask_consumed() == pos_b
+    for kind in (0, 1):
+        assert np.array_equal(a.get_mask(kind), b.get_mask(kind))
+    for n_ in STATE:
+        assert bits_equal(a.get(n_), b.get(n_)), n_
+    # a queue that runs dry is reported
+    c = M.Lattice(M.LYOTROPIC, p, LX, LY, 0, prec)
+    c.upload_state(st)
+    c.mask_supply(stream[:10])
+    c.draw_masks_queued(1, **args)
+    with pytest.raises(M.MassLBError):
+        c.mask_consumed()
+    for x in (a, b, c):
+        x.close()
