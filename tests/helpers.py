@@ -9,8 +9,8 @@ import numpy as np
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
-# BASELINE config 1 physics (CN->CC, Aphi->AA, Kphi->KK, Kn->LL,
-# Gammaphi->GammaP, tau -> tauNem = tauIso)
+# physics of the 256^2 CPU-runnable lyotropic configuration (CN->CC,
+# Aphi->AA, Kphi->KK, Kn->LL, Gammaphi->GammaP, tau -> tauNem = tauIso)
 LYO_C1 = dict(GammaQ=0.3, GammaP=0.1, xi=0.7, tauNem=1.5, tauIso=1.5, rho=40.0,
               friction=0.0, AA=0.1, CC=0.1, LL=0.05, KK=0.05, zeta=0.01,
               zetaI=0.0, conc=1.0, npc=1)
@@ -18,7 +18,7 @@ LYO_C1 = dict(GammaQ=0.3, GammaP=0.1, xi=0.7, tauNem=1.5, tauIso=1.5, rho=40.0,
 LYO_ALL = dict(GammaQ=0.3, GammaP=0.1, xi=0.7, tauNem=1.5, tauIso=1.2, rho=40.0,
                friction=0.02, AA=0.1, CC=0.1, LL=0.05, KK=0.05, zeta=0.03,
                zetaI=0.01, conc=0.9, npc=1)
-# BASELINE config 2 physics (CC fixed at 0.1 and stated)
+# physics of the 2048^2 nematic FP32-vs-FP64 configuration (CC fixed at 0.1)
 NEM_C2 = dict(Gamma=0.3, xi=0.7, tau=1.5, rho=40.0, friction=0.0, CC=0.1,
               LL=0.05, zeta=0.02, npc=1)
 NEM_ALL = dict(NEM_C2, friction=0.01)

@@ -4,7 +4,7 @@
   parameters.json and frame3.json must be text-identical to the reference's
   (same Configure() random stream, bit-exact steps, same JSON writer).
 * Configure() of every initial configuration against the reference's.
-* An FP32 run of the BASELINE initial state (random director, tanh disk)
+* An FP32 run of the benchmark's initial state (random director, tanh disk)
   through several output intervals, with the runtime checks on.
 """
 import json
