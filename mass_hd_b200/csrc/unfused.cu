@@ -240,7 +240,11 @@ uq_kernel(Dims d, Params P, State<T> s)
   }
 }
 
-template<typename T, bool DEV, int MODEL, bool FIRST>
+// PUSH (periodic lattices without a ghost ring, predictor only): the new ff
+// and fn of direction v go straight to the site they stream to, in the
+// ff_tmp/fn_tmp planes, which is Move (:371-386) fused into UpdateFields;
+// the same values land where move_kernel would put them.
+template<typename T, bool DEV, int MODEL, bool FIRST, bool PUSH = false>
 __global__ void __launch_bounds__(256)
 uf_kernel(Dims d, Params P, State<T> s)
 {
@@ -249,6 +253,11 @@ uf_kernel(Dims d, Params P, State<T> s)
   if(x >= d.LX || y >= d.LY) return;
   const Nbr<T> nb = neighbours<T>(d, x + d.g, y + d.g);
   const long long e = nb.e, NE = d.NE;
+  // where direction v streams to (PUSH)
+  auto dest = [&](int v) {
+    const int X = wrapi(x + d.g + CXv(v), d.EX), Y = wrapi(y + d.g + CYv(v), d.EY);
+    return Y + static_cast<long long>(d.EY)*X;
+  };
 
   const T nstore = s.n[e];
   const T nn = DEV ? T(P.rho) + nstore : nstore;
@@ -369,8 +378,11 @@ uf_kernel(Dims d, Params P, State<T> s)
       {
         const T f = FF[v*NE+e];
         const T force = T(Wv(v))*(Fx*T(CXv(v)) + Fy*T(CYv(v)));
-        FN[v*NE+e] = f + T(.5)*((fe[v]-f)/tau + force);
-        FF[v*NE+e] = f +      ((fe[v]-f)/tau + force);
+        const long long o = PUSH ? dest(v) : e;
+        T* fn_out = PUSH ? s.fn_tmp : FN;
+        T* ff_out = PUSH ? s.ff_tmp : FF;
+        fn_out[v*NE+o] = f + T(.5)*((fe[v]-f)/tau + force);
+        ff_out[v*NE+o] = f +      ((fe[v]-f)/tau + force);
       }
     }
     else
@@ -411,8 +423,11 @@ uf_kernel(Dims d, Params P, State<T> s)
         const T f = FF[v*NE+e];
         const T force = T(Wv(v))*(Fx*T(CXv(v)) + Fy*T(CYv(v)));
         const T fnv = f + T(.5)*((fe[v]-f)/tau + force) + T(0);
-        FN[v*NE+e] = fnv;
-        FF[v*NE+e] = fnv + T(.5)*((fe[v]-f)/tau + force);
+        const long long o = PUSH ? dest(v) : e;
+        T* fn_out = PUSH ? s.fn_tmp : FN;
+        T* ff_out = PUSH ? s.ff_tmp : FF;
+        fn_out[v*NE+o] = fnv;
+        ff_out[v*NE+o] = fnv + T(.5)*((fe[v]-f)/tau + force);
       }
     }
     else
@@ -899,10 +914,19 @@ int step_impl(const Dims& d, const Params& P, State<T>& s, int bc,
     uq_kernel<T, DEV, MODEL, false><<<grd, blk, 0, st>>>(d, P, s);
     fields2_bc();
     if(MODEL != NEM && s.conserve_phi) phi_sum<T>(d, s.phi, s.phisum, st);
-    uf_kernel<T, DEV, MODEL, true><<<grd, blk, 0, st>>>(d, P, s);
-    swap_fields();
-    if(bc) bc_lb_kernel<T><<<1, 1024, 0, st>>>(d, s.ff, s.fn, lbk);
-    move_kernel<T><<<egrd, blk, 0, st>>>(d, s.ff, s.fn, s.ff_tmp, s.fn_tmp);
+    if(bc)
+    {
+      uf_kernel<T, DEV, MODEL, true><<<grd, blk, 0, st>>>(d, P, s);
+      swap_fields();
+      bc_lb_kernel<T><<<1, 1024, 0, st>>>(d, s.ff, s.fn, lbk);
+      move_kernel<T><<<egrd, blk, 0, st>>>(d, s.ff, s.fn, s.ff_tmp, s.fn_tmp);
+    }
+    else
+    {
+      // no walls: Move happens inside UpdateFields
+      uf_kernel<T, DEV, MODEL, true, true><<<grd, blk, 0, st>>>(d, P, s);
+      swap_fields();
+    }
     std::swap(s.ff, s.ff_tmp);
     std::swap(s.fn, s.fn_tmp);
     for(unsigned c = 1; c <= P.npc; ++c)
@@ -947,10 +971,11 @@ int bc_mode(int model, int bc)
 
 int launches_unfused(int model, int bc, unsigned npc)
 {
-  // predictor: [bc] uq [bc] uf [bc] move ; corrector: [bc] uq [bc] uf
+  // predictor: [bc] uq [bc] uf [bc move] (periodic: Move inside uf);
+  // corrector: [bc] uq [bc] uf
   const int w = bc ? 1 : 0;
   (void)model;
-  return (2 + 3*w + 1) + (int)npc*(2 + 2*w);
+  return (2 + 4*w) + (int)npc*(2 + 2*w);
 }
 
 int step_unfused_f64(const Dims& d, const Params& P, State<double>& s, int bc,

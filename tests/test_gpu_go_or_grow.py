@@ -163,6 +163,34 @@ def test_fp32_go_or_grow_within_tolerance():
     b.close()
 
 
+@pytest.mark.parametrize("bc", [1, 2, 3, 4])
+def test_fp32_go_or_grow_walls_within_tolerance(bc):
+    """The FP32 sweeps with every wall type against FP64, masks on."""
+    p = params()
+    LX, LY = 48, 40
+    ref = O.RefOracle(O.GO_OR_GROW, p, LX, LY, bc)
+    ref.configure(8)
+    st = {n: ref.get(n) for n in STATE}
+    a = M.Lattice(M.GO_OR_GROW, p, LX, LY, bc, M.FP32)
+    b = M.Lattice(M.GO_OR_GROW, p, LX, LY, bc, M.FP64)
+    a.upload_state(st)
+    b.upload_state(st)
+    for _ in range(12):
+        ref.step(1)
+        rate, _ = rate_of(ref, p)
+        a.set_phi_source(rate)
+        b.set_phi_source(rate)
+        a.step(1)
+        b.step(1)
+    for n in STATE + ("chi",):
+        x, y = a.get(n), b.get(n)
+        if n == "ff":
+            x, y = ff_dev(x, 40.0), ff_dev(y, 40.0)
+        assert rel_l2(x, y) < 1e-4, (bc, n)
+    a.close()
+    b.close()
+
+
 def test_fp32_conserve_phi_parallel_sum():
     """FP32 sweeps take countphi from a parallel FP64 sum (FP64 keeps the
     serial site order): with division and death off, phi stays at its
