@@ -222,7 +222,7 @@ int alloc_state(mass_lb_handle* h, State<T>& s)
   const size_t NE = static_cast<size_t>(h->d.NE);
   T** lb[4] = {&s.ff, &s.fn, &s.ff_tmp, &s.fn_tmp};
   for(auto p : lb) if(int r = dalloc(h, p, 9*NE)) return r;
-  std::vector<T**> sc = {&s.Qxx, &s.Qyx, &s.QNxx, &s.QNyx, &s.n, &s.ux, &s.uy,
+  std::vector<T**> sc = {&s.Qxx, &s.Qyx, &s.Qxx_tmp, &s.Qyx_tmp, &s.QNxx, &s.QNyx, &s.n, &s.ux, &s.uy,
                          &s.Hxx, &s.Hyx, &s.dxQxx, &s.dyQxx, &s.dxQyx, &s.dyQyx,
                          &s.sXX, &s.sYY, &s.sYX, &s.sXY};
   if(h->model != NEM)
@@ -246,7 +246,7 @@ int zero_state(mass_lb_handle* h, State<T>& s)
   const size_t NE = static_cast<size_t>(h->d.NE);
   T* lb[4] = {s.ff, s.fn, s.ff_tmp, s.fn_tmp};
   for(T* p : lb) CU(cudaMemsetAsync(p, 0, 9*NE*sizeof(T), h->stream), "memset");
-  std::vector<T*> sc = {s.Qxx, s.Qyx, s.QNxx, s.QNyx, s.n, s.ux, s.uy, s.Hxx, s.Hyx,
+  std::vector<T*> sc = {s.Qxx, s.Qyx, s.Qxx_tmp, s.Qyx_tmp, s.QNxx, s.QNyx, s.n, s.ux, s.uy, s.Hxx, s.Hyx,
                         s.dxQxx, s.dyQxx, s.dxQyx, s.dyQyx, s.sXX, s.sYY, s.sYX, s.sXY};
   if(h->model != NEM)
   {

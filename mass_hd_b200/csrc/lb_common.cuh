@@ -72,6 +72,7 @@ struct State
 {
   T *ff, *fn, *ff_tmp, *fn_tmp;               // 9 planes each
   T *Qxx, *Qyx, *QNxx, *QNyx, *phi, *phn, *phi_tmp;
+  T *Qxx_tmp, *Qyx_tmp;  // the next Q, written beside Q by the sub-step kernel
   T *n, *ux, *uy, *uxp, *uyp, *Hxx, *Hyx, *MU;
   T *dxQxx, *dyQxx, *dxQyx, *dyQyx;
   T *sXX, *sYY, *sYX, *sXY;

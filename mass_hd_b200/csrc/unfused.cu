@@ -9,6 +9,9 @@
 //                        assigns every target exactly the value the
 //                        reference's push assigns it
 //   BoundaryConditions*-> bc_*_kernel (src/fields.hpp:620-930)
+//   periodic lattices -> substep_kernel: UpdateQuantities on a tile plus a
+//                        one-site ring in shared memory, then UpdateFields
+//                        (and, in the predictor, Move) in the same launch
 //
 // Two instantiations:
 //   T = double, DEV = false : the FP64 oracle mode. This file is compiled
@@ -91,15 +94,23 @@ __device__ __forceinline__ void equilibrium(T vx, T vy, T nn, T dn, T fe[9])
   }
 }
 
-template<typename T, bool DEV, int MODEL, bool DIAG>
-__global__ void __launch_bounds__(256)
-uq_kernel(Dims d, Params P, State<T> s)
+// The values one UpdateQuantities leaves at a site (src/models/lyotropic.cpp:
+// 215-247): density (n, or its deviation in DEV mode), velocity, phi flux,
+// molecular field, chemical potential, Q derivatives, stresses, and the
+// seven diagnostic stresses (DIAG).
+template<typename T>
+struct UQOut
 {
-  const int y = blockIdx.x*blockDim.x + threadIdx.x;
-  const int x = blockIdx.y*blockDim.y + threadIdx.y;
-  if(x >= d.LX || y >= d.LY) return;
-  const Nbr<T> nb = neighbours<T>(d, x + d.g, y + d.g);
-  const long long e = nb.e, NE = d.NE;
+  T n, ux, uy, uxp, uyp, Hxx, Hyx, MU, dxQxx, dyQxx, dxQyx, dyQyx, sXX, sYY, sXY, sYX;
+  T dg[7];
+};
+
+// UpdateQuantities of one site (the outputs in `o`)
+template<typename T, bool DEV, int MODEL, bool DIAG>
+__device__ __forceinline__ void uq_site(const Params& P, const State<T>& s, const Nbr<T>& nb,
+                                        const long long NE, UQOut<T>& o)
+{
+  const long long e = nb.e;
   const T* __restrict__ F = s.ff;
   const T f0 = F[e], f1 = F[NE+e], f2 = F[2*NE+e], f3 = F[3*NE+e], f4 = F[4*NE+e],
           f5 = F[5*NE+e], f6 = F[6*NE+e], f7 = F[7*NE+e], f8 = F[8*NE+e];
@@ -120,13 +131,13 @@ uq_kernel(Dims d, Params P, State<T> s)
 
   const T CC = T(P.CC), LL = T(P.LL), xi = T(P.xi), zeta = T(P.zeta);
 
-  s.n[e] = DEV ? dn : nn;   // DEV mode keeps the density deviation
-  s.ux[e] = vx;
-  s.uy[e] = vy;
-  s.dxQxx[e] = dxQxx;
-  s.dxQyx[e] = dxQyx;
-  s.dyQxx[e] = dyQxx;
-  s.dyQyx[e] = dyQyx;
+  o.n = DEV ? dn : nn;   // DEV mode keeps the density deviation
+  o.ux = vx;
+  o.uy = vy;
+  o.dxQxx = dxQxx;
+  o.dxQyx = dxQyx;
+  o.dyQxx = dyQxx;
+  o.dyQyx = dyQyx;
 
   if constexpr (MODEL == LYO)
   {
@@ -148,25 +159,25 @@ uq_kernel(Dims d, Params P, State<T> s)
       - T(2)*LL*(dxQxx*dyQxx+dxQyx*dyQyx);
     const T sigmaA = T(2)*(Qxx*Hyx - Qyx*Hxx);
 
-    s.uxp[e] = vx*p;
-    s.uyp[e] = vy*p;
-    s.Hxx[e] = Hxx;
-    s.Hyx[e] = Hyx;
-    s.MU[e] = mu;
-    s.sXX[e] = sigmaF + sigmaB + zetaI*(conc-p);
-    s.sYY[e] = -sigmaF + sigmaB + zetaI*(conc-p);
-    s.sXY[e] = sigmaS + sigmaA;
-    s.sYX[e] = sigmaS - sigmaA;
+    o.uxp = vx*p;
+    o.uyp = vy*p;
+    o.Hxx = Hxx;
+    o.Hyx = Hyx;
+    o.MU = mu;
+    o.sXX = sigmaF + sigmaB + zetaI*(conc-p);
+    o.sYY = -sigmaF + sigmaB + zetaI*(conc-p);
+    o.sXY = sigmaS + sigmaA;
+    o.sYX = sigmaS - sigmaA;
     if constexpr (DIAG)
     {
-      s.diag[0][e] = sigmaB + zetaI*(conc-p);
-      s.diag[1][e] = sigmaF - T(.5)*KK*(dyPhi*dyPhi-dxPhi*dxPhi) + zeta*Qxx*(T(1)-p);
+      o.dg[0] = sigmaB + zetaI*(conc-p);
+      o.dg[1] = sigmaF - T(.5)*KK*(dyPhi*dyPhi-dxPhi*dxPhi) + zeta*Qxx*(T(1)-p);
       // the reference uses zeta*Qxx here too (src/models/lyotropic.cpp:242)
-      s.diag[2][e] = sigmaS + KK*dxPhi*dyPhi + zeta*Qxx*(T(1)-p);
-      s.diag[3][e] = T(.5)*KK*(dyPhi*dyPhi-dxPhi*dxPhi);
-      s.diag[4][e] = -KK*dxPhi*dyPhi;
-      s.diag[5][e] = -zeta*Qxx*(T(1)-p);
-      s.diag[6][e] = -zeta*Qyx*(T(1)-p);
+      o.dg[2] = sigmaS + KK*dxPhi*dyPhi + zeta*Qxx*(T(1)-p);
+      o.dg[3] = T(.5)*KK*(dyPhi*dyPhi-dxPhi*dxPhi);
+      o.dg[4] = -KK*dxPhi*dyPhi;
+      o.dg[5] = -zeta*Qxx*(T(1)-p);
+      o.dg[6] = -zeta*Qyx*(T(1)-p);
     }
   }
   else if constexpr (MODEL == GOG)
@@ -199,24 +210,24 @@ uq_kernel(Dims d, Params P, State<T> s)
       - T(2)*LL*(dxQxx*dyQxx+dxQyx*dyQyx);
     const T sigmaA = T(2)*(Qxx*Hyx - Qyx*Hxx);
 
-    s.uxp[e] = vx*p;
-    s.uyp[e] = vy*p;
-    s.Hxx[e] = Hxx;
-    s.Hyx[e] = Hyx;
-    s.MU[e] = mu;
-    s.sXX[e] = sigmaF + sigmaB + zetaI*(conc-p);
-    s.sYY[e] = -sigmaF + sigmaB + zetaI*(conc-p);
-    s.sXY[e] = sigmaS + sigmaA;
-    s.sYX[e] = sigmaS - sigmaA;
+    o.uxp = vx*p;
+    o.uyp = vy*p;
+    o.Hxx = Hxx;
+    o.Hyx = Hyx;
+    o.MU = mu;
+    o.sXX = sigmaF + sigmaB + zetaI*(conc-p);
+    o.sYY = -sigmaF + sigmaB + zetaI*(conc-p);
+    o.sXY = sigmaS + sigmaA;
+    o.sYX = sigmaS - sigmaA;
     if constexpr (DIAG)
     {
-      s.diag[0][e] = sigmaB + zetaI*(conc-p);
-      s.diag[1][e] = sigmaF - T(.5)*KK*(dyPhi*dyPhi-dxPhi*dxPhi) + ap*Qxx;
-      s.diag[2][e] = sigmaS + KK*dxPhi*dyPhi + ap*Qyx;
-      s.diag[3][e] = T(.5)*KK*(dyPhi*dyPhi-dxPhi*dxPhi);
-      s.diag[4][e] = -KK*dxPhi*dyPhi;
-      s.diag[5][e] = -ap*Qxx;
-      s.diag[6][e] = -ap*Qyx;
+      o.dg[0] = sigmaB + zetaI*(conc-p);
+      o.dg[1] = sigmaF - T(.5)*KK*(dyPhi*dyPhi-dxPhi*dxPhi) + ap*Qxx;
+      o.dg[2] = sigmaS + KK*dxPhi*dyPhi + ap*Qyx;
+      o.dg[3] = T(.5)*KK*(dyPhi*dyPhi-dxPhi*dxPhi);
+      o.dg[4] = -KK*dxPhi*dyPhi;
+      o.dg[5] = -ap*Qxx;
+      o.dg[6] = -ap*Qyx;
     }
   }
   else
@@ -231,56 +242,127 @@ uq_kernel(Dims d, Params P, State<T> s)
     const T sigmaS = T(2)*xi*(Qyx*Qxx*Hxx + (Qyx*Qyx-T(1))*Hyx) - zeta*Qyx
       - T(2)*LL*(dxQxx*dyQxx+dxQyx*dyQyx);
     const T sigmaA = T(2)*(Qxx*Hyx - Qyx*Hxx);
-    s.Hxx[e] = Hxx;
-    s.Hyx[e] = Hyx;
-    s.sXX[e] = sigmaF + sigmaB;
-    s.sYY[e] = -sigmaF + sigmaB;
-    s.sXY[e] = sigmaS + sigmaA;
-    s.sYX[e] = sigmaS - sigmaA;
+    o.Hxx = Hxx;
+    o.Hyx = Hyx;
+    o.sXX = sigmaF + sigmaB;
+    o.sYY = -sigmaF + sigmaB;
+    o.sXY = sigmaS + sigmaA;
+    o.sYX = sigmaS - sigmaA;
   }
+}
+
+template<typename T, int MODEL, bool DIAG>
+__device__ __forceinline__ void store_uq(const State<T>& s, const long long e, const UQOut<T>& o)
+{
+  s.n[e] = o.n; s.ux[e] = o.ux; s.uy[e] = o.uy;
+  s.dxQxx[e] = o.dxQxx; s.dxQyx[e] = o.dxQyx; s.dyQxx[e] = o.dyQxx; s.dyQyx[e] = o.dyQyx;
+  s.Hxx[e] = o.Hxx; s.Hyx[e] = o.Hyx;
+  s.sXX[e] = o.sXX; s.sYY[e] = o.sYY; s.sXY[e] = o.sXY; s.sYX[e] = o.sYX;
+  if constexpr (MODEL != NEM)
+  {
+    s.uxp[e] = o.uxp; s.uyp[e] = o.uyp; s.MU[e] = o.MU;
+    if constexpr (DIAG)
+    {
+#pragma unroll
+      for(int k = 0; k < 7; ++k) s.diag[k][e] = o.dg[k];
+    }
+  }
+}
+
+template<typename T, bool DEV, int MODEL, bool DIAG>
+__global__ void __launch_bounds__(256)
+uq_kernel(Dims d, Params P, State<T> s)
+{
+  const int y = blockIdx.x*blockDim.x + threadIdx.x;
+  const int x = blockIdx.y*blockDim.y + threadIdx.y;
+  if(x >= d.LX || y >= d.LY) return;
+  const Nbr<T> nb = neighbours<T>(d, x + d.g, y + d.g);
+  UQOut<T> o;
+  uq_site<T, DEV, MODEL, DIAG>(P, s, nb, d.NE, o);
+  store_uq<T, MODEL, DIAG>(s, nb.e, o);
 }
 
 // PUSH (periodic lattices without a ghost ring, predictor only): the new ff
 // and fn of direction v go straight to the site they stream to, in the
 // ff_tmp/fn_tmp planes, which is Move (:371-386) fused into UpdateFields;
 // the same values land where move_kernel would put them.
-template<typename T, bool DEV, int MODEL, bool FIRST, bool PUSH = false>
-__global__ void __launch_bounds__(256)
-uf_kernel(Dims d, Params P, State<T> s)
+// UpdateQuantities fields, in the order of UQOut
+enum { Q_N = 0, Q_UX, Q_UY, Q_UXP, Q_UYP, Q_HXX, Q_HYX, Q_MU, Q_DXQXX, Q_DYQXX, Q_DXQYX,
+       Q_DYQYX, Q_SXX, Q_SYY, Q_SXY, Q_SYX, NUQ };
+
+// The UpdateQuantities values of a site (w = 0) and its neighbours +x, -x,
+// +y, -y (w = 1..4), with the stencils of src/lb.hpp in their operand order.
+template<typename T, class Derived>
+struct UQStencil
 {
-  const int y = blockIdx.x*blockDim.x + threadIdx.x;
-  const int x = blockIdx.y*blockDim.y + threadIdx.y;
-  if(x >= d.LX || y >= d.LY) return;
-  const Nbr<T> nb = neighbours<T>(d, x + d.g, y + d.g);
+  __device__ __forceinline__ T dx(int f) const
+  { const Derived& a = static_cast<const Derived&>(*this); return T(.5)*(a.at(f, 1)-a.at(f, 2)) + T(0); }
+  __device__ __forceinline__ T dy(int f) const
+  { const Derived& a = static_cast<const Derived&>(*this); return T(.5)*(a.at(f, 3)-a.at(f, 4)) + T(0); }
+  __device__ __forceinline__ T lap(int f) const
+  {
+    const Derived& a = static_cast<const Derived&>(*this);
+    return a.at(f, 1)+a.at(f, 2)+a.at(f, 3)+a.at(f, 4) - T(4)*a.at(f, 0) + T(0);
+  }
+};
+
+// ... read from the global planes of the state
+template<typename T>
+struct GlobalUQ : UQStencil<T, GlobalUQ<T>>
+{
+  const T* p[NUQ];
+  long long k[5];
+  __device__ __forceinline__ GlobalUQ(const State<T>& s, const Nbr<T>& nb)
+  {
+    p[Q_N] = s.n; p[Q_UX] = s.ux; p[Q_UY] = s.uy; p[Q_UXP] = s.uxp; p[Q_UYP] = s.uyp;
+    p[Q_HXX] = s.Hxx; p[Q_HYX] = s.Hyx; p[Q_MU] = s.MU; p[Q_DXQXX] = s.dxQxx;
+    p[Q_DYQXX] = s.dyQxx; p[Q_DXQYX] = s.dxQyx; p[Q_DYQYX] = s.dyQyx; p[Q_SXX] = s.sXX;
+    p[Q_SYY] = s.sYY; p[Q_SXY] = s.sXY; p[Q_SYX] = s.sYX;
+    k[0] = nb.e; k[1] = nb.e1; k[2] = nb.e2; k[3] = nb.e3; k[4] = nb.e4;
+  }
+  __device__ __forceinline__ T at(int f, int w) const { return __ldg(p[f] + k[w]); }
+};
+
+// UpdateFields of one site. `U` gives the UpdateQuantities values at the
+// site and its four neighbours (global planes, or a shared-memory tile).
+// SEP: the new Q goes to Qxx_tmp/Qyx_tmp and the corrector's populations to
+// ff_tmp (the sub-step kernel, whose blocks read Q and ff around their tile
+// while other blocks update theirs); otherwise both are updated in place.
+template<typename T, bool DEV, int MODEL, bool FIRST, bool PUSH, class UQA, bool SEP = false>
+__device__ __forceinline__ void uf_site(const Dims& d, const Params& P, const State<T>& s,
+                                        const Nbr<T>& nb, const int x, const int y, const UQA& U)
+{
   const long long e = nb.e, NE = d.NE;
+  T* const QXo = SEP ? s.Qxx_tmp : s.Qxx;
+  T* const QYo = SEP ? s.Qyx_tmp : s.Qyx;
   // where direction v streams to (PUSH)
   auto dest = [&](int v) {
     const int X = wrapi(x + d.g + CXv(v), d.EX), Y = wrapi(y + d.g + CYv(v), d.EY);
     return Y + static_cast<long long>(d.EY)*X;
   };
 
-  const T nstore = s.n[e];
+  const T nstore = U.at(Q_N, 0);
   const T nn = DEV ? T(P.rho) + nstore : nstore;
   const T dn = nstore;
-  const T vx = s.ux[e];
-  const T vy = s.uy[e];
+  const T vx = U.at(Q_UX, 0);
+  const T vy = U.at(Q_UY, 0);
   const T Qxx = s.Qxx[e];
   const T Qyx = s.Qyx[e];
-  const T Hxx = s.Hxx[e];
-  const T Hyx = s.Hyx[e];
-  const T dxQxx = s.dxQxx[e];
-  const T dyQxx = s.dyQxx[e];
-  const T dxQyx = s.dxQyx[e];
-  const T dyQyx = s.dyQyx[e];
+  const T Hxx = U.at(Q_HXX, 0);
+  const T Hyx = U.at(Q_HYX, 0);
+  const T dxQxx = U.at(Q_DXQXX, 0);
+  const T dyQxx = U.at(Q_DYQXX, 0);
+  const T dxQyx = U.at(Q_DXQYX, 0);
+  const T dyQyx = U.at(Q_DYQYX, 0);
 
-  const T dxux = dX(s.ux, nb);
-  const T dyux = dY(s.ux, nb);
-  const T dxuy = dX(s.uy, nb);
-  const T dyuy = dY(s.uy, nb);
-  const T dxSxx = dX(s.sXX, nb);
-  const T dySxy = dY(s.sXY, nb);
-  const T dxSyx = dX(s.sYX, nb);
-  const T dySyy = dY(s.sYY, nb);
+  const T dxux = U.dx(Q_UX);
+  const T dyux = U.dy(Q_UX);
+  const T dxuy = U.dx(Q_UY);
+  const T dyuy = U.dy(Q_UY);
+  const T dxSxx = U.dx(Q_SXX);
+  const T dySxy = U.dy(Q_SXY);
+  const T dxSyx = U.dx(Q_SYX);
+  const T dySyy = U.dy(Q_SYY);
 
   const T GammaQ = T(P.GammaQ), xi = T(P.xi), friction = T(P.friction);
 
@@ -315,16 +397,16 @@ uf_kernel(Dims d, Params P, State<T> s)
       const T rate = s.src ? s.src[e] : T(0);
       const T chi_eff = s.chi[e];
       R = chi_eff*p*rate;
-      const T mFlux = T(.5)*(s.ux[nb.e1]*s.m[nb.e1] - s.ux[nb.e2]*s.m[nb.e2])
-                    + T(.5)*(s.uy[nb.e3]*s.m[nb.e3] - s.uy[nb.e4]*s.m[nb.e4]);
+      const T mFlux = T(.5)*(U.at(Q_UX, 1)*s.m[nb.e1] - U.at(Q_UX, 2)*s.m[nb.e2])
+                    + T(.5)*(U.at(Q_UY, 3)*s.m[nb.e3] - U.at(Q_UY, 4)*s.m[nb.e4]);
       const T chi_px = s.chi[nb.e1], chi_mx = s.chi[nb.e2];
       const T chi_py = s.chi[nb.e3], chi_my = s.chi[nb.e4];
-      const T MUe = s.MU[e];
+      const T MUe = U.at(Q_MU, 0);
       const T diffusiveMFlux =
-        T(.5)*(chi_px + chi_eff)*(s.MU[nb.e1] - MUe)
-      - T(.5)*(chi_eff + chi_mx)*(MUe - s.MU[nb.e2])
-      + T(.5)*(chi_py + chi_eff)*(s.MU[nb.e3] - MUe)
-      - T(.5)*(chi_eff + chi_my)*(MUe - s.MU[nb.e4]);
+        T(.5)*(chi_px + chi_eff)*(U.at(Q_MU, 1) - MUe)
+      - T(.5)*(chi_eff + chi_mx)*(MUe - U.at(Q_MU, 2))
+      + T(.5)*(chi_py + chi_eff)*(U.at(Q_MU, 3) - MUe)
+      - T(.5)*(chi_eff + chi_my)*(MUe - U.at(Q_MU, 4));
       const T phenotypeDiffusion =
         T(.5)*(s.phi[nb.e1] + p)*(chi_px - chi_eff)
       - T(.5)*(p + s.phi[nb.e2])*(chi_eff - chi_mx)
@@ -346,8 +428,8 @@ uf_kernel(Dims d, Params P, State<T> s)
       s.m_tmp[e] = mt;
       s.chi_tmp[e] = pt > T(1e-12) ? mt/pt : T(0);
     };
-    const T del2mu = lap(s.MU, nb);
-    const T pFlux = dX(s.uxp, nb) + dY(s.uyp, nb);
+    const T del2mu = U.lap(Q_MU);
+    const T pFlux = U.dx(Q_UXP) + U.dy(Q_UYP);
     // conserve_phi is false for Lyotropic (src/models/lyotropic.hpp:46) and
     // set by the division models when division and death are off
     // (src/models/lyotropic-with-division.cpp:30)
@@ -360,8 +442,8 @@ uf_kernel(Dims d, Params P, State<T> s)
       s.QNxx[e] = s.Qxx[e] + T(.5)*Dxx;
       s.QNyx[e] = s.Qyx[e] + T(.5)*Dyx;
       s.phn[e]  = s.phi[e] + T(.5)*Dp;
-      s.Qxx[e]  = s.Qxx[e] + Dxx;
-      s.Qyx[e]  = s.Qyx[e] + Dyx;
+      QXo[e]  = s.Qxx[e] + Dxx;
+      QYo[e]  = s.Qyx[e] + Dyx;
       T pt = s.phi[e] + Dp;
       if constexpr (MODEL == GOG)
       {
@@ -387,8 +469,8 @@ uf_kernel(Dims d, Params P, State<T> s)
     }
     else
     {
-      s.Qxx[e] = s.QNxx[e] + T(.5)*Dxx;
-      s.Qyx[e] = s.QNyx[e] + T(.5)*Dyx;
+      QXo[e] = s.QNxx[e] + T(.5)*Dxx;
+      QYo[e] = s.QNyx[e] + T(.5)*Dyx;
       T pt = s.phn[e] + T(.5)*Dp;
       if constexpr (MODEL == GOG)
       {
@@ -402,7 +484,7 @@ uf_kernel(Dims d, Params P, State<T> s)
       {
         const T f = FF[v*NE+e];
         const T force = T(Wv(v))*(Fx*T(CXv(v)) + Fy*T(CYv(v)));
-        FF[v*NE+e] = FN[v*NE+e] + T(.5)*((fe[v]-f)/tau + force);
+        (SEP ? s.ff_tmp : FF)[v*NE+e] = FN[v*NE+e] + T(.5)*((fe[v]-f)/tau + force);
       }
     }
   }
@@ -415,8 +497,8 @@ uf_kernel(Dims d, Params P, State<T> s)
       const T qn_yx = s.Qyx[e] + T(.5)*Dyx + T(0);
       s.QNxx[e] = qn_xx;
       s.QNyx[e] = qn_yx;
-      s.Qxx[e] = qn_xx + T(.5)*Dxx;
-      s.Qyx[e] = qn_yx + T(.5)*Dyx;
+      QXo[e] = qn_xx + T(.5)*Dxx;
+      QYo[e] = qn_yx + T(.5)*Dyx;
 #pragma unroll
       for(int v=0; v<9; ++v)
       {
@@ -432,17 +514,92 @@ uf_kernel(Dims d, Params P, State<T> s)
     }
     else
     {
-      s.Qxx[e] = s.QNxx[e] + T(.5)*Dxx;
-      s.Qyx[e] = s.QNyx[e] + T(.5)*Dyx;
+      QXo[e] = s.QNxx[e] + T(.5)*Dxx;
+      QYo[e] = s.QNyx[e] + T(.5)*Dyx;
 #pragma unroll
       for(int v=0; v<9; ++v)
       {
         const T f = FF[v*NE+e];
         const T force = T(Wv(v))*(Fx*T(CXv(v)) + Fy*T(CYv(v)));
-        FF[v*NE+e] = FN[v*NE+e] + T(.5)*((fe[v]-f)/tau + force);
+        (SEP ? s.ff_tmp : FF)[v*NE+e] = FN[v*NE+e] + T(.5)*((fe[v]-f)/tau + force);
       }
     }
   }
+}
+
+template<typename T, bool DEV, int MODEL, bool FIRST, bool PUSH = false>
+__global__ void __launch_bounds__(256)
+uf_kernel(Dims d, Params P, State<T> s)
+{
+  const int y = blockIdx.x*blockDim.x + threadIdx.x;
+  const int x = blockIdx.y*blockDim.y + threadIdx.y;
+  if(x >= d.LX || y >= d.LY) return;
+  const Nbr<T> nb = neighbours<T>(d, x + d.g, y + d.g);
+  const GlobalUQ<T> U(s, nb);
+  uf_site<T, DEV, MODEL, FIRST, PUSH>(d, P, s, nb, x, y, U);
+}
+
+// One predictor or corrector sub-step on a periodic lattice in one launch:
+// UpdateQuantities over the block's tile plus a one-site ring into shared
+// memory, then UpdateFields over the tile reading its stencils from there.
+// The ring sites are computed by both neighbouring blocks with the same
+// expressions, so the values equal the two-sweep form's; nothing derived is
+// written to HBM except on the last sub-step of a call (storeq), which
+// leaves the same planes the two sweeps leave. Blocks read Q, phi, chi and
+// ff around their tile, so the new Q and (corrector) ff are written beside
+// them (SEP) and the host swaps the planes after the launch.
+constexpr int SUB_TY = 32, SUB_TX = 8;                 // tile: y (contiguous) x x
+constexpr int SUB_HY = SUB_TY + 2, SUB_HX = SUB_TX + 2;
+constexpr int SUB_HS = SUB_HY*SUB_HX;
+
+template<typename T>
+struct TileUQ : UQStencil<T, TileUQ<T>>
+{
+  const T (*a)[SUB_HS];
+  int c;
+  __device__ __forceinline__ T at(int f, int w) const
+  {
+    const int off = w == 0 ? 0 : w == 1 ? SUB_HY : w == 2 ? -SUB_HY : w == 3 ? 1 : -1;
+    return a[f][c + off];
+  }
+};
+
+template<typename T, bool DEV, int MODEL, bool FIRST, bool DIAG>
+__global__ void __launch_bounds__(SUB_TY*SUB_TX)
+substep_kernel(Dims d, Params P, State<T> s, int storeq)
+{
+  __shared__ T uq_s[NUQ][SUB_HS];
+  const int y0 = blockIdx.x*SUB_TY, x0 = blockIdx.y*SUB_TX;
+  const int tid = threadIdx.y*SUB_TY + threadIdx.x;
+  for(int i = tid; i < SUB_HS; i += SUB_TY*SUB_TX)
+  {
+    const int hx = i/SUB_HY, hy = i - hx*SUB_HY;
+    const int X = x0 - 1 + hx, Y = y0 - 1 + hy;
+    // the ring one past the lattice's end is the periodic image of site 0
+    if(X > d.LX || Y > d.LY) continue;
+    const Nbr<T> nb = neighbours<T>(d, wrapi(X, d.LX), wrapi(Y, d.LY));
+    UQOut<T> o;
+    uq_site<T, DEV, MODEL, DIAG>(P, s, nb, d.NE, o);
+    uq_s[Q_N][i] = o.n; uq_s[Q_UX][i] = o.ux; uq_s[Q_UY][i] = o.uy;
+    uq_s[Q_HXX][i] = o.Hxx; uq_s[Q_HYX][i] = o.Hyx;
+    uq_s[Q_DXQXX][i] = o.dxQxx; uq_s[Q_DYQXX][i] = o.dyQxx;
+    uq_s[Q_DXQYX][i] = o.dxQyx; uq_s[Q_DYQYX][i] = o.dyQyx;
+    uq_s[Q_SXX][i] = o.sXX; uq_s[Q_SYY][i] = o.sYY; uq_s[Q_SXY][i] = o.sXY; uq_s[Q_SYX][i] = o.sYX;
+    if constexpr (MODEL != NEM)
+    {
+      uq_s[Q_UXP][i] = o.uxp; uq_s[Q_UYP][i] = o.uyp; uq_s[Q_MU][i] = o.MU;
+    }
+    if(storeq && hx >= 1 && hx <= SUB_TX && hy >= 1 && hy <= SUB_TY && X < d.LX && Y < d.LY)
+      store_uq<T, MODEL, DIAG>(s, nb.e, o);
+  }
+  __syncthreads();
+  const int y = y0 + threadIdx.x, x = x0 + threadIdx.y;
+  if(x >= d.LX || y >= d.LY) return;
+  const Nbr<T> nb = neighbours<T>(d, x, y);
+  TileUQ<T> U;
+  U.a = uq_s;
+  U.c = (threadIdx.y + 1)*SUB_HY + threadIdx.x + 1;
+  uf_site<T, DEV, MODEL, FIRST, FIRST, TileUQ<T>, true>(d, P, s, nb, x, y, U);
 }
 
 // Streaming as a pull over every extended site.
@@ -908,6 +1065,37 @@ int step_impl(const Dims& d, const Params& P, State<T>& s, int bc,
     if(MODEL == GOG) { std::swap(s.m, s.m_tmp); std::swap(s.chi, s.chi_tmp); }
   };
 
+  if(!bc && d.g == 0 && P.npc >= 1)
+  {
+    // periodic: one launch per sub-step
+    const dim3 sblk(SUB_TY, SUB_TX);
+    const dim3 sgrd((d.LY + SUB_TY - 1)/SUB_TY, (d.LX + SUB_TX - 1)/SUB_TX);
+    auto swap_sub = [&]() {
+      swap_fields();
+      std::swap(s.Qxx, s.Qxx_tmp);
+      std::swap(s.Qyx, s.Qyx_tmp);
+      std::swap(s.ff, s.ff_tmp);
+    };
+    for(unsigned it = 0; it < nsteps; ++it)
+    {
+      if(MODEL != NEM && s.conserve_phi) phi_sum<T>(d, s.phi, s.phisum, st);
+      substep_kernel<T, DEV, MODEL, true, false><<<sgrd, sblk, 0, st>>>(d, P, s, 0);
+      swap_sub();
+      std::swap(s.fn, s.fn_tmp);
+      for(unsigned c = 1; c <= P.npc; ++c)
+      {
+        const bool last = it + 1 == nsteps && c == P.npc;
+        if(MODEL != NEM && s.conserve_phi) phi_sum<T>(d, s.phi, s.phisum, st);
+        if(last && diag_last)
+          substep_kernel<T, DEV, MODEL, false, true><<<sgrd, sblk, 0, st>>>(d, P, s, 1);
+        else
+          substep_kernel<T, DEV, MODEL, false, false><<<sgrd, sblk, 0, st>>>(d, P, s, last ? 1 : 0);
+        swap_sub();
+      }
+    }
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+  }
+
   for(unsigned it = 0; it < nsteps; ++it)
   {
     fields_bc();
@@ -971,10 +1159,11 @@ int bc_mode(int model, int bc)
 
 int launches_unfused(int model, int bc, unsigned npc)
 {
-  // predictor: [bc] uq [bc] uf [bc move] (periodic: Move inside uf);
-  // corrector: [bc] uq [bc] uf
-  const int w = bc ? 1 : 0;
+  // periodic: one sub-step kernel per predictor and corrector;
+  // walls: predictor [bc] uq [bc] uf [bc move], corrector [bc] uq [bc] uf
   (void)model;
+  if(!bc && npc >= 1) return 1 + (int)npc;
+  const int w = bc ? 1 : 0;
   return (2 + 4*w) + (int)npc*(2 + 2*w);
 }
 
