@@ -25,6 +25,7 @@
 #include "lb_common.cuh"
 #include "unfused.h"
 
+#include <atomic>
 #include <type_traits>
 #include <utility>
 
@@ -568,7 +569,8 @@ template<typename T, bool DEV, int MODEL, bool FIRST, bool DIAG>
 __global__ void __launch_bounds__(SUB_TY*SUB_TX)
 substep_kernel(Dims d, Params P, State<T> s, int storeq)
 {
-  __shared__ T uq_s[NUQ][SUB_HS];
+  extern __shared__ __align__(16) unsigned char sub_smem[];
+  T (*uq_s)[SUB_HS] = reinterpret_cast<T (*)[SUB_HS]>(sub_smem);
   const int y0 = blockIdx.x*SUB_TY, x0 = blockIdx.y*SUB_TX;
   const int tid = threadIdx.y*SUB_TY + threadIdx.x;
   for(int i = tid; i < SUB_HS; i += SUB_TY*SUB_TX)
@@ -600,6 +602,31 @@ substep_kernel(Dims d, Params P, State<T> s, int storeq)
   U.a = uq_s;
   U.c = (threadIdx.y + 1)*SUB_HY + threadIdx.x + 1;
   uf_site<T, DEV, MODEL, FIRST, FIRST, TileUQ<T>, true>(d, P, s, nb, x, y, U);
+}
+
+// Launch a sub-step; its tile needs NUQ*SUB_HS values of shared memory,
+// above the 48 KB default for larger tiles in FP64.
+template<typename T, bool DEV, int MODEL, bool FIRST, bool DIAG>
+void launch_substep(const Dims& d, const Params& P, const State<T>& s, int storeq,
+                    cudaStream_t st)
+{
+  constexpr size_t bytes = sizeof(T)*NUQ*SUB_HS;
+  if constexpr (bytes > 48*1024)
+  {
+    static std::atomic<unsigned long long> done{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = 1ull << (dev & 63);
+    if(!(done.load() & bit))
+    {
+      cudaFuncSetAttribute(substep_kernel<T, DEV, MODEL, FIRST, DIAG>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+      done.fetch_or(bit);
+    }
+  }
+  const dim3 blk(SUB_TY, SUB_TX);
+  const dim3 grd((d.LY + SUB_TY - 1)/SUB_TY, (d.LX + SUB_TX - 1)/SUB_TX);
+  substep_kernel<T, DEV, MODEL, FIRST, DIAG><<<grd, blk, bytes, st>>>(d, P, s, storeq);
 }
 
 // Streaming as a pull over every extended site.
@@ -1068,8 +1095,6 @@ int step_impl(const Dims& d, const Params& P, State<T>& s, int bc,
   if(!bc && d.g == 0 && P.npc >= 1)
   {
     // periodic: one launch per sub-step
-    const dim3 sblk(SUB_TY, SUB_TX);
-    const dim3 sgrd((d.LY + SUB_TY - 1)/SUB_TY, (d.LX + SUB_TX - 1)/SUB_TX);
     auto swap_sub = [&]() {
       swap_fields();
       std::swap(s.Qxx, s.Qxx_tmp);
@@ -1079,7 +1104,7 @@ int step_impl(const Dims& d, const Params& P, State<T>& s, int bc,
     for(unsigned it = 0; it < nsteps; ++it)
     {
       if(MODEL != NEM && s.conserve_phi) phi_sum<T>(d, s.phi, s.phisum, st);
-      substep_kernel<T, DEV, MODEL, true, false><<<sgrd, sblk, 0, st>>>(d, P, s, 0);
+      launch_substep<T, DEV, MODEL, true, false>(d, P, s, 0, st);
       swap_sub();
       std::swap(s.fn, s.fn_tmp);
       for(unsigned c = 1; c <= P.npc; ++c)
@@ -1087,9 +1112,9 @@ int step_impl(const Dims& d, const Params& P, State<T>& s, int bc,
         const bool last = it + 1 == nsteps && c == P.npc;
         if(MODEL != NEM && s.conserve_phi) phi_sum<T>(d, s.phi, s.phisum, st);
         if(last && diag_last)
-          substep_kernel<T, DEV, MODEL, false, true><<<sgrd, sblk, 0, st>>>(d, P, s, 1);
+          launch_substep<T, DEV, MODEL, false, true>(d, P, s, 1, st);
         else
-          substep_kernel<T, DEV, MODEL, false, false><<<sgrd, sblk, 0, st>>>(d, P, s, last ? 1 : 0);
+          launch_substep<T, DEV, MODEL, false, false>(d, P, s, last ? 1 : 0, st);
         swap_sub();
       }
     }
