@@ -2,10 +2,10 @@
 
     python -m mass_hd_b200.build [--verbose]
 
-Each .cu is compiled for sm_100a only. unfused.cu (the FP64 oracle mode)
-is compiled with --fmad=false so that no multiply-add is contracted and the
-FP64 path rounds every operation as the reference's double-precision build
-does; the other units may contract.
+Each .cu is compiled for sm_100a only. unfused.cu is compiled twice: its
+FP64 half (the oracle mode) with --fmad=false, so that no multiply-add is
+contracted and every operation rounds as the reference's double-precision
+build rounds it, and its FP32 half with contraction on, like the other units.
 """
 from __future__ import annotations
 
@@ -27,17 +27,19 @@ LIB = os.path.join(LIBDIR, "libmass_lb.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
           "-I", INCLUDE, "-I", CSRC]
+# object -> (source, flags)
 UNITS = {
-    "unfused.cu": ["--fmad=false"],
-    "masks.cu": ["--fmad=false"],
-    "fused32.cu": [],
-    "fused_warp.cu": [],
-    "reduce.cu": [],
-    "stats.cu": [],
-    "api.cu": [],
-    "noalloc.cu": [],
-    "conv_tc.cu": [],
-    "surrogate_ops.cu": [],
+    "unfused": ("unfused.cu", ["--fmad=false", "-DMLB_UNFUSED_PART=64"]),
+    "unfused_f32": ("unfused.cu", ["-DMLB_UNFUSED_PART=32"]),
+    "masks": ("masks.cu", ["--fmad=false"]),
+    "fused32": ("fused32.cu", []),
+    "fused_warp": ("fused_warp.cu", []),
+    "reduce": ("reduce.cu", []),
+    "stats": ("stats.cu", []),
+    "api": ("api.cu", []),
+    "noalloc": ("noalloc.cu", []),
+    "conv_tc": ("conv_tc.cu", []),
+    "surrogate_ops": ("surrogate_ops.cu", []),
 }
 
 
@@ -63,17 +65,17 @@ def build(verbose: bool = False, force: bool = False, ptxas_verbose: bool = Fals
     have not changed since the last build."""
     os.makedirs(BUILD, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
-    units = {u: f for u, f in UNITS.items() if os.path.exists(os.path.join(CSRC, u))}
+    units = {u: sf for u, sf in UNITS.items() if os.path.exists(os.path.join(CSRC, sf[0]))}
     stamp = os.path.join(BUILD, "stamp")
-    digest = _sources_hash(ARCH + COMMON + sorted(units))
+    digest = _sources_hash(ARCH + COMMON + [f"{u}:{sf[0]}:{' '.join(sf[1])}" for u, sf in sorted(units.items())])
     if not force and os.path.exists(LIB) and os.path.exists(stamp):
         with open(stamp) as fh:
             if fh.read().strip() == digest:
                 return LIB
     objs = []
-    for unit, flags in units.items():
-        obj = os.path.join(BUILD, unit.replace(".cu", ".o"))
-        cmd = [nvcc()] + ARCH + COMMON + flags + ["-c", os.path.join(CSRC, unit), "-o", obj]
+    for unit, (src, flags) in units.items():
+        obj = os.path.join(BUILD, unit + ".o")
+        cmd = [nvcc()] + ARCH + COMMON + flags + ["-c", os.path.join(CSRC, src), "-o", obj]
         if ptxas_verbose:
             cmd += ["-Xptxas", "-v"]
         if verbose:

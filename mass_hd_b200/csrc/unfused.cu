@@ -13,15 +13,16 @@
 //                        one-site ring in shared memory, then UpdateFields
 //                        (and, in the predictor, Move) in the same launch
 //
-// Two instantiations:
-//   T = double, DEV = false : the FP64 oracle mode. This file is compiled
+// Two instantiations, built as two objects (MLB_UNFUSED_PART = 64 / 32):
+//   T = double, DEV = false : the FP64 oracle mode. Its object is compiled
 //     with --fmad=false and every expression keeps the reference's operand
 //     order, so each value is rounded exactly as the reference's x86-64
 //     build rounds it.
-//   T = float,  DEV = true  : FP32 on wall lattices (the fused kernel covers
-//     periodic ones). Populations are stored as deviations g_v = f_v - t_v*rho
-//     from the rest state, so the O(1e-3) flow signal is not lost against
-//     rho = 40 in a 24-bit mantissa.
+//   T = float,  DEV = true  : FP32 for go-or-grow, wall lattices and shapes
+//     the fused kernels do not take. Populations are stored as deviations
+//     g_v = f_v - t_v*rho from the rest state, so the O(1e-3) flow signal is
+//     not lost against rho = 40 in a 24-bit mantissa. Its object contracts
+//     multiply-adds, and it multiplies by 1/tau and 1/n where FP64 divides.
 #include "lb_common.cuh"
 #include "unfused.h"
 
@@ -120,8 +121,18 @@ __device__ __forceinline__ void uq_site(const Params& P, const State<T>& s, cons
   T nn, dn;
   if constexpr (DEV) { dn = f0 + f1 + f2 + f3 + f4 + f5 + f6 + f7 + f8; nn = T(P.rho) + dn; }
   else { nn = f0 + f1 + f2 + f3 + f4 + f5 + f6 + f7 + f8; dn = nn; }
-  const T vx = (f1 - f2 + f5 - f6 - f7 + f8)/nn;
-  const T vy = (f3 - f4 + f5 - f6 + f7 - f8)/nn;
+  T vx, vy;
+  if constexpr (DEV)
+  {
+    const T inn = T(1)/nn;
+    vx = (f1 - f2 + f5 - f6 - f7 + f8)*inn;
+    vy = (f3 - f4 + f5 - f6 + f7 - f8)*inn;
+  }
+  else
+  {
+    vx = (f1 - f2 + f5 - f6 - f7 + f8)/nn;
+    vy = (f3 - f4 + f5 - f6 + f7 - f8)/nn;
+  }
 
   const T del2Qxx = lap(s.Qxx, nb);
   const T dxQxx = dX(s.Qxx, nb);
@@ -438,6 +449,9 @@ __device__ __forceinline__ void uf_site(const Dims& d, const Params& P, const St
                                   : T(0);
     const T Dp = T(P.GammaP)*del2mu - pFlux - corr;
     const T tau = T(P.tauNem)*p + T(P.tauIso)*(T(1)-p);
+    // FP32 multiplies by 1/tau; FP64 divides as the reference does
+    const T itau = DEV ? T(1)/tau : T(0);
+    auto over_tau = [&](T a) { return DEV ? a*itau : a/tau; };
     if constexpr (FIRST)
     {
       s.QNxx[e] = s.Qxx[e] + T(.5)*Dxx;
@@ -464,8 +478,8 @@ __device__ __forceinline__ void uf_site(const Dims& d, const Params& P, const St
         const long long o = PUSH ? dest(v) : e;
         T* fn_out = PUSH ? s.fn_tmp : FN;
         T* ff_out = PUSH ? s.ff_tmp : FF;
-        fn_out[v*NE+o] = f + T(.5)*((fe[v]-f)/tau + force);
-        ff_out[v*NE+o] = f +      ((fe[v]-f)/tau + force);
+        fn_out[v*NE+o] = f + T(.5)*(over_tau(fe[v]-f) + force);
+        ff_out[v*NE+o] = f +      (over_tau(fe[v]-f) + force);
       }
     }
     else
@@ -485,13 +499,16 @@ __device__ __forceinline__ void uf_site(const Dims& d, const Params& P, const St
       {
         const T f = FF[v*NE+e];
         const T force = T(Wv(v))*(Fx*T(CXv(v)) + Fy*T(CYv(v)));
-        (SEP ? s.ff_tmp : FF)[v*NE+e] = FN[v*NE+e] + T(.5)*((fe[v]-f)/tau + force);
+        (SEP ? s.ff_tmp : FF)[v*NE+e] = FN[v*NE+e] + T(.5)*(over_tau(fe[v]-f) + force);
       }
     }
   }
   else
   {
     const T tau = T(P.tauNem);
+    // FP32 multiplies by 1/tau; FP64 divides as the reference does
+    const T itau = DEV ? T(1)/tau : T(0);
+    auto over_tau = [&](T a) { return DEV ? a*itau : a/tau; };
     if constexpr (FIRST)
     {
       const T qn_xx = s.Qxx[e] + T(.5)*Dxx + T(0);
@@ -505,12 +522,12 @@ __device__ __forceinline__ void uf_site(const Dims& d, const Params& P, const St
       {
         const T f = FF[v*NE+e];
         const T force = T(Wv(v))*(Fx*T(CXv(v)) + Fy*T(CYv(v)));
-        const T fnv = f + T(.5)*((fe[v]-f)/tau + force) + T(0);
+        const T fnv = f + T(.5)*(over_tau(fe[v]-f) + force) + T(0);
         const long long o = PUSH ? dest(v) : e;
         T* fn_out = PUSH ? s.fn_tmp : FN;
         T* ff_out = PUSH ? s.ff_tmp : FF;
         fn_out[v*NE+o] = fnv;
-        ff_out[v*NE+o] = fnv + T(.5)*((fe[v]-f)/tau + force);
+        ff_out[v*NE+o] = fnv + T(.5)*(over_tau(fe[v]-f) + force);
       }
     }
     else
@@ -522,7 +539,7 @@ __device__ __forceinline__ void uf_site(const Dims& d, const Params& P, const St
       {
         const T f = FF[v*NE+e];
         const T force = T(Wv(v))*(Fx*T(CXv(v)) + Fy*T(CYv(v)));
-        (SEP ? s.ff_tmp : FF)[v*NE+e] = FN[v*NE+e] + T(.5)*((fe[v]-f)/tau + force);
+        (SEP ? s.ff_tmp : FF)[v*NE+e] = FN[v*NE+e] + T(.5)*(over_tau(fe[v]-f) + force);
       }
     }
   }
@@ -1159,6 +1176,11 @@ int step_impl(const Dims& d, const Params& P, State<T>& s, int bc,
 
 } // namespace
 
+#ifndef MLB_UNFUSED_PART
+#define MLB_UNFUSED_PART 0   // both precisions in one object
+#endif
+
+#if MLB_UNFUSED_PART != 32
 int lb_kind(int model, int bc)
 {
   if(model != NEM)
@@ -1203,6 +1225,23 @@ int step_unfused_f64(const Dims& d, const Params& P, State<double>& s, int bc,
   }
 }
 
+int relax_unfused_f64(const Dims& d, const Params& P, State<double>& s, int bc,
+                      unsigned nsteps, double dt, int relax_phi, int relax_Q,
+                      double* sum_out, cudaStream_t st)
+{
+  return relax_impl<double>(d, P, s, bc, nsteps, dt, relax_phi, relax_Q, sum_out, st);
+}
+
+int update_chi_f64(const Dims& d, State<double>& s, cudaStream_t st)
+{
+  const dim3 blk(64, 4);
+  chi_kernel<double><<<site_grid(d.LX, d.LY, blk), blk, 0, st>>>(d, s);
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+#endif
+
+#if MLB_UNFUSED_PART != 64
 int step_unfused_f32(const Dims& d, const Params& P, State<float>& s, int bc,
                      unsigned nsteps, bool diag_last, cudaStream_t st)
 {
@@ -1214,25 +1253,11 @@ int step_unfused_f32(const Dims& d, const Params& P, State<float>& s, int bc,
   }
 }
 
-int relax_unfused_f64(const Dims& d, const Params& P, State<double>& s, int bc,
-                      unsigned nsteps, double dt, int relax_phi, int relax_Q,
-                      double* sum_out, cudaStream_t st)
-{
-  return relax_impl<double>(d, P, s, bc, nsteps, dt, relax_phi, relax_Q, sum_out, st);
-}
-
 int relax_unfused_f32(const Dims& d, const Params& P, State<float>& s, int bc,
                       unsigned nsteps, double dt, int relax_phi, int relax_Q,
                       double* sum_out, cudaStream_t st)
 {
   return relax_impl<float>(d, P, s, bc, nsteps, dt, relax_phi, relax_Q, sum_out, st);
-}
-
-int update_chi_f64(const Dims& d, State<double>& s, cudaStream_t st)
-{
-  const dim3 blk(64, 4);
-  chi_kernel<double><<<site_grid(d.LX, d.LY, blk), blk, 0, st>>>(d, s);
-  return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 int update_chi_f32(const Dims& d, State<float>& s, cudaStream_t st)
@@ -1241,5 +1266,7 @@ int update_chi_f32(const Dims& d, State<float>& s, cudaStream_t st)
   chi_kernel<float><<<site_grid(d.LX, d.LY, blk), blk, 0, st>>>(d, s);
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
+
+#endif
 
 } // namespace mlb
