@@ -431,29 +431,33 @@ def run_ours_gog(args):
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind, "bytes_per_site": bps,
                 "traffic": None,
-                "note": "whole step (unfused sweeps, ~5 launches) against the primary state's "
-                        "bytes; small lattices are launch-bound"}
+                "note": "whole step (one sub-step kernel per predictor and corrector) against "
+                        "the primary state's bytes; small lattices are latency-bound"}
     lat.close()
 
-    # end to end: the driver on the runcard (host masks, Configure excluded)
-    n_e2e = max(args.steps, 30)
+    # end to end: the driver on the runcard (host masks, Configure excluded),
+    # long enough that the start (first supply, first checks) is amortised
+    # as in a production run
+    n_e2e = max(args.steps, 1000)
     with tempfile.TemporaryDirectory() as d:
         run_driver_gog(L, 3, args.precision, d)          # warm-up (build, first launch)
         t_loop = run_driver_gog(L, n_e2e, args.precision, d)
     t_loop = max_over_ranks(t_loop, world)
     # per step: one uniform (8 B) per phi >= 0.5 site up for every mask
-    # drawn (division every 3rd step, death every 2nd), and the 8-byte
-    # candidate count down on the steps that draw
+    # drawn (division every 3rd step, death every 2nd), and the 16-byte
+    # queue state (draws consumed, error flag) down on the steps that draw
     masks = sum((t % 3 == 0) + (t % 2 == 0) for t in range(n_e2e)) / n_e2e
     redraw = sum(1 for t in range(n_e2e) if t % 3 == 0 or t % 2 == 0) / n_e2e
     cand = int((st["phi"] >= 0.5).sum())
     e2e = {"value": whole_job_rate(sites, world, n_e2e, t_loop * 1e3), "unit": UNIT,
            "h2d_bytes_per_step": int(8 * cand * masks),
-           "d2h_bytes_per_step": int(8 * redraw),
+           "d2h_bytes_per_step": int(16 * redraw),
            "e2e_steps": n_e2e,
            "note": "mass-gpu driver on the runcard: Step() = host draws of the reference's "
-                   "random stream for the masks when due, masks and step on the device; "
-                   "driver clock around the time loop"}
+                   "random stream for the masks when due, written into pinned staging and "
+                   "queued up to three draws ahead; masks (one cooperative kernel per draw) "
+                   "and step on the device; driver clock around the time loop, device "
+                   "synchronised at its end"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -166,25 +166,40 @@ int mass_lb_get_mask(mass_lb_handle* h, int kind, unsigned char* out);
  * per candidate site and mask drawn.
  *
  * mass_lb_mask_supply: append n uniforms to the lattice's queue (a ring of
- * 3*LX*LY + 65536 draws; MASS_LB_EINVAL if the unconsumed draws would not
+ * 6*LX*LY + 65536 draws; MASS_LB_EINVAL if the unconsumed draws would not
  * fit). Asynchronous; `u` may be reused on return.
+ *
+ * mass_lb_mask_staging: a pinned host buffer of at least n doubles that the
+ * caller may fill and then pass as `u` to mass_lb_mask_supply, which sends
+ * it up without copying it first. It is free to write when this call
+ * returns (the previous supply's copy from it has been read); ask again
+ * before each fill.
  *
  * mass_lb_draw_masks_queued: `kinds` bit 0 draws the division mask, bit 1
  * the death mask. The candidates are counted on the device. The division
  * mask takes the next `count` queued draws, then the death mask the `count`
  * after those, as the reference draws them. Then the source becomes
  * alpha*division_mask - beta*death_mask, as mass_lb_draw_mask sets it.
- * Asynchronous. A caller that keeps at least 2*LX*LY draws unconsumed never
+ * Asynchronous: one cooperative kernel launch does the whole draw. A
+ * caller that keeps at least 2*LX*LY draws unconsumed never
  * runs the queue dry. When it does run dry, the next
  * mass_lb_mask_consumed fails with MASS_LB_EINVAL.
  *
  * mass_lb_mask_consumed: the number of queued draws taken so far, up to and
- * including the last mass_lb_draw_masks_queued (waits for that draw only). */
+ * including the last mass_lb_draw_masks_queued (waits for that draw only).
+ *
+ * mass_lb_mask_progress: the same count as far as the device has got,
+ * without waiting: `consumed` after the last queued draw that has finished,
+ * and `pending` queued draws issued after it. A caller that keeps
+ * 2*LX*LY*(pending + 1) draws beyond `consumed` supplied never runs the
+ * queue dry and, with pending <= 2, stays within the ring. */
 int mass_lb_mask_supply(mass_lb_handle* h, const double* u, long long n);
+int mass_lb_mask_staging(mass_lb_handle* h, long long n, double** buf);
 int mass_lb_draw_masks_queued(mass_lb_handle* h, int kinds, double division_coef,
                               double division_radius, double death_coef, double death_radius,
                               double phi_critical, double alpha, double beta);
 int mass_lb_mask_consumed(mass_lb_handle* h, long long* consumed);
+int mass_lb_mask_progress(mass_lb_handle* h, long long* consumed, int* pending);
 
 /* ---- go-or-grow -----------------------------------------------------------
  *

@@ -18,6 +18,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 using namespace mlb;
@@ -170,15 +171,20 @@ struct mass_lb_handle
   cudaEvent_t mk_copied = nullptr;   // the last staging copy has been read
 
   // queued uniforms (mass_lb_mask_supply / mass_lb_draw_masks_queued)
+  static constexpr int MQ_STAGES = 2;    // pinned staging buffers, used in turn
+  static constexpr int MQ_SLOTS = 4;     // queued draws whose counts may be in flight
   MaskQueue mq{};
-  double* mq_pinned = nullptr;        // staging of supplied draws
-  long long mq_pinned_cap = 0;
-  cudaEvent_t mq_copied = nullptr;    // the last supply copy has been read
-  long long* mq_host = nullptr;       // pinned: [0] draws consumed, [1] error flag
-  int* mq_err = nullptr;              // device: a mask needed more draws than supplied
-  cudaEvent_t mq_counted = nullptr;   // mq_host of the last queued draw has landed
-  long long mq_consumed = 0;          // last value read from mq_host[0]
-  bool mq_drawn = false;
+  double* mq_pinned[MQ_STAGES] = {};     // staging of supplied draws
+  long long mq_pinned_cap[MQ_STAGES] = {};
+  cudaEvent_t mq_copied[MQ_STAGES] = {}; // the last copy from each buffer has been read
+  int mq_stage = 0;                      // the buffer of the next supply
+  long long* mq_state = nullptr;         // device: [0] queue head, [1] error flag (low word)
+  int* mq_err = nullptr;                 // the error flag as the kernels set it
+  long long* mq_host = nullptr;          // pinned: mq_state of each draw slot
+  cudaEvent_t mq_counted[MQ_SLOTS] = {}; // a slot's mq_state has landed
+  long long mq_issued = 0;               // queued draws issued
+  long long mq_known = 0;                // draws whose counts have been read (a prefix)
+  long long mq_consumed = 0;             // draws consumed up to the last known draw
 };
 
 namespace {
@@ -497,10 +503,14 @@ void mass_lb_destroy(mass_lb_handle* h)
   for(void* p : h->allocs) cudaFree(p);
   if(h->mk_pinned) cudaFreeHost(h->mk_pinned);
   if(h->mk_copied) cudaEventDestroy(h->mk_copied);
-  if(h->mq_pinned) cudaFreeHost(h->mq_pinned);
+  for(int i = 0; i < mass_lb_handle::MQ_STAGES; ++i)
+  {
+    if(h->mq_pinned[i]) cudaFreeHost(h->mq_pinned[i]);
+    if(h->mq_copied[i]) cudaEventDestroy(h->mq_copied[i]);
+  }
+  for(int i = 0; i < mass_lb_handle::MQ_SLOTS; ++i)
+    if(h->mq_counted[i]) cudaEventDestroy(h->mq_counted[i]);
   if(h->mq_host) cudaFreeHost(h->mq_host);
-  if(h->mq_copied) cudaEventDestroy(h->mq_copied);
-  if(h->mq_counted) cudaEventDestroy(h->mq_counted);
   if(h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
@@ -1350,38 +1360,84 @@ namespace {
 int ensure_queue(mass_lb_handle* h)
 {
   if(h->mq.buf) return 0;
+  constexpr int S = mass_lb_handle::MQ_SLOTS, B = mass_lb_handle::MQ_STAGES;
   const long long N = static_cast<long long>(h->LX)*h->LY;
-  const long long cap = 3*N + (1ll << 16);
+  const long long cap = 6*N + (1ll << 16);
   if(int r = dalloc(h, &h->mq.buf, static_cast<size_t>(cap))) return r;
-  if(int r = dalloc(h, &h->mq.head, 1)) return r;
-  if(int r = dalloc(h, &h->mq_err, 1)) return r;
-  CU(cudaMemsetAsync(h->mq.head, 0, sizeof(long long), h->stream), "memset");
-  CU(cudaMemsetAsync(h->mq_err, 0, sizeof(int), h->stream), "memset");
-  CU(cudaMallocHost(reinterpret_cast<void**>(&h->mq_host), 2*sizeof(long long)), "pinned");
-  h->mq_host[0] = h->mq_host[1] = 0;
-  CU(cudaEventCreateWithFlags(&h->mq_copied, cudaEventDisableTiming), "event");
-  CU(cudaEventCreateWithFlags(&h->mq_counted, cudaEventDisableTiming), "event");
-  CU(cudaEventRecord(h->mq_copied, h->stream), "event");
+  if(int r = dalloc(h, &h->mq_state, 2)) return r;
+  h->mq.head = h->mq_state;
+  h->mq_err = reinterpret_cast<int*>(h->mq_state + 1);   // little-endian low word
+  CU(cudaMemsetAsync(h->mq_state, 0, 2*sizeof(long long), h->stream), "memset");
+  CU(cudaMallocHost(reinterpret_cast<void**>(&h->mq_host), 2*S*sizeof(long long)), "pinned");
+  for(int i = 0; i < 2*S; ++i) h->mq_host[i] = 0;
+  for(int i = 0; i < B; ++i)
+  {
+    CU(cudaEventCreateWithFlags(&h->mq_copied[i], cudaEventDisableTiming), "event");
+    CU(cudaEventRecord(h->mq_copied[i], h->stream), "event");
+  }
+  for(int i = 0; i < S; ++i)
+    CU(cudaEventCreateWithFlags(&h->mq_counted[i], cudaEventDisableTiming), "event");
   h->mq.cap = cap;
   h->mq.supplied = 0;
-  h->mq_consumed = 0;
+  h->mq_issued = h->mq_known = h->mq_consumed = 0;
   return 0;
 }
 
-// the consumed count and error flag of the last queued draw
-int queue_refresh(mass_lb_handle* h)
+// Read the counts of the queued draws that have landed, in order: all of
+// them up to draw `until` (waiting for them), then any later ones that are
+// already there.
+int queue_refresh(mass_lb_handle* h, long long until)
 {
-  if(!h->mq_drawn) return 0;
-  CU(cudaEventSynchronize(h->mq_counted), "queue count");
-  h->mq_consumed = h->mq_host[0];
-  if(h->mq_host[1])
-    return fail(MASS_LB_EINVAL, "a queued mask needed more draws than were supplied");
+  constexpr int S = mass_lb_handle::MQ_SLOTS;
+  while(h->mq_known < h->mq_issued)
+  {
+    const int sl = static_cast<int>(h->mq_known % S);
+    if(h->mq_known < until) CU(cudaEventSynchronize(h->mq_counted[sl]), "queue count");
+    else
+    {
+      const cudaError_t e = cudaEventQuery(h->mq_counted[sl]);
+      if(e == cudaErrorNotReady) break;
+      CU(e, "queue count");
+    }
+    h->mq_consumed = h->mq_host[2*sl];
+    if(h->mq_host[2*sl + 1])
+      return fail(MASS_LB_EINVAL, "a queued mask needed more draws than were supplied");
+    ++h->mq_known;
+  }
+  return 0;
+}
+
+// staging buffer i with room for n values (its previous copy has been
+// read: the caller waited on mq_copied[i])
+int ensure_staging(mass_lb_handle* h, int i, long long n)
+{
+  if(n <= h->mq_pinned_cap[i]) return 0;
+  if(h->mq_pinned[i]) cudaFreeHost(h->mq_pinned[i]);
+  h->mq_pinned[i] = nullptr;
+  h->mq_pinned_cap[i] = 0;
+  const long long cap = std::max(2*n, 1ll << 16);
+  CU(cudaMallocHost(reinterpret_cast<void**>(&h->mq_pinned[i]), cap*sizeof(double)), "pinned");
+  h->mq_pinned_cap[i] = cap;
   return 0;
 }
 
 } // namespace
 
 extern "C" {
+
+int mass_lb_mask_staging(mass_lb_handle* h, long long n, double** buf)
+{
+  if(!h || !buf) return fail(MASS_LB_EINVAL, "null argument");
+  if(h->model == NEM) return fail(MASS_LB_EUNSUPPORTED, "the nematic model has no phi");
+  if(n < 0) return fail(MASS_LB_EINVAL, "bad count");
+  DeviceGuard g(h->device);
+  if(int r = ensure_queue(h)) return r;
+  const int i = h->mq_stage;
+  CU(cudaEventSynchronize(h->mq_copied[i]), "staging wait");
+  if(int r = ensure_staging(h, i, n)) return r;
+  *buf = h->mq_pinned[i];
+  return 0;
+}
 
 int mass_lb_mask_supply(mass_lb_handle* h, const double* u, long long n)
 {
@@ -1394,30 +1450,34 @@ int mass_lb_mask_supply(mass_lb_handle* h, const double* u, long long n)
   MaskQueue& q = h->mq;
   if(q.supplied + n - h->mq_consumed > q.cap)
   {
-    if(int r = queue_refresh(h)) return r;
+    if(int r = queue_refresh(h, h->mq_issued)) return r;
     if(q.supplied + n - h->mq_consumed > q.cap)
-      return fail(MASS_LB_EINVAL, "mask queue full (more than 3*LX*LY + 65536 unconsumed draws)");
+      return fail(MASS_LB_EINVAL, "mask queue full (more than 6*LX*LY + 65536 unconsumed draws)");
   }
-  // the staging buffer is refilled once its previous copy has been read
-  CU(cudaEventSynchronize(h->mq_copied), "staging wait");
-  if(n > h->mq_pinned_cap)
+  // a staging buffer is refilled once its previous copy has been read;
+  // values written into it through mass_lb_mask_staging go up as they are
+  const int i = h->mq_stage;
+  const double* stage = h->mq_pinned[i];
+  const bool staged = u == stage;
+  if(staged && n > h->mq_pinned_cap[i])
+    return fail(MASS_LB_EINVAL, "more draws than the staging buffer holds");
+  CU(cudaEventSynchronize(h->mq_copied[i]), "staging wait");
+  if(!staged)
   {
-    if(h->mq_pinned) cudaFreeHost(h->mq_pinned);
-    h->mq_pinned = nullptr;
-    h->mq_pinned_cap = 0;
-    const long long cap = std::max(2*n, 1ll << 16);
-    CU(cudaMallocHost(reinterpret_cast<void**>(&h->mq_pinned), cap*sizeof(double)), "pinned");
-    h->mq_pinned_cap = cap;
+    if(int r = ensure_staging(h, i, n)) return r;
+    stage = h->mq_pinned[i];
+    std::memcpy(h->mq_pinned[i], u, n*sizeof(double));
   }
-  std::memcpy(h->mq_pinned, u, n*sizeof(double));
   const long long p = q.supplied % q.cap;
   const long long n1 = std::min(n, q.cap - p);
-  CU(cudaMemcpyAsync(q.buf + p, h->mq_pinned, n1*sizeof(double), cudaMemcpyHostToDevice,
+  CU(cudaMemcpyAsync(q.buf + p, stage, n1*sizeof(double), cudaMemcpyHostToDevice,
                      h->stream), "supply copy");
   if(n1 < n)
-    CU(cudaMemcpyAsync(q.buf, h->mq_pinned + n1, (n - n1)*sizeof(double),
+    CU(cudaMemcpyAsync(q.buf, stage + n1, (n - n1)*sizeof(double),
                        cudaMemcpyHostToDevice, h->stream), "supply copy");
-  CU(cudaEventRecord(h->mq_copied, h->stream), "event");
+  // the new count follows the values, so a draw sees both or neither
+  CU(cudaEventRecord(h->mq_copied[i], h->stream), "event");
+  h->mq_stage = i ^ 1;
   q.supplied += n;
   return 0;
 }
@@ -1432,47 +1492,26 @@ int mass_lb_draw_masks_queued(mass_lb_handle* h, int kinds, double division_coef
   DeviceGuard g(h->device);
   if(int r = ensure_masks(h)) return r;
   if(int r = ensure_queue(h)) return r;
-  MaskScratch& m = h->mk;
-  const MaskQueue& q = h->mq;
-  cudaError_t e = with_phi(h, [&](const auto& v) { return mask_count(v, m, h->stream); });
-  if(e != cudaSuccess) return cuda_fail(e, "mask candidates");
-  int slot = 0;
-  if(kinds & 1)
-  {
-    e = with_phi(h, [&](const auto& v) {
-      return mask_draw_queued(v, m, q, 0, slot, division_coef, phi_critical, division_radius,
-                              h->mq_err, h->stream);
-    });
-    if(e != cudaSuccess) return cuda_fail(e, "division mask");
-    ++slot;
-  }
-  if(kinds & 2)
-  {
-    e = with_phi(h, [&](const auto& v) {
-      return mask_draw_queued(v, m, q, 1, slot, death_coef, phi_critical, death_radius,
-                              h->mq_err, h->stream);
-    });
-    if(e != cudaSuccess) return cuda_fail(e, "death mask");
-    ++slot;
-  }
-  e = mask_queue_advance(m, q, slot, h->stream);
-  if(e != cudaSuccess) return cuda_fail(e, "queue advance");
-  // the consumed count and error flag travel to pinned memory behind the
-  // kernels; the caller reads them later without stalling this call
-  CU(cudaMemcpyAsync(h->mq_host, q.head, sizeof(long long), cudaMemcpyDeviceToHost, h->stream),
-     "queue count");
-  CU(cudaMemcpyAsync(h->mq_host + 1, h->mq_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream),
-     "queue flag");
-  CU(cudaEventRecord(h->mq_counted, h->stream), "event");
-  h->mq_drawn = true;
   void* plane = nullptr;
   int dbl = 0, gg = 0, EY = 0;
   if(int r = source_plane(h, &plane, &dbl, &gg, &EY)) return r;
-  e = dbl ? mask_rate<double>(static_cast<int>(h->LX), static_cast<int>(h->LY), gg, EY, m, alpha,
-                              beta, static_cast<double*>(plane), h->stream)
-          : mask_rate<float>(static_cast<int>(h->LX), static_cast<int>(h->LY), gg, EY, m, alpha,
-                             beta, static_cast<float*>(plane), h->stream);
-  if(e != cudaSuccess) return cuda_fail(e, "mask rate");
+  // this draw's count goes to a free slot (waiting for the draw that used it)
+  constexpr int S = mass_lb_handle::MQ_SLOTS;
+  if(int r = queue_refresh(h, h->mq_issued - S + 1)) return r;
+  const int sl = static_cast<int>(h->mq_issued % S);
+  // the source plane has phi's precision
+  const cudaError_t e = with_phi(h, [&](const auto& v) {
+    using T = std::remove_cv_t<std::remove_pointer_t<decltype(v.phi)>>;
+    if(dbl != (std::is_same<T, double>::value ? 1 : 0)) return cudaErrorInvalidValue;
+    const QueuedDraw<T> w{kinds, {division_coef, death_coef}, {division_radius, death_radius},
+                          phi_critical, alpha, beta, static_cast<T*>(plane), gg, EY, h->mq_err};
+    return mask_draw_queued_fused(v, h->mk, h->mq, w, h->stream);
+  });
+  if(e != cudaSuccess) return cuda_fail(e, "queued masks");
+  CU(cudaMemcpyAsync(h->mq_host + 2*sl, h->mq_state, 2*sizeof(long long), cudaMemcpyDeviceToHost,
+                     h->stream), "queue count");
+  CU(cudaEventRecord(h->mq_counted[sl], h->stream), "event");
+  ++h->mq_issued;
   if(h->fused && h->cfg.nt != 32) h->tuned = false;   // the source runs in the warp-strip kernel
   h->s64.src = h->src64;
   h->s32.src = h->src32;
@@ -1484,10 +1523,24 @@ int mass_lb_mask_consumed(mass_lb_handle* h, long long* consumed)
 {
   if(!h || !consumed) return fail(MASS_LB_EINVAL, "null argument");
   DeviceGuard g(h->device);
-  if(int r = queue_refresh(h)) return r;
+  if(int r = queue_refresh(h, h->mq_issued)) return r;
   *consumed = h->mq_consumed;
   return 0;
 }
+
+int mass_lb_mask_progress(mass_lb_handle* h, long long* consumed, int* pending)
+{
+  if(!h || !consumed || !pending) return fail(MASS_LB_EINVAL, "null argument");
+  DeviceGuard g(h->device);
+  if(int r = queue_refresh(h, 0)) return r;
+  *consumed = h->mq_consumed;
+  *pending = static_cast<int>(h->mq_issued - h->mq_known);
+  return 0;
+}
+
+} // extern "C"
+
+extern "C" {
 
 // ---- go-or-grow ------------------------------------------------------------
 

@@ -23,6 +23,8 @@
 
 #include <cmath>
 
+#include <cooperative_groups.h>
+
 namespace mlb {
 namespace {
 
@@ -31,6 +33,8 @@ constexpr int MB = 1024;   // sites per block in the counting/ranking kernels
 template<typename T>
 __device__ __forceinline__ double phi_at(const MaskView<T>& v, long long k)
 {
+  // without a ghost ring the plane is in site order already
+  if(v.g == 0 && v.EY == v.LY) return static_cast<double>(v.phi[k]);
   const int x = static_cast<int>(k / v.LY), y = static_cast<int>(k % v.LY);
   return static_cast<double>(v.phi[(y + v.g) + static_cast<long long>(v.EY)*(x + v.g)]);
 }
@@ -189,6 +193,146 @@ __global__ void rate_kernel(int LX, int LY, int g, int EY, const unsigned char* 
   }
 }
 
+// The circle of one centre site k, as stamp_kernel writes it (every writer
+// stores 1).
+__device__ __forceinline__ void stamp_circle(int LX, int LY, long long k,
+                                             unsigned char* __restrict__ mask, double r2, int R)
+{
+  const int cx = static_cast<int>(k / LY), cy = static_cast<int>(k % LY);
+  for(int dx = -R; dx <= R; ++dx)
+  {
+    const int x = ((cx + dx) % LX + LX) % LX;
+    for(int dy = -R; dy <= R; ++dy)
+    {
+      if(static_cast<double>(dx*dx + dy*dy) > r2) continue;
+      const int y = ((cy + dy) % LY + LY) % LY;
+      mask[y + static_cast<long long>(LY)*x] = 1;
+    }
+  }
+}
+
+// A queued draw in one cooperative launch (blocks of MB threads, each block
+// walking chunks of MB sites). Phases, separated by grid barriers:
+//  1. candidates per chunk; the masks being redrawn are cleared,
+//  2. every block forms the exclusive chunk offsets it needs and the total
+//     from all chunk counts (as scan_kernel), then the centres of its
+//     chunks: a candidate's draw for kind j is the queue entry
+//     head + slot_j*total + rank (division first), as center_queue_kernel,
+//     and a centre writes its circle into the mask of its kind (as
+//     stamp_kernel),
+//  3. the source plane alpha*division - beta*death (as rate_kernel) and
+//     head += kinds drawn * total.
+template<typename T>
+__global__ void __launch_bounds__(MB)
+queued_draw_kernel(MaskView<T> v, MaskScratch s, const double* __restrict__ queue, long long qcap,
+                   long long* head, long long supplied, QueuedDraw<T> w, double r2_0, int R0,
+                   double r2_1, int R1)
+{
+  namespace cg = cooperative_groups;
+  cg::grid_group grid = cg::this_grid();
+  __shared__ int warp_cnt[MB/32];
+  __shared__ long long part[MB];
+  const long long N = static_cast<long long>(v.LX)*v.LY;
+  const int nch = static_cast<int>((N + MB - 1)/MB);
+  const int tid = threadIdx.x;
+  const bool div = w.kinds & 1, dea = (w.kinds >> 1) & 1;
+
+  for(int c = blockIdx.x; c < nch; c += gridDim.x)
+  {
+    const long long k = static_cast<long long>(c)*MB + tid;
+    const int flag = k < N && phi_at(v, k) >= .5;
+    const int n = __syncthreads_count(flag);
+    if(tid == 0) s.block_cnt[c] = n;
+    if(k < N)
+    {
+      if(div) s.mask[0][k] = 0;
+      if(dea) s.mask[1][k] = 0;
+    }
+  }
+  grid.sync();
+
+  // exclusive prefix of the per-thread segments of the chunk counts
+  const int per = (nch + MB - 1)/MB;
+  {
+    const int lo = tid*per, hi = min(nch, lo + per);
+    long long sum = 0;
+    for(int i = lo; i < hi; ++i) sum += s.block_cnt[i];
+    part[tid] = sum;
+    __syncthreads();
+    for(int d = 1; d < MB; d <<= 1)
+    {
+      const long long add = tid >= d ? part[tid - d] : 0;
+      __syncthreads();
+      part[tid] += add;
+      __syncthreads();
+    }
+  }
+  const long long total = part[MB - 1], h0 = *head;
+  const unsigned lane = tid & 31u, warp = tid >> 5;
+  for(int c = blockIdx.x; c < nch; c += gridDim.x)
+  {
+    const long long k = static_cast<long long>(c)*MB + tid;
+    const double p = k < N ? phi_at(v, k) : 0.;
+    const bool flag = k < N && p >= .5;
+    const unsigned ballot = __ballot_sync(0xffffffffu, flag);
+    __syncthreads();   // warp_cnt of the previous chunk has been read
+    if(lane == 0) warp_cnt[warp] = __popc(ballot);
+    __syncthreads();
+    if(!flag) continue;
+    {
+      // chunk offset: the segments before c's, then the chunks before c in it
+      const int sg = c/per;
+      long long off = sg ? part[sg - 1] : 0;
+      for(int i = sg*per; i < c; ++i) off += s.block_cnt[i];
+      int before = 0;
+      for(unsigned i = 0; i < warp; ++i) before += warp_cnt[i];
+      before += __popc(ballot & ((1u << lane) - 1u));
+      const long long rank = off + before;
+      int slot = 0;
+      for(int j = 0; j < 2; ++j)
+      {
+        if(!((w.kinds >> j) & 1)) continue;
+        const long long idx = h0 + slot*total + rank;
+        ++slot;
+        if(idx < supplied)
+        {
+          // src/models/lyotropic-with-division.cpp:47 (division), :83 (death)
+          const double thr = j == 0 ? w.coef[0]*p*(1 - p/w.phi_critical) : w.coef[1]*p;
+          if(queue[idx % qcap] < thr)
+          {
+            if(j == 0 && R0 >= 0) stamp_circle(v.LX, v.LY, k, s.mask[0], r2_0, R0);
+            if(j == 1 && R1 >= 0) stamp_circle(v.LX, v.LY, k, s.mask[1], r2_1, R1);
+          }
+        }
+        else atomicOr(w.err, 1);
+      }
+    }
+  }
+  grid.sync();
+
+  const long long stride = static_cast<long long>(gridDim.x)*MB;
+  for(long long k = static_cast<long long>(blockIdx.x)*MB + tid; k < N; k += stride)
+  {
+    int x, y;
+    if(N <= 0xffffffffll)
+    {
+      const unsigned ku = static_cast<unsigned>(k), ly = static_cast<unsigned>(v.LY);
+      x = static_cast<int>(ku/ly);
+      y = static_cast<int>(ku - static_cast<unsigned>(x)*ly);
+    }
+    else
+    {
+      x = static_cast<int>(k / v.LY);
+      y = static_cast<int>(k % v.LY);
+    }
+    const unsigned char m0 = s.mask[0][k], m1 = s.mask[1][k];
+    // alpha*division_m - beta*death_m (src/models/lyotropic-with-division.cpp:121)
+    const double r = w.alpha*(m0 ? 1. : 0.) - w.beta*(m1 ? 1. : 0.);
+    w.src[(y + w.g) + static_cast<long long>(w.EY)*(x + w.g)] = static_cast<T>(r);
+  }
+  if(blockIdx.x == 0 && tid == 0) *head = h0 + (div + dea)*total;
+}
+
 inline int grid_for(long long n)
 {
   const long long b = (n + 255)/256;
@@ -268,6 +412,47 @@ cudaError_t mask_rate(int LX, int LY, int g, int EY, const MaskScratch& s, doubl
   return cudaGetLastError();
 }
 
+template<typename T>
+cudaError_t mask_draw_queued_fused(const MaskView<T>& v, const MaskScratch& s, const MaskQueue& q,
+                                   const QueuedDraw<T>& w, cudaStream_t st)
+{
+  // resident blocks only (a cooperative launch); per device, cached
+  static int grid_cache[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int& resident = grid_cache[dev & 63];
+  if(!resident)
+  {
+    int sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per_sm, queued_draw_kernel<T>, MB, 0);
+    if(e != cudaSuccess) return e;
+    resident = sms*(per_sm > 0 ? per_sm : 1);
+  }
+  const long long N = static_cast<long long>(v.LX)*v.LY;
+  const int nch = mask_blocks(N);
+  const int grid = nch < resident ? nch : resident;
+  // ceil(radius^2) as the reference computes it (:60, :96); R < 0: no circle
+  double r2[2];
+  int R[2];
+  for(int j = 0; j < 2; ++j)
+  {
+    r2[j] = std::ceil(w.radius[j]*w.radius[j]);
+    R[j] = r2[j] >= 0 ? static_cast<int>(std::floor(std::sqrt(r2[j]))) : -1;
+  }
+  MaskView<T> vv = v;
+  MaskScratch ss = s;
+  const double* qb = q.buf;
+  long long qcap = q.cap;
+  long long* head = q.head;
+  long long supplied = q.supplied;
+  QueuedDraw<T> ww = w;
+  void* args[] = {&vv, &ss, &qb, &qcap, &head, &supplied, &ww, &r2[0], &R[0], &r2[1], &R[1]};
+  return cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(queued_draw_kernel<T>),
+                                     dim3(grid), dim3(MB), args, 0, st);
+}
+
 template cudaError_t mask_count<double>(const MaskView<double>&, const MaskScratch&, cudaStream_t);
 template cudaError_t mask_count<float>(const MaskView<float>&, const MaskScratch&, cudaStream_t);
 template cudaError_t mask_draw<double>(const MaskView<double>&, const MaskScratch&, int, long long,
@@ -284,5 +469,12 @@ template cudaError_t mask_rate<double>(int, int, int, int, const MaskScratch&, d
                                        double*, cudaStream_t);
 template cudaError_t mask_rate<float>(int, int, int, int, const MaskScratch&, double, double,
                                       float*, cudaStream_t);
+
+template cudaError_t mask_draw_queued_fused<double>(const MaskView<double>&, const MaskScratch&,
+                                                   const MaskQueue&, const QueuedDraw<double>&,
+                                                   cudaStream_t);
+template cudaError_t mask_draw_queued_fused<float>(const MaskView<float>&, const MaskScratch&,
+                                                  const MaskQueue&, const QueuedDraw<float>&,
+                                                  cudaStream_t);
 
 } // namespace mlb

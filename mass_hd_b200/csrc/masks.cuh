@@ -36,6 +36,20 @@ struct MaskQueue
   long long supplied = 0;
 };
 
+// One queued draw: which masks, their coefficients and the source plane.
+template<typename T>
+struct QueuedDraw
+{
+  int kinds;             // bit 0 division, bit 1 death
+  double coef[2];        // division, death
+  double radius[2];
+  double phi_critical;
+  double alpha, beta;
+  T* src;                // the step kernels' source plane (ghost ring g, row stride EY)
+  int g, EY;
+  int* err;
+};
+
 int mask_blocks(long long nsites);
 
 template<typename T>
@@ -52,6 +66,12 @@ cudaError_t mask_draw_queued(const MaskView<T>& v, const MaskScratch& s, const M
 // head += nkinds * candidates, after the masks of one draw
 cudaError_t mask_queue_advance(const MaskScratch& s, const MaskQueue& q, int nkinds,
                                cudaStream_t st);
+// A whole queued draw in one cooperative launch: count, offsets, centres of
+// both kinds, circles, source plane and head advance, with grid barriers
+// between the phases.
+template<typename T>
+cudaError_t mask_draw_queued_fused(const MaskView<T>& v, const MaskScratch& s, const MaskQueue& q,
+                                   const QueuedDraw<T>& w, cudaStream_t st);
 template<typename T>
 cudaError_t mask_rate(int LX, int LY, int g, int EY, const MaskScratch& s, double alpha,
                       double beta, T* src, cudaStream_t st);

@@ -907,8 +907,9 @@ __global__ void phi_sum_serial(Dims d, const T* __restrict__ phi, double* out)
 // countphi for the FP32 sweeps, which do not reproduce the reference's
 // rounding anyway: per-block FP64 partial sums (PHI_PARTS blocks), then one
 // block adds the partials. Writes out[0]; out[1 .. PHI_PARTS] is scratch.
+template<typename T>
 __global__ void __launch_bounds__(256)
-phi_sum_partial(Dims d, const float* __restrict__ phi, double* __restrict__ out)
+phi_sum_partial(Dims d, const T* __restrict__ phi, double* __restrict__ out)
 {
   __shared__ double red[256];
   const long long N = static_cast<long long>(d.LX)*d.LY;
@@ -929,6 +930,7 @@ phi_sum_partial(Dims d, const float* __restrict__ phi, double* __restrict__ out)
   if(threadIdx.x == 0) out[1 + blockIdx.x] = red[0];
 }
 
+template<typename T>
 __global__ void __launch_bounds__(256)
 phi_sum_final(int nparts, double* __restrict__ out)
 {
@@ -952,8 +954,8 @@ void phi_sum(const Dims& d, const T* phi, double* out, cudaStream_t st)
 {
   if constexpr (std::is_same<T, float>::value)
   {
-    phi_sum_partial<<<PHI_PARTS, 256, 0, st>>>(d, phi, out);
-    phi_sum_final<<<1, 256, 0, st>>>(PHI_PARTS, out);
+    phi_sum_partial<T><<<PHI_PARTS, 256, 0, st>>>(d, phi, out);
+    phi_sum_final<T><<<1, 256, 0, st>>>(PHI_PARTS, out);
   }
   else phi_sum_serial<T><<<1, 1, 0, st>>>(d, phi, out);
 }

@@ -3,9 +3,70 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstring>
 #include <random>
 
 namespace {
+
+// The block loops below are built twice, for AVX2 and for the baseline
+// x86-64 vector unit, and the loader picks the one the CPU runs.
+#if defined(__x86_64__) && defined(__GNUC__) && defined(__ELF__)
+#define MT_CLONES __attribute__((target_clones("avx2", "default"), noinline))
+#else
+#define MT_CLONES
+#endif
+
+constexpr uint32_t MT_N = 624, MT_M = 397;
+
+inline uint32_t mt_step(uint32_t xk, uint32_t xk1, uint32_t xkm)
+{
+  const uint32_t y = (xk & 0x80000000u) | (xk1 & 0x7fffffffu);
+  return xkm ^ (y >> 1) ^ ((0u - (y & 1u)) & 0x9908b0dfu);
+}
+
+// X[k+N] from X[k], X[k+1], X[k+M], in place and in order: the first N-M
+// words read words not yet replaced, the rest read replaced ones at least
+// N-M = 227 places back
+MT_CLONES void mt_twist(uint32_t* x)
+{
+  for(uint32_t k = 0; k < MT_N - MT_M; ++k) x[k] = mt_step(x[k], x[k + 1], x[k + MT_M]);
+  for(uint32_t k = MT_N - MT_M; k < MT_N - 1; ++k) x[k] = mt_step(x[k], x[k + 1], x[k + MT_M - MT_N]);
+  x[MT_N - 1] = mt_step(x[MT_N - 1], x[0], x[MT_M - 1]);
+}
+
+MT_CLONES void mt_temper(const uint32_t* x, uint32_t* out)
+{
+  for(uint32_t k = 0; k < MT_N; ++k)
+  {
+    uint32_t y = x[k];
+    y ^= y >> 11;
+    y ^= (y << 7) & 0x9d2c5680u;
+    y ^= (y << 15) & 0xefc60000u;
+    y ^= y >> 18;
+    out[k] = y;
+  }
+}
+
+// generate_canonical<double, 53> of n word pairs (a, b) = (w[2j], w[2j+1]):
+// the 64-bit integer u = a + b*2^32 rounded to double, times 2^-64, kept
+// below 1. Both halves become exact doubles through the exponent field:
+// (2^84 + b*2^32) - (2^84 + 2^52) = b*2^32 - 2^52 and 2^52 + a; their sum
+// is u with the single rounding of a + b*2^32.
+MT_CLONES void mt_canonical_pairs(const uint32_t* w, double* d, size_t n)
+{
+  for(size_t j = 0; j < n; ++j)
+  {
+    uint64_t u;
+    std::memcpy(&u, w + 2*j, sizeof u);
+    const uint64_t hb = (u >> 32) | 0x4530000000000000ull;
+    const uint64_t lb = (u & 0xffffffffull) | 0x4330000000000000ull;
+    double h, l;
+    std::memcpy(&h, &hb, sizeof h);
+    std::memcpy(&l, &lb, sizeof l);
+    const double r = ((h - 19342813118337666422669312.0) + l)*0x1p-64;
+    d[j] = r >= 1.0 ? 0x1.fffffffffffffp-1 : r;
+  }
+}
 
 // The 32-bit Mersenne Twister of the C++ standard library
 // ([rand.eng.mers], [rand.predef]: std::mt19937 has word size 32, n = 624,
@@ -50,8 +111,7 @@ public:
       if(pos + 1 < N)
       {
         const size_t k = std::min(n - i, static_cast<size_t>((N - pos)/2));
-        const uint32_t* w = out + pos;
-        for(size_t j = 0; j < k; ++j) dst[i + j] = canonical(w[2*j], w[2*j + 1]);
+        mt_canonical_pairs(out + pos, dst + i, k);
         pos += static_cast<uint32_t>(2*k);
         i += k;
       }
@@ -65,34 +125,15 @@ public:
   }
 
 private:
-  static constexpr uint32_t N = 624, M = 397;
+  static constexpr uint32_t N = MT_N;
   uint32_t x[N];
   uint32_t out[N];
   uint32_t pos = N;
 
-  static uint32_t step(uint32_t xk, uint32_t xk1, uint32_t xkm)
-  {
-    const uint32_t y = (xk & 0x80000000u) | (xk1 & 0x7fffffffu);
-    return xkm ^ (y >> 1) ^ ((0u - (y & 1u)) & 0x9908b0dfu);
-  }
-
   void refill()
   {
-    // X[k+N] from X[k], X[k+1], X[k+M], in place and in order: the first
-    // N-M words read words not yet replaced, the rest read replaced ones
-    // at least N-M = 227 places back
-    for(uint32_t k = 0; k < N - M; ++k) x[k] = step(x[k], x[k + 1], x[k + M]);
-    for(uint32_t k = N - M; k < N - 1; ++k) x[k] = step(x[k], x[k + 1], x[k + M - N]);
-    x[N - 1] = step(x[N - 1], x[0], x[M - 1]);
-    for(uint32_t k = 0; k < N; ++k)
-    {
-      uint32_t y = x[k];
-      y ^= y >> 11;
-      y ^= (y << 7) & 0x9d2c5680u;
-      y ^= (y << 15) & 0xefc60000u;
-      y ^= y >> 18;
-      out[k] = y;
-    }
+    mt_twist(x);
+    mt_temper(x, out);
     pos = 0;
   }
 };

@@ -56,24 +56,35 @@ void LyotropicWithDivisionGPU::SetMasks()
   }
   if(!kinds) return;
   // The device takes one uniform per site with phi >= .5 and mask, in site
-  // order, from a queue of the reference generator's values. Keeping
-  // 2*LX*LY of them unconsumed covers two masks of any count, so the host
-  // never waits for the candidate count; it only learns, from the previous
-  // draw, how many values to add.
+  // order, from a queue of the reference generator's values. 2*LX*LY of
+  // them cover one draw of both masks of any count. The host learns how many
+  // were consumed from the draws the device has finished, without waiting,
+  // and keeps 2*LX*LY more for each draw still in flight and the next one,
+  // so it runs up to three draws ahead of the device.
   long long consumed = 0;
-  int r = mass_lb_mask_consumed(lattice, &consumed);
-  if(r != MASS_LB_OK) throw error_msg(mass_gpu::abi_error("mass_lb_mask_consumed", r));
-  const long long want = consumed + 2*static_cast<long long>(DomainSize);
+  int pending = 0;
+  int r = mass_lb_mask_progress(lattice, &consumed, &pending);
+  if(r != MASS_LB_OK) throw error_msg(mass_gpu::abi_error("mass_lb_mask_progress", r));
+  if(pending > 2)
+  {
+    r = mass_lb_mask_consumed(lattice, &consumed);
+    if(r != MASS_LB_OK) throw error_msg(mass_gpu::abi_error("mass_lb_mask_consumed", r));
+    pending = 0;
+  }
+  const long long want = consumed + 2*static_cast<long long>(DomainSize)*(pending + 1);
   if(supplied < want)
   {
     const size_t n = static_cast<size_t>(want - supplied);
-    draws.resize(n);
+    // the draws are written straight into the library's pinned staging
+    double* u = nullptr;
+    r = mass_lb_mask_staging(lattice, static_cast<long long>(n), &u);
+    if(r != MASS_LB_OK) throw error_msg(mass_gpu::abi_error("mass_lb_mask_staging", r));
 #ifdef MASS_GPU_STANDALONE
-    random_reals(draws.data(), n);   // the same values as n random_real() calls
+    random_reals(u, n);   // the same values as n random_real() calls
 #else
-    for(auto& u : draws) u = random_real();
+    for(size_t i = 0; i < n; ++i) u[i] = random_real();
 #endif
-    r = mass_lb_mask_supply(lattice, draws.data(), static_cast<long long>(n));
+    r = mass_lb_mask_supply(lattice, u, static_cast<long long>(n));
     if(r != MASS_LB_OK) throw error_msg(mass_gpu::abi_error("mass_lb_mask_supply", r));
     supplied = want;
   }

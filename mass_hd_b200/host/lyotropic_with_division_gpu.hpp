@@ -26,12 +26,11 @@ protected:
   double phi_critical = 1;
   unsigned division_count = 0, death_count = 0;
   bool conserve_phi = false;
-  /** random_real() values handed to the device's draw queue so far, and
-   * the buffer they pass through. Values are drawn ahead of need, in
-   * stream order; only the masks consume the generator after Configure(),
-   * so every value keeps its place in the reference's stream. */
+  /** random_real() values handed to the device's draw queue so far. Values
+   * are drawn ahead of need, in stream order, into the library's pinned
+   * staging buffer; only the masks consume the generator after
+   * Configure(), so every value keeps its place in the reference's stream. */
   long long supplied = 0;
-  std::vector<double> draws;
 
   /** Redraw the masks that are due (src/models/lyotropic-with-division.cpp:35-106). */
   void SetMasks();

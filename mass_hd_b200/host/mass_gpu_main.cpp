@@ -275,13 +275,16 @@ int run(int argc, char** argv)
   }
   if(!p.no_write && p.nsteps >= p.nstart) write_frame(p.nsteps);
   files.wait();
+  mass_lb_handle* h = nullptr;
+  if(auto* l = dynamic_cast<LyotropicGPU*>(model.operator->())) h = l->device_lattice();
+  else if(auto* n = dynamic_cast<NematicGPU*>(model.operator->())) h = n->device_lattice();
+  // the run time covers the device work the loop queued
+  if(h && mass_lb_synchronize(h) != MASS_LB_OK)
+    throw error_msg("mass_lb_synchronize: ", mass_lb_last_error());
   const auto dt = chrono::duration<double>(chrono::steady_clock::now() - start).count();
   model->Post();
   if(!p.save_state.empty())
   {
-    mass_lb_handle* h = nullptr;
-    if(auto* l = dynamic_cast<LyotropicGPU*>(model.operator->())) h = l->device_lattice();
-    else if(auto* n = dynamic_cast<NematicGPU*>(model.operator->())) h = n->device_lattice();
     if(!h) throw error_msg("model '", p.model_name, "' has no device lattice to save");
     if(mass_lb_save(h, p.save_state.c_str()) != MASS_LB_OK)
       throw error_msg("mass_lb_save: ", mass_lb_last_error());

@@ -135,8 +135,10 @@ def load_library(build_if_missing: bool = False):
                                         C.c_double, C.c_double, C.c_double]),
         "mass_lb_get_mask": (C.c_int, [vp, C.c_int, C.POINTER(C.c_ubyte)]),
         "mass_lb_mask_supply": (C.c_int, [vp, dp, C.c_longlong]),
+        "mass_lb_mask_staging": (C.c_int, [vp, C.c_longlong, C.POINTER(dp)]),
         "mass_lb_draw_masks_queued": (C.c_int, [vp, C.c_int] + [C.c_double] * 7),
         "mass_lb_mask_consumed": (C.c_int, [vp, C.POINTER(C.c_longlong)]),
+        "mass_lb_mask_progress": (C.c_int, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_int)]),
         "mass_lb_relax_free_energy": (C.c_int, [vp, C.c_uint, C.c_double, C.c_int, C.c_int, dp]),
         "mass_lb_ensemble_create": (C.c_int, [C.c_int, C.POINTER(Params), C.POINTER(C.c_uint),
                                               C.POINTER(C.c_uint), C.POINTER(vp)]),
@@ -306,10 +308,19 @@ class Lattice:
                                                 float(phi_critical), float(radius),
                                                 float(alpha), float(beta)))
 
-    def mask_supply(self, draws):
-        """Queue uniforms (stream order) for draw_masks_queued."""
+    def mask_supply(self, draws, staged: bool = False):
+        """Queue uniforms (stream order) for draw_masks_queued. staged: write
+        them into the library's pinned staging buffer first
+        (mass_lb_mask_staging), which the supply then sends up as it is."""
         d = np.ascontiguousarray(draws, dtype=np.float64)
-        _check(load_library().mass_lb_mask_supply(self.h, _dp(d), d.size))
+        lib = load_library()
+        if staged:
+            buf = C.POINTER(C.c_double)()
+            _check(lib.mass_lb_mask_staging(self.h, d.size, C.byref(buf)))
+            C.memmove(buf, d.ctypes.data, d.nbytes)
+            _check(lib.mass_lb_mask_supply(self.h, buf, d.size))
+        else:
+            _check(lib.mass_lb_mask_supply(self.h, _dp(d), d.size))
 
     def draw_masks_queued(self, kinds: int, division_coef: float, division_radius: float,
                           death_coef: float, death_radius: float, phi_critical: float,
@@ -323,6 +334,14 @@ class Lattice:
         n = C.c_longlong()
         _check(load_library().mass_lb_mask_consumed(self.h, C.byref(n)))
         return n.value
+
+    def mask_progress(self):
+        """(consumed, pending) without waiting: draws consumed up to the last
+        finished queued draw, and the queued draws issued after it."""
+        n = C.c_longlong()
+        k = C.c_int()
+        _check(load_library().mass_lb_mask_progress(self.h, C.byref(n), C.byref(k)))
+        return n.value, k.value
 
     def get_mask(self, kind: int) -> np.ndarray:
         out = np.empty(self.LX * self.LY, dtype=np.uint8)

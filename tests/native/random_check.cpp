@@ -30,6 +30,14 @@ int main()
     random_reals(bulk.data(), 7);
     for(int i = 0; i < 7; ++i) same(bulk[i], std::uniform_real_distribution<>(0., 1.)(g));
     same(random_real(), std::uniform_real_distribution<>(0., 1.)(g));
+    // bulk runs starting at odd word offsets, so pairs straddle the blocks
+    for(int k = 0; k < 5; ++k)
+    {
+      same(randu(), g());
+      const size_t m = 311 + 977*k;
+      random_reals(bulk.data(), m);
+      for(size_t i = 0; i < m; ++i) same(bulk[i], std::uniform_real_distribution<>(0., 1.)(g));
+    }
   }
   std::printf("%ld of %ld\n", bad, n);
   return bad != 0;

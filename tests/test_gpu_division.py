@@ -198,13 +198,15 @@ def test_device_masks_follow_reference_rule(LX, LY, bc, prec):
     b.close()
 
 
+@pytest.mark.parametrize("staged", [False, True])
 @pytest.mark.parametrize("prec", [M.FP64, M.FP32])
-def test_queued_masks_equal_direct_masks(prec):
+def test_queued_masks_equal_direct_masks(prec, staged):
     """mass_lb_draw_masks_queued takes the same uniforms in the same order as
     mass_lb_draw_mask: over a run whose masks are redrawn on a schedule
     (division alone, death alone, both in one step), two lattices, one fed
     through the queue and one draw by draw, keep bit-identical masks and
-    states, and the queue reports every draw it consumed."""
+    states, and the queue reports every draw it consumed. staged: the
+    uniforms go up from the library's pinned staging buffer."""
     LX, LY = 64, 64
     st = O.synthetic_state(O.LYOTROPIC, LX, LY, seed=12, flow=0.01, phi_kind="disk",
                            radius=LX / 3)
@@ -216,26 +218,28 @@ def test_queued_masks_equal_direct_masks(prec):
     rng = np.random.default_rng(3)
     stream = rng.uniform(0, 1, 200000)
     pos_b = 0
-    a.mask_supply(stream[:2 * LX * LY])
+    a.mask_supply(stream[:2 * LX * LY], staged)
     supplied = 2 * LX * LY
-    args = dict(division_coef=0.3, division_radius=2.5, death_coef=0.2, death_radius=1.5,
-                phi_critical=1.3, alpha=0.05, beta=0.03)
     for t in range(12):
+        # the coefficients change half-way
+        dc, dr, ec, er = (0.3, 2.5, 0.2, 1.5) if t < 6 else (0.45, 1.5, 0.1, 2.0)
+        args = dict(division_coef=dc, division_radius=dr, death_coef=ec, death_radius=er,
+                    phi_critical=1.3, alpha=0.05, beta=0.03)
         kinds = (1 if t % 3 == 0 else 0) | (2 if t % 2 == 0 else 0)
         if kinds:
             consumed = a.mask_consumed()
             assert consumed == pos_b
             if supplied - consumed < 2 * LX * LY:
                 n = consumed + 2 * LX * LY - supplied
-                a.mask_supply(stream[supplied:supplied + n])
+                a.mask_supply(stream[supplied:supplied + n], staged)
                 supplied += n
             a.draw_masks_queued(kinds, **args)
             n = b.mask_candidates()
             if kinds & 1:
-                b.draw_mask(0, stream[pos_b:pos_b + n], 0.3, 1.3, 2.5, 0.05, 0.03)
+                b.draw_mask(0, stream[pos_b:pos_b + n], dc, 1.3, dr, 0.05, 0.03)
                 pos_b += n
             if kinds & 2:
-                b.draw_mask(1, stream[pos_b:pos_b + n], 0.2, 1.3, 1.5, 0.05, 0.03)
+                b.draw_mask(1, stream[pos_b:pos_b + n], ec, 1.3, er, 0.05, 0.03)
                 pos_b += n
         a.step(1)
         b.step(1)
@@ -248,8 +252,90 @@ def test_queued_masks_equal_direct_masks(prec):
     c = M.Lattice(M.LYOTROPIC, p, LX, LY, 0, prec)
     c.upload_state(st)
     c.mask_supply(stream[:10])
-    c.draw_masks_queued(1, **args)
+    c.draw_masks_queued(1, 0.3, 2.5, 0.2, 1.5, 1.3, 0.05, 0.03)
     with pytest.raises(M.MassLBError):
         c.mask_consumed()
     for x in (a, b, c):
         x.close()
+
+
+@pytest.mark.parametrize("prec", [M.FP64, M.FP32])
+def test_queued_masks_running_ahead(prec):
+    """The plugin's supply policy: the host reads the consumed count of the
+    draws the device has finished (mass_lb_mask_progress, no wait) and keeps
+    2*LX*LY draws per draw in flight plus one more ahead, from the staging
+    buffer. Masks and states stay bit-identical to draw-by-draw masks, the
+    progress count never runs ahead of the true count, and it catches up
+    once the device is idle."""
+    LX, LY = 48, 40
+    N = LX * LY
+    st = O.synthetic_state(O.LYOTROPIC, LX, LY, seed=21, flow=0.01, phi_kind="disk",
+                           radius=LX / 3)
+    p = params()
+    a = M.Lattice(M.LYOTROPIC, p, LX, LY, 0, prec)
+    b = M.Lattice(M.LYOTROPIC, p, LX, LY, 0, prec)
+    a.upload_state(st)
+    b.upload_state(st)
+    stream = np.random.default_rng(5).uniform(0, 1, 40 * N)
+    supplied = pos_b = 0
+    for t in range(18):
+        kinds = (1 if t % 3 == 0 else 0) | (2 if t % 2 == 0 else 0)
+        if kinds:
+            consumed, pending = a.mask_progress()
+            assert 0 <= pending <= 4 and consumed <= pos_b
+            if pending > 2:
+                consumed, pending = a.mask_consumed(), 0
+            want = consumed + 2 * N * (pending + 1)
+            if supplied < want:
+                a.mask_supply(stream[supplied:want], True)
+                supplied = want
+            a.draw_masks_queued(kinds, 0.3, 2.5, 0.2, 1.5, 1.3, 0.05, 0.03)
+            n = b.mask_candidates()
+            if kinds & 1:
+                b.draw_mask(0, stream[pos_b:pos_b + n], 0.3, 1.3, 2.5, 0.05, 0.03)
+                pos_b += n
+            if kinds & 2:
+                b.draw_mask(1, stream[pos_b:pos_b + n], 0.2, 1.3, 1.5, 0.05, 0.03)
+                pos_b += n
+        a.step(1)
+        b.step(1)
+    a.synchronize()
+    assert a.mask_progress() == (pos_b, 0)
+    assert a.mask_consumed() == pos_b
+    for kind in (0, 1):
+        assert np.array_equal(a.get_mask(kind), b.get_mask(kind))
+    for n_ in STATE:
+        assert bits_equal(a.get(n_), b.get(n_)), n_
+    a.close()
+    b.close()
+
+
+def test_queued_circles_wrapping_the_lattice():
+    """Circles wider than half the lattice: the queued draw (each site looks
+    for centres around it) marks the same sites as the direct draw (each
+    centre writes its circle), both wrapping periodically."""
+    LX, LY = 16, 12
+    st = O.synthetic_state(O.LYOTROPIC, LX, LY, seed=4, flow=0.01, phi_kind="disk", radius=5)
+    p = params()
+    a = M.Lattice(M.LYOTROPIC, p, LX, LY, 0, M.FP64)
+    b = M.Lattice(M.LYOTROPIC, p, LX, LY, 0, M.FP64)
+    a.upload_state(st)
+    b.upload_state(st)
+    u = np.random.default_rng(8).uniform(0, 1, 64 * LX * LY)
+    a.mask_supply(u[:6 * LX * LY])
+    pos = 0
+    for radius in (6.5, 4.2, 0.0):
+        a.draw_masks_queued(3, 0.9, radius, 0.8, radius / 2, 1.3, 0.05, 0.03)
+        n = b.mask_candidates()
+        b.draw_mask(0, u[pos:pos + n], 0.9, 1.3, radius, 0.05, 0.03)
+        b.draw_mask(1, u[pos + n:pos + 2 * n], 0.8, 1.3, radius / 2, 0.05, 0.03)
+        pos += 2 * n
+        for kind in (0, 1):
+            assert np.array_equal(a.get_mask(kind), b.get_mask(kind)), (radius, kind)
+        if radius > 6:
+            assert a.get_mask(0).any()
+    a.step(1)
+    b.step(1)
+    assert bits_equal(a.get("phi"), b.get("phi"))
+    a.close()
+    b.close()
