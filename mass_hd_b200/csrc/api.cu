@@ -143,6 +143,7 @@ struct mass_lb_handle
   float* nxt = nullptr;
   float* diag = nullptr;     // NDIAG planes, allocated on first use
   bool has_prev = false;     // nxt holds the state before the last step
+  bool derived_pending = false;   // unfused: the derived planes await replay_derived
   FusedConfig cfg{128, 256};
   bool tuned = false;
 
@@ -515,6 +516,19 @@ void mass_lb_destroy(mass_lb_handle* h)
   delete h;
 }
 
+// The derived fields of the last step, computed now if the step left them
+// (before anything changes the state they come from, or when asked for).
+static int settle_derived(mass_lb_handle* h)
+{
+  if(!h->derived_pending) return 0;
+  h->derived_pending = false;
+  const int r = h->precision == MASS_LB_FP64
+    ? replay_derived_f64(h->d, h->P, h->s64, h->stream)
+    : replay_derived_f32(h->d, h->P, h->s32, h->stream);
+  if(r) return cuda_fail(cudaGetLastError(), "derived fields");
+  return 0;
+}
+
 static int put_field(mass_lb_handle* h, int field, const double* src)
 {
   const int LY = static_cast<int>(h->LY);
@@ -580,6 +594,7 @@ int mass_lb_upload_field(mass_lb_handle* h, int field, const double* src)
   if(field == MASS_LB_M && h->model != GOG)
     return fail(MASS_LB_EUNSUPPORTED, "m exists in the go-or-grow model only");
   DeviceGuard g(h->device);
+  if(int r = settle_derived(h)) return r;
   if(int r = put_field(h, field, src)) return r;
   h->has_prev = false;
   CU(cudaStreamSynchronize(h->stream), "upload sync");
@@ -592,6 +607,7 @@ int mass_lb_upload(mass_lb_handle* h, const double* ff, const double* QQxx,
   if(!h || !ff || !QQxx || !QQyx) return fail(MASS_LB_EINVAL, "null argument");
   if(h->model != NEM && !phi) return fail(MASS_LB_EINVAL, "lyotropic models need phi");
   DeviceGuard g(h->device);
+  if(int r = settle_derived(h)) return r;
   if(int r = put_field(h, MASS_LB_FF, ff)) return r;
   if(int r = put_field(h, MASS_LB_QQXX, QQxx)) return r;
   if(int r = put_field(h, MASS_LB_QQYX, QQyx)) return r;
@@ -613,17 +629,20 @@ int mass_lb_step(mass_lb_handle* h, unsigned nsteps)
   if(!h) return fail(MASS_LB_EINVAL, "null handle");
   if(nsteps == 0) return 0;
   DeviceGuard g(h->device);
+  const int bc = h->wall ? static_cast<int>(h->bc) : 0;
+  // sub-step kernels leave the derived fields to a replay on demand
+  const bool lazy = !h->fused && substep_path(h->d, h->P, bc);
   if(h->precision == MASS_LB_FP64)
   {
-    if(step_unfused_f64(h->d, h->P, h->s64, h->wall ? static_cast<int>(h->bc) : 0,
-                        nsteps, true, h->stream) != 0)
+    if(step_unfused_f64(h->d, h->P, h->s64, bc, nsteps, !lazy, h->stream) != 0)
       return cuda_fail(cudaGetLastError(), "fp64 step");
+    h->derived_pending = lazy;
   }
   else if(!h->fused)
   {
-    if(step_unfused_f32(h->d, h->P, h->s32, h->wall ? static_cast<int>(h->bc) : 0,
-                        nsteps, true, h->stream) != 0)
+    if(step_unfused_f32(h->d, h->P, h->s32, bc, nsteps, !lazy, h->stream) != 0)
       return cuda_fail(cudaGetLastError(), "fp32 step");
+    h->derived_pending = lazy;
   }
   else
   {
@@ -749,6 +768,8 @@ int mass_lb_download(mass_lb_handle* h, int field, double* out)
   if(h->precision == MASS_LB_FP32 && predictor)
     return fail(MASS_LB_EUNSUPPORTED, "step-internal predictor fields are FP64-mode only");
   DeviceGuard g(h->device);
+  if(!h->fused && field >= MASS_LB_N && field <= MASS_LB_SIGMA_ACTIVE_YX)
+    if(int r = settle_derived(h)) return r;
   if(h->fused && field >= MASS_LB_N && field <= MASS_LB_SIGMA_ACTIVE_YX)
   {
     if(!h->has_prev)
@@ -1048,6 +1069,10 @@ int mass_lb_save(mass_lb_handle* h, const char* path)
 int mass_lb_load(mass_lb_handle* h, const char* path)
 {
   if(!h || !path) return fail(MASS_LB_EINVAL, "null argument");
+  {
+    DeviceGuard g(h->device);
+    if(int r = settle_derived(h)) return r;
+  }
   FILE* f = std::fopen(path, "rb");
   if(!f) return fail(MASS_LB_EINVAL, std::string("cannot open ") + path);
   CkptHeader hd{};
@@ -1548,6 +1573,8 @@ int mass_lb_set_go_or_grow_params(mass_lb_handle* h, const mass_lb_go_or_grow_pa
 {
   if(!h || !p) return fail(MASS_LB_EINVAL, "null argument");
   if(h->model != GOG) return fail(MASS_LB_EUNSUPPORTED, "not a go-or-grow lattice");
+  DeviceGuard g(h->device);
+  if(int r = settle_derived(h)) return r;
   const Pheno ph{p->B, p->Snem, p->Dchi, p->Achi, p->Ochi, p->phiswitch, p->phi_critical,
                  p->growTogether ? 1 : 0};
   h->s64.ph = ph;
@@ -1561,6 +1588,7 @@ int mass_lb_relax_free_energy(mass_lb_handle* h, unsigned steps, double dt, int 
   if(!h) return fail(MASS_LB_EINVAL, "null handle");
   if(h->model != GOG) return fail(MASS_LB_EUNSUPPORTED, "not a go-or-grow lattice");
   DeviceGuard g(h->device);
+  if(int r = settle_derived(h)) return r;
   if(!h->relaxsum)
     if(int r = dalloc(h, &h->relaxsum, 1)) return r;
   const int bc = h->wall ? static_cast<int>(h->bc) : 0;

@@ -1111,7 +1111,7 @@ int step_impl(const Dims& d, const Params& P, State<T>& s, int bc,
     if(MODEL == GOG) { std::swap(s.m, s.m_tmp); std::swap(s.chi, s.chi_tmp); }
   };
 
-  if(!bc && d.g == 0 && P.npc >= 1)
+  if(substep_path(d, P, bc))
   {
     // periodic: one launch per sub-step
     auto swap_sub = [&]() {
@@ -1128,12 +1128,12 @@ int step_impl(const Dims& d, const Params& P, State<T>& s, int bc,
       std::swap(s.fn, s.fn_tmp);
       for(unsigned c = 1; c <= P.npc; ++c)
       {
-        const bool last = it + 1 == nsteps && c == P.npc;
+        // diag_last: the last sub-step also stores what its UpdateQuantities
+        // computed (else replay_derived recomputes it when it is asked for)
+        const bool last = diag_last && it + 1 == nsteps && c == P.npc;
         if(MODEL != NEM && s.conserve_phi) phi_sum<T>(d, s.phi, s.phisum, st);
-        if(last && diag_last)
-          launch_substep<T, DEV, MODEL, false, true>(d, P, s, 1, st);
-        else
-          launch_substep<T, DEV, MODEL, false, false>(d, P, s, last ? 1 : 0, st);
+        if(last) launch_substep<T, DEV, MODEL, false, true>(d, P, s, 1, st);
+        else launch_substep<T, DEV, MODEL, false, false>(d, P, s, 0, st);
         swap_sub();
       }
     }
@@ -1176,6 +1176,29 @@ int step_impl(const Dims& d, const Params& P, State<T>& s, int bc,
   return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
+// The derived fields of the last sub-step-kernel step: its last
+// UpdateQuantities again, on the state that sub-step read, which the step
+// leaves in the spare planes (ff_tmp, Qxx_tmp, Qyx_tmp, phi_tmp, chi_tmp).
+template<typename T, bool DEV>
+int replay_impl(const Dims& d, const Params& P, const State<T>& s, cudaStream_t st)
+{
+  State<T> r = s;
+  r.ff = s.ff_tmp;
+  r.Qxx = s.Qxx_tmp;
+  r.Qyx = s.Qyx_tmp;
+  r.phi = s.phi_tmp;
+  r.chi = s.chi_tmp;
+  const dim3 blk(64, 4);
+  const dim3 grd = site_grid(d.LX, d.LY, blk);
+  switch(P.model)
+  {
+    case LYO: uq_kernel<T, DEV, LYO, true><<<grd, blk, 0, st>>>(d, P, r); break;
+    case GOG: uq_kernel<T, DEV, GOG, true><<<grd, blk, 0, st>>>(d, P, r); break;
+    default: uq_kernel<T, DEV, NEM, true><<<grd, blk, 0, st>>>(d, P, r); break;
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
 } // namespace
 
 #ifndef MLB_UNFUSED_PART
@@ -1183,6 +1206,16 @@ int step_impl(const Dims& d, const Params& P, State<T>& s, int bc,
 #endif
 
 #if MLB_UNFUSED_PART != 32
+bool substep_path(const Dims& d, const Params& P, int bc)
+{
+  return !bc && d.g == 0 && P.npc >= 1;
+}
+
+int replay_derived_f64(const Dims& d, const Params& P, const State<double>& s, cudaStream_t st)
+{
+  return replay_impl<double, false>(d, P, s, st);
+}
+
 int lb_kind(int model, int bc)
 {
   if(model != NEM)
@@ -1244,6 +1277,11 @@ int update_chi_f64(const Dims& d, State<double>& s, cudaStream_t st)
 #endif
 
 #if MLB_UNFUSED_PART != 64
+int replay_derived_f32(const Dims& d, const Params& P, const State<float>& s, cudaStream_t st)
+{
+  return replay_impl<float, true>(d, P, s, st);
+}
+
 int step_unfused_f32(const Dims& d, const Params& P, State<float>& s, int bc,
                      unsigned nsteps, bool diag_last, cudaStream_t st)
 {

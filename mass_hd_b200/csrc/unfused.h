@@ -28,6 +28,15 @@ struct ScalarBC
 int lb_kind(int model, int bc);
 int bc_mode(int model, int bc);
 int launches_unfused(int model, int bc, unsigned npc);
+// Whether a step runs one sub-step kernel per predictor and corrector
+// (periodic lattice without a ghost ring, npc >= 1). Such a step called
+// with diag_last = false leaves the derived fields (n, u, H, mu, dQ,
+// stresses, diagnostic stresses) to replay_derived_*, which recomputes
+// them from the state its last UpdateQuantities read; valid until the next
+// step or change of the state.
+bool substep_path(const Dims& d, const Params& P, int bc);
+int replay_derived_f64(const Dims& d, const Params& P, const State<double>& s, cudaStream_t st);
+int replay_derived_f32(const Dims& d, const Params& P, const State<float>& s, cudaStream_t st);
 
 // Advance `nsteps` steps; swaps the ping-pong pointers held in `s`.
 // diag_last: the last corrector UpdateQuantities also writes the seven
