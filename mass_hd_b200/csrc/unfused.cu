@@ -570,6 +570,11 @@ constexpr int SUB_TY = 32, SUB_TX = 8;                 // tile: y (contiguous) x
 constexpr int SUB_HY = SUB_TY + 2, SUB_HX = SUB_TX + 2;
 constexpr int SUB_HS = SUB_HY*SUB_HX;
 
+__device__ __forceinline__ void prefetch_l2(const void* p)
+{
+  asm volatile("prefetch.global.L2 [%0];" :: "l"(p));
+}
+
 template<typename T>
 struct TileUQ : UQStencil<T, TileUQ<T>>
 {
@@ -584,12 +589,28 @@ struct TileUQ : UQStencil<T, TileUQ<T>>
 
 template<typename T, bool DEV, int MODEL, bool FIRST, bool DIAG>
 __global__ void __launch_bounds__(SUB_TY*SUB_TX)
-substep_kernel(Dims d, Params P, State<T> s, int storeq)
+substep_kernel(Dims d, Params P, State<T> s, int storeq, int prefetch)
 {
   extern __shared__ __align__(16) unsigned char sub_smem[];
   T (*uq_s)[SUB_HS] = reinterpret_cast<T (*)[SUB_HS]>(sub_smem);
   const int y0 = blockIdx.x*SUB_TY, x0 = blockIdx.y*SUB_TX;
   const int tid = threadIdx.y*SUB_TY + threadIdx.x;
+  if constexpr (!FIRST)
+  {
+    // the corrector's own-site inputs (fn, QN, phi_N, m_N) start towards L2
+    // while the tile's UpdateQuantities runs (states larger than L2)
+    const int y = y0 + threadIdx.x, x = x0 + threadIdx.y;
+    if(prefetch && x < d.LX && y < d.LY)
+    {
+      const long long e = y + static_cast<long long>(d.EY)*x;
+#pragma unroll
+      for(int v = 0; v < 9; ++v) prefetch_l2(s.fn + v*d.NE + e);
+      prefetch_l2(s.QNxx + e);
+      prefetch_l2(s.QNyx + e);
+      if constexpr (MODEL != NEM) prefetch_l2(s.phn + e);
+      if constexpr (MODEL == GOG) prefetch_l2(s.mN + e);
+    }
+  }
   for(int i = tid; i < SUB_HS; i += SUB_TY*SUB_TX)
   {
     const int hx = i/SUB_HY, hy = i - hx*SUB_HY;
@@ -643,7 +664,9 @@ void launch_substep(const Dims& d, const Params& P, const State<T>& s, int store
   }
   const dim3 blk(SUB_TY, SUB_TX);
   const dim3 grd((d.LY + SUB_TY - 1)/SUB_TY, (d.LX + SUB_TX - 1)/SUB_TX);
-  substep_kernel<T, DEV, MODEL, FIRST, DIAG><<<grd, blk, bytes, st>>>(d, P, s, storeq);
+  // about 60 planes of state and sweep fields; L2 holds 126 MB
+  const int prefetch = static_cast<double>(d.NE)*sizeof(T)*60 > 96e6 ? 1 : 0;
+  substep_kernel<T, DEV, MODEL, FIRST, DIAG><<<grd, blk, bytes, st>>>(d, P, s, storeq, prefetch);
 }
 
 // Streaming as a pull over every extended site.
