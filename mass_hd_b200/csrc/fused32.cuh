@@ -26,8 +26,6 @@ struct PairParams
 {
   float2 rho, GammaQ, GammaP, xi2, xi, tauIso, dtau, friction;
   float2 AA, hAA, nCC, hCC, LL, nLL2, KK, hKK, nKK, zeta, zetaI, conc;
-  float2 one, neg1, two, half, nhalf, quarter, nquarter, nfour, ntwo;
-  float2 third, twelfth, ninth, th36, zero;
 };
 
 struct FusedArgs

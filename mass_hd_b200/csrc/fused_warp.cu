@@ -93,6 +93,9 @@ __device__ __forceinline__ f2 fma(f2 a, f2 b, f2 c) { return f2{__ffma2_rn(a.v, 
 __device__ __forceinline__ f2 operator-(f2 a, f2 b) { return f2{__ffma2_rn(b.v, make_float2(-1.f, -1.f), a.v)}; }
 __device__ __forceinline__ f2 neg(f2 a) { return f2{__fmul2_rn(a.v, make_float2(-1.f, -1.f))}; }
 __device__ __forceinline__ f2 K(float c) { return bc(c); }
+// a literal pair: the compiler keeps these out of the registers the
+// parameter pairs would take
+#define KC(c) (f2{make_float2((c), (c))})
 __device__ __forceinline__ f2 W2(const float2& c) { return f2{c}; }
 
 __device__ __forceinline__ float rcp_approx(float x)
@@ -137,11 +140,6 @@ __host__ PairParams make_pp(const P32& p, int model)
   q.LL = b(p.LL); q.nLL2 = b(-2.f*p.LL);
   q.KK = b(p.KK); q.hKK = b(0.5f*p.KK); q.nKK = b(-p.KK);
   q.zeta = b(p.zeta); q.zetaI = b(p.zetaI); q.conc = b(p.conc);
-  q.one = b(1.f); q.neg1 = b(-1.f); q.two = b(2.f); q.half = b(0.5f);
-  q.nhalf = b(-0.5f); q.quarter = b(0.25f); q.nquarter = b(-0.25f);
-  q.nfour = b(-4.f); q.ntwo = b(-2.f); q.third = b(1.f/3.f);
-  q.twelfth = b(1.f/12.f); q.ninth = b(1.f/9.f); q.th36 = b(1.f/36.f);
-  q.zero = b(0.f);
   return q;
 }
 
@@ -176,10 +174,10 @@ __device__ __forceinline__ void uq_pair(const PP& P, const f2 g[9], const f2 Qa[
   const f2 vx = jx*inv, vy = jy*inv;
 
   const f2 Qxx = Qa[0], Qyx = Qb[0];
-  const f2 lQxx = fma(W2(P.nfour), Qxx, (Qa[1] + Qa[2]) + (Qa[3] + Qa[4]));
-  const f2 lQyx = fma(W2(P.nfour), Qyx, (Qb[1] + Qb[2]) + (Qb[3] + Qb[4]));
-  const f2 dxQxx = W2(P.half)*(Qa[1] - Qa[2]), dyQxx = W2(P.half)*(Qa[3] - Qa[4]);
-  const f2 dxQyx = W2(P.half)*(Qb[1] - Qb[2]), dyQyx = W2(P.half)*(Qb[3] - Qb[4]);
+  const f2 lQxx = fma(KC(-4.f), Qxx, (Qa[1] + Qa[2]) + (Qa[3] + Qa[4]));
+  const f2 lQyx = fma(KC(-4.f), Qyx, (Qb[1] + Qb[2]) + (Qb[3] + Qb[4]));
+  const f2 dxQxx = KC(.5f)*(Qa[1] - Qa[2]), dyQxx = KC(.5f)*(Qa[3] - Qa[4]);
+  const f2 dxQyx = KC(.5f)*(Qb[1] - Qb[2]), dyQyx = KC(.5f)*(Qb[3] - Qb[4]);
   const f2 S2 = fma(Qxx, Qxx, Qyx*Qyx);
   // cterm = CC*term with term = -S2 (lyotropic) or 1 - S2 (nematic)
   const f2 cterm = MODEL == LYO ? W2(P.nCC)*S2 : fma(W2(P.nCC), S2, neg(W2(P.nCC)));
@@ -187,13 +185,13 @@ __device__ __forceinline__ void uq_pair(const PP& P, const f2 g[9], const f2 Qa[
   const f2 Hyx = fma(cterm, Qyx, W2(P.LL)*lQyx);
   const f2 el = W2(P.LL)*(fma(dyQxx, dyQxx, dyQyx*dyQyx) - fma(dxQxx, dxQxx, dxQyx*dxQyx));
   const f2 elS = W2(P.nLL2)*fma(dxQxx, dyQxx, dxQyx*dyQyx);
-  const f2 sigmaA = W2(P.two)*fma(Qxx, Hyx, neg(Qyx*Hxx));
+  const f2 sigmaA = KC(2.f)*fma(Qxx, Hyx, neg(Qyx*Hxx));
   const f2 QQ = Qxx*Qyx;
-  const f2 flowF = W2(P.xi2)*fma(fma(Qxx, Qxx, W2(P.neg1)), Hxx, QQ*Hyx);
-  const f2 flowS = W2(P.xi2)*fma(QQ, Hxx, fma(Qyx, Qyx, W2(P.neg1))*Hyx);
+  const f2 flowF = W2(P.xi2)*fma(fma(Qxx, Qxx, KC(-1.f)), Hxx, QQ*Hyx);
+  const f2 flowS = W2(P.xi2)*fma(QQ, Hxx, fma(Qyx, Qyx, KC(-1.f))*Hyx);
   // sigmaB's nematic/lyotropic common part: 0.5 CC term^2 = 0.5 cterm^2/CC;
   // written as hCC*term*term with term recomputed from S2
-  const f2 term = MODEL == LYO ? neg(S2) : W2(P.one) - S2;
+  const f2 term = MODEL == LYO ? neg(S2) : KC(1.f) - S2;
   const f2 bulkQ = W2(P.hCC)*(term*term);
 
   o.dn = dn; o.ux = vx; o.uy = vy;
@@ -203,11 +201,11 @@ __device__ __forceinline__ void uq_pair(const PP& P, const f2 g[9], const f2 Qa[
   if constexpr (MODEL == LYO)
   {
     const f2 p = Ph[0];
-    const f2 omp = W2(P.one) - p;
-    const f2 lp = fma(W2(P.nfour), p, (Ph[1] + Ph[2]) + (Ph[3] + Ph[4]));
-    const f2 dxPhi = W2(P.half)*(Ph[1] - Ph[2]), dyPhi = W2(P.half)*(Ph[3] - Ph[4]);
+    const f2 omp = KC(1.f) - p;
+    const f2 lp = fma(KC(-4.f), p, (Ph[1] + Ph[2]) + (Ph[3] + Ph[4]));
+    const f2 dxPhi = KC(.5f)*(Ph[1] - Ph[2]), dyPhi = KC(.5f)*(Ph[3] - Ph[4]);
     const f2 pq = p*omp;
-    const f2 mu = fma(W2(P.AA)*pq, fma(W2(P.ntwo), p, W2(P.one)), W2(P.nKK)*lp);
+    const f2 mu = fma(W2(P.AA)*pq, fma(KC(-2.f), p, KC(1.f)), W2(P.nKK)*lp);
     const f2 sigmaB = fma(W2(P.hAA)*pq, pq, bulkQ) - mu*p;
     const f2 act = W2(P.zeta)*omp;
     const f2 pf = W2(P.hKK)*fma(dyPhi, dyPhi, neg(dxPhi*dxPhi));
@@ -237,7 +235,7 @@ __device__ __forceinline__ void uq_pair(const PP& P, const f2 g[9], const f2 Qa[
   {
     const f2 sigmaF = fma(neg(W2(P.zeta)), Qxx, flowF) + el;
     const f2 sigmaS = fma(neg(W2(P.zeta)), Qyx, flowS) + elS;
-    o.uxp = W2(P.zero); o.uyp = W2(P.zero); o.MU = W2(P.zero);
+    o.uxp = KC(0.f); o.uyp = KC(0.f); o.MU = KC(0.f);
     o.sXX = bulkQ + sigmaF;
     o.sYY = bulkQ - sigmaF;
     o.sXY = sigmaS + sigmaA;
@@ -283,55 +281,55 @@ __device__ __forceinline__ void uf_core(const PP& P, const UQ2o& c, const UQx& x
                                         const UQx& xm, const YN& y, f2 Qxx, f2 Qyx,
                                         UFcore& u)
 {
-  const f2 dxux = W2(P.half)*(xp.ux - xm.ux), dyux = W2(P.half)*(y.uxp_ - y.uxm);
-  const f2 dxuy = W2(P.half)*(xp.uy - xm.uy), dyuy = W2(P.half)*(y.uyp_ - y.uym);
-  const f2 dxSxx = W2(P.half)*(xp.sXX - xm.sXX), dySxy = W2(P.half)*(y.sxyp - y.sxym);
-  const f2 dxSyx = W2(P.half)*(xp.sYX - xm.sYX), dySyy = W2(P.half)*(y.syyp - y.syym);
+  const f2 dxux = KC(.5f)*(xp.ux - xm.ux), dyux = KC(.5f)*(y.uxp_ - y.uxm);
+  const f2 dxuy = KC(.5f)*(xp.uy - xm.uy), dyuy = KC(.5f)*(y.uyp_ - y.uym);
+  const f2 dxSxx = KC(.5f)*(xp.sXX - xm.sXX), dySxy = KC(.5f)*(y.sxyp - y.sxym);
+  const f2 dxSyx = KC(.5f)*(xp.sYX - xm.sYX), dySyy = KC(.5f)*(y.syyp - y.syym);
   const f2 expansion = dxux + dyuy;
-  const f2 shear = W2(P.half)*(dxuy + dyux);
-  const f2 vorticity = W2(P.half)*(dxuy - dyux);
-  const f2 Qs2 = W2(P.two)*(Qyx*shear);
+  const f2 shear = KC(.5f)*(dxuy + dyux);
+  const f2 vorticity = KC(.5f)*(dxuy - dyux);
+  const f2 Qs2 = KC(2.f)*(Qyx*shear);
   const f2 traceQL = fma(Qxx, dxux - dyuy, Qs2);
   const f2 vx = c.ux, vy = c.uy;
-  const f2 v2 = W2(P.two)*vorticity;
+  const f2 v2 = KC(2.f)*vorticity;
   // Dxx = G Hxx - vx dxQxx - vy dyQxx - 2 w Qyx + xi((Qxx+1)(2 dxux - trQL) + 2 Qyx shear - expansion)
-  const f2 bx = fma(Qxx + W2(P.one), fma(W2(P.two), dxux, neg(traceQL)), Qs2 - expansion);
+  const f2 bx = fma(Qxx + KC(1.f), fma(KC(2.f), dxux, neg(traceQL)), Qs2 - expansion);
   u.Dxx = fma(W2(P.GammaQ), c.Hxx, fma(W2(P.xi), bx, neg(fma(vx, c.dxQxx, fma(vy, c.dyQxx, v2*Qyx)))));
   // Dyx = G Hyx - vx dxQyx - vy dyQyx + 2 w Qxx + xi(Qyx(expansion - trQL) + 2 shear)
-  const f2 by = fma(Qyx, expansion - traceQL, W2(P.two)*shear);
+  const f2 by = fma(Qyx, expansion - traceQL, KC(2.f)*shear);
   u.Dyx = fma(W2(P.GammaQ), c.Hyx, fma(W2(P.xi), by, fma(v2, Qxx, neg(fma(vx, c.dxQyx, vy*c.dyQyx)))));
   const f2 Fx = (dxSxx + dySxy) - W2(P.friction)*vx;
   const f2 Fy = (dxSyx + dySyy) - W2(P.friction)*vy;
   if constexpr (MODEL == LYO)
   {
-    const f2 lMU = fma(W2(P.nfour), c.MU, (xp.MU + xm.MU) + (y.mup + y.mum));
-    const f2 pFlux = W2(P.half)*((xp.uxp - xm.uxp) + (y.uypp - y.uypm));
+    const f2 lMU = fma(KC(-4.f), c.MU, (xp.MU + xm.MU) + (y.mup + y.mum));
+    const f2 pFlux = KC(.5f)*((xp.uxp - xm.uxp) + (y.uypp - y.uypm));
     u.Dp = fma(W2(P.GammaP), lMU, neg(pFlux));
   }
-  else u.Dp = W2(P.zero);
+  else u.Dp = KC(0.f);
 
   const f2 dn = c.dn;
   const f2 nn = W2(P.rho) + dn;
   const f2 jx = nn*vx, jy = nn*vy;
   const f2 kxx = jx*vx, kyy = jy*vy, kxy = jx*vy, k2 = kxx + kyy;
-  const f2 dn9 = W2(P.ninth)*dn, dn36 = W2(P.th36)*dn;
-  const f2 a1 = fma(W2(P.nhalf), kyy, dn9), a3 = fma(W2(P.nhalf), kxx, dn9);
-  const f2 b5 = fma(W2(P.quarter), kxy, dn36), b7 = fma(W2(P.nquarter), kxy, dn36);
-  u.fe[1] = fma(k2 + jx, W2(P.third), a1);
-  u.fe[2] = fma(k2 - jx, W2(P.third), a1);
-  u.fe[3] = fma(k2 + jy, W2(P.third), a3);
-  u.fe[4] = fma(k2 - jy, W2(P.third), a3);
+  const f2 dn9 = KC((1.f/9.f))*dn, dn36 = KC((1.f/36.f))*dn;
+  const f2 a1 = fma(KC(-.5f), kyy, dn9), a3 = fma(KC(-.5f), kxx, dn9);
+  const f2 b5 = fma(KC(.25f), kxy, dn36), b7 = fma(KC(-.25f), kxy, dn36);
+  u.fe[1] = fma(k2 + jx, KC((1.f/3.f)), a1);
+  u.fe[2] = fma(k2 - jx, KC((1.f/3.f)), a1);
+  u.fe[3] = fma(k2 + jy, KC((1.f/3.f)), a3);
+  u.fe[4] = fma(k2 - jy, KC((1.f/3.f)), a3);
   const f2 s = jx + jy, d = jx - jy;
-  u.fe[5] = fma(k2 + s, W2(P.twelfth), b5);
-  u.fe[6] = fma(k2 - s, W2(P.twelfth), b5);
-  u.fe[7] = fma(k2 - d, W2(P.twelfth), b7);
-  u.fe[8] = fma(k2 + d, W2(P.twelfth), b7);
+  u.fe[5] = fma(k2 + s, KC((1.f/12.f)), b5);
+  u.fe[6] = fma(k2 - s, KC((1.f/12.f)), b5);
+  u.fe[7] = fma(k2 - d, KC((1.f/12.f)), b7);
+  u.fe[8] = fma(k2 + d, KC((1.f/12.f)), b7);
   u.fe[0] = dn - (((u.fe[1] + u.fe[2]) + (u.fe[3] + u.fe[4])) + ((u.fe[5] + u.fe[6]) + (u.fe[7] + u.fe[8])));
-  u.F[0] = W2(P.zero);
-  u.F[1] = W2(P.third)*Fx; u.F[2] = neg(u.F[1]);
-  u.F[3] = W2(P.third)*Fy; u.F[4] = neg(u.F[3]);
-  u.F[5] = W2(P.twelfth)*(Fx + Fy); u.F[6] = neg(u.F[5]);
-  u.F[7] = W2(P.twelfth)*(Fy - Fx); u.F[8] = neg(u.F[7]);
+  u.F[0] = KC(0.f);
+  u.F[1] = KC((1.f/3.f))*Fx; u.F[2] = neg(u.F[1]);
+  u.F[3] = KC((1.f/3.f))*Fy; u.F[4] = neg(u.F[3]);
+  u.F[5] = KC((1.f/12.f))*(Fx + Fy); u.F[6] = neg(u.F[5]);
+  u.F[7] = KC((1.f/12.f))*(Fy - Fx); u.F[8] = neg(u.F[7]);
 }
 
 template<int MODEL>
@@ -436,7 +434,7 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
   // fn v = 0,3,4 (3..5), ff v = 1,5,8 (6..8), fn v = 1,5,8 (9..11). C writes
   // them already shifted along y (column + cy); D reads its own columns.
 #pragma unroll
-  for(int k = 0; k < 3; ++k) { qa1[k] = qa2[k] = qn1[k] = qn2[k] = W2(P.zero); }
+  for(int k = 0; k < 3; ++k) { qa1[k] = qa2[k] = qn1[k] = qn2[k] = KC(0.f); }
   int s3 = 0;                              // i mod 3
   float* orow = a.out + static_cast<long long>(x0 - 6)*LY + yg;   // E's output row
 
@@ -478,7 +476,7 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
       else
       {
 #pragma unroll
-        for(int k = 0; k < 5; ++k) Ph[k] = W2(P.zero);
+        for(int k = 0; k < 5; ++k) Ph[k] = KC(0.f);
       }
       uq_pair<MODEL>(P, g, Qa, Qb, Ph, nq1, nullptr);
     }
@@ -488,7 +486,7 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
     {
       const YN y = ynbrs<MODEL>(q1c);
       const f2 Qxx = lds2(Rm + 9*RWW + cl), Qyx = lds2(Rm + 10*RWW + cl);
-      const f2 p = MODEL == LYO ? lds2(Rm + 11*RWW + cl) : W2(P.zero);
+      const f2 p = MODEL == LYO ? lds2(Rm + 11*RWW + cl) : KC(0.f);
       UFcore u;
       uf_core<MODEL>(P, q1c, xset(nq1), q1m, y, Qxx, Qyx, u);
       const f2 itau = itau_of<MODEL>(P, p);
@@ -497,24 +495,24 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
       {
         const f2 g = lds2(Rm + v*RWW + cl);
         const f2 coll = fma(u.fe[v] - g, itau, u.F[v]);
-        pn[v] = fma(W2(P.half), coll, g);
-        pf[v] = MODEL == LYO ? g + coll : fma(W2(P.half), coll, pn[v]);
+        pn[v] = fma(KC(.5f), coll, g);
+        pf[v] = MODEL == LYO ? g + coll : fma(KC(.5f), coll, pn[v]);
       }
-      nQN[0] = fma(W2(P.half), u.Dxx, Qxx);
-      nQN[1] = fma(W2(P.half), u.Dyx, Qyx);
+      nQN[0] = fma(KC(.5f), u.Dxx, Qxx);
+      nQN[1] = fma(KC(.5f), u.Dyx, Qyx);
       if constexpr (MODEL == LYO)
       {
         nQ[0] = Qxx + u.Dxx;
         nQ[1] = Qyx + u.Dyx;
-        nQN[2] = fma(W2(P.half), u.Dp, p);
+        nQN[2] = fma(KC(.5f), u.Dp, p);
         nQ[2] = p + u.Dp;
         if constexpr (SRC) nQ[2] = fma(p, src_at(x0 - 4 + i), nQ[2]);
       }
       else
       {
-        nQ[0] = fma(W2(P.half), u.Dxx, nQN[0]);
-        nQ[1] = fma(W2(P.half), u.Dyx, nQN[1]);
-        nQN[2] = nQ[2] = W2(P.zero);
+        nQ[0] = fma(KC(.5f), u.Dxx, nQN[0]);
+        nQ[1] = fma(KC(.5f), u.Dyx, nQN[1]);
+        nQN[2] = nQ[2] = KC(0.f);
       }
       // stream along y. Directions with cx = -1 (2, 6, 7) are used by D in
       // this same iteration: shift them by shuffles. The others go to the
@@ -563,11 +561,11 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
       else
       {
 #pragma unroll
-        for(int k = 0; k < 5; ++k) Ph[k] = W2(P.zero);
+        for(int k = 0; k < 5; ++k) Ph[k] = KC(0.f);
       }
       f2 dg[7];
       uq_pair<MODEL>(P, fs, Qa, Qb, Ph, nq2, DIAG ? dg : nullptr);
-      const f2 hitau = W2(P.nhalf)*itau_of<MODEL>(P, qa1[2]);
+      const f2 hitau = KC(-.5f)*itau_of<MODEL>(P, qa1[2]);
 #pragma unroll
       for(int v = 0; v < 9; ++v)
         *reinterpret_cast<float2*>(hrow + ((i & 1)*9 + v)*COLS + 2*lane) = fma(hitau, fs[v], ns[v]).v;
@@ -607,15 +605,15 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
       UFcore u;
       uf_core<MODEL>(P, q2c, xset(nq2), q2m, y, qa2[0], qa2[1], u);
       const f2 itau = itau_of<MODEL>(P, qa2[2]);
-      const f2 hitau = W2(P.half)*itau;
+      const f2 hitau = KC(.5f)*itau;
       f2 gout[9];
 #pragma unroll
       for(int v = 0; v < 9; ++v)
-        gout[v] = fma(W2(P.half), u.F[v],
+        gout[v] = fma(KC(.5f), u.F[v],
                       fma(hitau, u.fe[v], lds2(hrow + (((i + 1) & 1)*9 + v)*COLS + 2*lane)));
-      const f2 Qo0 = fma(W2(P.half), u.Dxx, qn2[0]);
-      const f2 Qo1 = fma(W2(P.half), u.Dyx, qn2[1]);
-      f2 Qo2 = fma(W2(P.half), u.Dp, qn2[2]);
+      const f2 Qo0 = fma(KC(.5f), u.Dxx, qn2[0]);
+      const f2 Qo1 = fma(KC(.5f), u.Dyx, qn2[1]);
+      f2 Qo2 = fma(KC(.5f), u.Dp, qn2[2]);
       // corrector source with the predicted phi of this row
       if constexpr (SRC) Qo2 = fma(qa2[2], src_at(x0 - 6 + i), Qo2);
       if(i >= 6)
