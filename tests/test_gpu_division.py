@@ -339,3 +339,35 @@ def test_queued_circles_wrapping_the_lattice():
     assert bits_equal(a.get("phi"), b.get("phi"))
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("prec", [M.FP64, M.FP32])
+def test_queued_masks_on_a_large_lattice(prec):
+    """More than 1024 chunks of 1024 sites: every block of the queued draw
+    walks several chunks and forms chunk offsets across segments of the
+    count array. Masks and queue count equal the draw-by-draw path's."""
+    LX, LY = 1100, 1000
+    N = LX * LY
+    st = O.synthetic_state(O.LYOTROPIC, LX, LY, seed=6, flow=0.01, phi_kind="disk",
+                           radius=450)
+    p = params()
+    a = M.Lattice(M.LYOTROPIC, p, LX, LY, 0, prec)
+    b = M.Lattice(M.LYOTROPIC, p, LX, LY, 0, prec)
+    a.upload_state(st)
+    b.upload_state(st)
+    u = np.random.default_rng(11).uniform(0, 1, 4 * N)
+    a.mask_supply(u[:4 * N], True)
+    a.draw_masks_queued(3, 0.02, 3.0, 0.01, 2.0, 1.3, 0.05, 0.03)
+    n = b.mask_candidates()
+    assert n > N // 2
+    b.draw_mask(0, u[:n], 0.02, 1.3, 3.0, 0.05, 0.03)
+    b.draw_mask(1, u[n:2 * n], 0.01, 1.3, 2.0, 0.05, 0.03)
+    assert a.mask_consumed() == 2 * n
+    for kind in (0, 1):
+        m = a.get_mask(kind)
+        assert m.any() and np.array_equal(m, b.get_mask(kind)), kind
+    a.step(1)
+    b.step(1)
+    assert bits_equal(a.get("phi"), b.get("phi"))
+    a.close()
+    b.close()
