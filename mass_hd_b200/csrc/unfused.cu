@@ -561,12 +561,15 @@ uf_kernel(Dims d, Params P, State<T> s)
 // UpdateQuantities over the block's tile plus a one-site ring into shared
 // memory, then UpdateFields over the tile reading its stencils from there.
 // The ring sites are computed by both neighbouring blocks with the same
-// expressions, so the values equal the two-sweep form's; nothing derived is
-// written to HBM except on the last sub-step of a call (storeq), which
-// leaves the same planes the two sweeps leave. Blocks read Q, phi, chi and
+// expressions, so the values equal the two-sweep form's. Nothing derived is
+// written to HBM unless storeq is set, which leaves the planes the two
+// sweeps leave (the library replays them on demand instead). Blocks read Q, phi, chi and
 // ff around their tile, so the new Q and (corrector) ff are written beside
 // them (SEP) and the host swaps the planes after the launch.
-constexpr int SUB_TY = 32, SUB_TX = 8;                 // tile: y (contiguous) x x
+// One thread per site of the tile and its ring (32 x 10 threads, a warp per
+// x row): every thread computes one UpdateQuantities, the 30 x 8 inner ones
+// then one UpdateFields.
+constexpr int SUB_TY = 30, SUB_TX = 8;                 // tile: y (contiguous) x x
 constexpr int SUB_HY = SUB_TY + 2, SUB_HX = SUB_TX + 2;
 constexpr int SUB_HS = SUB_HY*SUB_HX;
 
@@ -588,21 +591,23 @@ struct TileUQ : UQStencil<T, TileUQ<T>>
 };
 
 template<typename T, bool DEV, int MODEL, bool FIRST, bool DIAG>
-__global__ void __launch_bounds__(SUB_TY*SUB_TX)
+__global__ void __launch_bounds__(SUB_HY*SUB_HX)
 substep_kernel(Dims d, Params P, State<T> s, int storeq, int prefetch)
 {
   extern __shared__ __align__(16) unsigned char sub_smem[];
   T (*uq_s)[SUB_HS] = reinterpret_cast<T (*)[SUB_HS]>(sub_smem);
   const int y0 = blockIdx.x*SUB_TY, x0 = blockIdx.y*SUB_TX;
-  const int tid = threadIdx.y*SUB_TY + threadIdx.x;
+  const int i = threadIdx.y*SUB_HY + threadIdx.x;          // this thread's tile site
+  const int X = x0 - 1 + static_cast<int>(threadIdx.y), Y = y0 - 1 + static_cast<int>(threadIdx.x);
+  const bool inner = threadIdx.x >= 1 && threadIdx.x <= SUB_TY && threadIdx.y >= 1 &&
+                     threadIdx.y <= SUB_TX && X < d.LX && Y < d.LY;
   if constexpr (!FIRST)
   {
     // the corrector's own-site inputs (fn, QN, phi_N, m_N) start towards L2
     // while the tile's UpdateQuantities runs (states larger than L2)
-    const int y = y0 + threadIdx.x, x = x0 + threadIdx.y;
-    if(prefetch && x < d.LX && y < d.LY)
+    if(prefetch && inner)
     {
-      const long long e = y + static_cast<long long>(d.EY)*x;
+      const long long e = Y + static_cast<long long>(d.EY)*X;
 #pragma unroll
       for(int v = 0; v < 9; ++v) prefetch_l2(s.fn + v*d.NE + e);
       prefetch_l2(s.QNxx + e);
@@ -611,12 +616,9 @@ substep_kernel(Dims d, Params P, State<T> s, int storeq, int prefetch)
       if constexpr (MODEL == GOG) prefetch_l2(s.mN + e);
     }
   }
-  for(int i = tid; i < SUB_HS; i += SUB_TY*SUB_TX)
+  // the ring one past the lattice's end is the periodic image of site 0
+  if(X <= d.LX && Y <= d.LY)
   {
-    const int hx = i/SUB_HY, hy = i - hx*SUB_HY;
-    const int X = x0 - 1 + hx, Y = y0 - 1 + hy;
-    // the ring one past the lattice's end is the periodic image of site 0
-    if(X > d.LX || Y > d.LY) continue;
     const Nbr<T> nb = neighbours<T>(d, wrapi(X, d.LX), wrapi(Y, d.LY));
     UQOut<T> o;
     uq_site<T, DEV, MODEL, DIAG>(P, s, nb, d.NE, o);
@@ -629,17 +631,15 @@ substep_kernel(Dims d, Params P, State<T> s, int storeq, int prefetch)
     {
       uq_s[Q_UXP][i] = o.uxp; uq_s[Q_UYP][i] = o.uyp; uq_s[Q_MU][i] = o.MU;
     }
-    if(storeq && hx >= 1 && hx <= SUB_TX && hy >= 1 && hy <= SUB_TY && X < d.LX && Y < d.LY)
-      store_uq<T, MODEL, DIAG>(s, nb.e, o);
+    if(storeq && inner) store_uq<T, MODEL, DIAG>(s, nb.e, o);
   }
   __syncthreads();
-  const int y = y0 + threadIdx.x, x = x0 + threadIdx.y;
-  if(x >= d.LX || y >= d.LY) return;
-  const Nbr<T> nb = neighbours<T>(d, x, y);
+  if(!inner) return;
+  const Nbr<T> nb = neighbours<T>(d, X, Y);
   TileUQ<T> U;
   U.a = uq_s;
-  U.c = (threadIdx.y + 1)*SUB_HY + threadIdx.x + 1;
-  uf_site<T, DEV, MODEL, FIRST, FIRST, TileUQ<T>, true>(d, P, s, nb, x, y, U);
+  U.c = i;
+  uf_site<T, DEV, MODEL, FIRST, FIRST, TileUQ<T>, true>(d, P, s, nb, X, Y, U);
 }
 
 // Launch a sub-step; its tile needs NUQ*SUB_HS values of shared memory,
@@ -662,7 +662,7 @@ void launch_substep(const Dims& d, const Params& P, const State<T>& s, int store
       done.fetch_or(bit);
     }
   }
-  const dim3 blk(SUB_TY, SUB_TX);
+  const dim3 blk(SUB_HY, SUB_HX);
   const dim3 grd((d.LY + SUB_TY - 1)/SUB_TY, (d.LX + SUB_TX - 1)/SUB_TX);
   // about 60 planes of state and sweep fields; L2 holds 126 MB
   const int prefetch = static_cast<double>(d.NE)*sizeof(T)*60 > 96e6 ? 1 : 0;
