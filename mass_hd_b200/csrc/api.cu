@@ -179,6 +179,7 @@ struct mass_lb_handle
   long long mq_pinned_cap[MQ_STAGES] = {};
   cudaEvent_t mq_copied[MQ_STAGES] = {}; // the last copy from each buffer has been read
   int mq_stage = 0;                      // the buffer of the next supply
+  cudaStream_t mq_copy = nullptr;        // the supplies' copies (off the step stream)
   long long* mq_state = nullptr;         // device: [0] queue head, [1] error flag (low word)
   int* mq_err = nullptr;                 // the error flag as the kernels set it
   long long* mq_host = nullptr;          // pinned: mq_state of each draw slot
@@ -512,6 +513,7 @@ void mass_lb_destroy(mass_lb_handle* h)
   for(int i = 0; i < mass_lb_handle::MQ_SLOTS; ++i)
     if(h->mq_counted[i]) cudaEventDestroy(h->mq_counted[i]);
   if(h->mq_host) cudaFreeHost(h->mq_host);
+  if(h->mq_copy) cudaStreamDestroy(h->mq_copy);
   if(h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
@@ -1394,6 +1396,7 @@ int ensure_queue(mass_lb_handle* h)
   h->mq_err = reinterpret_cast<int*>(h->mq_state + 1);   // little-endian low word
   CU(cudaMemsetAsync(h->mq_state, 0, 2*sizeof(long long), h->stream), "memset");
   CU(cudaMallocHost(reinterpret_cast<void**>(&h->mq_host), 2*S*sizeof(long long)), "pinned");
+  CU(cudaStreamCreateWithFlags(&h->mq_copy, cudaStreamNonBlocking), "copy stream");
   for(int i = 0; i < 2*S; ++i) h->mq_host[i] = 0;
   for(int i = 0; i < B; ++i)
   {
@@ -1493,15 +1496,17 @@ int mass_lb_mask_supply(mass_lb_handle* h, const double* u, long long n)
     stage = h->mq_pinned[i];
     std::memcpy(h->mq_pinned[i], u, n*sizeof(double));
   }
+  // the values go up on the copy stream, so they need not wait for the
+  // steps queued before them; the next draw on the step stream waits for them
   const long long p = q.supplied % q.cap;
   const long long n1 = std::min(n, q.cap - p);
   CU(cudaMemcpyAsync(q.buf + p, stage, n1*sizeof(double), cudaMemcpyHostToDevice,
-                     h->stream), "supply copy");
+                     h->mq_copy), "supply copy");
   if(n1 < n)
     CU(cudaMemcpyAsync(q.buf, stage + n1, (n - n1)*sizeof(double),
-                       cudaMemcpyHostToDevice, h->stream), "supply copy");
-  // the new count follows the values, so a draw sees both or neither
-  CU(cudaEventRecord(h->mq_copied[i], h->stream), "event");
+                       cudaMemcpyHostToDevice, h->mq_copy), "supply copy");
+  CU(cudaEventRecord(h->mq_copied[i], h->mq_copy), "event");
+  CU(cudaStreamWaitEvent(h->stream, h->mq_copied[i], 0), "event wait");
   h->mq_stage = i ^ 1;
   q.supplied += n;
   return 0;
