@@ -182,8 +182,10 @@ struct mass_lb_handle
   cudaStream_t mq_copy = nullptr;        // the supplies' copies (off the step stream)
   long long* mq_state = nullptr;         // device: [0] queue head, [1] error flag (low word)
   int* mq_err = nullptr;                 // the error flag as the kernels set it
-  long long* mq_host = nullptr;          // pinned: mq_state of each draw slot
-  cudaEvent_t mq_counted[MQ_SLOTS] = {}; // a slot's mq_state has landed
+  long long* mq_snap = nullptr;          // device: (head, flag) after each draw slot's draw
+  long long* mq_host = nullptr;          // pinned: the same, per slot
+  cudaEvent_t mq_drew[MQ_SLOTS] = {};    // a slot's draw has finished (step stream)
+  cudaEvent_t mq_counted[MQ_SLOTS] = {}; // a slot's snapshot has landed
   long long mq_issued = 0;               // queued draws issued
   long long mq_known = 0;                // draws whose counts have been read (a prefix)
   long long mq_consumed = 0;             // draws consumed up to the last known draw
@@ -511,7 +513,10 @@ void mass_lb_destroy(mass_lb_handle* h)
     if(h->mq_copied[i]) cudaEventDestroy(h->mq_copied[i]);
   }
   for(int i = 0; i < mass_lb_handle::MQ_SLOTS; ++i)
+  {
     if(h->mq_counted[i]) cudaEventDestroy(h->mq_counted[i]);
+    if(h->mq_drew[i]) cudaEventDestroy(h->mq_drew[i]);
+  }
   if(h->mq_host) cudaFreeHost(h->mq_host);
   if(h->mq_copy) cudaStreamDestroy(h->mq_copy);
   if(h->stream) cudaStreamDestroy(h->stream);
@@ -1392,6 +1397,7 @@ int ensure_queue(mass_lb_handle* h)
   const long long cap = 6*N + (1ll << 16);
   if(int r = dalloc(h, &h->mq.buf, static_cast<size_t>(cap))) return r;
   if(int r = dalloc(h, &h->mq_state, 2)) return r;
+  if(int r = dalloc(h, &h->mq_snap, 2*S)) return r;
   h->mq.head = h->mq_state;
   h->mq_err = reinterpret_cast<int*>(h->mq_state + 1);   // little-endian low word
   CU(cudaMemsetAsync(h->mq_state, 0, 2*sizeof(long long), h->stream), "memset");
@@ -1404,7 +1410,10 @@ int ensure_queue(mass_lb_handle* h)
     CU(cudaEventRecord(h->mq_copied[i], h->stream), "event");
   }
   for(int i = 0; i < S; ++i)
+  {
     CU(cudaEventCreateWithFlags(&h->mq_counted[i], cudaEventDisableTiming), "event");
+    CU(cudaEventCreateWithFlags(&h->mq_drew[i], cudaEventDisableTiming), "event");
+  }
   h->mq.cap = cap;
   h->mq.supplied = 0;
   h->mq_issued = h->mq_known = h->mq_consumed = 0;
@@ -1534,13 +1543,17 @@ int mass_lb_draw_masks_queued(mass_lb_handle* h, int kinds, double division_coef
     using T = std::remove_cv_t<std::remove_pointer_t<decltype(v.phi)>>;
     if(dbl != (std::is_same<T, double>::value ? 1 : 0)) return cudaErrorInvalidValue;
     const QueuedDraw<T> w{kinds, {division_coef, death_coef}, {division_radius, death_radius},
-                          phi_critical, alpha, beta, static_cast<T*>(plane), gg, EY, h->mq_err};
+                          phi_critical, alpha, beta, static_cast<T*>(plane), gg, EY, h->mq_err,
+                          h->mq_snap + 2*sl};
     return mask_draw_queued_fused(v, h->mk, h->mq, w, h->stream);
   });
   if(e != cudaSuccess) return cuda_fail(e, "queued masks");
-  CU(cudaMemcpyAsync(h->mq_host + 2*sl, h->mq_state, 2*sizeof(long long), cudaMemcpyDeviceToHost,
-                     h->stream), "queue count");
-  CU(cudaEventRecord(h->mq_counted[sl], h->stream), "event");
+  // the snapshot comes down on the copy stream, off the step stream
+  CU(cudaEventRecord(h->mq_drew[sl], h->stream), "event");
+  CU(cudaStreamWaitEvent(h->mq_copy, h->mq_drew[sl], 0), "event wait");
+  CU(cudaMemcpyAsync(h->mq_host + 2*sl, h->mq_snap + 2*sl, 2*sizeof(long long),
+                     cudaMemcpyDeviceToHost, h->mq_copy), "queue count");
+  CU(cudaEventRecord(h->mq_counted[sl], h->mq_copy), "event");
   ++h->mq_issued;
   if(h->fused && h->cfg.nt != 32) h->tuned = false;   // the source runs in the warp-strip kernel
   h->s64.src = h->src64;

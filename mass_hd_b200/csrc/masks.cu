@@ -221,7 +221,8 @@ __device__ __forceinline__ void stamp_circle(int LX, int LY, long long k,
 //     and a centre writes its circle into the mask of its kind (as
 //     stamp_kernel),
 //  3. the source plane alpha*division - beta*death (as rate_kernel) and
-//     head += kinds drawn * total.
+//     head += kinds drawn * total, also written with the error flag to the
+//     draw's snapshot.
 template<typename T>
 __global__ void __launch_bounds__(MB)
 queued_draw_kernel(MaskView<T> v, MaskScratch s, const double* __restrict__ queue, long long qcap,
@@ -330,7 +331,14 @@ queued_draw_kernel(MaskView<T> v, MaskScratch s, const double* __restrict__ queu
     const double r = w.alpha*(m0 ? 1. : 0.) - w.beta*(m1 ? 1. : 0.);
     w.src[(y + w.g) + static_cast<long long>(w.EY)*(x + w.g)] = static_cast<T>(r);
   }
-  if(blockIdx.x == 0 && tid == 0) *head = h0 + (div + dea)*total;
+  if(blockIdx.x == 0 && tid == 0)
+  {
+    *head = h0 + (div + dea)*total;
+    // a copy of the queue state for the host, which this draw's slot owns
+    // until the host has read it (the live head moves with the next draw)
+    w.snap[0] = h0 + (div + dea)*total;
+    w.snap[1] = *w.err;
+  }
 }
 
 inline int grid_for(long long n)

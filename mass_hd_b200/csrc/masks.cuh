@@ -48,6 +48,7 @@ struct QueuedDraw
   T* src;                // the step kernels' source plane (ghost ring g, row stride EY)
   int g, EY;
   int* err;
+  long long* snap;       // after the draw: [0] queue head, [1] error flag
 };
 
 int mask_blocks(long long nsites);
