@@ -301,6 +301,9 @@ uq_kernel(Dims d, Params P, State<T> s)
 // UpdateQuantities fields, in the order of UQOut
 enum { Q_N = 0, Q_UX, Q_UY, Q_UXP, Q_UYP, Q_HXX, Q_HYX, Q_MU, Q_DXQXX, Q_DYQXX, Q_DXQYX,
        Q_DYQYX, Q_SXX, Q_SYY, Q_SXY, Q_SYX, NUQ };
+// state scalars UpdateFields reads around a site (phi, and m and chi for
+// go-or-grow), after the UpdateQuantities values in the tile
+enum { S_PHI = NUQ, S_CHI, S_M, NTILE };
 
 // The UpdateQuantities values of a site (w = 0) and its neighbours +x, -x,
 // +y, -y (w = 1..4), with the stencils of src/lb.hpp in their operand order.
@@ -322,10 +325,11 @@ struct UQStencil
 template<typename T>
 struct GlobalUQ : UQStencil<T, GlobalUQ<T>>
 {
-  const T* p[NUQ];
+  const T* p[NTILE];
   long long k[5];
   __device__ __forceinline__ GlobalUQ(const State<T>& s, const Nbr<T>& nb)
   {
+    p[S_PHI] = s.phi; p[S_CHI] = s.chi; p[S_M] = s.m;
     p[Q_N] = s.n; p[Q_UX] = s.ux; p[Q_UY] = s.uy; p[Q_UXP] = s.uxp; p[Q_UYP] = s.uyp;
     p[Q_HXX] = s.Hxx; p[Q_HYX] = s.Hyx; p[Q_MU] = s.MU; p[Q_DXQXX] = s.dxQxx;
     p[Q_DYQXX] = s.dyQxx; p[Q_DXQYX] = s.dxQyx; p[Q_DYQYX] = s.dyQyx; p[Q_SXX] = s.sXX;
@@ -399,7 +403,7 @@ __device__ __forceinline__ void uf_site(const Dims& d, const Params& P, const St
 
   if constexpr (MODEL != NEM)
   {
-    const T p = s.phi[e];
+    const T p = U.at(S_PHI, 0);
     // go-or-grow phenotype update (src/models/go-or-grow.cpp:331-362): the
     // growth R = chi*phi*(alpha*division_mask - beta*death_mask) and the
     // rate of change Dm of m = phi*chi
@@ -407,12 +411,12 @@ __device__ __forceinline__ void uf_site(const Dims& d, const Params& P, const St
     if constexpr (MODEL == GOG)
     {
       const T rate = s.src ? s.src[e] : T(0);
-      const T chi_eff = s.chi[e];
+      const T chi_eff = U.at(S_CHI, 0);
       R = chi_eff*p*rate;
-      const T mFlux = T(.5)*(U.at(Q_UX, 1)*s.m[nb.e1] - U.at(Q_UX, 2)*s.m[nb.e2])
-                    + T(.5)*(U.at(Q_UY, 3)*s.m[nb.e3] - U.at(Q_UY, 4)*s.m[nb.e4]);
-      const T chi_px = s.chi[nb.e1], chi_mx = s.chi[nb.e2];
-      const T chi_py = s.chi[nb.e3], chi_my = s.chi[nb.e4];
+      const T mFlux = T(.5)*(U.at(Q_UX, 1)*U.at(S_M, 1) - U.at(Q_UX, 2)*U.at(S_M, 2))
+                    + T(.5)*(U.at(Q_UY, 3)*U.at(S_M, 3) - U.at(Q_UY, 4)*U.at(S_M, 4));
+      const T chi_px = U.at(S_CHI, 1), chi_mx = U.at(S_CHI, 2);
+      const T chi_py = U.at(S_CHI, 3), chi_my = U.at(S_CHI, 4);
       const T MUe = U.at(Q_MU, 0);
       const T diffusiveMFlux =
         T(.5)*(chi_px + chi_eff)*(U.at(Q_MU, 1) - MUe)
@@ -420,10 +424,10 @@ __device__ __forceinline__ void uf_site(const Dims& d, const Params& P, const St
       + T(.5)*(chi_py + chi_eff)*(U.at(Q_MU, 3) - MUe)
       - T(.5)*(chi_eff + chi_my)*(MUe - U.at(Q_MU, 4));
       const T phenotypeDiffusion =
-        T(.5)*(s.phi[nb.e1] + p)*(chi_px - chi_eff)
-      - T(.5)*(p + s.phi[nb.e2])*(chi_eff - chi_mx)
-      + T(.5)*(s.phi[nb.e3] + p)*(chi_py - chi_eff)
-      - T(.5)*(p + s.phi[nb.e4])*(chi_eff - chi_my);
+        T(.5)*(U.at(S_PHI, 1) + p)*(chi_px - chi_eff)
+      - T(.5)*(p + U.at(S_PHI, 2))*(chi_eff - chi_mx)
+      + T(.5)*(U.at(S_PHI, 3) + p)*(chi_py - chi_eff)
+      - T(.5)*(p + U.at(S_PHI, 4))*(chi_eff - chi_my);
       const T Achi = T(s.ph.Achi);
       const T dVdChi = T(2)*Achi*chi_eff*(T(1)-chi_eff)*(T(1)-T(2)*chi_eff)
                      + T(s.ph.Ochi)*(p-T(s.ph.phiswitch));
@@ -456,19 +460,20 @@ __device__ __forceinline__ void uf_site(const Dims& d, const Params& P, const St
     {
       s.QNxx[e] = s.Qxx[e] + T(.5)*Dxx;
       s.QNyx[e] = s.Qyx[e] + T(.5)*Dyx;
-      s.phn[e]  = s.phi[e] + T(.5)*Dp;
+      s.phn[e]  = p + T(.5)*Dp;
       QXo[e]  = s.Qxx[e] + Dxx;
       QYo[e]  = s.Qyx[e] + Dyx;
-      T pt = s.phi[e] + Dp;
+      T pt = p + Dp;
       if constexpr (MODEL == GOG)
       {
         pt = pt + R;
-        s.mN[e] = s.m[e] + T(.5)*Dm;
-        phenotype_out(pt, s.m[e] + Dm);
+        const T me = U.at(S_M, 0);
+        s.mN[e] = me + T(.5)*Dm;
+        phenotype_out(pt, me + Dm);
       }
       // division source, added after the node update as the division model
       // does (src/models/lyotropic-with-division.cpp:121)
-      else if(s.src) pt = pt + s.phi[e]*s.src[e];
+      else if(s.src) pt = pt + p*s.src[e];
       s.phi_tmp[e] = pt;
 #pragma unroll
       for(int v=0; v<9; ++v)
@@ -492,7 +497,7 @@ __device__ __forceinline__ void uf_site(const Dims& d, const Params& P, const St
         pt = pt + R;
         phenotype_out(pt, s.mN[e] + T(.5)*Dm);
       }
-      else if(s.src) pt = pt + s.phi[e]*s.src[e];
+      else if(s.src) pt = pt + p*s.src[e];
       s.phi_tmp[e] = pt;
 #pragma unroll
       for(int v=0; v<9; ++v)
@@ -630,6 +635,12 @@ substep_kernel(Dims d, Params P, State<T> s, int storeq, int prefetch)
     if constexpr (MODEL != NEM)
     {
       uq_s[Q_UXP][i] = o.uxp; uq_s[Q_UYP][i] = o.uyp; uq_s[Q_MU][i] = o.MU;
+      uq_s[S_PHI][i] = s.phi[nb.e];
+    }
+    if constexpr (MODEL == GOG)
+    {
+      uq_s[S_CHI][i] = s.chi[nb.e];
+      uq_s[S_M][i] = s.m[nb.e];
     }
     if(storeq && inner) store_uq<T, MODEL, DIAG>(s, nb.e, o);
   }
@@ -642,13 +653,13 @@ substep_kernel(Dims d, Params P, State<T> s, int storeq, int prefetch)
   uf_site<T, DEV, MODEL, FIRST, FIRST, TileUQ<T>, true>(d, P, s, nb, X, Y, U);
 }
 
-// Launch a sub-step; its tile needs NUQ*SUB_HS values of shared memory,
+// Launch a sub-step; its tile needs NTILE*SUB_HS values of shared memory,
 // above the 48 KB default for larger tiles in FP64.
 template<typename T, bool DEV, int MODEL, bool FIRST, bool DIAG>
 void launch_substep(const Dims& d, const Params& P, const State<T>& s, int storeq,
                     cudaStream_t st)
 {
-  constexpr size_t bytes = sizeof(T)*NUQ*SUB_HS;
+  constexpr size_t bytes = sizeof(T)*NTILE*SUB_HS;
   if constexpr (bytes > 48*1024)
   {
     static std::atomic<unsigned long long> done{0};
