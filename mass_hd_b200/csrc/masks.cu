@@ -252,24 +252,39 @@ queued_draw_kernel(MaskView<T> v, MaskScratch s, const double* __restrict__ queu
   }
   grid.sync();
 
-  // exclusive prefix of the per-thread segments of the chunk counts
+  // inclusive prefix of the per-thread segments of the chunk counts: warp
+  // scans by shuffles, then the scan of the 32 warp totals
   const int per = (nch + MB - 1)/MB;
+  const unsigned lane = tid & 31u, warp = tid >> 5;
   {
+    __shared__ long long wsum[MB/32];
     const int lo = tid*per, hi = min(nch, lo + per);
     long long sum = 0;
     for(int i = lo; i < hi; ++i) sum += s.block_cnt[i];
-    part[tid] = sum;
-    __syncthreads();
-    for(int d = 1; d < MB; d <<= 1)
+#pragma unroll
+    for(int d = 1; d < 32; d <<= 1)
     {
-      const long long add = tid >= d ? part[tid - d] : 0;
-      __syncthreads();
-      part[tid] += add;
-      __syncthreads();
+      const long long add = __shfl_up_sync(0xffffffffu, sum, d);
+      if(lane >= static_cast<unsigned>(d)) sum += add;
     }
+    if(lane == 31) wsum[warp] = sum;
+    __syncthreads();
+    if(warp == 0)
+    {
+      long long ws = wsum[lane];
+#pragma unroll
+      for(int d = 1; d < 32; d <<= 1)
+      {
+        const long long add = __shfl_up_sync(0xffffffffu, ws, d);
+        if(lane >= static_cast<unsigned>(d)) ws += add;
+      }
+      wsum[lane] = ws;
+    }
+    __syncthreads();
+    part[tid] = sum + (warp ? wsum[warp - 1] : 0);
+    __syncthreads();
   }
   const long long total = part[MB - 1], h0 = *head;
-  const unsigned lane = tid & 31u, warp = tid >> 5;
   for(int c = blockIdx.x; c < nch; c += gridDim.x)
   {
     const long long k = static_cast<long long>(c)*MB + tid;
