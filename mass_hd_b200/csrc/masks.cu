@@ -193,21 +193,22 @@ __global__ void rate_kernel(int LX, int LY, int g, int EY, const unsigned char* 
   }
 }
 
-// The circle of one centre site k, as stamp_kernel writes it (every writer
-// stores 1).
-__device__ __forceinline__ void stamp_circle(int LX, int LY, long long k,
-                                             unsigned char* __restrict__ mask, double r2, int R)
+// The circle of centre site k as stamp_kernel writes it (every writer
+// stores 1), by a warp: lane l takes the offsets l, l+32, ... of the
+// (2R+1)^2 square.
+__device__ __forceinline__ void stamp_circle_warp(int LX, int LY, long long k,
+                                                  unsigned char* __restrict__ mask, double r2,
+                                                  int R, unsigned lane)
 {
   const int cx = static_cast<int>(k / LY), cy = static_cast<int>(k % LY);
-  for(int dx = -R; dx <= R; ++dx)
+  const int D = 2*R + 1;
+  for(int o = static_cast<int>(lane); o < D*D; o += 32)
   {
+    const int dx = o/D - R, dy = o - (o/D)*D - R;
+    if(static_cast<double>(dx*dx + dy*dy) > r2) continue;
     const int x = ((cx + dx) % LX + LX) % LX;
-    for(int dy = -R; dy <= R; ++dy)
-    {
-      if(static_cast<double>(dx*dx + dy*dy) > r2) continue;
-      const int y = ((cy + dy) % LY + LY) % LY;
-      mask[y + static_cast<long long>(LY)*x] = 1;
-    }
+    const int y = ((cy + dy) % LY + LY) % LY;
+    mask[y + static_cast<long long>(LY)*x] = 1;
   }
 }
 
@@ -294,7 +295,8 @@ queued_draw_kernel(MaskView<T> v, MaskScratch s, const double* __restrict__ queu
     __syncthreads();   // warp_cnt of the previous chunk has been read
     if(lane == 0) warp_cnt[warp] = __popc(ballot);
     __syncthreads();
-    if(!flag) continue;
+    unsigned cen = 0;   // bit j: a centre of kind j
+    if(flag)
     {
       // chunk offset: the segments before c's, then the chunks before c in it
       const int sg = c/per;
@@ -314,13 +316,23 @@ queued_draw_kernel(MaskView<T> v, MaskScratch s, const double* __restrict__ queu
         {
           // src/models/lyotropic-with-division.cpp:47 (division), :83 (death)
           const double thr = j == 0 ? w.coef[0]*p*(1 - p/w.phi_critical) : w.coef[1]*p;
-          if(queue[idx % qcap] < thr)
-          {
-            if(j == 0 && R0 >= 0) stamp_circle(v.LX, v.LY, k, s.mask[0], r2_0, R0);
-            if(j == 1 && R1 >= 0) stamp_circle(v.LX, v.LY, k, s.mask[1], r2_1, R1);
-          }
+          if(queue[idx % qcap] < thr) cen |= 1u << j;
         }
         else atomicOr(w.err, 1);
+      }
+    }
+    // the warp writes the circles of its centres together, one offset per lane
+    for(int j = 0; j < 2; ++j)
+    {
+      const int R = j ? R1 : R0;
+      if(!((w.kinds >> j) & 1) || R < 0) continue;
+      unsigned todo = __ballot_sync(0xffffffffu, (cen >> j) & 1u);
+      while(todo)
+      {
+        const int src = __ffs(todo) - 1;
+        todo &= todo - 1;
+        const long long kc = __shfl_sync(0xffffffffu, k, src);
+        stamp_circle_warp(v.LX, v.LY, kc, s.mask[j], j ? r2_1 : r2_0, R, lane);
       }
     }
   }
