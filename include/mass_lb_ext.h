@@ -88,6 +88,23 @@ int mass_lb_state_sums_noalloc(const float* planes, long long plane_stride, int 
                                unsigned LX, unsigned LY, double rho, void* stream,
                                double* fsum, double* phisum, int* nonfinite);
 
+/* ---- asynchronous transfers -------------------------------------------------
+ * The state's transfers without a wait on the host, for pipelines that keep
+ * several lattices busy: one lattice's input goes up and another's result
+ * comes down while a third steps. Both take pinned host buffers only
+ * (MASS_LB_EINVAL otherwise) and are ordered on the handle's stream with
+ * its steps. The host buffers must stay untouched, and `out` unread, until
+ * mass_lb_synchronize returns.
+ *
+ * mass_lb_upload_async: mass_lb_upload's work. The totals of the new state
+ * (mass_lb_initial_totals) are computed on the stream too and read when
+ * first asked for.
+ *
+ * mass_lb_download_async: mass_lb_download of ff, QQxx, QQyx or phi. */
+int mass_lb_upload_async(mass_lb_handle* h, const double* ff, const double* QQxx,
+                         const double* QQyx, const double* phi);
+int mass_lb_download_async(mass_lb_handle* h, int field, double* out);
+
 /* ---- checkpoints ------------------------------------------------------------
  *
  * Full-precision binary checkpoint of a lattice, filling the role of the

@@ -154,6 +154,9 @@ struct mass_lb_handle
   int* err = nullptr;
 
   double ftot = 0, ptot = 0;
+  double* tot_host = nullptr;   // pinned: the sums of an asynchronous upload
+  cudaEvent_t tot_ev = nullptr; // they have landed
+  bool tot_pending = false;     // ftot/ptot still to be read from tot_host
   unsigned long long steps = 0;
 
   // division-model hooks (mass_lb_set_phi_source / _conservation)
@@ -518,10 +521,18 @@ void mass_lb_destroy(mass_lb_handle* h)
     if(h->mq_drew[i]) cudaEventDestroy(h->mq_drew[i]);
   }
   if(h->mq_host) cudaFreeHost(h->mq_host);
+  if(h->tot_host) cudaFreeHost(h->tot_host);
+  if(h->tot_ev) cudaEventDestroy(h->tot_ev);
   if(h->mq_copy) cudaStreamDestroy(h->mq_copy);
   if(h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
+
+namespace {
+cudaError_t launch_sums(mass_lb_handle* h);
+int resolve_totals(mass_lb_handle* h);
+bool pinned_host(const void* p);
+} // namespace
 
 // The derived fields of the last step, computed now if the step left them
 // (before anything changes the state they come from, or when asked for).
@@ -626,8 +637,42 @@ int mass_lb_upload(mass_lb_handle* h, const double* ff, const double* QQxx,
   double fs = 0, ps = 0;
   int bad = 0;
   if(int r = mass_lb_checks(h, &fs, &ps, &bad)) return r;
+  if(int r = resolve_totals(h)) return r;   // an earlier asynchronous upload's
   h->ftot = fs;
   h->ptot = ps;
+  return 0;
+}
+
+int mass_lb_upload_async(mass_lb_handle* h, const double* ff, const double* QQxx,
+                         const double* QQyx, const double* phi)
+{
+  if(!h || !ff || !QQxx || !QQyx) return fail(MASS_LB_EINVAL, "null argument");
+  if(h->model != NEM && !phi) return fail(MASS_LB_EINVAL, "lyotropic models need phi");
+  DeviceGuard g(h->device);
+  if(!pinned_host(ff) || !pinned_host(QQxx) || !pinned_host(QQyx) ||
+     (h->model != NEM && !pinned_host(phi)))
+    return fail(MASS_LB_EINVAL, "asynchronous uploads take pinned host buffers");
+  if(int r = settle_derived(h)) return r;
+  if(int r = resolve_totals(h)) return r;
+  if(!h->tot_host)
+  {
+    CU(cudaMallocHost(reinterpret_cast<void**>(&h->tot_host), 3*sizeof(double)), "pinned");
+    CU(cudaEventCreateWithFlags(&h->tot_ev, cudaEventDisableTiming), "event");
+  }
+  if(int r = put_field(h, MASS_LB_FF, ff)) return r;
+  if(int r = put_field(h, MASS_LB_QQXX, QQxx)) return r;
+  if(int r = put_field(h, MASS_LB_QQYX, QQyx)) return r;
+  if(h->model != NEM)
+    if(int r = put_field(h, MASS_LB_PHI, phi)) return r;
+  h->has_prev = false;
+  h->steps = 0;
+  // the reference totals follow on the stream; read when first asked for
+  const cudaError_t e = launch_sums(h);
+  if(e != cudaSuccess) return cuda_fail(e, "sums");
+  CU(cudaMemcpyAsync(h->tot_host, h->red_out, 3*sizeof(double), cudaMemcpyDeviceToHost,
+                     h->stream), "sums copy");
+  CU(cudaEventRecord(h->tot_ev, h->stream), "event");
+  h->tot_pending = true;
   return 0;
 }
 
@@ -667,7 +712,7 @@ int mass_lb_step(mass_lb_handle* h, unsigned nsteps)
   return 0;
 }
 
-static int get_primary(mass_lb_handle* h, int field, double* out)
+static int get_primary(mass_lb_handle* h, int field, double* out, bool sync = true)
 {
   const int LY = static_cast<int>(h->LY);
   const long long rows_per = std::max<long long>(1, kStageSites/LY);
@@ -756,7 +801,7 @@ static int get_primary(mass_lb_handle* h, int field, double* out)
     CU(cudaMemcpyAsync(out + x0*LY*comps, h->stage, n*comps*sizeof(double),
                        cudaMemcpyDeviceToHost, h->stream), "download copy");
   }
-  CU(cudaStreamSynchronize(h->stream), "download sync");
+  if(sync) CU(cudaStreamSynchronize(h->stream), "download sync");
   return 0;
 }
 
@@ -791,10 +836,28 @@ int mass_lb_download(mass_lb_handle* h, int field, double* out)
   return get_primary(h, field, out);
 }
 
-int mass_lb_checks(mass_lb_handle* h, double* fsum, double* phisum, int* nonfinite)
+int mass_lb_download_async(mass_lb_handle* h, int field, double* out)
 {
-  if(!h) return fail(MASS_LB_EINVAL, "null handle");
+  if(!h || !out) return fail(MASS_LB_EINVAL, "null argument");
+  if(field != MASS_LB_FF && field != MASS_LB_QQXX && field != MASS_LB_QQYX &&
+     field != MASS_LB_PHI)
+    return fail(MASS_LB_EINVAL, "asynchronous downloads take ff, QQxx, QQyx or phi");
+  if(field == MASS_LB_PHI && h->model == NEM)
+    return fail(MASS_LB_EUNSUPPORTED, "field does not exist in the nematic model");
   DeviceGuard g(h->device);
+  if(!pinned_host(out))
+    return fail(MASS_LB_EINVAL, "asynchronous downloads take pinned host buffers");
+  return get_primary(h, field, out, false);
+}
+
+} // extern "C"
+
+namespace {
+
+// Sum of f and phi and the non-finite count into red_out (3 doubles), on
+// the handle's stream.
+cudaError_t launch_sums(mass_lb_handle* h)
+{
   cudaError_t e;
   if(h->fused)
   {
@@ -819,6 +882,40 @@ int mass_lb_checks(mass_lb_handle* h, double* fsum, double* phisum, int* nonfini
                      h->d.LX, h->d.LY, h->d.g, h->d.EY, h->P.rho};
     e = launch_sums_f32(v, h->red_scratch, h->red_out, h->stream);
   }
+  return e;
+}
+
+// ftot/ptot of an asynchronous upload, once its sums have landed
+int resolve_totals(mass_lb_handle* h)
+{
+  if(!h->tot_pending) return 0;
+  CU(cudaEventSynchronize(h->tot_ev), "totals");
+  h->ftot = h->tot_host[0];
+  h->ptot = h->tot_host[1];
+  h->tot_pending = false;
+  return 0;
+}
+
+bool pinned_host(const void* p)
+{
+  cudaPointerAttributes a{};
+  if(cudaPointerGetAttributes(&a, p) != cudaSuccess)
+  {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+} // namespace
+
+extern "C" {
+
+int mass_lb_checks(mass_lb_handle* h, double* fsum, double* phisum, int* nonfinite)
+{
+  if(!h) return fail(MASS_LB_EINVAL, "null handle");
+  DeviceGuard g(h->device);
+  const cudaError_t e = launch_sums(h);
   if(e != cudaSuccess) return cuda_fail(e, "sums");
   double r[3];
   CU(cudaMemcpyAsync(r, h->red_out, sizeof(r), cudaMemcpyDeviceToHost, h->stream), "sums copy");
@@ -834,6 +931,8 @@ int mass_lb_checks(mass_lb_handle* h, double* fsum, double* phisum, int* nonfini
 int mass_lb_initial_totals(mass_lb_handle* h, double* ftot, double* ptot)
 {
   if(!h) return fail(MASS_LB_EINVAL, "null handle");
+  DeviceGuard g(h->device);
+  if(int r = resolve_totals(h)) return r;
   if(ftot) *ftot = h->ftot;
   if(ptot) *ptot = h->ptot;
   return 0;
@@ -1060,6 +1159,10 @@ int mass_lb_save(mass_lb_handle* h, const char* path)
   hd.precision = h->precision;
   hd.LX = h->LX; hd.LY = h->LY; hd.bc = h->bc; hd.npc = h->P.npc;
   hd.steps = h->steps;
+  {
+    DeviceGuard g(h->device);
+    if(int r = resolve_totals(h)) return r;
+  }
   hd.ftot = h->ftot; hd.ptot = h->ptot;
   params_out(h->P, hd.params);
   hd.payload_doubles = buf.size();
@@ -1108,6 +1211,7 @@ int mass_lb_load(mass_lb_handle* h, const char* path)
   // continue the run the checkpoint came from: step count and the totals
   // the runtime checks compare against
   h->steps = hd.steps;
+  h->tot_pending = false;   // settled before the state was replaced
   h->ftot = hd.ftot;
   h->ptot = hd.ptot;
   return 0;

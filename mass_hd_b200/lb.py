@@ -136,6 +136,8 @@ def load_library(build_if_missing: bool = False):
         "mass_lb_get_mask": (C.c_int, [vp, C.c_int, C.POINTER(C.c_ubyte)]),
         "mass_lb_mask_supply": (C.c_int, [vp, dp, C.c_longlong]),
         "mass_lb_mask_staging": (C.c_int, [vp, C.c_longlong, C.POINTER(dp)]),
+        "mass_lb_upload_async": (C.c_int, [vp, dp, dp, dp, dp]),
+        "mass_lb_download_async": (C.c_int, [vp, C.c_int, dp]),
         "mass_lb_draw_masks_queued": (C.c_int, [vp, C.c_int] + [C.c_double] * 7),
         "mass_lb_mask_consumed": (C.c_int, [vp, C.POINTER(C.c_longlong)]),
         "mass_lb_mask_progress": (C.c_int, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_int)]),
@@ -259,6 +261,22 @@ class Lattice:
         out = np.empty(n, dtype=np.float64)
         _check(load_library().mass_lb_download(self.h, FIELD_ID[name], _dp(out)))
         return out.reshape(-1, 9) if name in ("ff", "fn") else out
+
+    def upload_async(self, ff, QQxx, QQyx, phi=None):
+        """mass_lb_upload_async: the arrays must be pinned, contiguous float64
+        and left untouched until synchronize()."""
+        arrs = [ff, QQxx, QQyx] + ([phi] if phi is not None else [])
+        for a in arrs:
+            assert a.dtype == np.float64 and a.flags.c_contiguous
+        _check(load_library().mass_lb_upload_async(self.h, _dp(ff), _dp(QQxx), _dp(QQyx),
+                                                   _dp(phi) if phi is not None else None))
+
+    def get_into_async(self, name: str, out: np.ndarray) -> np.ndarray:
+        """mass_lb_download_async into a pinned, contiguous float64 array;
+        valid after synchronize()."""
+        assert out.dtype == np.float64 and out.flags.c_contiguous
+        _check(load_library().mass_lb_download_async(self.h, FIELD_ID[name], _dp(out)))
+        return out
 
     def get_into(self, name: str, out: np.ndarray) -> np.ndarray:
         assert out.dtype == np.float64 and out.flags.c_contiguous

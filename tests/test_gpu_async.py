@@ -1,0 +1,64 @@
+"""Asynchronous transfers (mass_lb_upload_async / mass_lb_download_async):
+the same state, totals and results as the synchronous calls, ordered with
+the steps on the handle's stream, and pinned host buffers required."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.helpers import LYO_C1, NEM_C2, bits_equal
+
+pytestmark = pytest.mark.gpu
+
+import torch  # noqa: E402
+
+import mass_hd_b200 as M  # noqa: E402
+
+
+def pinned(a):
+    t = torch.empty(a.size, dtype=torch.float64, pin_memory=True)
+    out = t.numpy()
+    out[:] = a.reshape(-1)
+    return out, t
+
+
+@pytest.mark.parametrize("model,params,LX,LY,prec", [
+    (M.LYOTROPIC, LYO_C1, 64, 128, M.FP32),     # fused warp-strip kernel
+    (M.LYOTROPIC, LYO_C1, 48, 40, M.FP64),      # sub-step kernels
+    (M.NEMATIC, NEM_C2, 30, 66, M.FP32),        # unfused FP32
+])
+def test_async_transfers_equal_sync(model, params, LX, LY, prec):
+    st = O.synthetic_state(model, LX, LY, seed=5, flow=0.01)
+    names = ("ff", "QQxx", "QQyx", "phi") if model == M.LYOTROPIC else ("ff", "QQxx", "QQyx")
+    keep = []
+    host = {}
+    for k in names:
+        host[k], t = pinned(np.asarray(st[k], dtype=np.float64))
+        keep.append(t)
+    outs = {}
+    for k in names:
+        outs[k], t = pinned(np.zeros_like(host[k]))
+        keep.append(t)
+    a = M.Lattice(model, params, LX, LY, 0, prec)
+    b = M.Lattice(model, params, LX, LY, 0, prec)
+    a.upload(host["ff"], host["QQxx"], host["QQyx"], host.get("phi"))
+    a.step(3)
+    # two jobs back to back on b's stream, no wait in between
+    for _ in range(2):
+        b.upload_async(host["ff"], host["QQxx"], host["QQyx"], host.get("phi"))
+        b.step(3)
+        for k in names:
+            b.get_into_async(k, outs[k])
+    b.synchronize()
+    for k in names:
+        assert bits_equal(outs[k].reshape(a.get(k).shape), a.get(k)), k
+    assert a.initial_totals() == b.initial_totals()
+    # pageable buffers are refused
+    with pytest.raises(M.MassLBError):
+        b.get_into_async("QQxx", np.zeros(LX * LY))
+    with pytest.raises(M.MassLBError):
+        b.upload_async(np.asarray(st["ff"], dtype=np.float64).reshape(-1), host["QQxx"],
+                       host["QQyx"], host.get("phi"))
+    with pytest.raises(M.MassLBError):
+        b.get_into_async("sigmaXX", outs["QQxx"])
+    a.close()
+    b.close()
