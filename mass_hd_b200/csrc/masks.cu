@@ -17,6 +17,8 @@
 //     reference's minimum-image test of every site against every centre),
 //  5. rate_kernel forms alpha*division_mask - beta*death_mask in the
 //     source plane the step kernels read.
+// A draw from uniforms queued on the device ahead of need
+// (queued_draw_kernel) does the same in one cooperative launch.
 // Compiled with --fmad=false: the thresholds are rounded as the reference
 // rounds them.
 #include "masks.cuh"
@@ -111,50 +113,6 @@ center_kernel(MaskView<T> v, const long long* __restrict__ off, const double* __
   center[k] = c;
 }
 
-// The same centre test with the uniforms taken from a queue on the device:
-// the draws of this mask start `kslot` candidate counts past the queue head
-// (division first, then death, as the reference draws them). A draw past
-// what the caller has supplied sets *err and makes no centre.
-template<typename T>
-__global__ void __launch_bounds__(MB)
-center_queue_kernel(MaskView<T> v, const long long* __restrict__ off,
-                    const double* __restrict__ queue, long long qcap,
-                    const long long* __restrict__ head, const long long* __restrict__ total,
-                    int kslot, long long supplied, double coef, double phi_critical,
-                    int division, unsigned char* __restrict__ center, int* err)
-{
-  __shared__ int warp_cnt[MB/32];
-  const long long N = static_cast<long long>(v.LX)*v.LY;
-  const long long k = static_cast<long long>(blockIdx.x)*MB + threadIdx.x;
-  const double p = k < N ? phi_at(v, k) : 0.;
-  const bool flag = k < N && p >= .5;
-  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  const unsigned ballot = __ballot_sync(0xffffffffu, flag);
-  if(lane == 0) warp_cnt[warp] = __popc(ballot);
-  __syncthreads();
-  int before = 0;
-  for(unsigned w = 0; w < warp; ++w) before += warp_cnt[w];
-  before += __popc(ballot & ((1u << lane) - 1u));
-  if(k >= N) return;
-  unsigned char c = 0;
-  if(flag)
-  {
-    const long long idx = *head + kslot*(*total) + off[blockIdx.x] + before;
-    if(idx < supplied)
-    {
-      const double thr = division ? coef*p*(1 - p/phi_critical) : coef*p;
-      c = queue[idx % qcap] < thr;
-    }
-    else atomicOr(err, 1);
-  }
-  center[k] = c;
-}
-
-__global__ void advance_head_kernel(long long* head, const long long* total, int nkinds)
-{
-  if(blockIdx.x == 0 && threadIdx.x == 0) *head += nkinds*(*total);
-}
-
 __global__ void stamp_kernel(int LX, int LY, const unsigned char* __restrict__ center,
                              unsigned char* __restrict__ mask, double r2, int R)
 {
@@ -218,7 +176,7 @@ __device__ __forceinline__ void stamp_circle_warp(int LX, int LY, long long k,
 //  2. every block forms the exclusive chunk offsets it needs and the total
 //     from all chunk counts (as scan_kernel), then the centres of its
 //     chunks: a candidate's draw for kind j is the queue entry
-//     head + slot_j*total + rank (division first), as center_queue_kernel,
+//     head + slot_j*total + rank (division first),
 //     and a centre writes its circle into the mask of its kind (as
 //     stamp_kernel),
 //  3. the source plane alpha*division - beta*death (as rate_kernel) and
@@ -410,35 +368,6 @@ cudaError_t mask_draw(const MaskView<T>& v, const MaskScratch& s, int kind, long
 }
 
 template<typename T>
-cudaError_t mask_draw_queued(const MaskView<T>& v, const MaskScratch& s, const MaskQueue& q,
-                             int kind, int kslot, double coef, double phi_critical, double radius,
-                             int* err, cudaStream_t st)
-{
-  const long long N = static_cast<long long>(v.LX)*v.LY;
-  const int nb = mask_blocks(N);
-  center_queue_kernel<T><<<nb, MB, 0, st>>>(v, s.block_off, q.buf, q.cap, q.head, s.total, kslot,
-                                            q.supplied, coef, phi_critical, kind == 0 ? 1 : 0,
-                                            s.center, err);
-  unsigned char* mask = s.mask[kind];
-  cudaError_t e = cudaMemsetAsync(mask, 0, N, st);
-  if(e != cudaSuccess) return e;
-  const double r2 = std::ceil(radius*radius);
-  if(r2 >= 0)
-  {
-    const int R = static_cast<int>(std::floor(std::sqrt(r2)));
-    stamp_kernel<<<grid_for(N), 256, 0, st>>>(v.LX, v.LY, s.center, mask, r2, R);
-  }
-  return cudaGetLastError();
-}
-
-cudaError_t mask_queue_advance(const MaskScratch& s, const MaskQueue& q, int nkinds,
-                               cudaStream_t st)
-{
-  advance_head_kernel<<<1, 32, 0, st>>>(q.head, s.total, nkinds);
-  return cudaGetLastError();
-}
-
-template<typename T>
 cudaError_t mask_rate(int LX, int LY, int g, int EY, const MaskScratch& s, double alpha,
                       double beta, T* src, cudaStream_t st)
 {
@@ -494,12 +423,6 @@ template cudaError_t mask_draw<double>(const MaskView<double>&, const MaskScratc
                                        double, double, double, cudaStream_t);
 template cudaError_t mask_draw<float>(const MaskView<float>&, const MaskScratch&, int, long long,
                                       double, double, double, cudaStream_t);
-template cudaError_t mask_draw_queued<double>(const MaskView<double>&, const MaskScratch&,
-                                              const MaskQueue&, int, int, double, double, double,
-                                              int*, cudaStream_t);
-template cudaError_t mask_draw_queued<float>(const MaskView<float>&, const MaskScratch&,
-                                             const MaskQueue&, int, int, double, double, double,
-                                             int*, cudaStream_t);
 template cudaError_t mask_rate<double>(int, int, int, int, const MaskScratch&, double, double,
                                        double*, cudaStream_t);
 template cudaError_t mask_rate<float>(int, int, int, int, const MaskScratch&, double, double,

@@ -58,15 +58,6 @@ cudaError_t mask_count(const MaskView<T>& v, const MaskScratch& s, cudaStream_t 
 template<typename T>
 cudaError_t mask_draw(const MaskView<T>& v, const MaskScratch& s, int kind, long long ndraws,
                       double coef, double phi_critical, double radius, cudaStream_t st);
-// centre test and circles of one mask (kind 0 division, 1 death) from the
-// queue, its draws starting kslot candidate counts past the head
-template<typename T>
-cudaError_t mask_draw_queued(const MaskView<T>& v, const MaskScratch& s, const MaskQueue& q,
-                             int kind, int kslot, double coef, double phi_critical, double radius,
-                             int* err, cudaStream_t st);
-// head += nkinds * candidates, after the masks of one draw
-cudaError_t mask_queue_advance(const MaskScratch& s, const MaskQueue& q, int nkinds,
-                               cudaStream_t st);
 // A whole queued draw in one cooperative launch: count, offsets, centres of
 // both kinds, circles, source plane and head advance, with grid barriers
 // between the phases.
