@@ -256,3 +256,41 @@ def test_go_or_grow_rejections():
         g32.get("mN")
     for x in (lyo, g32):
         x.close()
+
+
+@pytest.mark.parametrize("change", ["relax", "params", "load"])
+def test_go_or_grow_derived_fields_survive_state_changes(change, tmp_path):
+    """On a periodic lattice the step leaves its derived fields (u, H, mu,
+    the stresses) to be recomputed on demand. A relaxation, new phenotype
+    parameters or a checkpoint load in between do not change them: they
+    stay those of the step, as on a lattice that downloaded them first (the
+    relaxation leaves its own H and mu, as it always has), and a loaded
+    state is the saved one."""
+    p = params()
+    ref = O.RefOracle(O.GO_OR_GROW, p, 40, 36, 0)
+    ref.configure(5)
+    st = {n: ref.get(n) for n in STATE}
+    rate = np.where(st["phi"] > 0.5, 0.002, 0.0)
+    a = M.Lattice(M.GO_OR_GROW, p, 40, 36, 0, M.FP64)
+    b = M.Lattice(M.GO_OR_GROW, p, 40, 36, 0, M.FP64)
+    path = os.path.join(tmp_path, "gog.ckpt")
+    for x in (a, b):
+        x.upload_state(st)
+        x.set_phi_source(rate)
+        x.step(4)
+    b.save(path)
+    want = {n: a.get(n) for n in DERIVED if n != "chi"}
+    if change == "relax":
+        b.relax_free_energy(5, 1.0, True, True)
+        for n in ("HHxx", "HHyx", "MU"):
+            del want[n]
+    elif change == "params":
+        b.set_go_or_grow_params(params(B=0.5, Snem=0.8, **{"phi-critical": 0.7}))
+    else:
+        b.step(3)
+        b.load(path)
+        want = {n: a.get(n) for n in ("ff", "QQxx", "phi", "m")}
+    for n, v in want.items():
+        assert bits_equal(b.get(n), v), n
+    a.close()
+    b.close()
