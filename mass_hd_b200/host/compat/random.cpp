@@ -10,7 +10,7 @@ namespace {
 
 // The block loops below are built twice, for AVX2 and for the baseline
 // x86-64 vector unit, and the loader picks the one the CPU runs.
-#if defined(__x86_64__) && defined(__GNUC__) && defined(__ELF__)
+#if defined(__x86_64__) && defined(__GNUC__) && defined(__ELF__) && !defined(MASS_GPU_NO_CLONES)
 #define MT_CLONES __attribute__((target_clones("avx2", "default"), noinline))
 #else
 #define MT_CLONES

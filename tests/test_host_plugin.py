@@ -55,11 +55,15 @@ def test_bulk_number_format_equals_stringstream(tmp_path):
     assert out.split()[-1] == "0", out
 
 
-def test_compat_generator_equals_std_mt19937(tmp_path):
+@pytest.mark.parametrize("clones", [True, False])
+def test_compat_generator_equals_std_mt19937(tmp_path, clones):
     """The standalone build's own Mersenne Twister (block-wise, vectorised)
     and its bulk random_reals give exactly the standard library's
-    std::mt19937 / uniform_real_distribution / normal_distribution values."""
-    exe = compile_native(tmp_path, "random_check.cpp", [os.path.join(COMPAT, "random.cpp")])
+    std::mt19937 / uniform_real_distribution / normal_distribution values,
+    in the build whose loader picks the AVX2 block loops where the CPU has
+    them and in the baseline-only build."""
+    extra = [os.path.join(COMPAT, "random.cpp")] + ([] if clones else ["-DMASS_GPU_NO_CLONES"])
+    exe = compile_native(tmp_path, "random_check.cpp", extra)
     out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout
     assert out.split()[0] == "0", out
 
