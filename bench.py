@@ -24,6 +24,10 @@ With --gpus N (torchrun), every rank advances its own lattice of the same
 size (independent runs, weak scaling, no collective on the data path); time
 is the max over ranks.
 
+The line also carries `fp64`: the FP64 mode (bit-identical to the
+reference's double-precision build) timed on the same seeded lattice, the
+like-for-like counterpart of the reference's FP64 CPU build.
+
 --impl reference times the reference's own OpenMP build of the same step
 (oracle/_ref, compiled from the reference sources) on the host cores, on a
 bounded sample of the same workload.
@@ -488,6 +492,48 @@ def run_ours_gog(args):
     return 0
 
 
+def fp64_record(model: str, st: dict, L: int, steps: int, warmup: int, world: int) -> dict:
+    """The FP64 mode (the reference's double-precision arithmetic, bit for
+    bit) on the same seeded workload: device time per step with CUDA events
+    on the library's stream, max over ranks, and its roofline against the
+    FP64 state's algorithmic bytes. It is the like-for-like counterpart of
+    the reference's FP64 OpenMP build."""
+    import torch
+
+    import mass_hd_b200 as M
+    mcode = M.LYOTROPIC if model == "lyotropic" else M.NEMATIC
+    params = LYO_C1 if model == "lyotropic" else NEM_C2
+    lat = M.Lattice(mcode, params, L, L, 0, M.FP64)
+    lat.upload_state(st)
+    stream = torch.cuda.ExternalStream(lat.stream)
+    for _ in range(max(warmup, 3)):
+        lat.step(1)
+    lat.synchronize()
+    barrier(world)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        lat.step(1)
+    e1.record(stream)
+    e1.synchronize()
+    lat.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    launches = steps * lat.launches_per_step
+    lat.close()
+    ms_per_step = ms / steps
+    bps = algorithmic_bytes(model, "fp64")
+    peak, peak_kind = measured_hbm_peak()
+    achieved = L * L * bps / (ms_per_step / 1e3) / 1e9
+    return {"value": whole_job_rate(L * L, world, steps, ms), "unit": UNIT,
+            "ms_per_step": ms_per_step, "steps": steps, "dtype": "f64", "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "bytes_per_site": bps},
+            "note": "FP64 mode (bit-identical to the reference's double-precision build) on "
+                    "the same seeded lattice: one sub-step kernel per predictor and corrector"}
+
+
 def run_ours(args):
     import torch
 
@@ -626,6 +672,10 @@ def run_ours(args):
                    "clock"}
     launches_e2e = n_pipe * NINFO * lat.launches_per_step
 
+    fp64 = None
+    if args.precision == "fp32" and not args.no_fp64:
+        fp64 = fp64_record(model, st, L, min(args.steps, 20), 3, world)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, kind, cores, sample = cpu_reference_run(model, L, 5, 1, 20.0)
@@ -651,6 +701,7 @@ def run_ours(args):
             "roofline": roofline,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "fp64": fp64,
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
@@ -672,6 +723,8 @@ def main():
     ap.add_argument("--model", default="lyotropic", choices=["lyotropic", "nematic", "go-or-grow"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true",
+                    help="skip the FP64-mode record beside the FP32 line")
     args = ap.parse_args()
     if args.size is None:
         args.size = 500 if args.model == "go-or-grow" else 4096

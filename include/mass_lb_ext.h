@@ -77,9 +77,14 @@ int mass_lb_statistics(mass_lb_handle* h, mass_lb_stats* out);
  * planes: nplanes (12 lyotropic, 11 nematic) float planes, plane_stride
  * apart, in the fused layout (g0..g8 as deviations from t_v*rho, Qxx, Qyx,
  * phi); rho: the rest density. Lattices above 67,108,864 sites (8192^2) are
- * rejected with MASS_LB_EINVAL. The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress) for that device; make that
- * first call before any stream capture. The array is shared by all calls and
+ * rejected with MASS_LB_EINVAL. The device that holds `planes` must be the
+ * current device and `stream` must belong to it (a handle's planes live on
+ * the device it was created on); otherwise the call returns MASS_LB_EINVAL
+ * without launching. The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) for that device; make that first call
+ * before any stream capture. The looked-up address is kept for the life of
+ * the device's context: after a cudaDeviceReset the library, this call
+ * included, is not to be used on that device again. The array is shared by all calls and
  * keeps the last call's contents (every call writes all it reads, so
  * nothing needs clearing); calls that overlap on the GPU race on it. Runs on
  * `stream` (a cudaStream_t, NULL = default stream) and returns after the
@@ -100,7 +105,13 @@ int mass_lb_state_sums_noalloc(const float* planes, long long plane_stride, int 
  * (mass_lb_initial_totals) are computed on the stream too and read when
  * first asked for.
  *
- * mass_lb_download_async: mass_lb_download of ff, QQxx, QQyx or phi. */
+ * mass_lb_download_async: mass_lb_download of ff, QQxx, QQyx or phi.
+ *
+ * End every asynchronous pipeline with mass_lb_synchronize, not with a wait
+ * on the stream of one's own: it is the call that reads the fused kernel's
+ * device error word (a copy wait that timed out inside a step) and turns it
+ * into MASS_LB_ECUDA. A pipeline that only synchronizes the stream could
+ * read a result that such a step left incomplete. */
 int mass_lb_upload_async(mass_lb_handle* h, const double* ff, const double* QQxx,
                          const double* QQyx, const double* phi);
 int mass_lb_download_async(mass_lb_handle* h, int field, double* out);

@@ -1711,6 +1711,9 @@ int mass_lb_relax_free_energy(mass_lb_handle* h, unsigned steps, double dt, int 
   if(h->model != GOG) return fail(MASS_LB_EUNSUPPORTED, "not a go-or-grow lattice");
   DeviceGuard g(h->device);
   if(int r = settle_derived(h)) return r;
+  // an earlier asynchronous upload's totals land first, so that they cannot
+  // later overwrite the relaxed phi total assigned below
+  if(int r = resolve_totals(h)) return r;
   if(!h->relaxsum)
     if(int r = dalloc(h, &h->relaxsum, 1)) return r;
   const int bc = h->wall ? static_cast<int>(h->bc) : 0;

@@ -156,15 +156,16 @@ noalloc_pass2(double* __restrict__ scratch, int nblocks)
 std::mutex g_noalloc_mu;
 double* g_noalloc_ptr[64] = {};   // device address of the array, per device
 
-// Set-up on the current device, once: the array's name in host code is a
-// host-side stand-in, not a device address, so the kernels get the address
-// that cudaGetSymbolAddress returns for this device.
-cudaError_t scratch_on_current_device(double** out)
+// Set-up on device `dev` (the current device), once: the array's name in
+// host code is a host-side stand-in, not a device address, so the kernels
+// get the address that cudaGetSymbolAddress returns for this device. The
+// cached address lives as long as the device's context: a cudaDeviceReset
+// ends the library's use of that device altogether (its handles' buffers
+// are gone too).
+cudaError_t scratch_on_current_device(int dev, double** out)
 {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if(e != cudaSuccess) return e;
   if(dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  cudaError_t e = cudaSuccess;
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
   if(!g_noalloc_ptr[dev])
   {
@@ -200,8 +201,37 @@ extern "C" int mass_lb_state_sums_noalloc(const float* planes, long long plane_s
                    "lattice of " + std::to_string(nsites) + " sites exceeds the " +
                    std::to_string(NA_MAX_SITES) + "-site limit of the static scratch");
   if(plane_stride < nsites) return na_fail(MASS_LB_EINVAL, "plane stride below LX*LY");
+  // The kernels run on the current device and use that device's copy of the
+  // array, so the planes and the stream must belong to it: a mismatch would
+  // make the kernels read another GPU's memory or fail to launch.
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if(e != cudaSuccess)
+    return na_fail(MASS_LB_ECUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+  cudaPointerAttributes pa{};
+  e = cudaPointerGetAttributes(&pa, planes);
+  if(e != cudaSuccess || pa.type != cudaMemoryTypeDevice)
+  {
+    cudaGetLastError();
+    return na_fail(MASS_LB_EINVAL, "planes are not device memory");
+  }
+  if(pa.device != dev)
+    return na_fail(MASS_LB_EINVAL,
+                   "planes live on device " + std::to_string(pa.device) + " but device " +
+                   std::to_string(dev) + " is current; make the planes' device current");
+  if(stream)
+  {
+    int sdev = -1;
+    e = cudaStreamGetDevice(static_cast<cudaStream_t>(stream), &sdev);
+    if(e != cudaSuccess)
+      return na_fail(MASS_LB_ECUDA, std::string("cudaStreamGetDevice: ") + cudaGetErrorString(e));
+    if(sdev != dev)
+      return na_fail(MASS_LB_EINVAL,
+                     "stream belongs to device " + std::to_string(sdev) + " but device " +
+                     std::to_string(dev) + " is current");
+  }
   double* scratch = nullptr;
-  cudaError_t e = scratch_on_current_device(&scratch);
+  e = scratch_on_current_device(dev, &scratch);
   if(e != cudaSuccess)
     return na_fail(MASS_LB_ECUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
   cudaStream_t st = static_cast<cudaStream_t>(stream);

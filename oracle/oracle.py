@@ -19,6 +19,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_SO = os.path.join(HERE, "_build", "libmass_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libmass_ref.so")
+# The reference checkout read by the oracle recipes and the fixture scripts:
+# MASS_REFERENCE_DIR when set, else the same default oracle/Makefile uses.
+REF_DIR = os.environ.get("MASS_REFERENCE_DIR") or "/root/reference"
 
 LYOTROPIC, NEMATIC, GO_OR_GROW = 0, 1, 2
 

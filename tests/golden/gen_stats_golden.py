@@ -29,10 +29,11 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = "/root/reference"
 sys.path.insert(0, ROOT)
 
 from oracle import oracle as O  # noqa: E402
+
+REF = O.REF_DIR
 
 
 def load_massPy():

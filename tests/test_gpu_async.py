@@ -62,3 +62,41 @@ def test_async_transfers_equal_sync(model, params, LX, LY, prec):
         b.get_into_async("sigmaXX", outs["QQxx"])
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("prec", [M.FP64, M.FP32])
+def test_async_go_or_grow_with_relaxation(prec):
+    """Go-or-grow: uploading phi through mass_lb_upload_async also refreshes
+    chi on the device. An asynchronous upload followed by a step and a dry
+    relaxation must leave the relaxed phi total as the reference total (the
+    upload's own sums, still in flight when the relaxation starts, must not
+    overwrite it later), and every field equal to the synchronous path."""
+    from tests.test_gpu_go_or_grow import GOG
+
+    LX, LY = 40, 36
+    ref = O.RefOracle(O.GO_OR_GROW, GOG, LX, LY, 0)
+    ref.configure(9)
+    names = ("ff", "QQxx", "QQyx", "phi")
+    keep, host = [], {}
+    for k in names:
+        host[k], t = pinned(np.asarray(ref.get(k), dtype=np.float64))
+        keep.append(t)
+    m = np.asarray(ref.get("m"), dtype=np.float64)
+    a = M.Lattice(M.GO_OR_GROW, GOG, LX, LY, 0, prec)
+    b = M.Lattice(M.GO_OR_GROW, GOG, LX, LY, 0, prec)
+    a.upload(host["ff"], host["QQxx"], host["QQyx"], host["phi"])
+    a.upload_field("m", m)
+    a.step(2)
+    ta = a.relax_free_energy(5, 0.8, True, True)
+    b.upload_async(host["ff"], host["QQxx"], host["QQyx"], host["phi"])
+    b.upload_field("m", m)
+    b.step(2)
+    tb = b.relax_free_energy(5, 0.8, True, True)
+    b.synchronize()
+    assert ta == tb
+    assert a.initial_totals() == b.initial_totals()
+    assert b.initial_totals()[1] == tb
+    for k in names + ("m", "chi"):
+        assert bits_equal(a.get(k), b.get(k)), k
+    a.close()
+    b.close()

@@ -1,7 +1,12 @@
 """mass_lb_statistics on the GPU: the reference's post-processing estimators
 (defect counts, <|u|^2>, enstrophy, phi-interface length) on the device,
 against values produced by the reference's own Python code; and FP32 vs
-FP64 agreement of window-averaged statistics in active turbulence."""
+FP64 agreement of window-averaged statistics in active turbulence, gated at
+2% on the nematic 2048^2 active-turbulence configuration (window steps
+2000-5000) and on a lyotropic 1024^2 run with the phi-interface length.
+
+MASS_LB_STATS_OUT=<dir> makes the gated comparisons write their JSON
+results there (the per-field errors and window means quoted in the docs)."""
 import glob
 import json
 import os
@@ -66,10 +71,44 @@ def test_statistics_match_restatement_on_walls():
         assert got[k] == pytest.approx(want[k], rel=1e-10), k
 
 
-def test_fp32_vs_fp64_window_statistics_active_turbulence():
-    r = CP.compare("nematic", 512, field_steps=100, steps=2500, window=1000, every=50)
+def _report(name, r):
+    out = os.environ.get("MASS_LB_STATS_OUT")
+    if out:
+        os.makedirs(out, exist_ok=True)
+        with open(os.path.join(out, name + ".json"), "w") as fh:
+            json.dump(r, fh, indent=1)
+
+
+# Active turbulence is chaotic, so runs longer than a few hundred steps are
+# compared through window means of the statistics, each within 2% of the
+# FP64 (oracle-mode) run started from the same seeded state.
+STAT_BOUND = 0.02
+
+
+def test_fp32_vs_fp64_nematic_2048_window_2000_5000():
+    """Nematic 2048^2, zeta = 0.02: per-field error after 100 steps, then
+    defect density, <|u|^2> and enstrophy averaged over steps 2000-5000,
+    sampled every 100 steps."""
+    r = CP.compare("nematic", 2048, field_steps=100, steps=5000, window=2000, every=100)
+    _report("nematic_2048", r)
+    print(json.dumps(r))
+    assert r["window"]["samples"] == 31
+    for n, e in r["field_rel_l2"].items():
+        assert e < 1e-4, (n, e)
+    for k in ("defect_density", "mean_u2", "enstrophy_density"):
+        assert r["window"]["means"][k]["rel_diff"] < STAT_BOUND, (k, r["window"]["means"][k])
+    # the run is in the turbulent regime the statistics are meant for
+    assert r["window"]["means"]["defect_density"]["fp64"] > 1e-4
+
+
+def test_fp32_vs_fp64_lyotropic_1024_with_interface():
+    """Lyotropic 1024^2 (tanh phi disk of radius 256): per-field error after
+    100 steps, then defect density, <|u|^2>, enstrophy and the phi-interface
+    length averaged over steps 1000-3000, sampled every 50 steps."""
+    r = CP.compare("lyotropic", 1024, field_steps=100, steps=3000, window=1000, every=50)
+    _report("lyotropic_1024", r)
     print(json.dumps(r))
     for n, e in r["field_rel_l2"].items():
-        assert e < 1e-3, (n, e)
-    for k in ("defect_density", "mean_u2", "enstrophy_density"):
-        assert r["window"]["means"][k]["rel_diff"] < 0.05, (k, r["window"]["means"][k])
+        assert e < 1e-4, (n, e)
+    for k in ("defect_density", "mean_u2", "enstrophy_density", "perimeter"):
+        assert r["window"]["means"][k]["rel_diff"] < STAT_BOUND, (k, r["window"]["means"][k])

@@ -12,12 +12,14 @@ import sys
 import numpy as np
 import pytest
 
+from oracle import oracle as O
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HOST = os.path.join(ROOT, "mass_hd_b200", "host")
 COMPAT = os.path.join(HOST, "compat")
 NATIVE = os.path.join(ROOT, "tests", "native")
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-REF = "/root/reference"
+REF = O.REF_DIR
 DRIVER = os.path.join(HOST, "_build", "mass-gpu")
 
 LYO_FIELDS = ["ff", "QQxx", "QQyx", "phi", "sigmaXX", "sigmaXY", "sigmaYX", "sigmaYY",

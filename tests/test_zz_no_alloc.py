@@ -91,3 +91,15 @@ def test_noalloc_rejects_lattices_above_the_limit():
     assert r == -1
     assert b"limit of the static scratch" in M.load_library().mass_lb_last_error()
     lat.close()
+
+
+def test_noalloc_rejects_host_planes():
+    """Planes that are not device memory of the current device are refused
+    before any launch."""
+    f = noalloc_fn()
+    host = np.zeros(12 * 64 * 64, dtype=np.float32)
+    fs, ps, bad = C.c_double(), C.c_double(), C.c_int()
+    r = f(host.ctypes.data, 64 * 64, 12, 64, 64, 40.0, None, C.byref(fs), C.byref(ps),
+          C.byref(bad))
+    assert r == -1
+    assert b"not device memory" in M.load_library().mass_lb_last_error()
