@@ -116,6 +116,35 @@ int mass_lb_upload_async(mass_lb_handle* h, const double* ff, const double* QQxx
                          const double* QQyx, const double* phi);
 int mass_lb_download_async(mass_lb_handle* h, int field, double* out);
 
+/* ---- rows of the primary state: domain decomposition ------------------------
+ * The reference runs one lattice in one process (its only mention of MPI is
+ * a comment, src/models.hpp:15); these calls have no counterpart there.
+ * They let a caller split one periodic lattice into x-slabs, one per GPU:
+ * each GPU holds its rows plus 4 halo rows on each side as an ordinary
+ * periodic lattice of (rows + 8) x LY sites, and before every step the
+ * halo rows are refreshed from the neighbouring slabs. One Step() reaches
+ * 4 rows in x (predictor UpdateQuantities, predictor UpdateFields with
+ * Move, corrector UpdateQuantities, corrector UpdateFields), so the owned
+ * rows then advance exactly as in the whole lattice, bit for bit.
+ *
+ * mass_lb_rows_layout: planes per site (12 lyotropic: 9 populations, Qxx,
+ *   Qyx, phi; 11 nematic) and bytes per value (4 in FP32, where the
+ *   populations are stored as deviations from t_v*rho; 8 in FP64).
+ * mass_lb_get_rows / mass_lb_put_rows: rows [x0, x0 + nrows) of every
+ *   primary plane to / from a DEVICE buffer of the handle's device laid out
+ *   [plane][row][y] in that storage format (nplanes * nrows * LY values),
+ *   ordered on the handle's stream, no host wait. put_rows replaces state:
+ *   it first settles the derived fields the last step left pending.
+ *   Lyotropic and nematic periodic lattices (MASS_LB_EUNSUPPORTED
+ *   otherwise).
+ * mass_lb_checks_rows: mass_lb_checks over rows [x0, x0 + nrows) only (the
+ *   owned rows of a slab), for a sum over slabs. Synchronous. */
+int mass_lb_rows_layout(mass_lb_handle* h, int* nplanes, int* elem_bytes);
+int mass_lb_get_rows(mass_lb_handle* h, unsigned x0, unsigned nrows, void* dst);
+int mass_lb_put_rows(mass_lb_handle* h, unsigned x0, unsigned nrows, const void* src);
+int mass_lb_checks_rows(mass_lb_handle* h, unsigned x0, unsigned nrows, double* fsum,
+                        double* phisum, int* nonfinite);
+
 /* ---- checkpoints ------------------------------------------------------------
  *
  * Full-precision binary checkpoint of a lattice, filling the role of the

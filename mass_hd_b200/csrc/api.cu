@@ -907,6 +907,66 @@ bool pinned_host(const void* p)
   return a.type == cudaMemoryTypeHost;
 }
 
+// ---- rows of the primary state (domain decomposition) ---------------------
+
+// Base pointer and plane geometry of primary plane q (0..8 populations, 9
+// Qxx, 10 Qyx, 11 phi) in the handle's own storage: element pointer of row
+// 0, column 0, and the row pitch in elements.
+template<typename T>
+T* primary_plane(mass_lb_handle* h, State<T>& s, int q, long long* pitch)
+{
+  *pitch = h->d.EY;
+  const long long off = static_cast<long long>(h->d.EY)*h->d.g + h->d.g;
+  T* base = q < 9 ? s.ff + q*h->d.NE : q == 9 ? s.Qxx : q == 10 ? s.Qyx : s.phi;
+  return base + off;
+}
+
+// Copies rows [x0, x0+nrows) of every primary plane between the handle's
+// state and a packed device buffer laid out [plane][row][y]. `to_rows`
+// selects the direction (packed -> state). The handle's stream orders it.
+int copy_rows(mass_lb_handle* h, unsigned x0, unsigned nrows, void* packed, bool to_rows)
+{
+  if(!h || !packed) return fail(MASS_LB_EINVAL, "null argument");
+  if(h->model == GOG)
+    return fail(MASS_LB_EUNSUPPORTED, "row transfers cover the lyotropic and nematic models");
+  if(h->wall) return fail(MASS_LB_EUNSUPPORTED, "row transfers need a periodic lattice");
+  if(nrows == 0 || x0 >= h->LX || nrows > h->LX - x0)
+    return fail(MASS_LB_EINVAL, "row range outside the lattice");
+  DeviceGuard g(h->device);
+  if(to_rows)
+    if(int r = settle_derived(h)) return r;
+  const int NP = nplanes(h);
+  const size_t LY = h->LY;
+  if(h->fused)
+  {
+    // planes of LX*LY floats: the rows of a plane are contiguous
+    const size_t width = nrows*LY*sizeof(float);
+    const size_t plane_b = static_cast<size_t>(h->LX)*LY*sizeof(float);
+    char* st = reinterpret_cast<char*>(h->cur) + static_cast<size_t>(x0)*LY*sizeof(float);
+    const cudaError_t e = to_rows
+      ? cudaMemcpy2DAsync(st, plane_b, packed, width, width, NP, cudaMemcpyDeviceToDevice, h->stream)
+      : cudaMemcpy2DAsync(packed, width, st, plane_b, width, NP, cudaMemcpyDeviceToDevice, h->stream);
+    CU(e, "row copy");
+    if(to_rows) h->has_prev = false;
+    return 0;
+  }
+  const size_t es = h->precision == MASS_LB_FP64 ? sizeof(double) : sizeof(float);
+  for(int q = 0; q < NP; ++q)
+  {
+    long long pitch = 0;
+    char* st = h->precision == MASS_LB_FP64
+      ? reinterpret_cast<char*>(primary_plane(h, h->s64, q, &pitch))
+      : reinterpret_cast<char*>(primary_plane(h, h->s32, q, &pitch));
+    st += static_cast<size_t>(x0)*pitch*es;
+    char* pk = static_cast<char*>(packed) + static_cast<size_t>(q)*nrows*LY*es;
+    const cudaError_t e = to_rows
+      ? cudaMemcpy2DAsync(st, pitch*es, pk, LY*es, LY*es, nrows, cudaMemcpyDeviceToDevice, h->stream)
+      : cudaMemcpy2DAsync(pk, LY*es, st, pitch*es, LY*es, nrows, cudaMemcpyDeviceToDevice, h->stream);
+    CU(e, "row copy");
+  }
+  return 0;
+}
+
 } // namespace
 
 extern "C" {
@@ -916,6 +976,69 @@ int mass_lb_checks(mass_lb_handle* h, double* fsum, double* phisum, int* nonfini
   if(!h) return fail(MASS_LB_EINVAL, "null handle");
   DeviceGuard g(h->device);
   const cudaError_t e = launch_sums(h);
+  if(e != cudaSuccess) return cuda_fail(e, "sums");
+  double r[3];
+  CU(cudaMemcpyAsync(r, h->red_out, sizeof(r), cudaMemcpyDeviceToHost, h->stream), "sums copy");
+  CU(cudaStreamSynchronize(h->stream), "sums sync");
+  if(h->fused)
+    if(int rc = check_err_flag(h)) return rc;
+  if(fsum) *fsum = r[0];
+  if(phisum) *phisum = r[1];
+  if(nonfinite) *nonfinite = r[2] != 0.0 ? 1 : 0;
+  return 0;
+}
+
+int mass_lb_rows_layout(mass_lb_handle* h, int* nplanes_out, int* elem_bytes)
+{
+  if(!h) return fail(MASS_LB_EINVAL, "null handle");
+  if(nplanes_out) *nplanes_out = nplanes(h);
+  if(elem_bytes) *elem_bytes = h->precision == MASS_LB_FP64 ? 8 : 4;
+  return 0;
+}
+
+int mass_lb_get_rows(mass_lb_handle* h, unsigned x0, unsigned nrows, void* dst)
+{
+  return copy_rows(h, x0, nrows, dst, false);
+}
+
+int mass_lb_put_rows(mass_lb_handle* h, unsigned x0, unsigned nrows, const void* src)
+{
+  return copy_rows(h, x0, nrows, const_cast<void*>(src), true);
+}
+
+int mass_lb_checks_rows(mass_lb_handle* h, unsigned x0, unsigned nrows, double* fsum,
+                        double* phisum, int* nonfinite)
+{
+  if(!h) return fail(MASS_LB_EINVAL, "null handle");
+  if(nrows == 0 || x0 >= h->LX || nrows > h->LX - x0)
+    return fail(MASS_LB_EINVAL, "row range outside the lattice");
+  DeviceGuard g(h->device);
+  cudaError_t e;
+  if(h->fused)
+  {
+    const long long plane = static_cast<long long>(h->LX)*h->LY;
+    const float* b = h->cur + static_cast<long long>(x0)*h->LY;
+    SumView<float> v{b, b + 9*plane, b + 10*plane, h->model == LYO ? b + 11*plane : nullptr,
+                     plane, static_cast<int>(nrows), static_cast<int>(h->LY), 0,
+                     static_cast<int>(h->LY), h->P.rho};
+    e = launch_sums_f32(v, h->red_scratch, h->red_out, h->stream);
+  }
+  else if(h->precision == MASS_LB_FP64)
+  {
+    const State<double>& s = h->s64;
+    const long long o = static_cast<long long>(h->d.EY)*x0;
+    SumView<double> v{s.ff + o, s.Qxx + o, s.Qyx + o, h->model != NEM ? s.phi + o : nullptr,
+                      h->d.NE, static_cast<int>(nrows), h->d.LY, h->d.g, h->d.EY, 0.0};
+    e = launch_sums_f64(v, h->red_scratch, h->red_out, h->stream);
+  }
+  else
+  {
+    const State<float>& s = h->s32;
+    const long long o = static_cast<long long>(h->d.EY)*x0;
+    SumView<float> v{s.ff + o, s.Qxx + o, s.Qyx + o, h->model != NEM ? s.phi + o : nullptr,
+                     h->d.NE, static_cast<int>(nrows), h->d.LY, h->d.g, h->d.EY, h->P.rho};
+    e = launch_sums_f32(v, h->red_scratch, h->red_out, h->stream);
+  }
   if(e != cudaSuccess) return cuda_fail(e, "sums");
   double r[3];
   CU(cudaMemcpyAsync(r, h->red_out, sizeof(r), cudaMemcpyDeviceToHost, h->stream), "sums copy");

@@ -124,6 +124,10 @@ def load_library(build_if_missing: bool = False):
         "mass_lb_autotune": (C.c_int, [vp]),
         "mass_lb_uses_fused": (C.c_int, [vp]),
         "mass_lb_device_state": (C.c_int, [vp, C.POINTER(vp), C.POINTER(C.c_longlong), ip]),
+        "mass_lb_rows_layout": (C.c_int, [vp, ip, ip]),
+        "mass_lb_get_rows": (C.c_int, [vp, C.c_uint, C.c_uint, vp]),
+        "mass_lb_put_rows": (C.c_int, [vp, C.c_uint, C.c_uint, vp]),
+        "mass_lb_checks_rows": (C.c_int, [vp, C.c_uint, C.c_uint, dp, dp, ip]),
         "mass_lb_statistics": (C.c_int, [vp, C.POINTER(Stats)]),
         "mass_lb_save": (C.c_int, [vp, C.c_char_p]),
         "mass_lb_load": (C.c_int, [vp, C.c_char_p]),
@@ -445,6 +449,28 @@ class Lattice:
         p, stride, n = C.c_void_p(), C.c_longlong(), C.c_int()
         _check(load_library().mass_lb_device_state(self.h, C.byref(p), C.byref(stride), C.byref(n)))
         return p.value, stride.value, n.value
+
+    # -- rows of the primary state (domain decomposition) ---------------------
+    def rows_layout(self):
+        """(planes per site, bytes per value) of get_rows / put_rows."""
+        n, b = C.c_int(), C.c_int()
+        _check(load_library().mass_lb_rows_layout(self.h, C.byref(n), C.byref(b)))
+        return n.value, b.value
+
+    def get_rows(self, x0: int, nrows: int, dst_ptr: int):
+        """Rows [x0, x0+nrows) of every primary plane into the device buffer
+        at dst_ptr ([plane][row][y], storage format), on the lattice's
+        stream."""
+        _check(load_library().mass_lb_get_rows(self.h, x0, nrows, C.c_void_p(dst_ptr)))
+
+    def put_rows(self, x0: int, nrows: int, src_ptr: int):
+        _check(load_library().mass_lb_put_rows(self.h, x0, nrows, C.c_void_p(src_ptr)))
+
+    def checks_rows(self, x0: int, nrows: int):
+        f, p, bad = C.c_double(), C.c_double(), C.c_int()
+        _check(load_library().mass_lb_checks_rows(self.h, x0, nrows, C.byref(f), C.byref(p),
+                                                  C.byref(bad)))
+        return f.value, p.value, bool(bad.value)
 
 
 class Ensemble:
