@@ -24,8 +24,9 @@ enum { NDIAG = 23 };
 // kernel (read straight from the constant bank as 64-bit operands).
 struct PairParams
 {
-  float2 rho, GammaQ, GammaP, xi2, xi, tauIso, dtau, friction;
-  float2 AA, hAA, nCC, hCC, LL, nLL2, KK, hKK, nKK, zeta, zetaI, conc;
+  float2 rho, GammaQ, GammaP, xi2, hxi, tauIso, dtau, itau, n2fric;
+  float2 AA, hAA, nCC, hCC, c4k, LL, q4LL, nh2LL;
+  float2 nKK, KK8, nKK4, zeta, nzeta, zetaI, conc;
 };
 
 struct FusedArgs

@@ -86,13 +86,10 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 
 struct f2 { float2 v; };
 __device__ __forceinline__ f2 mk(float a, float b) { return f2{make_float2(a, b)}; }
-__device__ __forceinline__ f2 bc(float s) { return f2{make_float2(s, s)}; }
 __device__ __forceinline__ f2 operator+(f2 a, f2 b) { return f2{__fadd2_rn(a.v, b.v)}; }
 __device__ __forceinline__ f2 operator*(f2 a, f2 b) { return f2{__fmul2_rn(a.v, b.v)}; }
 __device__ __forceinline__ f2 fma(f2 a, f2 b, f2 c) { return f2{__ffma2_rn(a.v, b.v, c.v)}; }
 __device__ __forceinline__ f2 operator-(f2 a, f2 b) { return f2{__ffma2_rn(b.v, make_float2(-1.f, -1.f), a.v)}; }
-__device__ __forceinline__ f2 neg(f2 a) { return f2{__fmul2_rn(a.v, make_float2(-1.f, -1.f))}; }
-__device__ __forceinline__ f2 K(float c) { return bc(c); }
 // a literal pair: the compiler keeps these out of the registers the
 // parameter pairs would take
 #define KC(c) (f2{make_float2((c), (c))})
@@ -129,213 +126,254 @@ using PP = PairParams;
 __host__ PairParams make_pp(const P32& p, int model)
 {
   auto b = [](float x) { return make_float2(x, x); };
+  const bool lyo = model == LYO;
   PairParams q;
   q.rho = b(p.rho); q.GammaQ = b(p.GammaQ); q.GammaP = b(p.GammaP);
-  q.xi2 = b(2.f*p.xi); q.xi = b(p.xi);
-  q.tauIso = b(model == LYO ? p.tauIso : p.tauNem);
-  q.dtau = b(model == LYO ? p.tauNem - p.tauIso : 0.f);
-  q.friction = b(p.friction);
-  q.AA = b(p.AA); q.hAA = b(0.5f*p.AA);
-  q.nCC = b(-p.CC); q.hCC = b(0.5f*p.CC);
-  q.LL = b(p.LL); q.nLL2 = b(-2.f*p.LL);
-  q.KK = b(p.KK); q.hKK = b(0.5f*p.KK); q.nKK = b(-p.KK);
-  q.zeta = b(p.zeta); q.zetaI = b(p.zetaI); q.conc = b(p.conc);
+  q.xi2 = b(2.f*p.xi); q.hxi = b(.5f*p.xi);
+  // tau(phi) = tauIso + (tauNem - tauIso) phi (lyotropic), tau (nematic)
+  q.tauIso = b(lyo ? p.tauIso : p.tauNem);
+  q.dtau = b(lyo ? p.tauNem - p.tauIso : 0.f);
+  q.itau = b(1.f/(lyo ? p.tauIso : p.tauNem));
+  q.n2fric = b(-2.f*p.friction);
+  q.AA = b(p.AA); q.hAA = b(.5f*p.AA);
+  q.nCC = b(-p.CC); q.hCC = b(.5f*p.CC);
+  // CC*term - 4 LL = -CC*S2 + c4k
+  q.c4k = b(lyo ? -4.f*p.LL : p.CC - 4.f*p.LL);
+  q.LL = b(p.LL);
+  q.q4LL = b(.25f*p.LL); q.nh2LL = b(-.5f*p.LL);
+  q.nKK = b(-p.KK); q.KK8 = b(.125f*p.KK); q.nKK4 = b(-.25f*p.KK);
+  q.zeta = b(p.zeta); q.nzeta = b(-p.zeta); q.zetaI = b(p.zetaI); q.conc = b(p.conc);
   return q;
 }
 
-// UpdateQuantities outputs of one row pair.
-// x-neighbour set: ux, uy, sXX, sYX, uxp, MU; y-neighbour set: ux, uy, sXY,
-// sYY, uyp, MU; centre only: dn, Hxx, Hyx, dQ.
-struct UQ2o
+// ---------------------------------------------------------------------------
+// The arithmetic of one step, restated for FP32 with fewer operations than
+// the reference's expression order (the FP64 mode keeps that order; FP32 is
+// held to tolerances against it):
+//  * central differences are kept as raw differences (twice the
+//    derivative) and their factors 1/2, 1/4 folded into the constants they
+//    meet (P.q4LL, P.nh2LL, P.KK8, P.nKK4, hxi, ...);
+//  * H = CC*term*Q + LL*lap(Q) is formed as (CC*term - 4 LL)*Q + LL*s, with
+//    s the sum of the four neighbours, and the antisymmetric stress
+//    Qxx*Hyx - Qyx*Hxx as LL*(Qxx*s_yx - Qyx*s_xx) (the bulk terms cancel);
+//  * the centre-only part of the Beris-Edwards rate, Gamma*H - u.grad(Q),
+//    is formed in UpdateQuantities, so UpdateFields carries 2 values
+//    instead of 6 per site;
+//  * the forcing term w_v*(F.c_v) is folded into the equilibrium: with
+//    j' = j + tau*F, fe'_v(j') = fe_v(j) + tau*w_v*(F.c_v), so
+//    (fe_v - f_v)/tau + F_v = (fe'_v - f_v)/tau, and the rest population
+//    is the closed form fe_0 = 4/9 dn - 2/3 k2 (dn and k2 = n|u|^2 as
+//    below), which is what nn - sum(fe_1..8) evaluates to;
+//  * y-neighbour differences and sums come from two shuffles and two scalar
+//    adds per pair, with no register repacking.
+
+// Values of one site after UpdateQuantities that a later UpdateFields reads
+// (centre, and through the neighbour sets). BEx/BEy: Gamma*H - u.grad(Q).
+struct UQc
 {
-  f2 dn, ux, uy, uxp, uyp, MU, Hxx, Hyx, dxQxx, dyQxx, dxQyx, dyQyx, sXX, sYY, sXY, sYX;
+  f2 dn, ux, uy, BEx, BEy, MU, uxp, uyp, sXX, sYY, sXY, sYX;
 };
+// x-neighbour set: what UpdateFields reads from the rows x +- 1
 struct UQx
 {
   f2 ux, uy, sXX, sYX, uxp, MU;
 };
-__device__ __forceinline__ UQx xset(const UQ2o& a)
+__device__ __forceinline__ UQx xset(const UQc& a)
 {
   return UQx{a.ux, a.uy, a.sXX, a.sYX, a.uxp, a.MU};
 }
+// Derived fields of the diagnostic replay (DIAG launches only)
+struct UQd
+{
+  f2 Hxx, Hyx, XA, YA, XB, YB, bi, sigmaF, sigmaS, pf, pfS, nact;
+};
 
-// Qa/Qb/Ph: centre, +x, -x, +y, -y
-template<int MODEL>
-__device__ __forceinline__ void uq_pair(const PP& P, const f2 g[9], const f2 Qa[5],
-                                        const f2 Qb[5], const f2 Ph[5], UQ2o& o,
-                                        f2* dg)
+// (v(y+1) + v(y-1), v(y+1) - v(y-1)) for both columns of every lane's pair:
+// lane l holds columns 2l, 2l+1; columns 2l-1 and 2l+2 come from the
+// neighbouring lanes.
+__device__ __forceinline__ void yboth(f2 a, f2& sum, f2& diff)
+{
+  const float lo = __shfl_up_sync(0xffffffffu, a.v.y, 1);
+  const float hi = __shfl_down_sync(0xffffffffu, a.v.x, 1);
+  sum = mk(a.v.y + lo, hi + a.v.x);
+  diff = mk(a.v.y - lo, hi - a.v.x);
+}
+__device__ __forceinline__ f2 ydiff(f2 a)
+{
+  const float lo = __shfl_up_sync(0xffffffffu, a.v.y, 1);
+  const float hi = __shfl_down_sync(0xffffffffu, a.v.x, 1);
+  return mk(a.v.y - lo, hi - a.v.x);
+}
+__device__ __forceinline__ f2 ysum(f2 a)
+{
+  const float lo = __shfl_up_sync(0xffffffffu, a.v.y, 1);
+  const float hi = __shfl_down_sync(0xffffffffu, a.v.x, 1);
+  return mk(a.v.y + lo, hi + a.v.x);
+}
+
+// Neighbour stencil of one scalar field at a site: s = sum of the four
+// neighbours, X = (+x) - (-x), Y = (+y) - (-y).
+struct Stn
+{
+  f2 c, s, X, Y;
+};
+
+// UpdateQuantities of one row pair (src/models/lyotropic.cpp:168-247,
+// src/models/nematic.cpp:76-131).
+template<int MODEL, bool DIAG>
+__device__ __forceinline__ void uq2(const PP& P, const f2 g[9], const Stn& A, const Stn& B,
+                                    const Stn& Ph, UQc& o, UQd& d)
 {
   const f2 dn = ((g[0] + g[1]) + (g[2] + g[3])) + ((g[4] + g[5]) + (g[6] + g[7])) + g[8];
-  const f2 nn = W2(P.rho) + dn;
-  const f2 inv = rcp2(nn, P);
-  const f2 d56 = g[5] - g[6];
-  const f2 jx = (g[1] - g[2]) + (d56 + (g[8] - g[7]));
-  const f2 jy = (g[3] - g[4]) + (d56 + (g[7] - g[8]));
+  const f2 inv = rcp2(W2(P.rho) + dn, P);
+  const f2 d56 = g[5] - g[6], d87 = g[8] - g[7];
+  const f2 jx = (g[1] - g[2]) + (d56 + d87);
+  const f2 jy = (g[3] - g[4]) + (d56 - d87);
   const f2 vx = jx*inv, vy = jy*inv;
 
-  const f2 Qxx = Qa[0], Qyx = Qb[0];
-  const f2 lQxx = fma(KC(-4.f), Qxx, (Qa[1] + Qa[2]) + (Qa[3] + Qa[4]));
-  const f2 lQyx = fma(KC(-4.f), Qyx, (Qb[1] + Qb[2]) + (Qb[3] + Qb[4]));
-  const f2 dxQxx = KC(.5f)*(Qa[1] - Qa[2]), dyQxx = KC(.5f)*(Qa[3] - Qa[4]);
-  const f2 dxQyx = KC(.5f)*(Qb[1] - Qb[2]), dyQyx = KC(.5f)*(Qb[3] - Qb[4]);
+  const f2 Qxx = A.c, Qyx = B.c;
   const f2 S2 = fma(Qxx, Qxx, Qyx*Qyx);
-  // cterm = CC*term with term = -S2 (lyotropic) or 1 - S2 (nematic)
-  const f2 cterm = MODEL == LYO ? W2(P.nCC)*S2 : fma(W2(P.nCC), S2, neg(W2(P.nCC)));
-  const f2 Hxx = fma(cterm, Qxx, W2(P.LL)*lQxx);
-  const f2 Hyx = fma(cterm, Qyx, W2(P.LL)*lQyx);
-  const f2 el = W2(P.LL)*(fma(dyQxx, dyQxx, dyQyx*dyQyx) - fma(dxQxx, dxQxx, dxQyx*dxQyx));
-  const f2 elS = W2(P.nLL2)*fma(dxQxx, dyQxx, dxQyx*dyQyx);
-  const f2 sigmaA = KC(2.f)*fma(Qxx, Hyx, neg(Qyx*Hxx));
+  // CC*term - 4*LL, term = -S2 (lyotropic) or 1 - S2 (nematic)
+  const f2 c4 = fma(W2(P.nCC), S2, W2(P.c4k));
+  const f2 LsA = W2(P.LL)*A.s, LsB = W2(P.LL)*B.s;
+  const f2 Hxx = fma(c4, Qxx, LsA);
+  const f2 Hyx = fma(c4, Qyx, LsB);
+  // Qxx*Hyx - Qyx*Hxx
+  const f2 aQ = Qxx*LsB - Qyx*LsA;
+  // 4/LL times the elastic normal stress, -2/LL times the shear one
+  const f2 elr = fma(A.Y, A.Y, B.Y*B.Y) - fma(A.X, A.X, B.X*B.X);
+  const f2 elSr = fma(A.X, A.Y, B.X*B.Y);
   const f2 QQ = Qxx*Qyx;
-  const f2 flowF = W2(P.xi2)*fma(fma(Qxx, Qxx, KC(-1.f)), Hxx, QQ*Hyx);
-  const f2 flowS = W2(P.xi2)*fma(QQ, Hxx, fma(Qyx, Qyx, KC(-1.f))*Hyx);
-  // sigmaB's nematic/lyotropic common part: 0.5 CC term^2 = 0.5 cterm^2/CC;
-  // written as hCC*term*term with term recomputed from S2
-  const f2 term = MODEL == LYO ? neg(S2) : KC(1.f) - S2;
-  const f2 bulkQ = W2(P.hCC)*(term*term);
-
-  o.dn = dn; o.ux = vx; o.uy = vy;
-  o.Hxx = Hxx; o.Hyx = Hyx;
-  o.dxQxx = dxQxx; o.dyQxx = dyQxx; o.dxQyx = dxQyx; o.dyQyx = dyQyx;
+  const f2 fF = fma(fma(Qxx, Qxx, KC(-1.f)), Hxx, QQ*Hyx);
+  const f2 fS = fma(QQ, Hxx, fma(Qyx, Qyx, KC(-1.f))*Hyx);
+  f2 sigmaF, sigmaS, bi, pf = KC(0.f), pfS = KC(0.f), nact;
 
   if constexpr (MODEL == LYO)
   {
-    const f2 p = Ph[0];
-    const f2 omp = KC(1.f) - p;
-    const f2 lp = fma(KC(-4.f), p, (Ph[1] + Ph[2]) + (Ph[3] + Ph[4]));
-    const f2 dxPhi = KC(.5f)*(Ph[1] - Ph[2]), dyPhi = KC(.5f)*(Ph[3] - Ph[4]);
-    const f2 pq = p*omp;
+    const f2 p = Ph.c;
+    nact = fma(W2(P.zeta), p, W2(P.nzeta));              // -zeta*(1 - p)
+    pf = W2(P.KK8)*((Ph.Y - Ph.X)*(Ph.Y + Ph.X));       // .5 KK (dyPhi^2 - dxPhi^2)
+    pfS = W2(P.nKK4)*(Ph.X*Ph.Y);                        // -KK dxPhi dyPhi
+    sigmaF = fma(W2(P.xi2), fF, fma(nact, Qxx, fma(W2(P.q4LL), elr, pf)));
+    sigmaS = fma(W2(P.xi2), fS, fma(nact, Qyx, fma(W2(P.nh2LL), elSr, pfS)));
+    const f2 pq = p*(KC(1.f) - p);
+    const f2 lp = fma(KC(-4.f), p, Ph.s);
     const f2 mu = fma(W2(P.AA)*pq, fma(KC(-2.f), p, KC(1.f)), W2(P.nKK)*lp);
-    const f2 sigmaB = fma(W2(P.hAA)*pq, pq, bulkQ) - mu*p;
-    const f2 act = W2(P.zeta)*omp;
-    const f2 pf = W2(P.hKK)*fma(dyPhi, dyPhi, neg(dxPhi*dxPhi));
-    const f2 pfS = W2(P.nKK)*(dxPhi*dyPhi);
-    const f2 sigmaF = fma(neg(act), Qxx, flowF) + (pf + el);
-    const f2 sigmaS = fma(neg(act), Qyx, flowS) + (pfS + elS);
-    const f2 bi = sigmaB + W2(P.zetaI)*(W2(P.conc) - p);
-    o.uxp = vx*p; o.uyp = vy*p; o.MU = mu;
-    o.sXX = bi + sigmaF;
-    o.sYY = bi - sigmaF;
-    o.sXY = sigmaS + sigmaA;
-    o.sYX = sigmaS - sigmaA;
-    if(dg)
-    {
-      dg[0] = bi;
-      dg[1] = fma(act, Qxx, sigmaF - pf);
-      // zeta*Qxx in the yx component as the reference has it
-      // (src/models/lyotropic.cpp:242)
-      dg[2] = fma(act, Qxx, sigmaS - pfS);
-      dg[3] = pf;
-      dg[4] = pfS;
-      dg[5] = neg(act*Qxx);
-      dg[6] = neg(act*Qyx);
-    }
+    // .5 AA (p(1-p))^2 + .5 CC term^2 - mu p, term^2 = S2^2
+    const f2 y = fma(W2(P.hCC)*S2, S2, (W2(P.hAA)*pq)*pq);
+    bi = fma(W2(P.zetaI), W2(P.conc) - p, y - mu*p);
+    o.MU = mu;
+    o.uxp = vx*p;
+    o.uyp = vy*p;
   }
   else
   {
-    const f2 sigmaF = fma(neg(W2(P.zeta)), Qxx, flowF) + el;
-    const f2 sigmaS = fma(neg(W2(P.zeta)), Qyx, flowS) + elS;
-    o.uxp = KC(0.f); o.uyp = KC(0.f); o.MU = KC(0.f);
-    o.sXX = bulkQ + sigmaF;
-    o.sYY = bulkQ - sigmaF;
-    o.sXY = sigmaS + sigmaA;
-    o.sYX = sigmaS - sigmaA;
+    nact = W2(P.nzeta);
+    sigmaF = fma(W2(P.xi2), fF, fma(nact, Qxx, W2(P.q4LL)*elr));
+    sigmaS = fma(W2(P.xi2), fS, fma(nact, Qyx, W2(P.nh2LL)*elSr));
+    const f2 term = KC(1.f) - S2;
+    bi = W2(P.hCC)*(term*term);
+    o.MU = o.uxp = o.uyp = KC(0.f);
+  }
+  o.dn = dn;
+  o.ux = vx;
+  o.uy = vy;
+  o.sXX = bi + sigmaF;
+  o.sYY = bi - sigmaF;
+  o.sXY = fma(KC(2.f), aQ, sigmaS);
+  o.sYX = fma(KC(-2.f), aQ, sigmaS);
+  o.BEx = fma(W2(P.GammaQ), Hxx, KC(-.5f)*fma(vx, A.X, vy*A.Y));
+  o.BEy = fma(W2(P.GammaQ), Hyx, KC(-.5f)*fma(vx, B.X, vy*B.Y));
+  if constexpr (DIAG)
+  {
+    d.Hxx = Hxx; d.Hyx = Hyx;
+    d.XA = A.X; d.YA = A.Y; d.XB = B.X; d.YB = B.Y;
+    d.bi = bi; d.sigmaF = sigmaF; d.sigmaS = sigmaS;
+    d.pf = pf; d.pfS = pfS; d.nact = nact;
   }
 }
 
-// y-neighbour values (+y, -y) of the y-set of a row, fetched from the
-// neighbouring lanes
-struct YN
+// y-neighbour differences (and the MU sum) of a row's UpdateQuantities
+struct YD
 {
-  f2 uxp_, uxm, uyp_, uym, sxyp, sxym, syyp, syym, uypp, uypm, mup, mum;
+  f2 ux, uy, sXY, sYY, uyp, MUs;
 };
 template<int MODEL>
-__device__ __forceinline__ YN ynbrs(const UQ2o& c)
+__device__ __forceinline__ YD ydiffs(const UQc& c)
 {
-  YN y;
-  y.uxp_ = yplus(c.ux); y.uxm = yminus(c.ux);
-  y.uyp_ = yplus(c.uy); y.uym = yminus(c.uy);
-  y.sxyp = yplus(c.sXY); y.sxym = yminus(c.sXY);
-  y.syyp = yplus(c.sYY); y.syym = yminus(c.sYY);
+  YD y;
+  y.ux = ydiff(c.ux);
+  y.uy = ydiff(c.uy);
+  y.sXY = ydiff(c.sXY);
+  y.sYY = ydiff(c.sYY);
   if constexpr (MODEL == LYO)
   {
-    y.uypp = yplus(c.uyp); y.uypm = yminus(c.uyp);
-    y.mup = yplus(c.MU); y.mum = yminus(c.MU);
+    y.uyp = ydiff(c.uyp);
+    y.MUs = ysum(c.MU);
   }
-  else
-  {
-    y.uypp = y.uypm = y.mup = y.mum = K(0.f);
-  }
+  else y.uyp = y.MUs = KC(0.f);
   return y;
-}
-
-// The flow part shared by both UpdateFields: Beris-Edwards D, force F,
-// Cahn-Hilliard Dp, equilibrium deviation fe and forcing term per direction.
-struct UFcore
-{
-  f2 Dxx, Dyx, Dp, fe[9], F[9];
-};
-
-template<int MODEL>
-__device__ __forceinline__ void uf_core(const PP& P, const UQ2o& c, const UQx& xp,
-                                        const UQx& xm, const YN& y, f2 Qxx, f2 Qyx,
-                                        UFcore& u)
-{
-  const f2 dxux = KC(.5f)*(xp.ux - xm.ux), dyux = KC(.5f)*(y.uxp_ - y.uxm);
-  const f2 dxuy = KC(.5f)*(xp.uy - xm.uy), dyuy = KC(.5f)*(y.uyp_ - y.uym);
-  const f2 dxSxx = KC(.5f)*(xp.sXX - xm.sXX), dySxy = KC(.5f)*(y.sxyp - y.sxym);
-  const f2 dxSyx = KC(.5f)*(xp.sYX - xm.sYX), dySyy = KC(.5f)*(y.syyp - y.syym);
-  const f2 expansion = dxux + dyuy;
-  const f2 shear = KC(.5f)*(dxuy + dyux);
-  const f2 vorticity = KC(.5f)*(dxuy - dyux);
-  const f2 Qs2 = KC(2.f)*(Qyx*shear);
-  const f2 traceQL = fma(Qxx, dxux - dyuy, Qs2);
-  const f2 vx = c.ux, vy = c.uy;
-  const f2 v2 = KC(2.f)*vorticity;
-  // Dxx = G Hxx - vx dxQxx - vy dyQxx - 2 w Qyx + xi((Qxx+1)(2 dxux - trQL) + 2 Qyx shear - expansion)
-  const f2 bx = fma(Qxx + KC(1.f), fma(KC(2.f), dxux, neg(traceQL)), Qs2 - expansion);
-  u.Dxx = fma(W2(P.GammaQ), c.Hxx, fma(W2(P.xi), bx, neg(fma(vx, c.dxQxx, fma(vy, c.dyQxx, v2*Qyx)))));
-  // Dyx = G Hyx - vx dxQyx - vy dyQyx + 2 w Qxx + xi(Qyx(expansion - trQL) + 2 shear)
-  const f2 by = fma(Qyx, expansion - traceQL, KC(2.f)*shear);
-  u.Dyx = fma(W2(P.GammaQ), c.Hyx, fma(W2(P.xi), by, fma(v2, Qxx, neg(fma(vx, c.dxQyx, vy*c.dyQyx)))));
-  const f2 Fx = (dxSxx + dySxy) - W2(P.friction)*vx;
-  const f2 Fy = (dxSyx + dySyy) - W2(P.friction)*vy;
-  if constexpr (MODEL == LYO)
-  {
-    const f2 lMU = fma(KC(-4.f), c.MU, (xp.MU + xm.MU) + (y.mup + y.mum));
-    const f2 pFlux = KC(.5f)*((xp.uxp - xm.uxp) + (y.uypp - y.uypm));
-    u.Dp = fma(W2(P.GammaP), lMU, neg(pFlux));
-  }
-  else u.Dp = KC(0.f);
-
-  const f2 dn = c.dn;
-  const f2 nn = W2(P.rho) + dn;
-  const f2 jx = nn*vx, jy = nn*vy;
-  const f2 kxx = jx*vx, kyy = jy*vy, kxy = jx*vy, k2 = kxx + kyy;
-  const f2 dn9 = KC((1.f/9.f))*dn, dn36 = KC((1.f/36.f))*dn;
-  const f2 a1 = fma(KC(-.5f), kyy, dn9), a3 = fma(KC(-.5f), kxx, dn9);
-  const f2 b5 = fma(KC(.25f), kxy, dn36), b7 = fma(KC(-.25f), kxy, dn36);
-  u.fe[1] = fma(k2 + jx, KC((1.f/3.f)), a1);
-  u.fe[2] = fma(k2 - jx, KC((1.f/3.f)), a1);
-  u.fe[3] = fma(k2 + jy, KC((1.f/3.f)), a3);
-  u.fe[4] = fma(k2 - jy, KC((1.f/3.f)), a3);
-  const f2 s = jx + jy, d = jx - jy;
-  u.fe[5] = fma(k2 + s, KC((1.f/12.f)), b5);
-  u.fe[6] = fma(k2 - s, KC((1.f/12.f)), b5);
-  u.fe[7] = fma(k2 - d, KC((1.f/12.f)), b7);
-  u.fe[8] = fma(k2 + d, KC((1.f/12.f)), b7);
-  u.fe[0] = dn - (((u.fe[1] + u.fe[2]) + (u.fe[3] + u.fe[4])) + ((u.fe[5] + u.fe[6]) + (u.fe[7] + u.fe[8])));
-  u.F[0] = KC(0.f);
-  u.F[1] = KC((1.f/3.f))*Fx; u.F[2] = neg(u.F[1]);
-  u.F[3] = KC((1.f/3.f))*Fy; u.F[4] = neg(u.F[3]);
-  u.F[5] = KC((1.f/12.f))*(Fx + Fy); u.F[6] = neg(u.F[5]);
-  u.F[7] = KC((1.f/12.f))*(Fy - Fx); u.F[8] = neg(u.F[7]);
 }
 
 template<int MODEL>
 __device__ __forceinline__ f2 itau_of(const PP& P, f2 p)
 {
-  return MODEL == LYO ? rcp2(fma(W2(P.dtau), p, W2(P.tauIso)), P) : rcp2(W2(P.tauIso), P);
+  return MODEL == LYO ? rcp2(fma(W2(P.dtau), p, W2(P.tauIso)), P) : W2(P.itau);
+}
+
+// UpdateFields of one row pair up to the node update
+// (src/models/lyotropic.cpp:249-306, src/models/nematic.cpp:132-199):
+// Beris-Edwards rates Dxx, Dyx, the Cahn-Hilliard rate Dp, and the
+// equilibrium fe' with the forcing folded in (see above), so that the
+// collision is (fe'_v - f_v)*itau. itau = 1/tau(phi).
+template<int MODEL>
+__device__ __forceinline__ void uf2(const PP& P, const UQc& c, const UQx& xp, const UQx& xm,
+                                    const YD& y, f2 Qxx, f2 Qyx, f2 itau, f2 tau, f2 fe[9],
+                                    f2& Dxx, f2& Dyx, f2& Dp)
+{
+  const f2 Dxux = xp.ux - xm.ux, Dxuy = xp.uy - xm.uy;
+  const f2 E2 = Dxux + y.uy;          // 2 expansion
+  const f2 S4 = Dxuy + y.ux;          // 4 shear
+  const f2 V4 = Dxuy - y.ux;          // 4 vorticity
+  const f2 QS = Qyx*S4;
+  const f2 T2 = fma(Qxx, Dxux - y.uy, QS);     // 2 traceQL
+  // xi*((Qxx+1)(2dxux - trQL) + 2Qyx shear - expansion) = hxi*bx2
+  const f2 bx2 = fma(Qxx + KC(1.f), KC(2.f)*Dxux - T2, QS - E2);
+  // xi*(Qyx(expansion - trQL) + 2 shear) = hxi*by2
+  const f2 by2 = fma(Qyx, E2 - T2, S4);
+  Dxx = fma(W2(P.hxi), bx2, fma(KC(-.5f)*V4, Qyx, c.BEx));
+  Dyx = fma(W2(P.hxi), by2, fma(KC(.5f)*V4, Qxx, c.BEy));
+  // twice the force: (d_x s_xx + d_y s_xy - friction u_x), ...
+  const f2 Fx2 = fma(W2(P.n2fric), c.ux, (xp.sXX - xm.sXX) + y.sXY);
+  const f2 Fy2 = fma(W2(P.n2fric), c.uy, (xp.sYX - xm.sYX) + y.sYY);
+  if constexpr (MODEL == LYO)
+  {
+    const f2 lMU = fma(KC(-4.f), c.MU, (xp.MU + xm.MU) + y.MUs);
+    Dp = fma(W2(P.GammaP), lMU, KC(-.5f)*((xp.uxp - xm.uxp) + y.uyp));
+  }
+  else Dp = KC(0.f);
+
+  const f2 dn = c.dn;
+  const f2 nn = W2(P.rho) + dn;
+  const f2 jx = nn*c.ux, jy = nn*c.uy;
+  const f2 kxx = jx*c.ux, kyy = jy*c.uy, kxy = jx*c.uy, k2 = kxx + kyy;
+  const f2 th = KC(.5f)*tau;
+  const f2 jxF = fma(th, Fx2, jx), jyF = fma(th, Fy2, jy);
+  const f2 A = fma(KC((1.f/3.f)), k2, KC((1.f/9.f))*dn);
+  const f2 E1 = fma(KC(-.5f), kyy, A), E3 = fma(KC(-.5f), kxx, A);
+  fe[1] = fma(KC((1.f/3.f)), jxF, E1);
+  fe[2] = fma(KC((-1.f/3.f)), jxF, E1);
+  fe[3] = fma(KC((1.f/3.f)), jyF, E3);
+  fe[4] = fma(KC((-1.f/3.f)), jyF, E3);
+  const f2 B = fma(KC((1.f/12.f)), k2, KC((1.f/36.f))*dn);
+  const f2 Bp = fma(KC(.25f), kxy, B), Bm = fma(KC(-.25f), kxy, B);
+  const f2 s = jxF + jyF, d = jxF - jyF;
+  fe[5] = fma(KC((1.f/12.f)), s, Bp);
+  fe[6] = fma(KC((-1.f/12.f)), s, Bp);
+  fe[7] = fma(KC((-1.f/12.f)), d, Bm);
+  fe[8] = fma(KC((1.f/12.f)), d, Bm);
+  fe[0] = fma(KC((4.f/9.f)), dn, KC((-2.f/3.f))*k2);
+  (void)itau;
 }
 
 // One lattice as one work item sees it.
@@ -426,8 +464,9 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
     return f2{__ldg(reinterpret_cast<const float2*>(a.src + static_cast<long long>(x)*LY + yw))};
   };
 
-  UQ2o q1c{}, q2c{};
+  UQc q1c{}, q2c{};
   UQx q1m{}, q2m{};
+  UQd dq{};
   f2 qa1[3], qa2[3], qn1[3], qn2[3];
   // Delayed populations live in shared memory: row slot s (the row C
   // produced s iterations ago, mod 3), array k: ff v = 0,3,4 (k = 0..2),
@@ -437,6 +476,29 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
   for(int k = 0; k < 3; ++k) { qa1[k] = qa2[k] = qn1[k] = qn2[k] = KC(0.f); }
   int s3 = 0;                              // i mod 3
   float* orow = a.out + static_cast<long long>(x0 - 6)*LY + yg;   // E's output row
+
+  // stencil of plane q at ring row R0 (centre), Rp (+x), Rm (-x)
+  auto ring_stn = [&](const float* Rm, const float* R0, const float* Rp, int q) {
+    const float* c = R0 + q*RWW + cl;
+    Stn t;
+    t.c = lds2(c);
+    const f2 xp = lds2(Rp + q*RWW + cl), xm = lds2(Rm + q*RWW + cl);
+    const float lo = c[-1], hi = c[2];
+    t.s = (xp + xm) + mk(t.c.v.y + lo, hi + t.c.v.x);
+    t.X = xp - xm;
+    t.Y = mk(t.c.v.y - lo, hi - t.c.v.x);
+    return t;
+  };
+  // stencil from register rows: centre (held by this lane), +x, -x
+  auto reg_stn = [&](f2 cen, f2 xp, f2 xm) {
+    Stn t;
+    t.c = cen;
+    f2 ys;
+    yboth(cen, ys, t.Y);
+    t.s = (xp + xm) + ys;
+    t.X = xp - xm;
+    return t;
+  };
 
   const int nit = rows + 6;
   for(int i = 0; i < nit; ++i)
@@ -455,63 +517,51 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
     const float* dp_2 = dpop + (s3 == 2 ? 0 : s3 + 1)*NDP*PW + 2 + 2*lane;   // two iterations ago
 
     // ---- B: predictor UpdateQuantities at row b ----
-    UQ2o nq1;
+    UQc nq1;
     {
       f2 g[9];
 #pragma unroll
       for(int v = 0; v < 9; ++v) g[v] = lds2(R0 + v*RWW + cl);
-      f2 Qa[5], Qb[5], Ph[5];
-      const float* q0 = R0 + 9*RWW + cl;
-      Qa[0] = lds2(q0); Qa[1] = lds2(Rp + 9*RWW + cl); Qa[2] = lds2(Rm + 9*RWW + cl);
-      Qa[3] = mk(Qa[0].v.y, q0[2]); Qa[4] = mk(q0[-1], Qa[0].v.x);
-      const float* q1 = R0 + 10*RWW + cl;
-      Qb[0] = lds2(q1); Qb[1] = lds2(Rp + 10*RWW + cl); Qb[2] = lds2(Rm + 10*RWW + cl);
-      Qb[3] = mk(Qb[0].v.y, q1[2]); Qb[4] = mk(q1[-1], Qb[0].v.x);
-      if constexpr (MODEL == LYO)
-      {
-        const float* q2 = R0 + 11*RWW + cl;
-        Ph[0] = lds2(q2); Ph[1] = lds2(Rp + 11*RWW + cl); Ph[2] = lds2(Rm + 11*RWW + cl);
-        Ph[3] = mk(Ph[0].v.y, q2[2]); Ph[4] = mk(q2[-1], Ph[0].v.x);
-      }
-      else
-      {
-#pragma unroll
-        for(int k = 0; k < 5; ++k) Ph[k] = KC(0.f);
-      }
-      uq_pair<MODEL>(P, g, Qa, Qb, Ph, nq1, nullptr);
+      const Stn A = ring_stn(Rm, R0, Rp, 9), B = ring_stn(Rm, R0, Rp, 10);
+      Stn Ph{};
+      if constexpr (MODEL == LYO) Ph = ring_stn(Rm, R0, Rp, 11);
+      UQd unused;
+      uq2<MODEL, false>(P, g, A, B, Ph, nq1, unused);
     }
 
     // ---- C: predictor UpdateFields at row b-1, then y-part of Move ----
     f2 nQ[3], nQN[3], pf[9], pn[9];
     {
-      const YN y = ynbrs<MODEL>(q1c);
+      const YD y = ydiffs<MODEL>(q1c);
       const f2 Qxx = lds2(Rm + 9*RWW + cl), Qyx = lds2(Rm + 10*RWW + cl);
       const f2 p = MODEL == LYO ? lds2(Rm + 11*RWW + cl) : KC(0.f);
-      UFcore u;
-      uf_core<MODEL>(P, q1c, xset(nq1), q1m, y, Qxx, Qyx, u);
-      const f2 itau = itau_of<MODEL>(P, p);
+      const f2 tau = MODEL == LYO ? fma(W2(P.dtau), p, W2(P.tauIso)) : W2(P.tauIso);
+      const f2 itau = MODEL == LYO ? rcp2(tau, P) : W2(P.itau);
+      const f2 hitau = KC(.5f)*itau;
+      f2 fe[9], Dxx, Dyx, Dp;
+      uf2<MODEL>(P, q1c, xset(nq1), q1m, y, Qxx, Qyx, itau, tau, fe, Dxx, Dyx, Dp);
 #pragma unroll
       for(int v = 0; v < 9; ++v)
       {
         const f2 g = lds2(Rm + v*RWW + cl);
-        const f2 coll = fma(u.fe[v] - g, itau, u.F[v]);
-        pn[v] = fma(KC(.5f), coll, g);
-        pf[v] = MODEL == LYO ? g + coll : fma(KC(.5f), coll, pn[v]);
+        const f2 dv = fe[v] - g;
+        pn[v] = fma(hitau, dv, g);
+        pf[v] = fma(itau, dv, g);
       }
-      nQN[0] = fma(KC(.5f), u.Dxx, Qxx);
-      nQN[1] = fma(KC(.5f), u.Dyx, Qyx);
+      nQN[0] = fma(KC(.5f), Dxx, Qxx);
+      nQN[1] = fma(KC(.5f), Dyx, Qyx);
       if constexpr (MODEL == LYO)
       {
-        nQ[0] = Qxx + u.Dxx;
-        nQ[1] = Qyx + u.Dyx;
-        nQN[2] = fma(KC(.5f), u.Dp, p);
-        nQ[2] = p + u.Dp;
+        nQ[0] = Qxx + Dxx;
+        nQ[1] = Qyx + Dyx;
+        nQN[2] = fma(KC(.5f), Dp, p);
+        nQ[2] = p + Dp;
         if constexpr (SRC) nQ[2] = fma(p, src_at(x0 - 4 + i), nQ[2]);
       }
       else
       {
-        nQ[0] = fma(KC(.5f), u.Dxx, nQN[0]);
-        nQ[1] = fma(KC(.5f), u.Dyx, nQN[1]);
+        nQ[0] = Qxx + Dxx;
+        nQ[1] = Qyx + Dyx;
         nQN[2] = nQ[2] = KC(0.f);
       }
       // stream along y. Directions with cx = -1 (2, 6, 7) are used by D in
@@ -540,7 +590,7 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
     }
 
     // ---- D: corrector UpdateQuantities at row s = b-2 (x-part of Move) ----
-    UQ2o nq2;
+    UQc nq2;
     {
       // direction v at (s, y) left row s - cx: cx = -1 is the row C just
       // produced, cx = 0 the previous one, cx = +1 the one before that
@@ -551,20 +601,11 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
       ns[0] = lds2(dp_1 + 3*PW); ns[3] = lds2(dp_1 + 4*PW); ns[4] = lds2(dp_1 + 5*PW);
       fs[1] = lds2(dp_2 + 6*PW); fs[5] = lds2(dp_2 + 7*PW); fs[8] = lds2(dp_2 + 8*PW);
       ns[1] = lds2(dp_2 + 9*PW); ns[5] = lds2(dp_2 + 10*PW); ns[8] = lds2(dp_2 + 11*PW);
-      f2 Qa[5], Qb[5], Ph[5];
-      Qa[0] = qa1[0]; Qa[1] = nQ[0]; Qa[2] = qa2[0]; Qa[3] = yplus(qa1[0]); Qa[4] = yminus(qa1[0]);
-      Qb[0] = qa1[1]; Qb[1] = nQ[1]; Qb[2] = qa2[1]; Qb[3] = yplus(qa1[1]); Qb[4] = yminus(qa1[1]);
-      if constexpr (MODEL == LYO)
-      {
-        Ph[0] = qa1[2]; Ph[1] = nQ[2]; Ph[2] = qa2[2]; Ph[3] = yplus(qa1[2]); Ph[4] = yminus(qa1[2]);
-      }
-      else
-      {
-#pragma unroll
-        for(int k = 0; k < 5; ++k) Ph[k] = KC(0.f);
-      }
-      f2 dg[7];
-      uq_pair<MODEL>(P, fs, Qa, Qb, Ph, nq2, DIAG ? dg : nullptr);
+      const Stn A = reg_stn(qa1[0], nQ[0], qa2[0]);
+      const Stn B = reg_stn(qa1[1], nQ[1], qa2[1]);
+      Stn Ph{};
+      if constexpr (MODEL == LYO) Ph = reg_stn(qa1[2], nQ[2], qa2[2]);
+      uq2<MODEL, DIAG>(P, fs, A, B, Ph, nq2, dq);
       const f2 hitau = KC(-.5f)*itau_of<MODEL>(P, qa1[2]);
 #pragma unroll
       for(int v = 0; v < 9; ++v)
@@ -576,9 +617,9 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
         {
           const long long pl = a.plane;
           float* o = a.diag + static_cast<long long>(xs)*LY + yg;
-          const f2 vals[16] = {W2(P.rho) + nq2.dn, nq2.ux, nq2.uy, nq2.uxp, nq2.uyp, nq2.Hxx,
-                               nq2.Hyx, nq2.MU, nq2.dxQxx, nq2.dyQxx, nq2.dxQyx, nq2.dyQyx,
-                               nq2.sXX, nq2.sYY, nq2.sYX, nq2.sXY};
+          const f2 vals[16] = {W2(P.rho) + nq2.dn, nq2.ux, nq2.uy, nq2.uxp, nq2.uyp, dq.Hxx,
+                               dq.Hyx, nq2.MU, KC(.5f)*dq.XA, KC(.5f)*dq.YA, KC(.5f)*dq.XB,
+                               KC(.5f)*dq.YB, nq2.sXX, nq2.sYY, nq2.sYX, nq2.sXY};
 #pragma unroll
           for(int k = 0; k < 16; ++k)
           {
@@ -587,6 +628,11 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
           }
           if constexpr (MODEL == LYO)
           {
+            const f2 aQxx = dq.nact*qa1[0];
+            // the elastic yx stress carries +zeta*Qxx*(1-phi) as the
+            // reference has it (src/models/lyotropic.cpp:242)
+            const f2 dg[7] = {dq.bi, (dq.sigmaF - dq.pf) - aQxx, (dq.sigmaS - dq.pfS) - aQxx,
+                              dq.pf, dq.pfS, aQxx, dq.nact*qa1[1]};
 #pragma unroll
             for(int k = 0; k < 7; ++k)
             {
@@ -601,19 +647,19 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
     // ---- E: corrector UpdateFields at row b-3, store ----
     if constexpr (!DIAG)
     {
-      const YN y = ynbrs<MODEL>(q2c);
-      UFcore u;
-      uf_core<MODEL>(P, q2c, xset(nq2), q2m, y, qa2[0], qa2[1], u);
-      const f2 itau = itau_of<MODEL>(P, qa2[2]);
+      const YD y = ydiffs<MODEL>(q2c);
+      const f2 tau = MODEL == LYO ? fma(W2(P.dtau), qa2[2], W2(P.tauIso)) : W2(P.tauIso);
+      const f2 itau = MODEL == LYO ? rcp2(tau, P) : W2(P.itau);
       const f2 hitau = KC(.5f)*itau;
+      f2 fe[9], Dxx, Dyx, Dp;
+      uf2<MODEL>(P, q2c, xset(nq2), q2m, y, qa2[0], qa2[1], itau, tau, fe, Dxx, Dyx, Dp);
       f2 gout[9];
 #pragma unroll
       for(int v = 0; v < 9; ++v)
-        gout[v] = fma(KC(.5f), u.F[v],
-                      fma(hitau, u.fe[v], lds2(hrow + (((i + 1) & 1)*9 + v)*COLS + 2*lane)));
-      const f2 Qo0 = fma(KC(.5f), u.Dxx, qn2[0]);
-      const f2 Qo1 = fma(KC(.5f), u.Dyx, qn2[1]);
-      f2 Qo2 = fma(KC(.5f), u.Dp, qn2[2]);
+        gout[v] = fma(hitau, fe[v], lds2(hrow + (((i + 1) & 1)*9 + v)*COLS + 2*lane));
+      const f2 Qo0 = fma(KC(.5f), Dxx, qn2[0]);
+      const f2 Qo1 = fma(KC(.5f), Dyx, qn2[1]);
+      f2 Qo2 = fma(KC(.5f), Dp, qn2[2]);
       // corrector source with the predicted phi of this row
       if constexpr (SRC) Qo2 = fma(qa2[2], src_at(x0 - 6 + i), Qo2);
       if(i >= 6)

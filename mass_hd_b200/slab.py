@@ -10,7 +10,7 @@ contiguous in every plane:
   with HALO = 4 halo rows on each side as an ordinary periodic lattice of
   (n_r + 8) x LY sites: local row i is global row x0_r - 4 + i (mod LX);
 * before every step the halo rows are refreshed from the neighbouring
-  slabs (`exchange_halos`): the first 4 owned rows go to the left
+  slabs (`DistExchange.exchange`): the first 4 owned rows go to the left
   neighbour's upper halo, the last 4 to the right neighbour's lower halo,
   each as one packed [plane][row][y] buffer (mass_lb_get_rows /
   mass_lb_put_rows on the device);
