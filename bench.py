@@ -22,7 +22,9 @@ the serial rate (one handle, one job after another) is reported beside it.
 
 With --gpus N (torchrun), every rank advances its own lattice of the same
 size (independent runs, weak scaling, no collective on the data path); time
-is the max over ranks.
+is the max over ranks. --decomp slab instead splits ONE lattice into
+x-slabs over the ranks, with a halo-row exchange over NCCL before every
+step (strong scaling).
 
 The line also carries `fp64`: the FP64 mode (bit-identical to the
 reference's double-precision build) timed on the same seeded lattice, the
@@ -534,6 +536,63 @@ def fp64_record(model: str, st: dict, L: int, steps: int, warmup: int, world: in
                     "the same seeded lattice: one sub-step kernel per predictor and corrector"}
 
 
+def run_ours_slab(args):
+    """--decomp slab: ONE lattice of size^2 split into x-slabs over the ranks
+    (strong scaling), halo rows exchanged before every step over NCCL
+    (mass_hd_b200/slab.py). A step is the exchange plus the step of every
+    slab; time is the slowest rank's, with CUDA events on its lattice
+    stream."""
+    import torch
+
+    import mass_hd_b200 as M
+    from mass_hd_b200 import slab as S
+
+    rank, world, local = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    model = args.model
+    mcode = M.LYOTROPIC if model == "lyotropic" else M.NEMATIC
+    params = LYO_C1 if model == "lyotropic" else NEM_C2
+    prec = M.FP32 if args.precision == "fp32" else M.FP64
+    L = args.size
+    x0, n = S.partition(L, world)[rank]
+    sl = S.LatticeSlab(mcode, params, L, L, prec, x0, n)
+    sl.upload_global(synthetic_state(model, L, seed=1))
+    run = S.SlabRun(sl, S.DistExchange())
+    run.step(max(args.warmup, 3))
+    sl.synchronize()
+    barrier(world)
+    stream = torch.cuda.ExternalStream(sl.lat.stream)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    run.step(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    sl.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    f, p, bad = run.checks()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": L * L * args.steps / (ms / 1e3), "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f64",
+            "data": "synthetic (seeded random director S=1, tanh phi disk R=L/4)",
+            "config": {"workload": f"{model} {args.precision.upper()} {L}x{L} periodic, one "
+                                   f"lattice in x-slabs", "model": model, "LX": L, "LY": L,
+                       "precision": args.precision, "parallelism": f"x-slabs over {world} ranks",
+                       "halo_bytes_per_step_per_rank": sl.bufs.bytes_per_exchange},
+            "gpu_launches": args.steps * sl.lat.launches_per_step,
+            "checks": {"fsum": f, "phisum": p, "nonfinite": bad},
+        }
+        print(json.dumps(line), flush=True)
+    sl.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
 def run_ours(args):
     import torch
 
@@ -541,6 +600,8 @@ def run_ours(args):
 
     if args.model == "go-or-grow":
         return run_ours_gog(args)
+    if args.decomp == "slab":
+        return run_ours_slab(args)
     rank, world, local = dist_setup(args.gpus)
     torch.cuda.set_device(local)
     model = args.model
@@ -723,6 +784,9 @@ def main():
     ap.add_argument("--model", default="lyotropic", choices=["lyotropic", "nematic", "go-or-grow"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--decomp", default="independent", choices=["independent", "slab"],
+                    help="independent: a lattice per rank (weak scaling, default); slab: one "
+                         "lattice split into x-slabs over the ranks (strong scaling)")
     ap.add_argument("--no-fp64", action="store_true",
                     help="skip the FP64-mode record beside the FP32 line")
     args = ap.parse_args()

@@ -1,6 +1,7 @@
 """Batched parameter sweep: many lyotropic runs of uneven size advanced together.
 
     python -m mass_hd_b200.ensemble_case [--runs 96] [--steps 1000] [--seed 7]
+    torchrun --nproc-per-node N -m mass_hd_b200.ensemble_case --sharded [...]
 
 The sweep: each run's lattice is L x L with L drawn uniformly from
 {128, 192, 256, 384, 512}; zeta log-uniform in [1e-3, 5e-2]; the nematic
@@ -14,6 +15,13 @@ mass_lb_ensemble_step) and once run after run through the single-lattice
 path (mass_lb_step, autotuned tile per run), checks that both give
 bit-identical states, and prints one JSON object with both times and their
 ratio. Timing is wall-clock around device-synchronised calls.
+
+--sharded (one process per GPU): the runs are independent, so they are
+split over the ranks with no communication on the data path
+(`partition_runs`: largest lattice first onto the rank with the fewest
+sites so far), each rank steps its share as one ensemble, and the time is
+the slowest rank's (an all-reduce of one number). Rank 0 prints the sites,
+the per-rank loads and the whole job's site-updates per second.
 """
 from __future__ import annotations
 
@@ -53,6 +61,47 @@ def sweep(nruns: int = 96, seed: int = 7, sizes=SIZES):
             st["phi"] = rng.normal(0.5, 0.05, L * L)
         out.append((p, (L, L), st))
     return out
+
+
+def partition_runs(sizes, world: int):
+    """Run indices per rank: runs sorted by site count, largest first, each
+    given to the rank with the fewest sites so far (ties to the lowest
+    rank). Every run lands on exactly one rank; the loads differ by at most
+    the largest run."""
+    load = [0] * world
+    share = [[] for _ in range(world)]
+    order = sorted(range(len(sizes)), key=lambda i: (-sizes[i][0] * sizes[i][1], i))
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        share[r].append(i)
+        load[r] += sizes[i][0] * sizes[i][1]
+    return [sorted(x) for x in share], load
+
+
+def run_sharded(nruns: int, steps: int, seed: int = 7) -> dict:
+    """This rank's share of the sweep as one ensemble (see --sharded)."""
+    import os
+
+    import torch
+
+    import bench
+    rank, world, local = bench.dist_setup(int(os.environ.get("WORLD_SIZE", "1")))
+    torch.cuda.set_device(local)
+    cases = sweep(nruns, seed)
+    share, load = partition_runs([c[1] for c in cases], world)
+    mine = [cases[i] for i in share[rank]]
+    t = 0.0
+    if mine:
+        ens, t = run_batched(mine, steps)
+        ens.close()
+    t_max = bench.max_over_ranks(t, world)
+    out = {"runs": nruns, "steps": steps, "ranks": world, "rank_sites": load,
+           "rank_runs": [len(x) for x in share], "slowest_rank_s": t_max,
+           "site_updates_per_s": site_updates(cases, steps) / t_max if t_max > 0 else None}
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return out if rank == 0 else None
 
 
 def site_updates(cases, steps: int) -> int:
@@ -110,7 +159,14 @@ def main(argv=None) -> int:
     ap.add_argument("--runs", type=int, default=96)
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--seed", type=int, default=7)
+    ap.add_argument("--sharded", action="store_true",
+                    help="split the runs over the ranks of a torchrun launch")
     a = ap.parse_args(argv)
+    if a.sharded:
+        r = run_sharded(a.runs, a.steps, a.seed)
+        if r is not None:
+            print(json.dumps(r))
+        return 0
     print(json.dumps(compare(a.runs, a.steps, a.seed)))
     return 0
 

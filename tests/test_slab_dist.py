@@ -171,3 +171,18 @@ def test_slab_rows_wrap_periodically():
     assert list(loc["phi"][:4]) == [0.0, 1.0, 2.0, 3.0]
     assert S.owned_part(loc["phi"], 2, 2).tolist() == [8.0, 9.0, 10.0, 11.0]
     assert S.owned_part(loc["ff"], 2, 2).shape == (4, 2)
+
+
+def test_ensemble_runs_split_over_ranks_once_and_balanced():
+    from mass_hd_b200 import ensemble_case as E
+    cases = E.sweep(96, seed=7)
+    sizes = [c[1] for c in cases]
+    for world in (1, 2, 3, 8):
+        share, load = E.partition_runs(sizes, world)
+        flat = sorted(i for s in share for i in s)
+        assert flat == list(range(96))
+        assert load == [sum(sizes[i][0] * sizes[i][1] for i in s) for s in share]
+        assert max(load) - min(load) <= 512 * 512
+    # more ranks than runs: some ranks get nothing, none gets a run twice
+    share, load = E.partition_runs([(128, 128), (256, 256)], 4)
+    assert sorted(i for s in share for i in s) == [0, 1] and load.count(0) == 2
