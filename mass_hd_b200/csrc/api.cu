@@ -286,7 +286,19 @@ P32 p32_of(const Params& P)
              static_cast<float>(P.friction), static_cast<float>(P.AA),
              static_cast<float>(P.CC), static_cast<float>(P.LL),
              static_cast<float>(P.KK), static_cast<float>(P.zeta),
-             static_cast<float>(P.zetaI), static_cast<float>(P.conc)};
+             static_cast<float>(P.zetaI), static_cast<float>(P.conc),
+             0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0};
+}
+
+// the same with the go-or-grow phenotype terms
+P32 p32_of(const Params& P, const Pheno& ph)
+{
+  P32 q = p32_of(P);
+  q.B = static_cast<float>(ph.B); q.Snem = static_cast<float>(ph.Snem);
+  q.Dchi = static_cast<float>(ph.Dchi); q.Achi = static_cast<float>(ph.Achi);
+  q.Ochi = static_cast<float>(ph.Ochi); q.phiswitch = static_cast<float>(ph.phiswitch);
+  q.phi_critical = static_cast<float>(ph.phi_critical); q.growTogether = ph.growTogether;
+  return q;
 }
 
 FusedArgs fused_args(mass_lb_handle* h, const float* in, float* out, bool diag)
@@ -299,8 +311,9 @@ FusedArgs fused_args(mass_lb_handle* h, const float* in, float* out, bool diag)
   a.LX = static_cast<int>(h->LX);
   a.LY = static_cast<int>(h->LY);
   a.plane = static_cast<long long>(h->LX)*h->LY;
-  a.p = p32_of(h->P);
-  a.src = h->src_on ? h->src_fused : nullptr;
+  a.p = h->model == GOG ? p32_of(h->P, h->s32.ph) : p32_of(h->P);
+  // go-or-grow always reads its growth-rate plane (zero until a source is set)
+  a.src = h->src_on || h->model == GOG ? h->src_fused : nullptr;
   return a;
 }
 

@@ -12,6 +12,9 @@ struct P32
 {
   float rho, GammaQ, GammaP, xi, tauNem, tauIso, friction;
   float AA, CC, LL, KK, zeta, zetaI, conc;
+  // go-or-grow phenotype terms (Pheno)
+  float B, Snem, Dchi, Achi, Ochi, phiswitch, phi_critical;
+  int growTogether;
 };
 
 // Diagnostic outputs of the corrector UpdateQuantities (the values the
@@ -27,6 +30,9 @@ struct PairParams
   float2 rho, GammaQ, GammaP, xi2, hxi, tauIso, dtau, itau, n2fric;
   float2 AA, hAA, nCC, hCC, c4k, LL, q4LL, nh2LL;
   float2 nKK, KK8, nKK4, zeta, nzeta, zetaI, conc;
+  // go-or-grow: Snem, phi_critical, B, B/2, GammaP/2, Dchi/2, 2 Achi, Ochi,
+  // phiswitch, growTogether (0 or 1)
+  float2 Snem, phic, Bc, hB, hGP, hDchi, A2chi, Ochi, phisw, gt;
 };
 
 struct FusedArgs
@@ -42,6 +48,7 @@ struct FusedArgs
   P32 p;
   PairParams pp;       // filled by the warp-strip launcher
   const float* src;    // per-site phi source rate (LX*LY) or null; warp-strip kernel only
+                       // (go-or-grow: the growth rate, always present)
 };
 
 // Tile shapes the autotuner may pick.

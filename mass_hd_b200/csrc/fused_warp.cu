@@ -126,7 +126,8 @@ using PP = PairParams;
 __host__ PairParams make_pp(const P32& p, int model)
 {
   auto b = [](float x) { return make_float2(x, x); };
-  const bool lyo = model == LYO;
+  const bool lyo = model != NEM;      // lyotropic and go-or-grow: tau(phi)
+  const bool gog = model == GOG;
   PairParams q;
   q.rho = b(p.rho); q.GammaQ = b(p.GammaQ); q.GammaP = b(p.GammaP);
   q.xi2 = b(2.f*p.xi); q.hxi = b(.5f*p.xi);
@@ -136,13 +137,17 @@ __host__ PairParams make_pp(const P32& p, int model)
   q.itau = b(1.f/(lyo ? p.tauIso : p.tauNem));
   q.n2fric = b(-2.f*p.friction);
   q.AA = b(p.AA); q.hAA = b(.5f*p.AA);
-  q.nCC = b(-p.CC); q.hCC = b(.5f*p.CC);
-  // CC*term - 4 LL = -CC*S2 + c4k
-  q.c4k = b(lyo ? -4.f*p.LL : p.CC - 4.f*p.LL);
+  // the bulk factor of H minus 4 LL, as -nCC*S2 + c4k: CC*(-S2) (lyotropic),
+  // CC*(1 - S2) (nematic), 2 CC*(Snem - S2) (go-or-grow)
+  q.nCC = b(gog ? -2.f*p.CC : -p.CC); q.hCC = b(.5f*p.CC);
+  q.c4k = b(gog ? 2.f*p.CC*p.Snem - 4.f*p.LL : lyo ? -4.f*p.LL : p.CC - 4.f*p.LL);
   q.LL = b(p.LL);
   q.q4LL = b(.25f*p.LL); q.nh2LL = b(-.5f*p.LL);
   q.nKK = b(-p.KK); q.KK8 = b(.125f*p.KK); q.nKK4 = b(-.25f*p.KK);
   q.zeta = b(p.zeta); q.nzeta = b(-p.zeta); q.zetaI = b(p.zetaI); q.conc = b(p.conc);
+  q.Snem = b(p.Snem); q.phic = b(p.phi_critical); q.Bc = b(p.B); q.hB = b(.5f*p.B);
+  q.hGP = b(.5f*p.GammaP); q.hDchi = b(.5f*p.Dchi); q.A2chi = b(2.f*p.Achi);
+  q.Ochi = b(p.Ochi); q.phisw = b(p.phiswitch); q.gt = b(p.growTogether ? 1.f : 0.f);
   return q;
 }
 
@@ -464,28 +469,17 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
     return f2{__ldg(reinterpret_cast<const float2*>(a.src + static_cast<long long>(x)*LY + yw))};
   };
 
-  // Row windows, rotated by the unrolled loop below instead of copied:
-  // slot k of each holds the row of iteration i with i mod 3 = k.
-  //   Pq: predictor UpdateQuantities (B) of its row,
-  //   Cq: corrector UpdateQuantities (D) of its row,
-  //   Aq: predicted Qxx, Qyx, phi (C) of its row, Nq: QN of its row (C).
-  // In iteration i (k = i mod 3) the newest is slot k, the one before slot
-  // (k + 2) mod 3 and the one before that slot (k + 1) mod 3.
-  UQc Pq[3], Cq[3];
-  f2 Aq[3][3], Nq[3][3];
-#pragma unroll
-  for(int k = 0; k < 3; ++k)
-  {
-    Pq[k] = UQc{};
-    Cq[k] = UQc{};
-#pragma unroll
-    for(int q = 0; q < 3; ++q) Aq[k][q] = Nq[k][q] = KC(0.f);
-  }
+  UQc q1c{}, q2c{};
+  UQx q1m{}, q2m{};
   UQd dq{};
+  f2 qa1[3], qa2[3], qn1[3], qn2[3];
   // Delayed populations live in shared memory: row slot s (the row C
   // produced s iterations ago, mod 3), array k: ff v = 0,3,4 (k = 0..2),
   // fn v = 0,3,4 (3..5), ff v = 1,5,8 (6..8), fn v = 1,5,8 (9..11). C writes
   // them already shifted along y (column + cy); D reads its own columns.
+#pragma unroll
+  for(int k = 0; k < 3; ++k) { qa1[k] = qa2[k] = qn1[k] = qn2[k] = KC(0.f); }
+  int s3 = 0;                              // i mod 3
   float* orow = a.out + static_cast<long long>(x0 - 6)*LY + yg;   // E's output row
 
   // stencil of plane q at ring row R0 (centre), Rp (+x), Rm (-x)
@@ -512,16 +506,14 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
   };
 
   const int nit = rows + 6;
-  // One row iteration; false once a bounded wait has given up.
-  auto body = [&](const int i, const int s3, UQc& Pn, const UQc& Pc, const UQc& Po, UQc& Cn,
-                  const UQc& Cc, const UQc& Co, f2 (&An)[3], const f2 (&Ac)[3],
-                  const f2 (&Ao)[3], f2 (&Nn)[3], const f2 (&No)[3]) -> bool {
+  for(int i = 0; i < nit; ++i)
+  {
     if(i + 2 < nload)
     {
       const int rr = i + 2;
       if(!mbar_wait_bounded(&mbar[(rb + rr) & (RING - 1)], ((rb + rr) / RING) & 1)) abort = true;
     }
-    if(__any_sync(0xffffffffu, abort)) return false;
+    if(__any_sync(0xffffffffu, abort)) break;
     const float* Rm = ring + ((rb + i    ) & (RING - 1))*NP*RWW;   // row b-1
     const float* R0 = ring + ((rb + i + 1) & (RING - 1))*NP*RWW;   // row b
     const float* Rp = ring + ((rb + i + 2) & (RING - 1))*NP*RWW;   // row b+1
@@ -530,7 +522,7 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
     const float* dp_2 = dpop + (s3 == 2 ? 0 : s3 + 1)*NDP*PW + 2 + 2*lane;   // two iterations ago
 
     // ---- B: predictor UpdateQuantities at row b ----
-    UQc& nq1 = Pn;
+    UQc nq1;
     {
       f2 g[9];
 #pragma unroll
@@ -543,18 +535,16 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
     }
 
     // ---- C: predictor UpdateFields at row b-1, then y-part of Move ----
-    f2 (&nQ)[3] = An;
-    f2 (&nQN)[3] = Nn;
-    f2 pf[9], pn[9];
+    f2 nQ[3], nQN[3], pf[9], pn[9];
     {
-      const YD y = ydiffs<MODEL>(Pc);
+      const YD y = ydiffs<MODEL>(q1c);
       const f2 Qxx = lds2(Rm + 9*RWW + cl), Qyx = lds2(Rm + 10*RWW + cl);
       const f2 p = MODEL == LYO ? lds2(Rm + 11*RWW + cl) : KC(0.f);
       const f2 tau = MODEL == LYO ? fma(W2(P.dtau), p, W2(P.tauIso)) : W2(P.tauIso);
       const f2 itau = MODEL == LYO ? rcp2(tau, P) : W2(P.itau);
       const f2 hitau = KC(.5f)*itau;
       f2 fe[9], Dxx, Dyx, Dp;
-      uf2<MODEL>(P, Pc, xset(nq1), xset(Po), y, Qxx, Qyx, itau, tau, fe, Dxx, Dyx, Dp);
+      uf2<MODEL>(P, q1c, xset(nq1), q1m, y, Qxx, Qyx, itau, tau, fe, Dxx, Dyx, Dp);
 #pragma unroll
       for(int v = 0; v < 9; ++v)
       {
@@ -605,7 +595,7 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
     }
 
     // ---- D: corrector UpdateQuantities at row s = b-2 (x-part of Move) ----
-    UQc& nq2 = Cn;
+    UQc nq2;
     {
       // direction v at (s, y) left row s - cx: cx = -1 is the row C just
       // produced, cx = 0 the previous one, cx = +1 the one before that
@@ -616,12 +606,12 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
       ns[0] = lds2(dp_1 + 3*PW); ns[3] = lds2(dp_1 + 4*PW); ns[4] = lds2(dp_1 + 5*PW);
       fs[1] = lds2(dp_2 + 6*PW); fs[5] = lds2(dp_2 + 7*PW); fs[8] = lds2(dp_2 + 8*PW);
       ns[1] = lds2(dp_2 + 9*PW); ns[5] = lds2(dp_2 + 10*PW); ns[8] = lds2(dp_2 + 11*PW);
-      const Stn A = reg_stn(Ac[0], nQ[0], Ao[0]);
-      const Stn B = reg_stn(Ac[1], nQ[1], Ao[1]);
+      const Stn A = reg_stn(qa1[0], nQ[0], qa2[0]);
+      const Stn B = reg_stn(qa1[1], nQ[1], qa2[1]);
       Stn Ph{};
-      if constexpr (MODEL == LYO) Ph = reg_stn(Ac[2], nQ[2], Ao[2]);
+      if constexpr (MODEL == LYO) Ph = reg_stn(qa1[2], nQ[2], qa2[2]);
       uq2<MODEL, DIAG>(P, fs, A, B, Ph, nq2, dq);
-      const f2 hitau = KC(-.5f)*itau_of<MODEL>(P, Ac[2]);
+      const f2 hitau = KC(-.5f)*itau_of<MODEL>(P, qa1[2]);
 #pragma unroll
       for(int v = 0; v < 9; ++v)
         *reinterpret_cast<float2*>(hrow + ((i & 1)*9 + v)*COLS + 2*lane) = fma(hitau, fs[v], ns[v]).v;
@@ -643,11 +633,11 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
           }
           if constexpr (MODEL == LYO)
           {
-            const f2 aQxx = dq.nact*Ac[0];
+            const f2 aQxx = dq.nact*qa1[0];
             // the elastic yx stress carries +zeta*Qxx*(1-phi) as the
             // reference has it (src/models/lyotropic.cpp:242)
             const f2 dg[7] = {dq.bi, (dq.sigmaF - dq.pf) - aQxx, (dq.sigmaS - dq.pfS) - aQxx,
-                              dq.pf, dq.pfS, aQxx, dq.nact*Ac[1]};
+                              dq.pf, dq.pfS, aQxx, dq.nact*qa1[1]};
 #pragma unroll
             for(int k = 0; k < 7; ++k)
             {
@@ -662,21 +652,21 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
     // ---- E: corrector UpdateFields at row b-3, store ----
     if constexpr (!DIAG)
     {
-      const YD y = ydiffs<MODEL>(Cc);
-      const f2 tau = MODEL == LYO ? fma(W2(P.dtau), Ao[2], W2(P.tauIso)) : W2(P.tauIso);
+      const YD y = ydiffs<MODEL>(q2c);
+      const f2 tau = MODEL == LYO ? fma(W2(P.dtau), qa2[2], W2(P.tauIso)) : W2(P.tauIso);
       const f2 itau = MODEL == LYO ? rcp2(tau, P) : W2(P.itau);
       const f2 hitau = KC(.5f)*itau;
       f2 fe[9], Dxx, Dyx, Dp;
-      uf2<MODEL>(P, Cc, xset(nq2), xset(Co), y, Ao[0], Ao[1], itau, tau, fe, Dxx, Dyx, Dp);
+      uf2<MODEL>(P, q2c, xset(nq2), q2m, y, qa2[0], qa2[1], itau, tau, fe, Dxx, Dyx, Dp);
       f2 gout[9];
 #pragma unroll
       for(int v = 0; v < 9; ++v)
         gout[v] = fma(hitau, fe[v], lds2(hrow + (((i + 1) & 1)*9 + v)*COLS + 2*lane));
-      const f2 Qo0 = fma(KC(.5f), Dxx, No[0]);
-      const f2 Qo1 = fma(KC(.5f), Dyx, No[1]);
-      f2 Qo2 = fma(KC(.5f), Dp, No[2]);
+      const f2 Qo0 = fma(KC(.5f), Dxx, qn2[0]);
+      const f2 Qo1 = fma(KC(.5f), Dyx, qn2[1]);
+      f2 Qo2 = fma(KC(.5f), Dp, qn2[2]);
       // corrector source with the predicted phi of this row
-      if constexpr (SRC) Qo2 = fma(Ao[2], src_at(x0 - 6 + i), Qo2);
+      if constexpr (SRC) Qo2 = fma(qa2[2], src_at(x0 - 6 + i), Qo2);
       if(i >= 6)
       {
         const long long pl = a.plane;
@@ -700,6 +690,16 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
       }
     }
 
+    // ---- advance the row windows ----
+    q1m = xset(q1c); q1c = nq1;
+    q2m = xset(q2c); q2c = nq2;
+#pragma unroll
+    for(int k = 0; k < 3; ++k)
+    {
+      qa2[k] = qa1[k]; qa1[k] = nQ[k];
+      qn2[k] = qn1[k]; qn1[k] = nQN[k];
+    }
+    s3 = s3 == 2 ? 0 : s3 + 1;
     orow += LY;
 
     __syncwarp();
@@ -709,19 +709,6 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
       issue(issued);
       ++issued;
     }
-    return true;
-  };
-
-  for(int i = 0; i < nit; i += 3)
-  {
-    if(!body(i, 0, Pq[0], Pq[2], Pq[1], Cq[0], Cq[2], Cq[1], Aq[0], Aq[2], Aq[1], Nq[0], Nq[1]))
-      break;
-    if(i + 1 >= nit ||
-       !body(i + 1, 1, Pq[1], Pq[0], Pq[2], Cq[1], Cq[0], Cq[2], Aq[1], Aq[0], Aq[2], Nq[1], Nq[2]))
-      break;
-    if(i + 2 >= nit ||
-       !body(i + 2, 2, Pq[2], Pq[1], Pq[0], Cq[2], Cq[1], Cq[0], Aq[2], Aq[1], Aq[0], Nq[2], Nq[0]))
-      break;
   }
 
   rowbase = rb + issued;
