@@ -31,12 +31,17 @@ int mass_lb_set_tile(mass_lb_handle* h, int threads, int rows);
 int mass_lb_autotune(mass_lb_handle* h);
 
 /* 1 if mass_lb_step runs the fused FP32 kernel (FP32, periodic lattice,
- * npc = 1, LY % 4 == 0, LY >= 64), else 0. */
+ * npc = 1, LY % 4 == 0, LY >= 64; every model), else 0. A go-or-grow or
+ * division lattice leaves the fused kernel for the unfused FP32 sweeps when
+ * conserve_phi is switched on (mass_lb_set_phi_conservation), which needs a
+ * lattice-wide phi sum inside a sub-step; the dry relaxation of go-or-grow
+ * runs on the sweeps and hands the state back. */
 int mass_lb_uses_fused(mass_lb_handle* h);
 
 /* Device view of the fused FP32 state (read-only for the caller): `*planes`
  * receives the base of NP float planes of LX*LY values each (g0..g8 as
- * deviations from t_v*rho, then Qxx, Qyx and, for lyotropic, phi), valid
+ * deviations from t_v*rho, then Qxx, Qyx, then phi for the lyotropic
+ * models and m for go-or-grow: 11, 12 or 13 planes), valid
  * until the next mass_lb_step / upload call. */
 int mass_lb_device_state(mass_lb_handle* h, void** planes, long long* plane_stride,
                          int* nplanes);
@@ -155,7 +160,10 @@ int mass_lb_checks_rows(mass_lb_handle* h, unsigned x0, unsigned nrows, double* 
  * doubles in the reference's
  * site order, guarded by an FNV-1a checksum. Everything else a step uses is
  * recomputed from these, so a loaded lattice continues bit for bit as if it
- * had never stopped (FP32 values are stored exactly as doubles). A
+ * had never stopped (FP32 values are stored exactly as doubles; an FP32
+ * handle writes its populations as the deviations from t_v*rho it holds,
+ * format version 2, so that sites near rest keep every bit; version 1
+ * files still load). A
  * checkpoint loads into a handle of the same model and lattice size; the
  * precision and boundary may differ. Errors (MASS_LB_EINVAL): unreadable
  * file, wrong magic or version, other model or size, short or corrupted

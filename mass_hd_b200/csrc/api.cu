@@ -112,6 +112,20 @@ __global__ void k_get_scalar(double* __restrict__ st, const T* a, int x0, int nr
   }
 }
 
+// chi = m/phi (0 where phi <= 1e-12) from the fused go-or-grow planes, in
+// FP32 as the unfused sweeps store it (src/models/go-or-grow.cpp:208-216)
+__global__ void k_get_chi(double* __restrict__ st, const float* phi, const float* m, int x0,
+                          int nrows, int LY)
+{
+  const long long n = static_cast<long long>(nrows)*LY;
+  const long long base = static_cast<long long>(x0)*LY;
+  for(long long k = blockIdx.x*256ll + threadIdx.x; k < n; k += 256ll*gridDim.x)
+  {
+    const float p = phi[base + k];
+    st[k] = p > 1e-12f ? static_cast<double>(m[base + k]/p) : 0.0;
+  }
+}
+
 inline int blocks_for(long long n)
 {
   long long b = (n + 255)/256;
@@ -133,6 +147,7 @@ struct mass_lb_handle
   Dims d{};
   cudaStream_t stream = nullptr;
   bool fused = false;
+  bool in_ensemble = false;  // a run of a mass_lb_ensemble (its buffers step there)
 
   State<double> s64{};       // FP64 (any bc)
   State<float> s32{};        // FP32 with walls
@@ -227,7 +242,9 @@ int dalloc(mass_lb_handle* h, T** p, size_t n)
   return 0;
 }
 
-int nplanes(const mass_lb_handle* h) { return h->model == LYO ? 12 : 11; }
+// planes of the FP32 fused state: g0..g8, Qxx, Qyx, then phi (lyotropic,
+// go-or-grow) and m (go-or-grow)
+int nplanes(const mass_lb_handle* h) { return h->model == NEM ? 11 : h->model == LYO ? 12 : 13; }
 
 template<typename T>
 int alloc_state(mass_lb_handle* h, State<T>& s)
@@ -317,6 +334,63 @@ FusedArgs fused_args(mass_lb_handle* h, const float* in, float* out, bool diag)
   return a;
 }
 
+// Moves an FP32 fused state into the unfused sweeps' state (allocated on
+// first use) or back. The layouts agree plane for plane on a periodic
+// lattice (no ghost ring, populations as deviations in both), so each is a
+// device copy. The sweeps take over where the fused kernel cannot run: the
+// dry relaxation of go-or-grow's Configure() and conserve_phi.
+int fused_to_sweeps(mass_lb_handle* h)
+{
+  if(!h->fused) return 0;
+  if(!h->s32.ff)
+  {
+    if(int r = alloc_state(h, h->s32)) return r;
+    if(int r = zero_state(h, h->s32)) return r;
+  }
+  const size_t plane = static_cast<size_t>(h->LX)*h->LY;
+  const size_t b = plane*sizeof(float);
+  State<float>& s = h->s32;
+  CU(cudaMemcpyAsync(s.ff, h->cur, 9*b, cudaMemcpyDeviceToDevice, h->stream), "state copy");
+  CU(cudaMemcpyAsync(s.Qxx, h->cur + 9*plane, b, cudaMemcpyDeviceToDevice, h->stream), "state copy");
+  CU(cudaMemcpyAsync(s.Qyx, h->cur + 10*plane, b, cudaMemcpyDeviceToDevice, h->stream), "state copy");
+  if(h->model != NEM)
+    CU(cudaMemcpyAsync(s.phi, h->cur + 11*plane, b, cudaMemcpyDeviceToDevice, h->stream), "state copy");
+  if(h->model == GOG)
+    CU(cudaMemcpyAsync(s.m, h->cur + 12*plane, b, cudaMemcpyDeviceToDevice, h->stream), "state copy");
+  if(h->src_on && h->src_fused)
+  {
+    if(!h->src32)
+      if(int r = dalloc(h, &h->src32, h->d.NE)) return r;
+    CU(cudaMemcpyAsync(h->src32, h->src_fused, b, cudaMemcpyDeviceToDevice, h->stream), "copy");
+    s.src = h->src32;
+  }
+  if(h->model == GOG && update_chi_f32(h->d, s, h->stream))
+    return cuda_fail(cudaGetLastError(), "chi update");
+  h->fused = false;
+  h->has_prev = false;
+  h->derived_pending = false;
+  return 0;
+}
+
+int sweeps_to_fused(mass_lb_handle* h)
+{
+  if(h->fused) return 0;
+  const size_t plane = static_cast<size_t>(h->LX)*h->LY;
+  const size_t b = plane*sizeof(float);
+  const State<float>& s = h->s32;
+  CU(cudaMemcpyAsync(h->cur, s.ff, 9*b, cudaMemcpyDeviceToDevice, h->stream), "state copy");
+  CU(cudaMemcpyAsync(h->cur + 9*plane, s.Qxx, b, cudaMemcpyDeviceToDevice, h->stream), "state copy");
+  CU(cudaMemcpyAsync(h->cur + 10*plane, s.Qyx, b, cudaMemcpyDeviceToDevice, h->stream), "state copy");
+  if(h->model != NEM)
+    CU(cudaMemcpyAsync(h->cur + 11*plane, s.phi, b, cudaMemcpyDeviceToDevice, h->stream), "state copy");
+  if(h->model == GOG)
+    CU(cudaMemcpyAsync(h->cur + 12*plane, s.m, b, cudaMemcpyDeviceToDevice, h->stream), "state copy");
+  h->fused = true;
+  h->has_prev = false;
+  h->derived_pending = false;
+  return 0;
+}
+
 int check_err_flag(mass_lb_handle* h)
 {
   int e = 0;
@@ -334,10 +408,15 @@ std::vector<FusedConfig> tile_candidates(const mass_lb_handle* h)
   for(int nt : {32, 64, 128, 256})
   {
     if(!fused_supported(static_cast<int>(h->LX), static_cast<int>(h->LY), nt)) continue;
-    if(h->src_on && nt != 32) continue;   // the phi source is in the warp-strip kernel only
-    for(int rows : {32, 64, 128, 256, 512, 1024})
+    // the phi source and go-or-grow are in the warp-strip kernel only
+    if((h->src_on || h->model == GOG) && nt != 32) continue;
+    for(int rows : {8, 16, 32, 64, 128, 256, 512, 1024})
     {
-      if(rows > static_cast<int>(h->LX) && rows != 32) continue;
+      if(rows > static_cast<int>(h->LX) && rows != 8) continue;
+      // short chunks only where a lattice has few strips to spread: each
+      // warp's rows are a serial chain, and on a lattice whose state fits
+      // in L2 more, shorter chains win over the pipeline fill they repeat
+      if(rows < 32 && h->LX >= 32 && static_cast<long long>(h->LX)*h->LY > (1ll << 21)) continue;
       c.push_back(FusedConfig{nt, std::min(rows, static_cast<int>(h->LX))});
     }
   }
@@ -473,9 +552,9 @@ int mass_lb_create(const mass_lb_params* params, unsigned LX, unsigned LY,
   }
   else
   {
-    // the fused kernel covers lyotropic and nematic; go-or-grow runs the
-    // unfused sweeps in FP32
-    h->fused = !h->wall && h->P.npc == 1 && h->model != GOG &&
+    // the fused warp-strip kernel: every model on periodic lattices with
+    // npc = 1; the rest runs the unfused sweeps in FP32
+    h->fused = !h->wall && h->P.npc == 1 &&
                fused_supported(static_cast<int>(LX), static_cast<int>(LY), 64);
     if(h->fused)
     {
@@ -485,6 +564,14 @@ int mass_lb_create(const mass_lb_params* params, unsigned LX, unsigned LY,
       if(cudaMemsetAsync(h->cur, 0, n*sizeof(float), h->stream) != cudaSuccess ||
          cudaMemsetAsync(h->nxt, 0, n*sizeof(float), h->stream) != cudaSuccess)
         return bail(fail(MASS_LB_ECUDA, "memset"));
+      if(h->model == GOG)
+      {
+        // the growth-rate plane every go-or-grow step reads, zero until set
+        const size_t np = static_cast<size_t>(LX)*LY;
+        if(int r = dalloc(h, &h->src_fused, np)) return bail(r);
+        if(cudaMemsetAsync(h->src_fused, 0, np*sizeof(float), h->stream) != cudaSuccess)
+          return bail(fail(MASS_LB_ECUDA, "memset"));
+      }
       if(const char* env = std::getenv("MASS_LB_TILE"))
       {
         int nt = 0, rows = 0;
@@ -560,14 +647,16 @@ static int settle_derived(mass_lb_handle* h)
   return 0;
 }
 
-static int put_field(mass_lb_handle* h, int field, const double* src)
+// ff_raw: FP32 populations given as the deviations from t_v*rho the FP32
+// state holds (a checkpoint's exact values), not as populations
+static int put_field(mass_lb_handle* h, int field, const double* src, bool ff_raw = false)
 {
   const int LY = static_cast<int>(h->LY);
   const long long rows_per = std::max<long long>(1, kStageSites/LY);
   const bool f64 = h->precision == MASS_LB_FP64;
   const bool isff = field == MASS_LB_FF;
   const int comps = isff ? 9 : 1;
-  const double rest = f64 ? 0.0 : h->P.rho;
+  const double rest = f64 || ff_raw ? 0.0 : h->P.rho;
   for(long long x0 = 0; x0 < h->LX; x0 += rows_per)
   {
     const int nrows = static_cast<int>(std::min<long long>(rows_per, h->LX - x0));
@@ -583,7 +672,8 @@ static int put_field(mass_lb_handle* h, int field, const double* src)
         k_put_ff<float><<<nb, 256, 0, h->stream>>>(h->stage, base, plane, x0, nrows, LY, 0, LY, rest);
       else
       {
-        const int p = field == MASS_LB_QQXX ? 9 : field == MASS_LB_QQYX ? 10 : 11;
+        const int p = field == MASS_LB_QQXX ? 9 : field == MASS_LB_QQYX ? 10
+                    : field == MASS_LB_M ? 12 : 11;
         k_put_scalar<float><<<nb, 256, 0, h->stream>>>(h->stage, base + p*plane, x0, nrows, LY, 0, LY);
       }
     }
@@ -605,7 +695,8 @@ static int put_field(mass_lb_handle* h, int field, const double* src)
     }
     CU(cudaGetLastError(), "upload kernel");
   }
-  if(h->model == GOG && (field == MASS_LB_PHI || field == MASS_LB_M))
+  // chi follows phi and m (the fused kernel forms chi = m/phi itself)
+  if(h->model == GOG && !h->fused && (field == MASS_LB_PHI || field == MASS_LB_M))
   {
     const int r = h->precision == MASS_LB_FP64 ? update_chi_f64(h->d, h->s64, h->stream)
                                                : update_chi_f32(h->d, h->s32, h->stream);
@@ -632,14 +723,23 @@ int mass_lb_upload_field(mass_lb_handle* h, int field, const double* src)
   return 0;
 }
 
+static int upload_state(mass_lb_handle* h, const double* ff, const double* QQxx,
+                        const double* QQyx, const double* phi, bool ff_raw);
+
 int mass_lb_upload(mass_lb_handle* h, const double* ff, const double* QQxx,
                    const double* QQyx, const double* phi)
+{
+  return upload_state(h, ff, QQxx, QQyx, phi, false);
+}
+
+static int upload_state(mass_lb_handle* h, const double* ff, const double* QQxx,
+                        const double* QQyx, const double* phi, bool ff_raw)
 {
   if(!h || !ff || !QQxx || !QQyx) return fail(MASS_LB_EINVAL, "null argument");
   if(h->model != NEM && !phi) return fail(MASS_LB_EINVAL, "lyotropic models need phi");
   DeviceGuard g(h->device);
   if(int r = settle_derived(h)) return r;
-  if(int r = put_field(h, MASS_LB_FF, ff)) return r;
+  if(int r = put_field(h, MASS_LB_FF, ff, ff_raw)) return r;
   if(int r = put_field(h, MASS_LB_QQXX, QQxx)) return r;
   if(int r = put_field(h, MASS_LB_QQYX, QQyx)) return r;
   if(h->model != NEM)
@@ -725,8 +825,11 @@ int mass_lb_step(mass_lb_handle* h, unsigned nsteps)
   return 0;
 }
 
-static int get_primary(mass_lb_handle* h, int field, double* out, bool sync = true)
+// ff_raw: FP32 populations as the stored deviations from t_v*rho
+static int get_primary(mass_lb_handle* h, int field, double* out, bool sync = true,
+                       bool ff_raw = false)
 {
+  const double rest32 = ff_raw ? 0.0 : h->P.rho;
   const int LY = static_cast<int>(h->LY);
   const long long rows_per = std::max<long long>(1, kStageSites/LY);
   const bool isff = field == MASS_LB_FF || field == MASS_LB_FN;
@@ -739,9 +842,14 @@ static int get_primary(mass_lb_handle* h, int field, double* out, bool sync = tr
     if(h->fused)
     {
       const long long plane = static_cast<long long>(h->LX)*h->LY;
-      if(field <= MASS_LB_PHI)
+      if(field == MASS_LB_M)
+        k_get_scalar<float><<<nb, 256, 0, h->stream>>>(h->stage, h->cur + 12*plane, x0, nrows, LY, 0, LY, 0.0);
+      else if(field == MASS_LB_CHI)
+        k_get_chi<<<nb, 256, 0, h->stream>>>(h->stage, h->cur + 11*plane, h->cur + 12*plane,
+                                             x0, nrows, LY);
+      else if(field <= MASS_LB_PHI)
       {
-        if(isff) k_get_ff<float><<<nb, 256, 0, h->stream>>>(h->stage, h->cur, plane, x0, nrows, LY, 0, LY, h->P.rho);
+        if(isff) k_get_ff<float><<<nb, 256, 0, h->stream>>>(h->stage, h->cur, plane, x0, nrows, LY, 0, LY, rest32);
         else
         {
           const int p = field == MASS_LB_QQXX ? 9 : field == MASS_LB_QQYX ? 10 : 11;
@@ -807,7 +915,7 @@ static int get_primary(mass_lb_handle* h, int field, double* out, bool sync = tr
           if(field >= MASS_LB_SIGMA_BULK && field <= MASS_LB_SIGMA_ACTIVE_YX)
             a = s.diag[field - MASS_LB_SIGMA_BULK];
       }
-      if(field == MASS_LB_FF) k_get_ff<float><<<nb, 256, 0, h->stream>>>(h->stage, s.ff, d.NE, x0, nrows, LY, d.g, d.EY, h->P.rho);
+      if(field == MASS_LB_FF) k_get_ff<float><<<nb, 256, 0, h->stream>>>(h->stage, s.ff, d.NE, x0, nrows, LY, d.g, d.EY, rest32);
       else k_get_scalar<float><<<nb, 256, 0, h->stream>>>(h->stage, a, x0, nrows, LY, d.g, d.EY, add);
     }
     CU(cudaGetLastError(), "download kernel");
@@ -876,7 +984,7 @@ cudaError_t launch_sums(mass_lb_handle* h)
   {
     const long long plane = static_cast<long long>(h->LX)*h->LY;
     SumView<float> v{h->cur, h->cur + 9*plane, h->cur + 10*plane,
-                     h->model == LYO ? h->cur + 11*plane : nullptr, plane,
+                     h->model != NEM ? h->cur + 11*plane : nullptr, plane,
                      static_cast<int>(h->LX), static_cast<int>(h->LY), 0,
                      static_cast<int>(h->LY), h->P.rho};
     e = launch_sums_f32(v, h->red_scratch, h->red_out, h->stream);
@@ -1031,7 +1139,7 @@ int mass_lb_checks_rows(mass_lb_handle* h, unsigned x0, unsigned nrows, double* 
   {
     const long long plane = static_cast<long long>(h->LX)*h->LY;
     const float* b = h->cur + static_cast<long long>(x0)*h->LY;
-    SumView<float> v{b, b + 9*plane, b + 10*plane, h->model == LYO ? b + 11*plane : nullptr,
+    SumView<float> v{b, b + 9*plane, b + 10*plane, h->model != NEM ? b + 11*plane : nullptr,
                      plane, static_cast<int>(nrows), static_cast<int>(h->LY), 0,
                      static_cast<int>(h->LY), h->P.rho};
     e = launch_sums_f32(v, h->red_scratch, h->red_out, h->stream);
@@ -1146,7 +1254,7 @@ int mass_lb_statistics(mass_lb_handle* h, mass_lb_stats* out)
   {
     const long long plane = N;
     StatView<float> v{h->cur, plane, h->cur + 9*plane, h->cur + 10*plane,
-                      h->model == LYO ? h->cur + 11*plane : nullptr,
+                      h->model != NEM ? h->cur + 11*plane : nullptr,
                       static_cast<int>(h->LX), static_cast<int>(h->LY), 0,
                       static_cast<int>(h->LY), h->P.rho};
     e = launch_stats_f32(v, h->stats, 0.4, h->stream);
@@ -1245,7 +1353,7 @@ namespace {
 struct CkptHeader
 {
   char magic[8];             // "MASSLBCK"
-  int32_t version;           // 1
+  int32_t version;           // 2 (1: FP32 populations stored with t_v*rho added)
   int32_t model, precision;  // of the handle that wrote it
   uint32_t LX, LY, bc, npc;
   uint64_t steps;
@@ -1284,13 +1392,21 @@ int mass_lb_save(mass_lb_handle* h, const char* path)
   const size_t N = static_cast<size_t>(h->LX)*h->LY;
   const int nf = ckpt_scalars(h->model);
   std::vector<double> buf(N*9 + nf*N);
-  if(int r = mass_lb_download(h, MASS_LB_FF, buf.data())) return r;
+  {
+    // FP32 populations go out as the deviations from t_v*rho the state
+    // holds: exact in double, where f = deviation + t_v*rho would round
+    // the deviations of sites near rest
+    DeviceGuard g(h->device);
+    if(int r = settle_derived(h)) return r;
+    if(int r = get_primary(h, MASS_LB_FF, buf.data(), true, h->precision == MASS_LB_FP32))
+      return r;
+  }
   const int fields[4] = {MASS_LB_QQXX, MASS_LB_QQYX, MASS_LB_PHI, MASS_LB_M};
   for(int i = 0; i < nf; ++i)
     if(int r = mass_lb_download(h, fields[i], buf.data() + N*9 + i*N)) return r;
   CkptHeader hd{};
   std::memcpy(hd.magic, "MASSLBCK", 8);
-  hd.version = 1;
+  hd.version = 2;
   hd.model = h->model;
   hd.precision = h->precision;
   hd.LX = h->LX; hd.LY = h->LY; hd.bc = h->bc; hd.npc = h->P.npc;
@@ -1328,7 +1444,7 @@ int mass_lb_load(mass_lb_handle* h, const char* path)
   };
   if(std::fread(&hd, sizeof(hd), 1, f) != 1) return bad("short header");
   if(std::memcmp(hd.magic, "MASSLBCK", 8) != 0) return bad("not a mass_lb checkpoint");
-  if(hd.version != 1) return bad("unknown checkpoint version");
+  if(hd.version != 1 && hd.version != 2) return bad("unknown checkpoint version");
   if(hd.model != h->model) return bad("checkpoint of another model");
   if(hd.LX != h->LX || hd.LY != h->LY) return bad("checkpoint of another lattice size");
   const size_t N = static_cast<size_t>(h->LX)*h->LY;
@@ -1339,11 +1455,22 @@ int mass_lb_load(mass_lb_handle* h, const char* path)
   std::fclose(f);
   if(fnv1a(buf.data(), buf.size()*sizeof(double), kFnvOffset) != hd.checksum)
     return fail(MASS_LB_EINVAL, std::string(path) + ": checksum mismatch (corrupted file)");
-  const double* ff = buf.data();
+  double* ff = buf.data();
   const double* q = buf.data() + N*9;
+  // version 2 from an FP32 handle: populations as deviations from t_v*rho
+  // (rho of the writer); an FP32 handle of the same rho takes them as they
+  // are, anything else gets the populations
+  const double rho_file = hd.params[5];
+  bool raw = hd.version >= 2 && hd.precision == MASS_LB_FP32;
+  if(raw && !(h->precision == MASS_LB_FP32 && h->P.rho == rho_file))
+  {
+    for(size_t k = 0; k < N; ++k)
+      for(int v = 0; v < 9; ++v) ff[9*k + v] += Tv(v)*rho_file;
+    raw = false;
+  }
   if(h->model == GOG)
     if(int r = mass_lb_upload_field(h, MASS_LB_M, q + 3*N)) return r;
-  if(int r = mass_lb_upload(h, ff, q, q + N, h->model != NEM ? q + 2*N : nullptr)) return r;
+  if(int r = upload_state(h, ff, q, q + N, h->model != NEM ? q + 2*N : nullptr, raw)) return r;
   // continue the run the checkpoint came from: step count and the totals
   // the runtime checks compare against
   h->steps = hd.steps;
@@ -1393,6 +1520,13 @@ int mass_lb_set_phi_source(mass_lb_handle* h, const double* rate)
     h->src_on = false;
     h->s64.src = nullptr;
     h->s32.src = nullptr;
+    // go-or-grow's fused step reads its rate plane in any case
+    if(h->fused && h->model == GOG)
+    {
+      CU(cudaMemsetAsync(h->src_fused, 0, static_cast<size_t>(h->LX)*h->LY*sizeof(float),
+                         h->stream), "memset");
+      CU(cudaStreamSynchronize(h->stream), "sync");
+    }
     return 0;
   }
   if(h->fused)
@@ -1431,10 +1565,16 @@ int mass_lb_set_phi_conservation(mass_lb_handle* h, int on, double totalphi)
 {
   if(!h) return fail(MASS_LB_EINVAL, "null handle");
   if(h->model == NEM) return fail(MASS_LB_EUNSUPPORTED, "the nematic model has no phi");
-  if(on && h->fused)
-    return fail(MASS_LB_EUNSUPPORTED, "conserve_phi needs a lattice-wide sum between the two "
-                                      "halves of a sub-step; use precision FP64");
   DeviceGuard g(h->device);
+  // conserve_phi needs a lattice-wide phi sum between the two halves of a
+  // sub-step, which the one-launch fused step does not have: the lattice
+  // continues on the unfused FP32 sweeps
+  if(on && h->fused)
+  {
+    if(h->in_ensemble)
+      return fail(MASS_LB_EUNSUPPORTED, "conserve_phi is not available to ensemble runs");
+    if(int r = fused_to_sweeps(h)) return r;
+  }
   if(on && !h->phisum)
     if(int r = dalloc(h, &h->phisum, 1 + PHI_PARTS)) return r;
   for(int i = 0; i < 2; ++i)
@@ -1852,6 +1992,10 @@ int mass_lb_relax_free_energy(mass_lb_handle* h, unsigned steps, double dt, int 
   if(int r = resolve_totals(h)) return r;
   if(!h->relaxsum)
     if(int r = dalloc(h, &h->relaxsum, 1)) return r;
+  // the relaxation runs on the sweeps' state; a fused lattice goes there
+  // and back
+  const bool was_fused = h->fused;
+  if(int r = fused_to_sweeps(h)) return r;
   const int bc = h->wall ? static_cast<int>(h->bc) : 0;
   const int r = h->precision == MASS_LB_FP64
     ? relax_unfused_f64(h->d, h->P, h->s64, bc, steps, dt, relax_phi, relax_Q, h->relaxsum, h->stream)
@@ -1865,6 +2009,11 @@ int mass_lb_relax_free_energy(mass_lb_handle* h, unsigned steps, double dt, int 
   CU(cudaMemcpyAsync(&sum, h->relaxsum, sizeof(double), cudaMemcpyDeviceToHost, h->stream),
      "relaxation sum");
   CU(cudaStreamSynchronize(h->stream), "relaxation sync");
+  if(was_fused)
+  {
+    if(int r = sweeps_to_fused(h)) return r;
+    CU(cudaStreamSynchronize(h->stream), "state copy sync");
+  }
   h->ptot = sum;
   h->has_prev = false;
   if(phisum) *phisum = sum;
@@ -2034,6 +2183,7 @@ int mass_lb_ensemble_create(int nruns, const mass_lb_params* params, const unsig
     mass_lb_handle* h = nullptr;
     if(int r = mass_lb_create(&params[i], LX[i], LY[i], 0, MASS_LB_FP32, &h)) return bail(r);
     h->tuned = true;   // the ensemble kernel steps this lattice
+    h->in_ensemble = true;
     e->runs.push_back(h);
     const long long strips = (LY[i] + ENS_WOUT - 1)/ENS_WOUT;
     items_max += strips*((LX[i] + 31)/32);

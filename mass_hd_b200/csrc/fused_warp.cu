@@ -30,7 +30,11 @@ constexpr int RING = 4;     // input rows per warp in shared memory (power of 2)
 constexpr int PADY = 4;     // ring row padding (floats, each side)
 constexpr int COLS = 64;    // columns per warp strip
 constexpr int WOUT = COLS - 8;
-constexpr int RWW = COLS + 2*PADY;   // ring row stride (floats)
+// ring row stride (floats): a 16-byte-aligned left pad, then the strip. The
+// lane holding columns 62-63 reads one value past its row (its +y
+// neighbour, a halo column whose result is never stored); that read stays
+// inside this warp's shared memory.
+constexpr int RWW = COLS + PADY;
 constexpr int WPB = 4;      // warps per CTA
 constexpr int PW = COLS + 4;         // stride of a delayed-population row
 constexpr int NDP = 12;              // delayed populations (see below)
@@ -174,18 +178,21 @@ __host__ PairParams make_pp(const P32& p, int model)
 
 // Values of one site after UpdateQuantities that a later UpdateFields reads
 // (centre, and through the neighbour sets). BEx/BEy: Gamma*H - u.grad(Q).
+// Go-or-grow also carries chi = m/phi, phi and u*m (its phenotype update
+// reads them at the neighbours); the other models leave them zero.
 struct UQc
 {
   f2 dn, ux, uy, BEx, BEy, MU, uxp, uyp, sXX, sYY, sXY, sYX;
+  f2 chi, p, uxm, uym;
 };
 // x-neighbour set: what UpdateFields reads from the rows x +- 1
 struct UQx
 {
-  f2 ux, uy, sXX, sYX, uxp, MU;
+  f2 ux, uy, sXX, sYX, uxp, MU, chi, p, uxm;
 };
 __device__ __forceinline__ UQx xset(const UQc& a)
 {
-  return UQx{a.ux, a.uy, a.sXX, a.sYX, a.uxp, a.MU};
+  return UQx{a.ux, a.uy, a.sXX, a.sYX, a.uxp, a.MU, a.chi, a.p, a.uxm};
 }
 // Derived fields of the diagnostic replay (DIAG launches only)
 struct UQd
@@ -227,7 +234,7 @@ struct Stn
 // src/models/nematic.cpp:76-131).
 template<int MODEL, bool DIAG>
 __device__ __forceinline__ void uq2(const PP& P, const f2 g[9], const Stn& A, const Stn& B,
-                                    const Stn& Ph, UQc& o, UQd& d)
+                                    const Stn& Ph, const f2 m, UQc& o, UQd& d)
 {
   const f2 dn = ((g[0] + g[1]) + (g[2] + g[3])) + ((g[4] + g[5]) + (g[6] + g[7])) + g[8];
   const f2 inv = rcp2(W2(P.rho) + dn, P);
@@ -270,6 +277,39 @@ __device__ __forceinline__ void uq2(const PP& P, const f2 g[9], const Stn& A, co
     o.MU = mu;
     o.uxp = vx*p;
     o.uyp = vy*p;
+    o.chi = o.p = o.uxm = o.uym = KC(0.f);
+  }
+  else if constexpr (MODEL == GOG)
+  {
+    // GoOrGrow::UpdateQuantitiesAtNode (src/models/go-or-grow.cpp:230-308):
+    // H and the bulk stress with term = Snem - q^2 (H's factor 2 CC is in
+    // nCC and c4k), the crowding penalty B above phi_critical, and the
+    // active stress weighted by the go fraction 1 - chi, chi = m/phi
+    const f2 p = Ph.c;
+    const f2 mp = m*rcp2(p, P);
+    const f2 chi = mk(p.v.x > 1e-12f ? mp.v.x : 0.f, p.v.y > 1e-12f ? mp.v.y : 0.f);
+    nact = (W2(P.nzeta)*p)*(KC(1.f) - chi);             // -zeta*phi*(1 - chi)
+    pf = W2(P.KK8)*((Ph.Y - Ph.X)*(Ph.Y + Ph.X));
+    pfS = W2(P.nKK4)*(Ph.X*Ph.Y);
+    sigmaF = fma(W2(P.xi2), fF, fma(nact, Qxx, fma(W2(P.q4LL), elr, pf)));
+    sigmaS = fma(W2(P.xi2), fS, fma(nact, Qyx, fma(W2(P.nh2LL), elSr, pfS)));
+    const f2 pq = p*(KC(1.f) - p);
+    const f2 lp = fma(KC(-4.f), p, Ph.s);
+    const f2 dpc = p - W2(P.phic);
+    const f2 pos = mk(fmaxf(dpc.v.x, 0.f), fmaxf(dpc.v.y, 0.f));
+    const f2 mu = fma(W2(P.AA)*pq, fma(KC(-2.f), p, KC(1.f)),
+                      fma(W2(P.Bc), pos, W2(P.nKK)*lp));
+    // .5 AA (p(1-p))^2 + .5 B pos^2 + .5 CC term^2 - mu p
+    const f2 term = W2(P.Snem) - S2;
+    const f2 y = fma(W2(P.hCC)*term, term, fma(W2(P.hAA)*pq, pq, (W2(P.hB)*pos)*pos));
+    bi = fma(W2(P.zetaI), W2(P.conc) - p, y - mu*p);
+    o.MU = mu;
+    o.uxp = vx*p;
+    o.uyp = vy*p;
+    o.chi = chi;
+    o.p = p;
+    o.uxm = vx*m;
+    o.uym = vy*m;
   }
   else
   {
@@ -279,6 +319,7 @@ __device__ __forceinline__ void uq2(const PP& P, const f2 g[9], const Stn& A, co
     const f2 term = KC(1.f) - S2;
     bi = W2(P.hCC)*(term*term);
     o.MU = o.uxp = o.uyp = KC(0.f);
+    o.chi = o.p = o.uxm = o.uym = KC(0.f);
   }
   o.dn = dn;
   o.ux = vx;
@@ -299,9 +340,12 @@ __device__ __forceinline__ void uq2(const PP& P, const f2 g[9], const Stn& A, co
 }
 
 // y-neighbour differences (and the MU sum) of a row's UpdateQuantities
+// (go-or-grow: the y+-1 values of chi, phi and MU themselves, and the
+// y-difference of uy*m)
 struct YD
 {
   f2 ux, uy, sXY, sYY, uyp, MUs;
+  f2 chip, chim, pp, pm, MUp, MUm, uym;
 };
 template<int MODEL>
 __device__ __forceinline__ YD ydiffs(const UQc& c)
@@ -316,14 +360,62 @@ __device__ __forceinline__ YD ydiffs(const UQc& c)
     y.uyp = ydiff(c.uyp);
     y.MUs = ysum(c.MU);
   }
+  else if constexpr (MODEL == GOG)
+  {
+    y.uyp = ydiff(c.uyp);
+    y.MUp = yplus(c.MU); y.MUm = yminus(c.MU);
+    y.MUs = y.MUp + y.MUm;
+    y.chip = yplus(c.chi); y.chim = yminus(c.chi);
+    y.pp = yplus(c.p); y.pm = yminus(c.p);
+    y.uym = ydiff(c.uym);
+  }
   else y.uyp = y.MUs = KC(0.f);
   return y;
+}
+
+// Go-or-grow's rate of change of m (src/models/go-or-grow.cpp:331-362)
+// and its growth term R = chi*phi*rate, at a site whose UpdateQuantities
+// values are c, with the x-neighbour sets xp, xm and the y-neighbours in y.
+// Dm = GammaP*sum_n .5(chi_n + chi)(MU_n - MU) + Dchi*sum_n .5(phi_n + phi)(chi_n - chi)
+//      - div(u m) - phi*V'(chi) + (growTogether ? chi R : R)
+__device__ __forceinline__ void pheno_rate(const PP& P, const UQc& c, const UQx& xp,
+                                           const UQx& xm, const YD& y, const f2 rate,
+                                           f2& Dm, f2& R)
+{
+  const f2 chi = c.chi, MU = c.MU, p = c.p;
+  f2 dmf = (xp.chi + chi)*(xp.MU - MU);
+  f2 pd = (xp.p + p)*(xp.chi - chi);
+  dmf = fma(xm.chi + chi, xm.MU - MU, dmf);
+  pd = fma(xm.p + p, xm.chi - chi, pd);
+  dmf = fma(y.chip + chi, y.MUp - MU, dmf);
+  pd = fma(y.pp + p, y.chip - chi, pd);
+  dmf = fma(y.chim + chi, y.MUm - MU, dmf);
+  pd = fma(y.pm + p, y.chim - chi, pd);
+  // twice the divergence of u m
+  const f2 mF2 = (xp.uxm - xm.uxm) + y.uym;
+  // V'(chi) = 2 Achi chi (1 - chi)(1 - 2 chi) + Ochi (phi - phiswitch)
+  const f2 dV = fma(W2(P.A2chi)*chi, (KC(1.f) - chi)*fma(KC(-2.f), chi, KC(1.f)),
+                    W2(P.Ochi)*(p - W2(P.phisw)));
+  R = (chi*p)*rate;
+  // growTogether: chi R, else R
+  const f2 mG = fma(W2(P.gt), chi - KC(1.f), KC(1.f))*R;
+  Dm = fma(W2(P.hGP), dmf, W2(P.hDchi)*pd);
+  Dm = fma(KC(-.5f), mF2, Dm) - p*dV;
+  Dm = Dm + mG;
+}
+
+// m after a sub-step clamped to [0, max(phi after the sub-step, 0)]
+// (src/models/go-or-grow.cpp:378-383)
+__device__ __forceinline__ f2 clamp_m(f2 mt, f2 pt)
+{
+  return mk(fminf(fmaxf(mt.v.x, 0.f), fmaxf(pt.v.x, 0.f)),
+            fminf(fmaxf(mt.v.y, 0.f), fmaxf(pt.v.y, 0.f)));
 }
 
 template<int MODEL>
 __device__ __forceinline__ f2 itau_of(const PP& P, f2 p)
 {
-  return MODEL == LYO ? rcp2(fma(W2(P.dtau), p, W2(P.tauIso)), P) : W2(P.itau);
+  return MODEL != NEM ? rcp2(fma(W2(P.dtau), p, W2(P.tauIso)), P) : W2(P.itau);
 }
 
 // UpdateFields of one row pair up to the node update
@@ -351,7 +443,7 @@ __device__ __forceinline__ void uf2(const PP& P, const UQc& c, const UQx& xp, co
   // twice the force: (d_x s_xx + d_y s_xy - friction u_x), ...
   const f2 Fx2 = fma(W2(P.n2fric), c.ux, (xp.sXX - xm.sXX) + y.sXY);
   const f2 Fy2 = fma(W2(P.n2fric), c.uy, (xp.sYX - xm.sYX) + y.sYY);
-  if constexpr (MODEL == LYO)
+  if constexpr (MODEL != NEM)
   {
     const f2 lMU = fma(KC(-4.f), c.MU, (xp.MU + xm.MU) + y.MUs);
     Dp = fma(W2(P.GammaP), lMU, KC(-.5f)*((xp.uxp - xm.uxp) + y.uyp));
@@ -399,7 +491,7 @@ struct ItemView
 template<int MODEL>
 struct WarpSmem
 {
-  static constexpr int NP = MODEL == LYO ? 12 : 11;
+  static constexpr int NP = MODEL == NEM ? 11 : MODEL == LYO ? 12 : 13;
   static constexpr int FLOATS = RING*NP*RWW + 3*NDP*PW + 2*9*COLS;
 };
 
@@ -414,7 +506,7 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
                                           const int chunk, float* ring, float* dpop, float* hrow,
                                           uint64_t* mbar, const int lane, unsigned& rowbase)
 {
-  constexpr int NP = MODEL == LYO ? 12 : 11;
+  constexpr int NP = MODEL == NEM ? 11 : MODEL == LYO ? 12 : 13;
   const int y0 = strip*WOUT;
   const int x0 = chunk*a.rows;
   const int rows = min(a.rows, a.LX - x0);
@@ -472,13 +564,15 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
   UQc q1c{}, q2c{};
   UQx q1m{}, q2m{};
   UQd dq{};
-  f2 qa1[3], qa2[3], qn1[3], qn2[3];
+  // predicted (Qxx, Qyx, phi, m) and QN (QNxx, QNyx, phn, mN) of the rows
+  // one and two iterations back; m only in go-or-grow
+  f2 qa1[4], qa2[4], qn1[4], qn2[4];
   // Delayed populations live in shared memory: row slot s (the row C
   // produced s iterations ago, mod 3), array k: ff v = 0,3,4 (k = 0..2),
   // fn v = 0,3,4 (3..5), ff v = 1,5,8 (6..8), fn v = 1,5,8 (9..11). C writes
   // them already shifted along y (column + cy); D reads its own columns.
 #pragma unroll
-  for(int k = 0; k < 3; ++k) { qa1[k] = qa2[k] = qn1[k] = qn2[k] = KC(0.f); }
+  for(int k = 0; k < 4; ++k) { qa1[k] = qa2[k] = qn1[k] = qn2[k] = KC(0.f); }
   int s3 = 0;                              // i mod 3
   float* orow = a.out + static_cast<long long>(x0 - 6)*LY + yg;   // E's output row
 
@@ -529,19 +623,20 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
       for(int v = 0; v < 9; ++v) g[v] = lds2(R0 + v*RWW + cl);
       const Stn A = ring_stn(Rm, R0, Rp, 9), B = ring_stn(Rm, R0, Rp, 10);
       Stn Ph{};
-      if constexpr (MODEL == LYO) Ph = ring_stn(Rm, R0, Rp, 11);
+      if constexpr (MODEL != NEM) Ph = ring_stn(Rm, R0, Rp, 11);
+      const f2 m0 = MODEL == GOG ? lds2(R0 + 12*RWW + cl) : KC(0.f);
       UQd unused;
-      uq2<MODEL, false>(P, g, A, B, Ph, nq1, unused);
+      uq2<MODEL, false>(P, g, A, B, Ph, m0, nq1, unused);
     }
 
     // ---- C: predictor UpdateFields at row b-1, then y-part of Move ----
-    f2 nQ[3], nQN[3], pf[9], pn[9];
+    f2 nQ[4], nQN[4], pf[9], pn[9];
     {
       const YD y = ydiffs<MODEL>(q1c);
       const f2 Qxx = lds2(Rm + 9*RWW + cl), Qyx = lds2(Rm + 10*RWW + cl);
-      const f2 p = MODEL == LYO ? lds2(Rm + 11*RWW + cl) : KC(0.f);
-      const f2 tau = MODEL == LYO ? fma(W2(P.dtau), p, W2(P.tauIso)) : W2(P.tauIso);
-      const f2 itau = MODEL == LYO ? rcp2(tau, P) : W2(P.itau);
+      const f2 p = MODEL != NEM ? lds2(Rm + 11*RWW + cl) : KC(0.f);
+      const f2 tau = MODEL != NEM ? fma(W2(P.dtau), p, W2(P.tauIso)) : W2(P.tauIso);
+      const f2 itau = MODEL != NEM ? rcp2(tau, P) : W2(P.itau);
       const f2 hitau = KC(.5f)*itau;
       f2 fe[9], Dxx, Dyx, Dp;
       uf2<MODEL>(P, q1c, xset(nq1), q1m, y, Qxx, Qyx, itau, tau, fe, Dxx, Dyx, Dp);
@@ -562,12 +657,25 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
         nQN[2] = fma(KC(.5f), Dp, p);
         nQ[2] = p + Dp;
         if constexpr (SRC) nQ[2] = fma(p, src_at(x0 - 4 + i), nQ[2]);
+        nQN[3] = nQ[3] = KC(0.f);
+      }
+      else if constexpr (MODEL == GOG)
+      {
+        f2 Dm, R;
+        pheno_rate(P, q1c, xset(nq1), q1m, y, src_at(x0 - 4 + i), Dm, R);
+        const f2 me = lds2(Rm + 12*RWW + cl);
+        nQ[0] = Qxx + Dxx;
+        nQ[1] = Qyx + Dyx;
+        nQN[2] = fma(KC(.5f), Dp, p);
+        nQ[2] = (p + Dp) + R;
+        nQN[3] = fma(KC(.5f), Dm, me);
+        nQ[3] = clamp_m(me + Dm, nQ[2]);
       }
       else
       {
         nQ[0] = Qxx + Dxx;
         nQ[1] = Qyx + Dyx;
-        nQN[2] = nQ[2] = KC(0.f);
+        nQN[2] = nQ[2] = nQN[3] = nQ[3] = KC(0.f);
       }
       // stream along y. Directions with cx = -1 (2, 6, 7) are used by D in
       // this same iteration: shift them by shuffles. The others go to the
@@ -609,8 +717,8 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
       const Stn A = reg_stn(qa1[0], nQ[0], qa2[0]);
       const Stn B = reg_stn(qa1[1], nQ[1], qa2[1]);
       Stn Ph{};
-      if constexpr (MODEL == LYO) Ph = reg_stn(qa1[2], nQ[2], qa2[2]);
-      uq2<MODEL, DIAG>(P, fs, A, B, Ph, nq2, dq);
+      if constexpr (MODEL != NEM) Ph = reg_stn(qa1[2], nQ[2], qa2[2]);
+      uq2<MODEL, DIAG>(P, fs, A, B, Ph, qa1[3], nq2, dq);
       const f2 hitau = KC(-.5f)*itau_of<MODEL>(P, qa1[2]);
 #pragma unroll
       for(int v = 0; v < 9; ++v)
@@ -631,13 +739,15 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
             if(colx_ok) o[k*pl] = vals[k].v.x;
             if(coly_ok) o[k*pl + 1] = vals[k].v.y;
           }
-          if constexpr (MODEL == LYO)
+          if constexpr (MODEL != NEM)
           {
-            const f2 aQxx = dq.nact*qa1[0];
-            // the elastic yx stress carries +zeta*Qxx*(1-phi) as the
-            // reference has it (src/models/lyotropic.cpp:242)
-            const f2 dg[7] = {dq.bi, (dq.sigmaF - dq.pf) - aQxx, (dq.sigmaS - dq.pfS) - aQxx,
-                              dq.pf, dq.pfS, aQxx, dq.nact*qa1[1]};
+            const f2 aQxx = dq.nact*qa1[0], aQyx = dq.nact*qa1[1];
+            // the lyotropic elastic yx stress carries +zeta*Qxx*(1-phi) as
+            // the reference has it (src/models/lyotropic.cpp:242); the
+            // go-or-grow one the Qyx term (src/models/go-or-grow.cpp:300)
+            const f2 dg[7] = {dq.bi, (dq.sigmaF - dq.pf) - aQxx,
+                              (dq.sigmaS - dq.pfS) - (MODEL == GOG ? aQyx : aQxx),
+                              dq.pf, dq.pfS, aQxx, aQyx};
 #pragma unroll
             for(int k = 0; k < 7; ++k)
             {
@@ -653,8 +763,8 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
     if constexpr (!DIAG)
     {
       const YD y = ydiffs<MODEL>(q2c);
-      const f2 tau = MODEL == LYO ? fma(W2(P.dtau), qa2[2], W2(P.tauIso)) : W2(P.tauIso);
-      const f2 itau = MODEL == LYO ? rcp2(tau, P) : W2(P.itau);
+      const f2 tau = MODEL != NEM ? fma(W2(P.dtau), qa2[2], W2(P.tauIso)) : W2(P.tauIso);
+      const f2 itau = MODEL != NEM ? rcp2(tau, P) : W2(P.itau);
       const f2 hitau = KC(.5f)*itau;
       f2 fe[9], Dxx, Dyx, Dp;
       uf2<MODEL>(P, q2c, xset(nq2), q2m, y, qa2[0], qa2[1], itau, tau, fe, Dxx, Dyx, Dp);
@@ -667,6 +777,14 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
       f2 Qo2 = fma(KC(.5f), Dp, qn2[2]);
       // corrector source with the predicted phi of this row
       if constexpr (SRC) Qo2 = fma(qa2[2], src_at(x0 - 6 + i), Qo2);
+      f2 Qo3 = KC(0.f);
+      if constexpr (MODEL == GOG)
+      {
+        f2 Dm, R;
+        pheno_rate(P, q2c, xset(nq2), q2m, y, src_at(x0 - 6 + i), Dm, R);
+        Qo2 = Qo2 + R;
+        Qo3 = clamp_m(fma(KC(.5f), Dm, qn2[3]), Qo2);
+      }
       if(i >= 6)
       {
         const long long pl = a.plane;
@@ -677,7 +795,8 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
           for(int v = 0; v < 9; ++v) *reinterpret_cast<float2*>(o + v*pl) = gout[v].v;
           *reinterpret_cast<float2*>(o + 9*pl) = Qo0.v;
           *reinterpret_cast<float2*>(o + 10*pl) = Qo1.v;
-          if constexpr (MODEL == LYO) *reinterpret_cast<float2*>(o + 11*pl) = Qo2.v;
+          if constexpr (MODEL != NEM) *reinterpret_cast<float2*>(o + 11*pl) = Qo2.v;
+          if constexpr (MODEL == GOG) *reinterpret_cast<float2*>(o + 12*pl) = Qo3.v;
         }
         else if(colx_ok)
         {
@@ -685,7 +804,8 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
           for(int v = 0; v < 9; ++v) o[v*pl] = gout[v].v.x;
           o[9*pl] = Qo0.v.x;
           o[10*pl] = Qo1.v.x;
-          if constexpr (MODEL == LYO) o[11*pl] = Qo2.v.x;
+          if constexpr (MODEL != NEM) o[11*pl] = Qo2.v.x;
+          if constexpr (MODEL == GOG) o[12*pl] = Qo3.v.x;
         }
       }
     }
@@ -694,7 +814,7 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
     q1m = xset(q1c); q1c = nq1;
     q2m = xset(q2c); q2c = nq2;
 #pragma unroll
-    for(int k = 0; k < 3; ++k)
+    for(int k = 0; k < 4; ++k)
     {
       qa2[k] = qa1[k]; qa1[k] = nQ[k];
       qn2[k] = qn1[k]; qn1[k] = nQN[k];
@@ -904,6 +1024,12 @@ cudaError_t launch_fused_warp_step(const FusedArgs& a, int model, int rows, bool
     if(a.src)
       return diag ? launch_t<LYO, true, true>(a, rows, st) : launch_t<LYO, false, true>(a, rows, st);
     return diag ? launch_t<LYO, true, false>(a, rows, st) : launch_t<LYO, false, false>(a, rows, st);
+  }
+  if(model == GOG)
+  {
+    // the growth-rate plane is part of every go-or-grow step
+    if(!a.src) return cudaErrorInvalidValue;
+    return diag ? launch_t<GOG, true, false>(a, rows, st) : launch_t<GOG, false, false>(a, rows, st);
   }
   return diag ? launch_t<NEM, true, false>(a, rows, st) : launch_t<NEM, false, false>(a, rows, st);
 }

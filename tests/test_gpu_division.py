@@ -115,11 +115,26 @@ def test_fp32_fused_division_within_tolerance():
         lat.close()
 
 
+def test_conserve_phi_moves_a_fused_lattice_to_the_sweeps():
+    """conserve_phi needs a lattice-wide phi sum inside each sub-step, which
+    the one-launch fused step has not: switching it on hands the FP32 state
+    to the unfused sweeps, which hold phi at the given total."""
+    p = params(alpha=0.0, beta=0.0)
+    st = O.synthetic_state(O.LYOTROPIC, 64, 64, seed=12, flow=0.01)
+    a = M.Lattice(M.LYOTROPIC, p, 64, 64, 0, M.FP32)
+    assert a.uses_fused
+    a.upload_state(st)
+    a.step(2)
+    total = float(a.get("phi").sum())
+    a.set_phi_conservation(True, total)
+    assert not a.uses_fused
+    a.step(20)
+    assert abs(a.get("phi").sum() - total) < 1e-4 * total
+    a.close()
+
+
 def test_unsupported_combinations_are_rejected():
     p = params()
-    a = M.Lattice(M.LYOTROPIC, p, 64, 64, 0, M.FP32)
-    with pytest.raises(M.MassLBError):
-        a.set_phi_conservation(True, 1.0)
     n = M.Lattice(M.NEMATIC, {"Gamma": 0.3, "xi": 0.7, "tau": 1.5, "CC": 0.1, "LL": 0.05},
                   64, 64, 0, M.FP64)
     with pytest.raises(M.MassLBError):
@@ -130,9 +145,11 @@ def test_unsupported_combinations_are_rejected():
     ens.runs[0].set_phi_source(np.full(64 * 64, 0.01))
     with pytest.raises(M.MassLBError):
         ens.step(1)
+    with pytest.raises(M.MassLBError):
+        ens.runs[0].set_phi_conservation(True, 1.0)
     ens.runs[0].set_phi_source(None)
     ens.step(1)
-    for x in (a, n, ens):
+    for x in (n, ens):
         x.close()
 
 
