@@ -437,8 +437,10 @@ def run_ours_gog(args):
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind, "bytes_per_site": bps,
                 "traffic": None,
-                "note": "whole step (one sub-step kernel per predictor and corrector) against "
-                        "the primary state's bytes; small lattices are latency-bound"}
+                "note": ("whole step in one fused launch" if lat.uses_fused else
+                         "whole step (one sub-step kernel per predictor and corrector)") +
+                        " against the primary state's bytes (13 planes); lattices whose state "
+                        "fits in L2 are latency-bound"}
     lat.close()
 
     # end to end: the driver on the runcard (host masks, Configure excluded),
