@@ -294,19 +294,25 @@ def training_params(zeta: float) -> dict:
     return p
 
 
-def initial_state(L: int, rng: np.random.Generator) -> dict:
+def initial_state(L: int, rng: np.random.Generator, phi: str = "disk") -> dict:
+    """Random director (S = 1) and either a tanh phi disk of radius L/4
+    (phi="disk") or phi ~ N(0.5, 0.05) i.i.d. (phi="random")."""
     from .run_case import REST
     theta = rng.uniform(0.0, np.pi, L * L)
-    x = np.arange(L)[:, None] - L / 2
-    y = np.arange(L)[None, :] - L / 2
-    r = np.sqrt(x * x + y * y).reshape(-1)
-    return {"QQxx": np.cos(2 * theta), "QQyx": np.sin(2 * theta),
-            "ff": np.tile(REST * 40.0, (L * L, 1)),
-            "phi": 0.5 * (1 - np.tanh((r - L / 4) / 2))}
+    st = {"QQxx": np.cos(2 * theta), "QQyx": np.sin(2 * theta),
+          "ff": np.tile(REST * 40.0, (L * L, 1))}
+    if phi == "random":
+        st["phi"] = rng.normal(0.5, 0.05, L * L)
+    else:
+        x = np.arange(L)[:, None] - L / 2
+        y = np.arange(L)[None, :] - L / 2
+        r = np.sqrt(x * x + y * y).reshape(-1)
+        st["phi"] = 0.5 * (1 - np.tanh((r - L / 4) / 2))
+    return st
 
 
 def generate_dataset(ntraj=40, L=256, pairs=50, jump=50, t_min=2000, t_max=22000, seed=0,
-                     zeta_range=(0.005, 0.03)):
+                     zeta_range=(0.005, 0.03), phi="disk"):
     """Simulate ntraj lattices together (one ensemble) and record the raw
     fields of `pairs` (t, t+jump) pairs per trajectory, t evenly spaced over
     [t_min, t_max). Returns (fields [ntraj*2*pairs, L, L, 5] device fp32,
@@ -315,7 +321,7 @@ def generate_dataset(ntraj=40, L=256, pairs=50, jump=50, t_min=2000, t_max=22000
     zetas = rng.uniform(*zeta_range, ntraj)
     ens = lb.Ensemble(lb.LYOTROPIC, [training_params(z) for z in zetas], [(L, L)] * ntraj)
     for run in ens.runs:
-        run.upload_state(initial_state(L, rng))
+        run.upload_state(initial_state(L, rng, phi))
     per = 2 * pairs
     fields = torch.empty((ntraj * per, L, L, NF), dtype=torch.float32, device="cuda")
     zero, one = np.zeros(NF), np.ones(NF)
@@ -460,6 +466,121 @@ def hybrid(params: Params, ens: lb.Ensemble, steps: int, jump=50, M=10, threshol
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     net.check_error_flag()
+    return {"steps": t, "wall_s": wall, "surrogate_jumps": taken, "plain_jumps_rejected": rejected,
+            "checks": checks, "nonfinite_rollouts": nonfinite, "check_errors": errors,
+            "samples": samples}
+
+
+# -- one large lattice, tile by tile --------------------------------------------
+
+RECEPTIVE = 2 * NBLOCKS + 2   # sites one forward pass reaches: 14 3x3 convolutions
+
+
+class TiledSurrogate:
+    """The surrogate applied to one large periodic lattice tile by tile.
+
+    Each tile x tile interior is predicted from a (tile + 2 halo)^2 window
+    cut from the lattice's fields with circular indices. The network pads
+    every image circularly, so the window's own wrap reaches RECEPTIVE
+    sites into it; with halo >= RECEPTIVE the interior sees only true
+    neighbours, and the interiors together equal the network applied to the
+    whole torus. `batch` windows go through the network at once."""
+
+    def __init__(self, params: Params, LX: int, LY: int, tile: int = 1024, halo: int = 64,
+                 batch: int = 8):
+        if halo < RECEPTIVE:
+            raise ValueError(f"halo must be at least {RECEPTIVE}")
+        if LX % tile or LY % tile:
+            raise ValueError("the lattice must be a whole number of tiles")
+        self.P, self.LX, self.LY, self.T, self.h = params, LX, LY, tile, halo
+        W = tile + 2 * halo
+        self.W = W
+        self.batch = batch
+        self.net = Net(params, batch, W, W, train=False)
+        self.cur = torch.empty((LX, LY, NF), dtype=torch.float32, device="cuda")
+        self.pred = torch.empty_like(self.cur)
+        self.win = torch.empty((batch, W, W, NF), dtype=torch.float32, device="cuda")
+        self.tiles = [(tx, ty) for tx in range(LX // tile) for ty in range(LY // tile)]
+        self.idx = np.arange(batch)
+
+    def _rows(self, t0, n):
+        return (torch.arange(-self.h, self.T + self.h, device="cuda") + t0) % n
+
+    def predict(self, cur: torch.Tensor, out: torch.Tensor):
+        """out <- the network's prediction for the normalised fields cur
+        [LX, LY, 5], window by window."""
+        T, h = self.T, self.h
+        for b0 in range(0, len(self.tiles), self.batch):
+            chunk = self.tiles[b0:b0 + self.batch]
+            for k, (tx, ty) in enumerate(chunk):
+                rows = self._rows(tx * T, self.LX)
+                cols = self._rows(ty * T, self.LY)
+                self.win[k].copy_(cur.index_select(0, rows).index_select(1, cols))
+            self.net.pack(self.win, self.idx)
+            p = self.net.forward()
+            for k, (tx, ty) in enumerate(chunk):
+                out[tx * T:(tx + 1) * T, ty * T:(ty + 1) * T].copy_(p[k, h:h + T, h:h + T])
+        return out
+
+
+def hybrid_tiled(params: Params, lat: lb.Lattice, steps: int, jump=50, M=10, threshold=0.5,
+                 stats_every=None, tiler: TiledSurrogate = None):
+    """hybrid() for one large lattice: every M jumps the plain method runs
+    one jump while the tiled surrogate predicts it; if the surrogate's error
+    relative to the plain change is below `threshold` it takes the next M-1
+    jumps (the lattice rebuilt from its fields with equilibrium
+    populations), else the plain method does. Returns wall time, jumps per
+    method, the check errors and statistics samples every stats_every steps."""
+    tiler = tiler or TiledSurrogate(params, lat.LX, lat.LY)
+    cur, pred = tiler.cur, tiler.pred
+    after = torch.empty_like(cur)
+    t = 0
+    taken = rejected = checks = nonfinite = 0
+    errors, samples = [], []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    # The lattice steps on its own stream and the field conversions run on
+    # torch's: each hand-over waits for the other side (a read of the state
+    # before its steps have finished would see the old state).
+    while t < steps:
+        lat.synchronize()
+        fields_from_lattice(lat, cur, params.mean, params.scale)
+        tiler.predict(cur, pred)
+        torch.cuda.current_stream().synchronize()
+        lat.step(jump)
+        lat.synchronize()
+        fields_from_lattice(lat, after, params.mean, params.scale)
+        err = float((torch.linalg.vector_norm(pred - after) /
+                     torch.linalg.vector_norm(after - cur).clamp_min(1e-12)).item())
+        errors.append(err)
+        checks += 1
+        accepted = False
+        if err < threshold:
+            # roll the surrogate M - 1 jumps on from the plain state,
+            # ping-ponging two scratch buffers
+            a, b = after, pred
+            for _ in range(M - 1):
+                tiler.predict(a, b)
+                a, b = b, a
+            if bool(torch.isfinite(a).all().item()):
+                lattice_from_fields(lat, a, params.mean, params.scale)
+                torch.cuda.current_stream().synchronize()
+                taken += M - 1
+                accepted = True
+            else:
+                nonfinite += 1
+            after, pred = a, b
+        if not accepted:
+            torch.cuda.current_stream().synchronize()
+            lat.step(jump * (M - 1))
+            rejected += M - 1
+        t += jump * M
+        if stats_every and t % stats_every == 0:
+            samples.append((t, lat.statistics()))
+    lat.synchronize()
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    tiler.net.check_error_flag()
     return {"steps": t, "wall_s": wall, "surrogate_jumps": taken, "plain_jumps_rejected": rejected,
             "checks": checks, "nonfinite_rollouts": nonfinite, "check_errors": errors,
             "samples": samples}

@@ -295,3 +295,55 @@ def test_short_training_lowers_the_loss():
     P = G.Params(seed=1)
     losses = G.train(P, F, pairs, epochs=30, batch=B, lr=2e-3)
     assert losses[-1] < 0.3 * losses[0], losses
+
+
+def test_tiled_prediction_equals_the_whole_torus():
+    """TiledSurrogate: windows of tile + 2*halo with circular halos give,
+    on their interiors, what the network gives applied to the whole
+    periodic lattice at once (the halo covers the 14-site receptive
+    field)."""
+    torch.manual_seed(3)
+    P = G.Params(seed=4)
+    P.mean = np.zeros(G.NF, dtype=np.float32)
+    P.scale = np.ones(G.NF, dtype=np.float32)
+    L = 512
+    cur = torch.randn((L, L, G.NF), device="cuda") * 0.5
+    whole = G.Net(P, 1, L, L, train=False)
+    whole.pack(cur[None].contiguous(), np.array([0]))
+    want = whole.forward()[0].clone()
+    tiler = G.TiledSurrogate(P, L, L, tile=256, halo=64, batch=2)
+    got = tiler.predict(cur, torch.empty_like(cur))
+    err = (got - want).abs().max().item()
+    assert err <= 1e-6 * want.abs().max().item(), err
+    with pytest.raises(ValueError):
+        G.TiledSurrogate(P, L, L, tile=256, halo=8)
+
+
+def test_tiled_hybrid_at_threshold_zero_is_plain_lb():
+    """hybrid_tiled with threshold 0 never accepts a surrogate jump: the
+    lattice ends bit-identical to the plain method stepped as long, and
+    every check error is an honest ratio (a read of the state before its
+    steps had finished would give ratios near 1e12)."""
+    from oracle import oracle as O
+    from mass_hd_b200 import lb
+    from mass_hd_b200.run_case import PARAMS
+    L = 512
+    P = G.Params(seed=2)
+    st = O.synthetic_state(O.LYOTROPIC, L, L, seed=5, flow=0.02)
+    a = lb.Lattice(lb.LYOTROPIC, PARAMS["lyotropic"], L, L, 0, lb.FP32)
+    b = lb.Lattice(lb.LYOTROPIC, PARAMS["lyotropic"], L, L, 0, lb.FP32)
+    for x in (a, b):
+        x.set_tile(32, 64)
+        x.upload_state(st)
+        x.step(20)
+    P.mean = np.zeros(G.NF, dtype=np.float32)
+    P.scale = np.ones(G.NF, dtype=np.float32)
+    tiler = G.TiledSurrogate(P, L, L, tile=256, halo=64, batch=4)
+    res = G.hybrid_tiled(P, a, 200, jump=20, M=5, threshold=0.0, tiler=tiler)
+    b.step(200)
+    assert res["surrogate_jumps"] == 0 and res["checks"] == 2
+    assert all(0 < e < 1e6 for e in res["check_errors"]), res["check_errors"]
+    for n in ("ff", "QQxx", "QQyx", "phi"):
+        assert np.array_equal(a.get(n), b.get(n)), n
+    a.close()
+    b.close()
