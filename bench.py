@@ -28,7 +28,9 @@ step (strong scaling).
 
 The line also carries `fp64`: the FP64 mode (bit-identical to the
 reference's double-precision build) timed on the same seeded lattice, the
-like-for-like counterpart of the reference's FP64 CPU build.
+like-for-like counterpart of the reference's FP64 CPU build; and
+`ensemble`: the 96-run batched sweep against the same runs one after
+another (a bounded sample of 200 steps per run).
 
 --impl reference times the reference's own OpenMP build of the same step
 (oracle/_ref, compiled from the reference sources) on the host cores, on a
@@ -538,6 +540,25 @@ def fp64_record(model: str, st: dict, L: int, steps: int, warmup: int, world: in
                     "the same seeded lattice: one sub-step kernel per predictor and corrector"}
 
 
+def ensemble_record(steps: int = 200, nruns: int = 96) -> dict:
+    """The batched ensemble (configuration 3: 96 lyotropic runs, L from
+    {128, 192, 256, 384, 512}, zeta, LL and xi swept, FP32) against the same
+    runs stepped one after another through mass_lb_step, on a bounded
+    sample of `steps` steps per run (the configuration runs 10k). Both from
+    the same seeded states, device-synchronised wall clock; the states must
+    come out bit-identical."""
+    from mass_hd_b200 import ensemble_case as E
+    r = E.compare(nruns, steps)
+    return {"runs": nruns, "steps_per_run": steps, "sites": r["sites"],
+            "batched_site_updates_per_s": r["batched_site_updates_per_s"],
+            "sequential_site_updates_per_s": r["sequential_site_updates_per_s"],
+            "speedup": r["speedup"], "bit_identical": r["bit_identical"],
+            "chunk_rows": r["ensemble_rows"],
+            "note": "one persistent warp-strip launch per step for all runs, replayed from a "
+                    "CUDA graph, against mass_lb_step per run with its own autotuned tile; "
+                    f"{steps} steps per run as a bounded sample of the 10k-step sweep"}
+
+
 def run_ours_slab(args):
     """--decomp slab: ONE lattice of size^2 split into x-slabs over the ranks
     (strong scaling), halo rows exchanged before every step over NCCL
@@ -738,6 +759,9 @@ def run_ours(args):
     fp64 = None
     if args.precision == "fp32" and not args.no_fp64:
         fp64 = fp64_record(model, st, L, min(args.steps, 20), 3, world)
+    ens = None
+    if model == "lyotropic" and world == 1 and not args.no_ensemble:
+        ens = ensemble_record()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -765,6 +789,7 @@ def run_ours(args):
             "e2e": e2e,
             "cpu_baseline": cpu,
             "fp64": fp64,
+            "ensemble": ens,
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
@@ -789,6 +814,8 @@ def main():
     ap.add_argument("--decomp", default="independent", choices=["independent", "slab"],
                     help="independent: a lattice per rank (weak scaling, default); slab: one "
                          "lattice split into x-slabs over the ranks (strong scaling)")
+    ap.add_argument("--no-ensemble", action="store_true",
+                    help="skip the batched-ensemble record beside the lyotropic line")
     ap.add_argument("--no-fp64", action="store_true",
                     help="skip the FP64-mode record beside the FP32 line")
     args = ap.parse_args()
