@@ -202,3 +202,37 @@ def test_step_errors_surface_in_runtime_checks(tmp_path):
     runcard(card, "lyotropic", opts)
     r = subprocess.run([DRIVER, str(card), "-o", str(tmp_path / "o")], capture_output=True, text=True)
     assert r.returncode == 1 and "precision 'fp16' unknown" in r.stderr
+
+
+def test_fp32_go_or_grow_driver_tracks_fp64(tmp_path):
+    """mass-gpu on a go-or-grow runcard in FP32, the fused one-launch step on
+    this periodic lattice (relaxation on the sweeps, masks drawn on the
+    device from the reference's stream), against the same runcard in FP64:
+    every frame field within FP32 tolerance after 8 steps."""
+    gog = {"B": 0.1, "Snem": 1.0, "Dchi": 0.01, "Achi": 0.1, "Ochi": 0.05,
+           "phiswitch": 0.5, "growTogether": 0, "chi0": 0.6, "chi-noise": 0.05,
+           "chi-length": 1.5, "relax-steps": 20, "relax-dt": 1.0, "relax-phi": 1,
+           "relax-Q": 1, "alpha": 0.01, "beta": 0.005, "division-rate": 0.6,
+           "division-time": 1, "division-radius": 2.5, "death-rate": 0.3,
+           "death-time": 2, "death-radius": 1.5, "phi-critical": 0.9, "chi-config": "noise"}
+    frames = {}
+    for prec in ("fp32", "fp64"):
+        opts = dict(LYO, config="circle", radius=20, level=0.0, conc=1.0, angle=0.0, noise=1.0,
+                    zeta=0.02)
+        opts.update(gog)
+        opts.update(LX=64, LY=64, nsteps=8, ninfo=8, seed=11, precision=prec)
+        card = tmp_path / f"{prec}.dat"
+        runcard(card, "go-or-grow", opts)
+        run(card, tmp_path / prec)
+        frames[prec] = load_frame(tmp_path / prec / "frame8.json")
+    a, b = frames["fp32"], frames["fp64"]
+    for k in ("QQxx", "QQyx", "phi", "m", "chi", "division_mask", "death_mask"):
+        assert k in a, k
+    for k in ("division_mask", "death_mask"):
+        assert np.array_equal(a[k], b[k]), k
+    rest = np.array([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4) * 40.0
+    for k in ("ff", "QQxx", "QQyx", "phi", "m"):
+        x, y = a[k], b[k]
+        if k == "ff":
+            x, y = x.reshape(-1, 9) - rest, y.reshape(-1, 9) - rest
+        assert np.linalg.norm(x - y) <= 1e-4 * np.linalg.norm(y), k
