@@ -438,7 +438,9 @@ def run_ours_gog(args):
     achieved = sites * bps / (ms_per_step / 1e3) / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind, "bytes_per_site": bps,
-                "traffic": None,
+                "traffic": (traffic_per_site("go-or-grow", args.precision) * sites
+                            if lat.uses_fused and traffic_per_site("go-or-grow", args.precision)
+                            else None),
                 "note": ("whole step in one fused launch" if lat.uses_fused else
                          "whole step (one sub-step kernel per predictor and corrector)") +
                         " against the primary state's bytes (13 planes); lattices whose state "
