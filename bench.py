@@ -710,52 +710,73 @@ def run_ours(args):
     dt = time.perf_counter() - t0
     dt_serial = max_over_ranks(dt, world)
 
-    # The same jobs on two handles, so that one job's transfers overlap the
-    # other's steps: handle X uploads while handle Y steps, then Y's result
-    # comes down while X steps. Every job still uploads its input from
-    # pinned host memory and downloads its result.
-    lat2 = M.Lattice(mcode, params, L, L, 0, prec)
-    if lat.uses_fused:
-        lat2.set_tile(*lat.tile())
-    outs2 = {}
-    for k, a in host.items():
-        o, t = pinned_copy(np.zeros_like(a))
-        outs2[k] = o
-        keep.append(t)
-    lats, outsets = (lat, lat2), (outs, outs2)
+    # The same jobs pipelined over NBUF handles: each job's upload and the
+    # previous job's download run on their handles' transfer streams while
+    # another handle steps, and mass_lb_stream_wait keeps the runs of steps
+    # one after another on the device, so each has the whole GPU. Every job
+    # still uploads its input from pinned host memory and downloads its
+    # result into pinned host memory; the host reuses a handle (and its
+    # output buffers) only after synchronizing on it.
+    NBUF = 3
+    lats = [lat] + [M.Lattice(mcode, params, L, L, 0, prec) for _ in range(NBUF - 1)]
+    outsets = [outs]
+    for x in lats[1:]:
+        if lat.uses_fused:
+            x.set_tile(*lat.tile())
+        o2 = {}
+        for k, a in host.items():
+            o, t = pinned_copy(np.zeros_like(a))
+            o2[k] = o
+            keep.append(t)
+        outsets.append(o2)
 
-    def upload(x):
-        x.upload(host["ff"], host["QQxx"], host["QQyx"], host.get("phi"))
+    def upload_async(x):
+        x.upload_async(host["ff"], host["QQxx"], host["QQyx"], host.get("phi"))
 
-    upload(lat2)
-    lat2.step(NINFO)                 # warm-up of the second handle
-    lat2.synchronize()
-    n_pipe = 8
+    def download_async(i):
+        for k, o in outsets[i].items():
+            lats[i].get_into_async(k, o)
+
+    def pipeline(njobs):
+        for j in range(njobs):
+            i = j % NBUF
+            x = lats[i]
+            if j >= NBUF:
+                x.synchronize()                    # job j - NBUF has landed
+            upload_async(x)                        # beside the previous job's steps
+            if j < NBUF - 1:
+                # filling the pipeline: one upload at a time, so that the
+                # first job's input is not slowed by the next ones' sharing
+                # the host link (the GPU steps the previous job meanwhile)
+                x.synchronize()
+            if j > 0:
+                x.wait_for(lats[(j - 1) % NBUF])   # steps after the previous job's
+            x.step(NINFO)
+            if j > 0:
+                download_async((j - 1) % NBUF)     # beside this job's steps
+        download_async((njobs - 1) % NBUF)
+        for x in lats:
+            x.synchronize()
+
+    pipeline(NBUF)                   # warm-up of every handle
+    n_pipe = 16
     barrier(world)
     t0 = time.perf_counter()
-    upload(lats[0])
-    lats[0].step(NINFO)              # asynchronous
-    for j in range(1, n_pipe):
-        cur, prev = lats[j % 2], lats[(j - 1) % 2]
-        upload(cur)                  # overlaps prev's steps
-        cur.step(NINFO)
-        for k, o in outsets[(j - 1) % 2].items():
-            prev.get_into(k, o)      # waits for prev; overlaps cur's steps
-    last = (n_pipe - 1) % 2
-    for k, o in outsets[last].items():
-        lats[last].get_into(k, o)
+    pipeline(n_pipe)
     dt = time.perf_counter() - t0
     dt_pipe = max_over_ranks(dt, world)
-    lat2.close()
+    for x in lats[1:]:
+        x.close()
     e2e = {"value": whole_job_rate(sites, world, NINFO * n_pipe, dt_pipe * 1e3), "unit": UNIT,
            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-           "steps_per_e2e_step": NINFO, "e2e_steps": n_pipe,
+           "steps_per_e2e_step": NINFO, "e2e_steps": n_pipe, "handles": NBUF,
            "serial_value": whole_job_rate(sites, world, NINFO * n_e2e, dt_serial * 1e3),
            "note": "per e2e step (a job): upload the state from pinned host memory, 100 Step() "
-                   "calls, download ff/QQxx/QQyx/phi, through the C ABI; jobs alternate between "
-                   "two handles so that one job's transfers overlap the other's steps; "
-                   "serial_value: the same jobs one after another on one handle; host wall "
-                   "clock"}
+                   "calls, download ff/QQxx/QQyx/phi into pinned host memory, through the C "
+                   "ABI; jobs rotate over 3 handles with asynchronous transfers and "
+                   "mass_lb_stream_wait ordering the runs of steps, the first upload and the "
+                   "last download inside the timed region; serial_value: the same jobs one "
+                   "after another on one handle with synchronous calls; host wall clock"}
     launches_e2e = n_pipe * NINFO * lat.launches_per_step
 
     fp64 = None

@@ -104,7 +104,11 @@ int mass_lb_state_sums_noalloc(const float* planes, long long plane_stride, int 
  * comes down while a third steps. Both take pinned host buffers only
  * (MASS_LB_EINVAL otherwise) and are ordered on the handle's stream with
  * its steps. The host buffers must stay untouched, and `out` unread, until
- * mass_lb_synchronize returns.
+ * mass_lb_synchronize returns. The copies and their FP64<->FP32 conversion
+ * kernels run on a transfer stream of the device's highest priority that
+ * is forked from the handle's stream and joined back to it, so that they
+ * take the SMs ahead of other handles' queued steps; the order seen on the
+ * handle's stream is unchanged.
  *
  * mass_lb_upload_async: mass_lb_upload's work. The totals of the new state
  * (mass_lb_initial_totals) are computed on the stream too and read when
@@ -120,6 +124,14 @@ int mass_lb_state_sums_noalloc(const float* planes, long long plane_stride, int 
 int mass_lb_upload_async(mass_lb_handle* h, const double* ff, const double* QQxx,
                          const double* QQyx, const double* phi);
 int mass_lb_download_async(mass_lb_handle* h, int field, double* out);
+
+/* Device-side order between two handles, without a wait on the host: the
+ * work queued on `h` after this call starts only when the work queued on
+ * `before` up to this call has finished. A pipeline over several lattices
+ * uses it to keep their steps one after another (each run of steps then has
+ * the whole GPU) while the other lattices' transfers run beside them. The
+ * handles may be on different devices; h == before is a no-op. */
+int mass_lb_stream_wait(mass_lb_handle* h, mass_lb_handle* before);
 
 /* ---- rows of the primary state: domain decomposition ------------------------
  * The reference runs one lattice in one process (its only mention of MPI is

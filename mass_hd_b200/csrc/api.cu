@@ -48,7 +48,7 @@ const char* kFieldNames[MASS_LB_NUM_FIELDS] = {
   "sigma_phase_field_xx", "sigma_phase_field_yx", "sigma_active_xx",
   "sigma_active_yx", "fn", "QNxx", "QNyx", "phn", "m", "chi", "mN"};
 
-constexpr long long kStageSites = 1ll << 22;   // sites per transfer chunk
+constexpr long long kStageSites = 1ll << 24;   // sites per transfer chunk
 
 // --------------------------------------------------------------------------
 // host <-> device conversion kernels (one chunk of whole rows at a time)
@@ -146,6 +146,15 @@ struct mass_lb_handle
   Params P{};
   Dims d{};
   cudaStream_t stream = nullptr;
+  // Host<->device transfers of whole fields run on `xfer`, a stream of the
+  // device's highest priority, forked from `stream` and joined back to it by
+  // two events, so that their conversion kernels take the SMs ahead of other
+  // handles' queued steps. `io` is the stream the transfer code issues on:
+  // `xfer` inside an XferScope, `stream` elsewhere.
+  cudaStream_t xfer = nullptr;
+  cudaEvent_t xfer_in = nullptr, xfer_out = nullptr;
+  cudaStream_t io = nullptr;
+  cudaEvent_t order_ev = nullptr;   // mass_lb_stream_wait's mark on this stream
   bool fused = false;
   bool in_ensemble = false;  // a run of a mass_lb_ensemble (its buffers step there)
 
@@ -533,6 +542,16 @@ int mass_lb_create(const mass_lb_params* params, unsigned LX, unsigned LY,
   auto bail = [&](int r) { mass_lb_destroy(h); return r; };
   if(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
     return bail(fail(MASS_LB_ECUDA, "stream create"));
+  h->io = h->stream;
+  {
+    int least = 0, greatest = 0;
+    if(cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess ||
+       cudaStreamCreateWithPriority(&h->xfer, cudaStreamNonBlocking, greatest) != cudaSuccess ||
+       cudaEventCreateWithFlags(&h->xfer_in, cudaEventDisableTiming) != cudaSuccess ||
+       cudaEventCreateWithFlags(&h->xfer_out, cudaEventDisableTiming) != cudaSuccess ||
+       cudaEventCreateWithFlags(&h->order_ev, cudaEventDisableTiming) != cudaSuccess)
+      return bail(fail(MASS_LB_ECUDA, "transfer stream create"));
+  }
 
   if(int r = dalloc(h, &h->err, 1)) return bail(r);
   if(int r = dalloc(h, &h->red_scratch, sums_scratch_doubles())) return bail(r);
@@ -624,6 +643,10 @@ void mass_lb_destroy(mass_lb_handle* h)
   if(h->tot_host) cudaFreeHost(h->tot_host);
   if(h->tot_ev) cudaEventDestroy(h->tot_ev);
   if(h->mq_copy) cudaStreamDestroy(h->mq_copy);
+  if(h->xfer) { cudaStreamSynchronize(h->xfer); cudaStreamDestroy(h->xfer); }
+  if(h->xfer_in) cudaEventDestroy(h->xfer_in);
+  if(h->xfer_out) cudaEventDestroy(h->xfer_out);
+  if(h->order_ev) cudaEventDestroy(h->order_ev);
   if(h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
@@ -647,6 +670,33 @@ static int settle_derived(mass_lb_handle* h)
   return 0;
 }
 
+// One field transfer on the handle's high-priority transfer stream: it
+// starts after the work queued on the step stream before it, and the step
+// stream waits for it, so the order the caller sees on the handle's stream
+// is unchanged. Only the conversion kernels and copies move; what follows
+// the transfer is queued on the step stream again.
+struct XferScope
+{
+  mass_lb_handle* h;
+  explicit XferScope(mass_lb_handle* hh) : h(hh)
+  {
+    if(cudaEventRecord(h->xfer_in, h->stream) == cudaSuccess &&
+       cudaStreamWaitEvent(h->xfer, h->xfer_in, 0) == cudaSuccess)
+      h->io = h->xfer;
+  }
+  ~XferScope()
+  {
+    if(h->io == h->xfer)
+    {
+      cudaEventRecord(h->xfer_out, h->xfer);
+      cudaStreamWaitEvent(h->stream, h->xfer_out, 0);
+    }
+    h->io = h->stream;
+  }
+  XferScope(const XferScope&) = delete;
+  XferScope& operator=(const XferScope&) = delete;
+};
+
 // ff_raw: FP32 populations given as the deviations from t_v*rho the FP32
 // state holds (a checkpoint's exact values), not as populations
 static int put_field(mass_lb_handle* h, int field, const double* src, bool ff_raw = false)
@@ -657,24 +707,26 @@ static int put_field(mass_lb_handle* h, int field, const double* src, bool ff_ra
   const bool isff = field == MASS_LB_FF;
   const int comps = isff ? 9 : 1;
   const double rest = f64 || ff_raw ? 0.0 : h->P.rho;
+  {
+  XferScope scope(h);   // joined before the chi update below
   for(long long x0 = 0; x0 < h->LX; x0 += rows_per)
   {
     const int nrows = static_cast<int>(std::min<long long>(rows_per, h->LX - x0));
     const long long n = static_cast<long long>(nrows)*LY;
     CU(cudaMemcpyAsync(h->stage, src + x0*LY*comps, n*comps*sizeof(double),
-                       cudaMemcpyHostToDevice, h->stream), "upload copy");
+                       cudaMemcpyHostToDevice, h->io), "upload copy");
     const int nb = blocks_for(n);
     if(h->fused)
     {
       const long long plane = static_cast<long long>(h->LX)*h->LY;
       float* base = h->cur;
       if(isff)
-        k_put_ff<float><<<nb, 256, 0, h->stream>>>(h->stage, base, plane, x0, nrows, LY, 0, LY, rest);
+        k_put_ff<float><<<nb, 256, 0, h->io>>>(h->stage, base, plane, x0, nrows, LY, 0, LY, rest);
       else
       {
         const int p = field == MASS_LB_QQXX ? 9 : field == MASS_LB_QQYX ? 10
                     : field == MASS_LB_M ? 12 : 11;
-        k_put_scalar<float><<<nb, 256, 0, h->stream>>>(h->stage, base + p*plane, x0, nrows, LY, 0, LY);
+        k_put_scalar<float><<<nb, 256, 0, h->io>>>(h->stage, base + p*plane, x0, nrows, LY, 0, LY);
       }
     }
     else if(f64)
@@ -682,18 +734,19 @@ static int put_field(mass_lb_handle* h, int field, const double* src, bool ff_ra
       State<double>& s = h->s64;
       double* a = field == MASS_LB_QQXX ? s.Qxx : field == MASS_LB_QQYX ? s.Qyx
                 : field == MASS_LB_M ? s.m : s.phi;
-      if(isff) k_put_ff<double><<<nb, 256, 0, h->stream>>>(h->stage, s.ff, h->d.NE, x0, nrows, LY, h->d.g, h->d.EY, 0.0);
-      else k_put_scalar<double><<<nb, 256, 0, h->stream>>>(h->stage, a, x0, nrows, LY, h->d.g, h->d.EY);
+      if(isff) k_put_ff<double><<<nb, 256, 0, h->io>>>(h->stage, s.ff, h->d.NE, x0, nrows, LY, h->d.g, h->d.EY, 0.0);
+      else k_put_scalar<double><<<nb, 256, 0, h->io>>>(h->stage, a, x0, nrows, LY, h->d.g, h->d.EY);
     }
     else
     {
       State<float>& s = h->s32;
       float* a = field == MASS_LB_QQXX ? s.Qxx : field == MASS_LB_QQYX ? s.Qyx
                : field == MASS_LB_M ? s.m : s.phi;
-      if(isff) k_put_ff<float><<<nb, 256, 0, h->stream>>>(h->stage, s.ff, h->d.NE, x0, nrows, LY, h->d.g, h->d.EY, rest);
-      else k_put_scalar<float><<<nb, 256, 0, h->stream>>>(h->stage, a, x0, nrows, LY, h->d.g, h->d.EY);
+      if(isff) k_put_ff<float><<<nb, 256, 0, h->io>>>(h->stage, s.ff, h->d.NE, x0, nrows, LY, h->d.g, h->d.EY, rest);
+      else k_put_scalar<float><<<nb, 256, 0, h->io>>>(h->stage, a, x0, nrows, LY, h->d.g, h->d.EY);
     }
     CU(cudaGetLastError(), "upload kernel");
+  }
   }
   // chi follows phi and m (the fused kernel forms chi = m/phi itself)
   if(h->model == GOG && !h->fused && (field == MASS_LB_PHI || field == MASS_LB_M))
@@ -834,6 +887,8 @@ static int get_primary(mass_lb_handle* h, int field, double* out, bool sync = tr
   const long long rows_per = std::max<long long>(1, kStageSites/LY);
   const bool isff = field == MASS_LB_FF || field == MASS_LB_FN;
   const int comps = isff ? 9 : 1;
+  {
+  XferScope scope(h);
   for(long long x0 = 0; x0 < h->LX; x0 += rows_per)
   {
     const int nrows = static_cast<int>(std::min<long long>(rows_per, h->LX - x0));
@@ -843,24 +898,24 @@ static int get_primary(mass_lb_handle* h, int field, double* out, bool sync = tr
     {
       const long long plane = static_cast<long long>(h->LX)*h->LY;
       if(field == MASS_LB_M)
-        k_get_scalar<float><<<nb, 256, 0, h->stream>>>(h->stage, h->cur + 12*plane, x0, nrows, LY, 0, LY, 0.0);
+        k_get_scalar<float><<<nb, 256, 0, h->io>>>(h->stage, h->cur + 12*plane, x0, nrows, LY, 0, LY, 0.0);
       else if(field == MASS_LB_CHI)
-        k_get_chi<<<nb, 256, 0, h->stream>>>(h->stage, h->cur + 11*plane, h->cur + 12*plane,
+        k_get_chi<<<nb, 256, 0, h->io>>>(h->stage, h->cur + 11*plane, h->cur + 12*plane,
                                              x0, nrows, LY);
       else if(field <= MASS_LB_PHI)
       {
-        if(isff) k_get_ff<float><<<nb, 256, 0, h->stream>>>(h->stage, h->cur, plane, x0, nrows, LY, 0, LY, rest32);
+        if(isff) k_get_ff<float><<<nb, 256, 0, h->io>>>(h->stage, h->cur, plane, x0, nrows, LY, 0, LY, rest32);
         else
         {
           const int p = field == MASS_LB_QQXX ? 9 : field == MASS_LB_QQYX ? 10 : 11;
-          k_get_scalar<float><<<nb, 256, 0, h->stream>>>(h->stage, h->cur + p*plane, x0, nrows, LY, 0, LY, 0.0);
+          k_get_scalar<float><<<nb, 256, 0, h->io>>>(h->stage, h->cur + p*plane, x0, nrows, LY, 0, LY, 0.0);
         }
       }
       else
       {
         // derived fields from the replayed diagnostics, mass_lb_field order
         const int p = field - MASS_LB_N;
-        k_get_scalar<float><<<nb, 256, 0, h->stream>>>(h->stage, h->diag + p*plane, x0, nrows, LY, 0, LY, 0.0);
+        k_get_scalar<float><<<nb, 256, 0, h->io>>>(h->stage, h->diag + p*plane, x0, nrows, LY, 0, LY, 0.0);
       }
     }
     else if(h->precision == MASS_LB_FP64)
@@ -888,9 +943,9 @@ static int get_primary(mass_lb_handle* h, int field, double* out, bool sync = tr
           if(field >= MASS_LB_SIGMA_BULK && field <= MASS_LB_SIGMA_ACTIVE_YX)
             a = s.diag[field - MASS_LB_SIGMA_BULK];
       }
-      if(field == MASS_LB_FF) k_get_ff<double><<<nb, 256, 0, h->stream>>>(h->stage, s.ff, d.NE, x0, nrows, LY, d.g, d.EY, 0.0);
-      else if(field == MASS_LB_FN) k_get_ff<double><<<nb, 256, 0, h->stream>>>(h->stage, s.fn, d.NE, x0, nrows, LY, d.g, d.EY, 0.0);
-      else k_get_scalar<double><<<nb, 256, 0, h->stream>>>(h->stage, a, x0, nrows, LY, d.g, d.EY, 0.0);
+      if(field == MASS_LB_FF) k_get_ff<double><<<nb, 256, 0, h->io>>>(h->stage, s.ff, d.NE, x0, nrows, LY, d.g, d.EY, 0.0);
+      else if(field == MASS_LB_FN) k_get_ff<double><<<nb, 256, 0, h->io>>>(h->stage, s.fn, d.NE, x0, nrows, LY, d.g, d.EY, 0.0);
+      else k_get_scalar<double><<<nb, 256, 0, h->io>>>(h->stage, a, x0, nrows, LY, d.g, d.EY, 0.0);
     }
     else
     {
@@ -915,12 +970,13 @@ static int get_primary(mass_lb_handle* h, int field, double* out, bool sync = tr
           if(field >= MASS_LB_SIGMA_BULK && field <= MASS_LB_SIGMA_ACTIVE_YX)
             a = s.diag[field - MASS_LB_SIGMA_BULK];
       }
-      if(field == MASS_LB_FF) k_get_ff<float><<<nb, 256, 0, h->stream>>>(h->stage, s.ff, d.NE, x0, nrows, LY, d.g, d.EY, rest32);
-      else k_get_scalar<float><<<nb, 256, 0, h->stream>>>(h->stage, a, x0, nrows, LY, d.g, d.EY, add);
+      if(field == MASS_LB_FF) k_get_ff<float><<<nb, 256, 0, h->io>>>(h->stage, s.ff, d.NE, x0, nrows, LY, d.g, d.EY, rest32);
+      else k_get_scalar<float><<<nb, 256, 0, h->io>>>(h->stage, a, x0, nrows, LY, d.g, d.EY, add);
     }
     CU(cudaGetLastError(), "download kernel");
     CU(cudaMemcpyAsync(out + x0*LY*comps, h->stage, n*comps*sizeof(double),
-                       cudaMemcpyDeviceToHost, h->stream), "download copy");
+                       cudaMemcpyDeviceToHost, h->io), "download copy");
+  }
   }
   if(sync) CU(cudaStreamSynchronize(h->stream), "download sync");
   return 0;
@@ -1192,6 +1248,19 @@ int mass_lb_synchronize(mass_lb_handle* h)
 }
 
 void* mass_lb_stream(mass_lb_handle* h) { return h ? static_cast<void*>(h->stream) : nullptr; }
+
+int mass_lb_stream_wait(mass_lb_handle* h, mass_lb_handle* before)
+{
+  if(!h || !before) return fail(MASS_LB_EINVAL, "null handle");
+  if(h == before) return 0;
+  {
+    DeviceGuard g(before->device);
+    CU(cudaEventRecord(before->order_ev, before->stream), "order mark");
+  }
+  DeviceGuard g(h->device);
+  CU(cudaStreamWaitEvent(h->stream, before->order_ev, 0), "order wait");
+  return 0;
+}
 
 int mass_lb_launches_per_step(mass_lb_handle* h)
 {

@@ -142,6 +142,7 @@ def load_library(build_if_missing: bool = False):
         "mass_lb_mask_staging": (C.c_int, [vp, C.c_longlong, C.POINTER(dp)]),
         "mass_lb_upload_async": (C.c_int, [vp, dp, dp, dp, dp]),
         "mass_lb_download_async": (C.c_int, [vp, C.c_int, dp]),
+        "mass_lb_stream_wait": (C.c_int, [vp, vp]),
         "mass_lb_draw_masks_queued": (C.c_int, [vp, C.c_int] + [C.c_double] * 7),
         "mass_lb_mask_consumed": (C.c_int, [vp, C.POINTER(C.c_longlong)]),
         "mass_lb_mask_progress": (C.c_int, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_int)]),
@@ -390,6 +391,11 @@ class Lattice:
 
     def synchronize(self):
         _check(load_library().mass_lb_synchronize(self.h))
+
+    def wait_for(self, before: "Lattice"):
+        """mass_lb_stream_wait: work queued on this lattice from now on starts
+        after the work queued on `before` so far (no wait on the host)."""
+        _check(load_library().mass_lb_stream_wait(self.h, before.h))
 
     def checks(self):
         f, p, bad = C.c_double(), C.c_double(), C.c_int()

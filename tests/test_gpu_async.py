@@ -100,3 +100,51 @@ def test_async_go_or_grow_with_relaxation(prec):
         assert bits_equal(a.get(k), b.get(k)), k
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("prec,LX,LY", [(M.FP32, 256, 192), (M.FP64, 40, 48)])
+def test_pipeline_over_handles_equals_jobs_run_alone(prec, LX, LY):
+    """Jobs with different inputs rotated over three handles, the runs of
+    steps ordered with mass_lb_stream_wait and the transfers asynchronous
+    (the bench's end-to-end pipeline): every job's result equals the job run
+    alone with synchronous calls, bit for bit."""
+    model, params, names = M.LYOTROPIC, LYO_C1, ("ff", "QQxx", "QQyx", "phi")
+    njobs, nbuf, steps = 7, 3, 4
+    keep, ins, outs = [], [], []
+    for j in range(njobs):
+        st = O.synthetic_state(model, LX, LY, seed=40 + j, flow=0.02)
+        d, o = {}, {}
+        for k in names:
+            d[k], t = pinned(np.asarray(st[k], dtype=np.float64))
+            keep.append(t)
+            o[k], t = pinned(np.zeros_like(d[k]))
+            keep.append(t)
+        ins.append(d)
+        outs.append(o)
+    lats = [M.Lattice(model, params, LX, LY, 0, prec) for _ in range(nbuf)]
+    for j in range(njobs):
+        x = lats[j % nbuf]
+        if j >= nbuf:
+            x.synchronize()
+        x.upload_async(*(ins[j][k] for k in names))
+        if j > 0:
+            x.wait_for(lats[(j - 1) % nbuf])
+        x.step(steps)
+        if j > 0:
+            for k in names:
+                lats[(j - 1) % nbuf].get_into_async(k, outs[j - 1][k])
+    for k in names:
+        lats[(njobs - 1) % nbuf].get_into_async(k, outs[njobs - 1][k])
+    for x in lats:
+        x.synchronize()
+    ref = M.Lattice(model, params, LX, LY, 0, prec)
+    for j in range(njobs):
+        ref.upload(*(ins[j][k] for k in names))
+        ref.step(steps)
+        for k in names:
+            want = ref.get(k)
+            assert bits_equal(outs[j][k].reshape(want.shape), want), (j, k)
+    # ordering calls: the same handle is a no-op, a null handle an error
+    lats[0].wait_for(lats[0])
+    from mass_hd_b200 import lb
+    assert lb.load_library().mass_lb_stream_wait(lats[0].h, None) != 0
