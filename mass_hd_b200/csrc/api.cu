@@ -132,6 +132,122 @@ inline int blocks_for(long long n)
   return static_cast<int>(std::min<long long>(std::max<long long>(b, 1), 4096));
 }
 
+// ---- wall bands of a fused lattice ----------------------------------------
+// A fused FP32 lattice with walls steps in two parts. The warp-strip kernel
+// steps the whole lattice as if it were periodic. One Step() reaches 4
+// sites (predictor UpdateQuantities, UpdateFields and Move, corrector
+// UpdateQuantities and UpdateFields), so every site at least 4 sites from a
+// wall gets exactly what the wall step gives it: its dependence cone holds
+// no ghost value and no site whose update a wall changes. The sites nearer
+// a wall come from a band lattice: the kBandHalf rows next to each wall of
+// one axis, side by side, stepped by the wall-aware sweeps
+// (step_unfused_f32) with the lattice's own boundary kind. The band's
+// outer kBandKeep rows on each side are exact; the cut between its halves
+// reaches only rows that are discarded. Channels (walls across y) take one
+// band of LX x 2*kBandHalf sites, boxes a second of 2*kBandHalf x LY.
+constexpr int kBandHalf = 8;
+constexpr int kBandKeep = 4;
+
+struct BandMap
+{
+  int axis;            // 0: the band crosses y (walls front/back), 1: crosses x
+  int LX, LY;          // the whole lattice
+  int BX, BY;          // the band's sites
+  int EY;              // the band's extended row (BY + 2, ghost ring g = 1)
+  long long NE;        // the band's extended plane
+  long long plane;     // LX*LY, the fused plane
+};
+
+// band planes: ff (9 planes), the scalars Qxx, Qyx, [phi], [m] in the fused
+// plane order 9, 10, 11, 12, and the phi source rate
+struct BandPtrs
+{
+  float* ff;
+  float* sc[4];
+  int nsc;
+  float* src;
+  const float* src_fused;
+};
+
+// the band's derived planes in the fused diagnostic order (fields n ..
+// sigma_active_yx); null where the model has none
+struct BandDiag
+{
+  const float* a[NDIAG];
+  float rho;
+};
+
+__device__ __forceinline__ int band_row(int i, int N)
+{
+  return i < kBandHalf ? i : N - 2*kBandHalf + i;
+}
+
+// band site k -> fused index gi, band extended index bi; keep: the site is
+// one of the rows the band step leaves exact
+__device__ __forceinline__ bool band_site(const BandMap& m, long long k, long long& gi,
+                                          long long& bi)
+{
+  const int bx = static_cast<int>(k / m.BY), by = static_cast<int>(k % m.BY);
+  const int x = m.axis == 1 ? band_row(bx, m.LX) : bx;
+  const int y = m.axis == 0 ? band_row(by, m.LY) : by;
+  gi = static_cast<long long>(x)*m.LY + y;
+  bi = static_cast<long long>(bx + 1)*m.EY + (by + 1);
+  const int r = m.axis == 0 ? by : bx;
+  return r < kBandKeep || r >= 2*kBandHalf - kBandKeep;
+}
+
+__global__ void __launch_bounds__(256)
+k_band_gather(BandMap m, const float* __restrict__ from, BandPtrs p)
+{
+  const long long n = static_cast<long long>(m.BX)*m.BY;
+  for(long long k = blockIdx.x*256ll + threadIdx.x; k < n; k += 256ll*gridDim.x)
+  {
+    long long gi, bi;
+    band_site(m, k, gi, bi);
+#pragma unroll
+    for(int v = 0; v < 9; ++v) p.ff[v*m.NE + bi] = from[v*m.plane + gi];
+    for(int i = 0; i < p.nsc; ++i) p.sc[i][bi] = from[(9 + i)*m.plane + gi];
+    if(p.src) p.src[bi] = p.src_fused[gi];
+  }
+}
+
+__global__ void __launch_bounds__(256)
+k_band_scatter(BandMap m, float* __restrict__ to, BandPtrs p)
+{
+  const long long n = static_cast<long long>(m.BX)*m.BY;
+  for(long long k = blockIdx.x*256ll + threadIdx.x; k < n; k += 256ll*gridDim.x)
+  {
+    long long gi, bi;
+    if(!band_site(m, k, gi, bi)) continue;
+#pragma unroll
+    for(int v = 0; v < 9; ++v) to[v*m.plane + gi] = p.ff[v*m.NE + bi];
+    for(int i = 0; i < p.nsc; ++i) to[(9 + i)*m.plane + gi] = p.sc[i][bi];
+  }
+}
+
+__global__ void __launch_bounds__(256)
+k_band_diag(BandMap m, float* __restrict__ diag, BandDiag d)
+{
+  const long long n = static_cast<long long>(m.BX)*m.BY;
+  for(long long k = blockIdx.x*256ll + threadIdx.x; k < n; k += 256ll*gridDim.x)
+  {
+    long long gi, bi;
+    if(!band_site(m, k, gi, bi)) continue;
+    // the fused diagnostics hold the density n, the sweeps its deviation
+    if(d.a[0]) diag[gi] = d.rho + d.a[0][bi];
+    for(int p = 1; p < NDIAG; ++p)
+      if(d.a[p]) diag[p*m.plane + gi] = d.a[p][bi];
+  }
+}
+
+struct WallBand
+{
+  BandMap map{};
+  Dims d{};
+  State<float> s{};
+  float* src = nullptr;   // the phi source rate on the band's extended torus
+};
+
 } // namespace
 
 // --------------------------------------------------------------------------
@@ -166,6 +282,8 @@ struct mass_lb_handle
   float* cur = nullptr;
   float* nxt = nullptr;
   float* diag = nullptr;     // NDIAG planes, allocated on first use
+  WallBand band[2];          // FP32 fused with walls: the band lattices
+  int nbands = 0;
   bool has_prev = false;     // nxt holds the state before the last step
   bool derived_pending = false;   // unfused: the derived planes await replay_derived
   FusedConfig cfg{128, 256};
@@ -256,9 +374,9 @@ int dalloc(mass_lb_handle* h, T** p, size_t n)
 int nplanes(const mass_lb_handle* h) { return h->model == NEM ? 11 : h->model == LYO ? 12 : 13; }
 
 template<typename T>
-int alloc_state(mass_lb_handle* h, State<T>& s)
+int alloc_state(mass_lb_handle* h, State<T>& s, const Dims& d)
 {
-  const size_t NE = static_cast<size_t>(h->d.NE);
+  const size_t NE = static_cast<size_t>(d.NE);
   T** lb[4] = {&s.ff, &s.fn, &s.ff_tmp, &s.fn_tmp};
   for(auto p : lb) if(int r = dalloc(h, p, 9*NE)) return r;
   std::vector<T**> sc = {&s.Qxx, &s.Qyx, &s.Qxx_tmp, &s.Qyx_tmp, &s.QNxx, &s.QNyx, &s.n, &s.ux, &s.uy,
@@ -280,9 +398,9 @@ int alloc_state(mass_lb_handle* h, State<T>& s)
 }
 
 template<typename T>
-int zero_state(mass_lb_handle* h, State<T>& s)
+int zero_state(mass_lb_handle* h, State<T>& s, const Dims& d)
 {
-  const size_t NE = static_cast<size_t>(h->d.NE);
+  const size_t NE = static_cast<size_t>(d.NE);
   T* lb[4] = {s.ff, s.fn, s.ff_tmp, s.fn_tmp};
   for(T* p : lb) CU(cudaMemsetAsync(p, 0, 9*NE*sizeof(T), h->stream), "memset");
   std::vector<T*> sc = {s.Qxx, s.Qyx, s.Qxx_tmp, s.Qyx_tmp, s.QNxx, s.QNyx, s.n, s.ux, s.uy, s.Hxx, s.Hyx,
@@ -301,6 +419,11 @@ int zero_state(mass_lb_handle* h, State<T>& s)
   for(T* p : sc) CU(cudaMemsetAsync(p, 0, NE*sizeof(T), h->stream), "memset");
   return 0;
 }
+
+template<typename T>
+int alloc_state(mass_lb_handle* h, State<T>& s) { return alloc_state(h, s, h->d); }
+template<typename T>
+int zero_state(mass_lb_handle* h, State<T>& s) { return zero_state(h, s, h->d); }
 
 // FP32 parameters of the fused kernels (the same rounding for single
 // lattices and ensemble runs, so both step bit-identically)
@@ -348,6 +471,22 @@ FusedArgs fused_args(mass_lb_handle* h, const float* in, float* out, bool diag)
 // lattice (no ghost ring, populations as deviations in both), so each is a
 // device copy. The sweeps take over where the fused kernel cannot run: the
 // dry relaxation of go-or-grow's Configure() and conserve_phi.
+// One LX x LY plane between the fused layout (x*LY + y) and the sweeps'
+// extended torus ((x+g)*EY + y + g); with walls (g = 1) the ghost ring is
+// left to the boundary kernels of the next step.
+cudaError_t plane_copy(const mass_lb_handle* h, float* dst, const float* src, bool to_sweeps)
+{
+  const Dims& d = h->d;
+  const size_t row = static_cast<size_t>(d.LY)*sizeof(float);
+  if(d.g == 0)
+    return cudaMemcpyAsync(dst, src, row*d.LX, cudaMemcpyDeviceToDevice, h->stream);
+  const long long off = static_cast<long long>(d.g)*d.EY + d.g;
+  const size_t ext = static_cast<size_t>(d.EY)*sizeof(float);
+  return to_sweeps
+    ? cudaMemcpy2DAsync(dst + off, ext, src, row, row, d.LX, cudaMemcpyDeviceToDevice, h->stream)
+    : cudaMemcpy2DAsync(dst, row, src + off, ext, row, d.LX, cudaMemcpyDeviceToDevice, h->stream);
+}
+
 int fused_to_sweeps(mass_lb_handle* h)
 {
   if(!h->fused) return 0;
@@ -356,21 +495,22 @@ int fused_to_sweeps(mass_lb_handle* h)
     if(int r = alloc_state(h, h->s32)) return r;
     if(int r = zero_state(h, h->s32)) return r;
   }
-  const size_t plane = static_cast<size_t>(h->LX)*h->LY;
-  const size_t b = plane*sizeof(float);
+  const long long plane = static_cast<long long>(h->LX)*h->LY;
   State<float>& s = h->s32;
-  CU(cudaMemcpyAsync(s.ff, h->cur, 9*b, cudaMemcpyDeviceToDevice, h->stream), "state copy");
-  CU(cudaMemcpyAsync(s.Qxx, h->cur + 9*plane, b, cudaMemcpyDeviceToDevice, h->stream), "state copy");
-  CU(cudaMemcpyAsync(s.Qyx, h->cur + 10*plane, b, cudaMemcpyDeviceToDevice, h->stream), "state copy");
-  if(h->model != NEM)
-    CU(cudaMemcpyAsync(s.phi, h->cur + 11*plane, b, cudaMemcpyDeviceToDevice, h->stream), "state copy");
-  if(h->model == GOG)
-    CU(cudaMemcpyAsync(s.m, h->cur + 12*plane, b, cudaMemcpyDeviceToDevice, h->stream), "state copy");
+  for(int v = 0; v < 9; ++v)
+    CU(plane_copy(h, s.ff + v*h->d.NE, h->cur + v*plane, true), "state copy");
+  CU(plane_copy(h, s.Qxx, h->cur + 9*plane, true), "state copy");
+  CU(plane_copy(h, s.Qyx, h->cur + 10*plane, true), "state copy");
+  if(h->model != NEM) CU(plane_copy(h, s.phi, h->cur + 11*plane, true), "state copy");
+  if(h->model == GOG) CU(plane_copy(h, s.m, h->cur + 12*plane, true), "state copy");
   if(h->src_on && h->src_fused)
   {
     if(!h->src32)
+    {
       if(int r = dalloc(h, &h->src32, h->d.NE)) return r;
-    CU(cudaMemcpyAsync(h->src32, h->src_fused, b, cudaMemcpyDeviceToDevice, h->stream), "copy");
+      CU(cudaMemsetAsync(h->src32, 0, h->d.NE*sizeof(float), h->stream), "memset");
+    }
+    CU(plane_copy(h, h->src32, h->src_fused, true), "copy");
     s.src = h->src32;
   }
   if(h->model == GOG && update_chi_f32(h->d, s, h->stream))
@@ -384,19 +524,103 @@ int fused_to_sweeps(mass_lb_handle* h)
 int sweeps_to_fused(mass_lb_handle* h)
 {
   if(h->fused) return 0;
-  const size_t plane = static_cast<size_t>(h->LX)*h->LY;
-  const size_t b = plane*sizeof(float);
+  const long long plane = static_cast<long long>(h->LX)*h->LY;
   const State<float>& s = h->s32;
-  CU(cudaMemcpyAsync(h->cur, s.ff, 9*b, cudaMemcpyDeviceToDevice, h->stream), "state copy");
-  CU(cudaMemcpyAsync(h->cur + 9*plane, s.Qxx, b, cudaMemcpyDeviceToDevice, h->stream), "state copy");
-  CU(cudaMemcpyAsync(h->cur + 10*plane, s.Qyx, b, cudaMemcpyDeviceToDevice, h->stream), "state copy");
-  if(h->model != NEM)
-    CU(cudaMemcpyAsync(h->cur + 11*plane, s.phi, b, cudaMemcpyDeviceToDevice, h->stream), "state copy");
-  if(h->model == GOG)
-    CU(cudaMemcpyAsync(h->cur + 12*plane, s.m, b, cudaMemcpyDeviceToDevice, h->stream), "state copy");
+  for(int v = 0; v < 9; ++v)
+    CU(plane_copy(h, h->cur + v*plane, s.ff + v*h->d.NE, false), "state copy");
+  CU(plane_copy(h, h->cur + 9*plane, s.Qxx, false), "state copy");
+  CU(plane_copy(h, h->cur + 10*plane, s.Qyx, false), "state copy");
+  if(h->model != NEM) CU(plane_copy(h, h->cur + 11*plane, s.phi, false), "state copy");
+  if(h->model == GOG) CU(plane_copy(h, h->cur + 12*plane, s.m, false), "state copy");
   h->fused = true;
   h->has_prev = false;
   h->derived_pending = false;
+  return 0;
+}
+
+// ---- wall bands (the scheme is described above k_band_gather) -------------
+
+bool walls_box(const mass_lb_handle* h)
+{
+  return h->model != NEM && (h->bc == 3 || h->bc == 4);
+}
+
+// the bands need two disjoint halves on every walled axis
+bool bands_fit(const mass_lb_handle* h)
+{
+  return h->LY >= 2u*kBandHalf && (!walls_box(h) || h->LX >= 2u*kBandHalf);
+}
+
+int init_bands(mass_lb_handle* h)
+{
+  h->nbands = walls_box(h) ? 2 : 1;
+  const int LX = static_cast<int>(h->LX), LY = static_cast<int>(h->LY);
+  for(int i = 0; i < h->nbands; ++i)
+  {
+    WallBand& b = h->band[i];
+    const int BX = i == 0 ? LX : 2*kBandHalf, BY = i == 0 ? 2*kBandHalf : LY;
+    b.d = Dims{BX, BY, 1, BX + 2, BY + 2, static_cast<long long>(BX + 2)*(BY + 2)};
+    b.map = BandMap{i, LX, LY, BX, BY, BY + 2, b.d.NE, static_cast<long long>(LX)*LY};
+    if(int r = alloc_state(h, b.s, b.d)) return r;
+    if(int r = zero_state(h, b.s, b.d)) return r;
+    if(h->model != NEM)
+    {
+      if(int r = dalloc(h, &b.src, b.d.NE)) return r;
+      CU(cudaMemsetAsync(b.src, 0, b.d.NE*sizeof(float), h->stream), "memset");
+    }
+  }
+  return 0;
+}
+
+BandPtrs band_ptrs(const mass_lb_handle* h, const WallBand& b)
+{
+  BandPtrs p{};
+  p.ff = b.s.ff;
+  p.sc[0] = b.s.Qxx;
+  p.sc[1] = b.s.Qyx;
+  p.nsc = 2;
+  if(h->model != NEM) p.sc[p.nsc++] = b.s.phi;
+  if(h->model == GOG) p.sc[p.nsc++] = b.s.m;
+  // the fused go-or-grow step reads a zero rate plane when no source is
+  // set, the sweeps none: both leave phi as it is
+  p.src = h->src_on && h->src_fused ? b.src : nullptr;
+  p.src_fused = h->src_fused;
+  return p;
+}
+
+// The band part of one step of a fused lattice with walls: gather the bands
+// from the state `from`, step them with the walls, then write their exact
+// rows into the state `to` or, with `diag`, their derived fields (those of
+// the last UpdateQuantities) into the diagnostic planes.
+int step_bands(mass_lb_handle* h, const float* from, float* to, bool diag)
+{
+  for(int i = 0; i < h->nbands; ++i)
+  {
+    WallBand& b = h->band[i];
+    const int nb = blocks_for(static_cast<long long>(b.map.BX)*b.map.BY);
+    const BandPtrs p = band_ptrs(h, b);
+    k_band_gather<<<nb, 256, 0, h->stream>>>(b.map, from, p);
+    CU(cudaGetLastError(), "band gather");
+    b.s.src = p.src;
+    b.s.conserve_phi = 0;
+    b.s.phisum = nullptr;
+    b.s.ph = h->s32.ph;
+    if(h->model == GOG && update_chi_f32(b.d, b.s, h->stream))
+      return cuda_fail(cudaGetLastError(), "band chi");
+    if(step_unfused_f32(b.d, h->P, b.s, static_cast<int>(h->bc), 1, diag, h->stream) != 0)
+      return cuda_fail(cudaGetLastError(), "band step");
+    if(diag)
+    {
+      const State<float>& s = b.s;
+      const BandDiag dd{{s.n, s.ux, s.uy, s.uxp, s.uyp, s.Hxx, s.Hyx, s.MU, s.dxQxx, s.dyQxx,
+                         s.dxQyx, s.dyQyx, s.sXX, s.sYY, s.sYX, s.sXY, s.diag[0], s.diag[1],
+                         s.diag[2], s.diag[3], s.diag[4], s.diag[5], s.diag[6]},
+                        static_cast<float>(h->P.rho)};
+      k_band_diag<<<nb, 256, 0, h->stream>>>(b.map, h->diag, dd);
+    }
+    else k_band_scatter<<<nb, 256, 0, h->stream>>>(b.map, to, band_ptrs(h, b));
+    CU(cudaGetLastError(), "band scatter");
+  }
   return 0;
 }
 
@@ -571,9 +795,10 @@ int mass_lb_create(const mass_lb_params* params, unsigned LX, unsigned LY,
   }
   else
   {
-    // the fused warp-strip kernel: every model on periodic lattices with
-    // npc = 1; the rest runs the unfused sweeps in FP32
-    h->fused = !h->wall && h->P.npc == 1 &&
+    // the fused warp-strip kernel: every model with npc = 1, on periodic
+    // lattices and, with the wall bands beside it, on walled ones; the rest
+    // runs the unfused sweeps in FP32
+    h->fused = h->P.npc == 1 && (!h->wall || bands_fit(h)) &&
                fused_supported(static_cast<int>(LX), static_cast<int>(LY), 64);
     if(h->fused)
     {
@@ -583,6 +808,8 @@ int mass_lb_create(const mass_lb_params* params, unsigned LX, unsigned LY,
       if(cudaMemsetAsync(h->cur, 0, n*sizeof(float), h->stream) != cudaSuccess ||
          cudaMemsetAsync(h->nxt, 0, n*sizeof(float), h->stream) != cudaSuccess)
         return bail(fail(MASS_LB_ECUDA, "memset"));
+      if(h->wall)
+        if(int r = init_bands(h)) return bail(r);
       if(h->model == GOG)
       {
         // the growth-rate plane every go-or-grow step reads, zero until set
@@ -870,6 +1097,8 @@ int mass_lb_step(mass_lb_handle* h, unsigned nsteps)
     {
       const FusedArgs a = fused_args(h, h->cur, h->nxt, false);
       CU(launch_fused_step(a, h->model, h->cfg, false, h->stream), "fused step");
+      if(h->nbands)
+        if(int r = step_bands(h, h->cur, h->nxt, false)) return r;
       std::swap(h->cur, h->nxt);
     }
     h->has_prev = true;
@@ -1008,6 +1237,8 @@ int mass_lb_download(mass_lb_handle* h, int field, double* out)
     // outputs on (the replay does not write the state)
     const FusedArgs a = fused_args(h, h->nxt, h->cur, true);
     CU(launch_fused_step(a, h->model, h->cfg, true, h->stream), "diag replay");
+    if(h->nbands)
+      if(int r = step_bands(h, h->nxt, nullptr, true)) return r;
     if(int r = check_err_flag(h)) return r;
   }
   return get_primary(h, field, out);
@@ -1265,7 +1496,10 @@ int mass_lb_stream_wait(mass_lb_handle* h, mass_lb_handle* before)
 int mass_lb_launches_per_step(mass_lb_handle* h)
 {
   if(!h) return fail(MASS_LB_EINVAL, "null handle");
-  if(h->fused) return 1;
+  // fused with walls: per band a gather, [chi,] the wall sweeps, a scatter
+  if(h->fused)
+    return 1 + h->nbands*(2 + (h->model == GOG ? 1 : 0) +
+                          launches_unfused(h->model, static_cast<int>(h->bc), 1));
   return launches_unfused(h->model, h->wall ? static_cast<int>(h->bc) : 0, h->P.npc);
 }
 

@@ -773,15 +773,17 @@ __device__ __forceinline__ void s_apply(const Dims& d, T* a, XY i, int in, int k
   else a[at(d, i)] = T(2)*a[at(d, j)] - a[at(d, step_xy(d, j, in))];
 }
 
-// Scalar fields. Phase 1: walls (they read domain values only); phase 2:
-// corners (channel corners read the left/right ghosts written in phase 1).
+// Scalar fields, in two launches: the walls (they read domain values only),
+// then the corners (channel corners read the left/right ghosts the walls
+// wrote). Every ghost value is a copy, a negation or a 2a - b of values the
+// launch before has settled, so the grid's layout does not change a bit.
 template<typename T>
-__global__ void __launch_bounds__(1024)
-bc_scalar_kernel(Dims d, ScalarBC<T> job)
+__global__ void __launch_bounds__(256)
+bc_scalar_walls(Dims d, ScalarBC<T> job)
 {
   const int LX = d.LX, LY = d.LY;
   const int nwall = 2*LY + 2*LX;
-  for(int idx = threadIdx.x; idx < nwall; idx += blockDim.x)
+  for(int idx = blockIdx.x*blockDim.x + threadIdx.x; idx < nwall; idx += blockDim.x*gridDim.x)
   {
     int w, k;
     if(idx < LY) { w = W_LEFT; k = idx; }
@@ -802,27 +804,38 @@ bc_scalar_kernel(Dims d, ScalarBC<T> job)
       else s_apply(d, a, i, OPPv(w), job.kind[f]);
     }
   }
-  __syncthreads();
-  if(threadIdx.x < 4)
+}
+
+template<typename T>
+__global__ void __launch_bounds__(32)
+bc_scalar_corners(Dims d, ScalarBC<T> job)
+{
+  if(threadIdx.x >= 4) return;
+  // order of the reference's corner calls does not matter: each corner
+  // reads a wall ghost or a domain site, never another corner
+  const int cs[4] = {C_RIGHTBACK, C_RIGHTFRONT, C_LEFTBACK, C_LEFTFRONT};
+  const int c = cs[threadIdx.x];
+  const XY i = corner_xy(d, c);
+  for(int f = 0; f < job.nf; ++f)
   {
-    // order of the reference's corner calls does not matter: each corner
-    // reads a wall ghost or a domain site, never another corner
-    const int cs[4] = {C_RIGHTBACK, C_RIGHTFRONT, C_LEFTBACK, C_LEFTFRONT};
-    const int c = cs[threadIdx.x];
-    const XY i = corner_xy(d, c);
-    for(int f = 0; f < job.nf; ++f)
+    T* a = job.f[f];
+    if(job.mode == BCM_PBC)
+      a[at(d, i)] = a[at(d, step_xy(d, corner_xy(d, OPPv(c)), c))];
+    else if(job.mode == BCM_CHANNEL)
     {
-      T* a = job.f[f];
-      if(job.mode == BCM_PBC)
-        a[at(d, i)] = a[at(d, step_xy(d, corner_xy(d, OPPv(c)), c))];
-      else if(job.mode == BCM_CHANNEL)
-      {
-        const int w = (c == C_RIGHTBACK || c == C_LEFTBACK) ? W_BACK : W_FRONT;
-        s_apply(d, a, i, OPPv(w), job.kind[f]);
-      }
-      else s_apply(d, a, i, OPPv(c), job.kind[f]);
+      const int w = (c == C_RIGHTBACK || c == C_LEFTBACK) ? W_BACK : W_FRONT;
+      s_apply(d, a, i, OPPv(w), job.kind[f]);
     }
+    else s_apply(d, a, i, OPPv(c), job.kind[f]);
   }
+}
+
+template<typename T>
+void launch_bc_scalar(const Dims& d, const ScalarBC<T>& j, cudaStream_t st)
+{
+  const int n = 2*d.LY + 2*d.LX;
+  bc_scalar_walls<T><<<(n + 255)/256, 256, 0, st>>>(d, j);
+  bc_scalar_corners<T><<<1, 32, 0, st>>>(d, j);
 }
 
 template<typename T>
@@ -847,18 +860,19 @@ __device__ __forceinline__ void f_wall(const Dims& d, T* f, int w, int k, bool n
     }
 }
 
-// Population fields ff and fn. Phase 1: left/right walls, and every wall
-// whose update reads domain values only; phase 2: front/back no-slip walls
-// (their diagonal bounce reads the left/right ghosts, which the reference
-// has already updated by then); phase 3: corners.
+// Population fields ff and fn, in up to three launches: (1) left/right
+// walls, and every wall whose update reads domain values only (a no-slip
+// box's left/right walls read the front/back ghosts as the last Move left
+// them, the reference's order); (2) front/back no-slip walls, whose
+// diagonal bounce reads the left/right ghosts (1) wrote; (3) the corners.
 template<typename T>
-__global__ void __launch_bounds__(1024)
-bc_lb_kernel(Dims d, T* ff, T* fn, int kind)
+__global__ void __launch_bounds__(256)
+bc_lb_walls(Dims d, T* ff, T* fn, int kind)
 {
   const int LX = d.LX, LY = d.LY;
   T* arrs[2] = {ff, fn};
-  // phase 1
-  for(int idx = threadIdx.x; idx < 2*LY + 2*LX; idx += blockDim.x)
+  for(int idx = blockIdx.x*blockDim.x + threadIdx.x; idx < 2*LY + 2*LX;
+      idx += blockDim.x*gridDim.x)
   {
     int w, k;
     if(idx < LY) { w = W_LEFT; k = idx; }
@@ -877,44 +891,61 @@ bc_lb_kernel(Dims d, T* ff, T* fn, int kind)
         f_wall(d, f, w, k, true);
     }
   }
-  __syncthreads();
-  // phase 2
-  if(kind == LBK_NOSLIP_CHANNEL || kind == LBK_NOSLIP_BOX)
+}
+
+template<typename T>
+__global__ void __launch_bounds__(256)
+bc_lb_noslip_fb(Dims d, T* ff, T* fn)
+{
+  const int LX = d.LX;
+  T* arrs[2] = {ff, fn};
+  for(int idx = blockIdx.x*blockDim.x + threadIdx.x; idx < 2*LX; idx += blockDim.x*gridDim.x)
   {
-    for(int idx = threadIdx.x; idx < 2*LX; idx += blockDim.x)
+    const int w = idx < LX ? W_FRONT : W_BACK;
+    const int k = idx < LX ? idx : idx - LX;
+    for(int a = 0; a < 2; ++a) f_wall(d, arrs[a], w, k, true);
+  }
+}
+
+template<typename T>
+__global__ void __launch_bounds__(32)
+bc_lb_corners(Dims d, T* ff, T* fn, int kind)
+{
+  if(threadIdx.x >= 4) return;
+  T* arrs[2] = {ff, fn};
+  const int cs[4] = {C_RIGHTBACK, C_RIGHTFRONT, C_LEFTBACK, C_LEFTFRONT};
+  const int c = cs[threadIdx.x];
+  const XY i = corner_xy(d, c);
+  for(int a = 0; a < 2; ++a)
+  {
+    T* f = arrs[a];
+    if(kind == LBK_PBC)
+      f_pbc_node(d, f, i, step_xy(d, corner_xy(d, OPPv(c)), c));
+    else if(kind == LBK_FREESLIP_CHANNEL)
     {
-      const int w = idx < LX ? W_FRONT : W_BACK;
-      const int k = idx < LX ? idx : idx - LX;
-      for(int a = 0; a < 2; ++a) f_wall(d, arrs[a], w, k, true);
+      const int w = (c == C_RIGHTBACK || c == C_LEFTBACK) ? W_BACK : W_FRONT;
+      const int p = c_proj[w][c];
+      const int v = OPPv(c);
+      const XY l = step_xy(d, corner_xy(d, c_refl[p][c]), p);
+      f[v*d.NE + at(d, i)] = f[v*d.NE + at(d, l)];
+    }
+    else
+    {
+      const int v = OPPv(c);
+      f[v*d.NE + at(d, i)] = f[c*d.NE + at(d, step_xy(d, i, v))];
     }
   }
-  __syncthreads();
-  // phase 3
-  if(threadIdx.x < 4)
-  {
-    const int cs[4] = {C_RIGHTBACK, C_RIGHTFRONT, C_LEFTBACK, C_LEFTFRONT};
-    const int c = cs[threadIdx.x];
-    const XY i = corner_xy(d, c);
-    for(int a = 0; a < 2; ++a)
-    {
-      T* f = arrs[a];
-      if(kind == LBK_PBC)
-        f_pbc_node(d, f, i, step_xy(d, corner_xy(d, OPPv(c)), c));
-      else if(kind == LBK_FREESLIP_CHANNEL)
-      {
-        const int w = (c == C_RIGHTBACK || c == C_LEFTBACK) ? W_BACK : W_FRONT;
-        const int p = c_proj[w][c];
-        const int v = OPPv(c);
-        const XY l = step_xy(d, corner_xy(d, c_refl[p][c]), p);
-        f[v*d.NE + at(d, i)] = f[v*d.NE + at(d, l)];
-      }
-      else
-      {
-        const int v = OPPv(c);
-        f[v*d.NE + at(d, i)] = f[c*d.NE + at(d, step_xy(d, i, v))];
-      }
-    }
-  }
+}
+
+bool lb_noslip(int kind) { return kind == LBK_NOSLIP_CHANNEL || kind == LBK_NOSLIP_BOX; }
+
+template<typename T>
+void launch_bc_lb(const Dims& d, T* ff, T* fn, int kind, cudaStream_t st)
+{
+  const int n = 2*d.LY + 2*d.LX;
+  bc_lb_walls<T><<<(n + 255)/256, 256, 0, st>>>(d, ff, fn, kind);
+  if(lb_noslip(kind)) bc_lb_noslip_fb<T><<<(2*d.LX + 255)/256, 256, 0, st>>>(d, ff, fn);
+  bc_lb_corners<T><<<1, 32, 0, st>>>(d, ff, fn, kind);
 }
 
 inline dim3 site_grid(int nx, int ny, dim3 blk)
@@ -1074,7 +1105,7 @@ int relax_impl(const Dims& d, const Params& P, State<T>& s, int bc, unsigned nst
     j.f[0] = a; j.f[1] = b; j.f[2] = c;
     j.nf = c ? 3 : 1;
     for(int i = 0; i < j.nf; ++i) j.kind[i] = BC_NEUMANN;
-    bc_scalar_kernel<T><<<1, 1024, 0, st>>>(d, j);
+    launch_bc_scalar<T>(d, j, st);
   };
   if(nsteps > 0 && (relax_phi || relax_Q))
   {
@@ -1114,7 +1145,7 @@ int step_impl(const Dims& d, const Params& P, State<T>& s, int bc,
     // go-or-grow walls treat m and chi as phi (src/models/go-or-grow.cpp:393-418)
     if(MODEL == GOG) { j.f[3] = s.m; j.f[4] = s.chi; j.nf = 5; }
     for(int i = 0; i < j.nf; ++i) j.kind[i] = BC_NEUMANN;
-    bc_scalar_kernel<T><<<1, 1024, 0, st>>>(d, j);
+    launch_bc_scalar<T>(d, j, st);
   };
   auto fields2_bc = [&]() {
     if(!bc) return;
@@ -1135,7 +1166,7 @@ int step_impl(const Dims& d, const Params& P, State<T>& s, int bc,
       for(int i = 0; i < 6; ++i) { j.f[i] = fs[i]; j.kind[i] = BC_NEUMANN; }
       j.nf = 6;
     }
-    bc_scalar_kernel<T><<<1, 1024, 0, st>>>(d, j);
+    launch_bc_scalar<T>(d, j, st);
   };
 
   // after UpdateFields: the new phi (and, for go-or-grow, m and chi =
@@ -1184,7 +1215,7 @@ int step_impl(const Dims& d, const Params& P, State<T>& s, int bc,
     {
       uf_kernel<T, DEV, MODEL, true><<<grd, blk, 0, st>>>(d, P, s);
       swap_fields();
-      bc_lb_kernel<T><<<1, 1024, 0, st>>>(d, s.ff, s.fn, lbk);
+      launch_bc_lb<T>(d, s.ff, s.fn, lbk, st);
       move_kernel<T><<<egrd, blk, 0, st>>>(d, s.ff, s.fn, s.ff_tmp, s.fn_tmp);
     }
     else
@@ -1275,12 +1306,12 @@ int bc_mode(int model, int bc)
 
 int launches_unfused(int model, int bc, unsigned npc)
 {
-  // periodic: one sub-step kernel per predictor and corrector;
-  // walls: predictor [bc] uq [bc] uf [bc move], corrector [bc] uq [bc] uf
-  (void)model;
-  if(!bc && npc >= 1) return 1 + (int)npc;
-  const int w = bc ? 1 : 0;
-  return (2 + 4*w) + (int)npc*(2 + 2*w);
+  // periodic: one sub-step kernel per predictor and corrector; walls:
+  // predictor [bc] uq [bc] uf [bc] move, corrector [bc] uq [bc] uf, where
+  // a scalar [bc] is two launches and the populations' two or three
+  if(!bc) return 1 + (int)npc;
+  const int lb = lb_noslip(lb_kind(model, bc)) ? 3 : 2;
+  return (2 + 1 + 2 + 1 + lb + 1) + (int)npc*6;
 }
 
 int step_unfused_f64(const Dims& d, const Params& P, State<double>& s, int bc,
