@@ -284,6 +284,8 @@ struct mass_lb_handle
   float* diag = nullptr;     // NDIAG planes, allocated on first use
   WallBand band[2];          // FP32 fused with walls: the band lattices
   int nbands = 0;
+  cudaStream_t bstream = nullptr;   // their work beside the fused kernel
+  cudaEvent_t band_in = nullptr, band_out = nullptr;
   bool has_prev = false;     // nxt holds the state before the last step
   bool derived_pending = false;   // unfused: the derived planes await replay_derived
   FusedConfig cfg{128, 256};
@@ -554,6 +556,11 @@ bool bands_fit(const mass_lb_handle* h)
 int init_bands(mass_lb_handle* h)
 {
   h->nbands = walls_box(h) ? 2 : 1;
+  int least = 0, greatest = 0;
+  CU(cudaDeviceGetStreamPriorityRange(&least, &greatest), "priorities");
+  CU(cudaStreamCreateWithPriority(&h->bstream, cudaStreamNonBlocking, greatest), "band stream");
+  CU(cudaEventCreateWithFlags(&h->band_in, cudaEventDisableTiming), "event");
+  CU(cudaEventCreateWithFlags(&h->band_out, cudaEventDisableTiming), "event");
   const int LX = static_cast<int>(h->LX), LY = static_cast<int>(h->LY);
   for(int i = 0; i < h->nbands; ++i)
   {
@@ -588,27 +595,38 @@ BandPtrs band_ptrs(const mass_lb_handle* h, const WallBand& b)
   return p;
 }
 
-// The band part of one step of a fused lattice with walls: gather the bands
-// from the state `from`, step them with the walls, then write their exact
-// rows into the state `to` or, with `diag`, their derived fields (those of
-// the last UpdateQuantities) into the diagnostic planes.
-int step_bands(mass_lb_handle* h, const float* from, float* to, bool diag)
+// The band part of one step of a fused lattice with walls, on stream `st`:
+// gather the bands from the state `from` and step them with the walls
+// (with `diag`, keeping the derived fields of the last UpdateQuantities).
+int band_compute(mass_lb_handle* h, const float* from, bool diag, cudaStream_t st)
 {
   for(int i = 0; i < h->nbands; ++i)
   {
     WallBand& b = h->band[i];
     const int nb = blocks_for(static_cast<long long>(b.map.BX)*b.map.BY);
     const BandPtrs p = band_ptrs(h, b);
-    k_band_gather<<<nb, 256, 0, h->stream>>>(b.map, from, p);
+    k_band_gather<<<nb, 256, 0, st>>>(b.map, from, p);
     CU(cudaGetLastError(), "band gather");
     b.s.src = p.src;
     b.s.conserve_phi = 0;
     b.s.phisum = nullptr;
     b.s.ph = h->s32.ph;
-    if(h->model == GOG && update_chi_f32(b.d, b.s, h->stream))
+    if(h->model == GOG && update_chi_f32(b.d, b.s, st))
       return cuda_fail(cudaGetLastError(), "band chi");
-    if(step_unfused_f32(b.d, h->P, b.s, static_cast<int>(h->bc), 1, diag, h->stream) != 0)
+    if(step_unfused_f32(b.d, h->P, b.s, static_cast<int>(h->bc), 1, diag, st) != 0)
       return cuda_fail(cudaGetLastError(), "band step");
+  }
+  return 0;
+}
+
+// Then, on stream `st`: the bands' exact rows into the state `to` or, with
+// `diag`, their derived fields into the diagnostic planes.
+int band_emit(mass_lb_handle* h, float* to, bool diag, cudaStream_t st)
+{
+  for(int i = 0; i < h->nbands; ++i)
+  {
+    const WallBand& b = h->band[i];
+    const int nb = blocks_for(static_cast<long long>(b.map.BX)*b.map.BY);
     if(diag)
     {
       const State<float>& s = b.s;
@@ -616,12 +634,27 @@ int step_bands(mass_lb_handle* h, const float* from, float* to, bool diag)
                          s.dxQyx, s.dyQyx, s.sXX, s.sYY, s.sYX, s.sXY, s.diag[0], s.diag[1],
                          s.diag[2], s.diag[3], s.diag[4], s.diag[5], s.diag[6]},
                         static_cast<float>(h->P.rho)};
-      k_band_diag<<<nb, 256, 0, h->stream>>>(b.map, h->diag, dd);
+      k_band_diag<<<nb, 256, 0, st>>>(b.map, h->diag, dd);
     }
-    else k_band_scatter<<<nb, 256, 0, h->stream>>>(b.map, to, band_ptrs(h, b));
+    else k_band_scatter<<<nb, 256, 0, st>>>(b.map, to, band_ptrs(h, b));
     CU(cudaGetLastError(), "band scatter");
   }
   return 0;
+}
+
+// One fused step of a walled lattice, cur -> nxt: the band work runs on the
+// high-priority band stream beside the warp-strip kernel (both only read
+// cur), and the step stream writes the band rows after both.
+int fused_step_with_bands(mass_lb_handle* h)
+{
+  CU(cudaEventRecord(h->band_in, h->stream), "band fork");
+  CU(cudaStreamWaitEvent(h->bstream, h->band_in, 0), "band fork");
+  if(int r = band_compute(h, h->cur, false, h->bstream)) return r;
+  CU(cudaEventRecord(h->band_out, h->bstream), "band join");
+  const FusedArgs a = fused_args(h, h->cur, h->nxt, false);
+  CU(launch_fused_step(a, h->model, h->cfg, false, h->stream), "fused step");
+  CU(cudaStreamWaitEvent(h->stream, h->band_out, 0), "band join");
+  return band_emit(h, h->nxt, false, h->stream);
 }
 
 int check_err_flag(mass_lb_handle* h)
@@ -871,6 +904,9 @@ void mass_lb_destroy(mass_lb_handle* h)
   if(h->tot_ev) cudaEventDestroy(h->tot_ev);
   if(h->mq_copy) cudaStreamDestroy(h->mq_copy);
   if(h->xfer) { cudaStreamSynchronize(h->xfer); cudaStreamDestroy(h->xfer); }
+  if(h->bstream) { cudaStreamSynchronize(h->bstream); cudaStreamDestroy(h->bstream); }
+  if(h->band_in) cudaEventDestroy(h->band_in);
+  if(h->band_out) cudaEventDestroy(h->band_out);
   if(h->xfer_in) cudaEventDestroy(h->xfer_in);
   if(h->xfer_out) cudaEventDestroy(h->xfer_out);
   if(h->order_ev) cudaEventDestroy(h->order_ev);
@@ -1095,10 +1131,15 @@ int mass_lb_step(mass_lb_handle* h, unsigned nsteps)
       if(int r = autotune(h)) return r;
     for(unsigned i = 0; i < nsteps; ++i)
     {
-      const FusedArgs a = fused_args(h, h->cur, h->nxt, false);
-      CU(launch_fused_step(a, h->model, h->cfg, false, h->stream), "fused step");
       if(h->nbands)
-        if(int r = step_bands(h, h->cur, h->nxt, false)) return r;
+      {
+        if(int r = fused_step_with_bands(h)) return r;
+      }
+      else
+      {
+        const FusedArgs a = fused_args(h, h->cur, h->nxt, false);
+        CU(launch_fused_step(a, h->model, h->cfg, false, h->stream), "fused step");
+      }
       std::swap(h->cur, h->nxt);
     }
     h->has_prev = true;
@@ -1238,7 +1279,10 @@ int mass_lb_download(mass_lb_handle* h, int field, double* out)
     const FusedArgs a = fused_args(h, h->nxt, h->cur, true);
     CU(launch_fused_step(a, h->model, h->cfg, true, h->stream), "diag replay");
     if(h->nbands)
-      if(int r = step_bands(h, h->nxt, nullptr, true)) return r;
+    {
+      if(int r = band_compute(h, h->nxt, true, h->stream)) return r;
+      if(int r = band_emit(h, nullptr, true, h->stream)) return r;
+    }
     if(int r = check_err_flag(h)) return r;
   }
   return get_primary(h, field, out);
