@@ -63,6 +63,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "site-updates/s"
+BC_NAMES = {1: "free-slip channel walls", 2: "no-slip channel walls",
+            3: "free-slip box walls", 4: "no-slip box walls"}
 UNIT = "site-updates/s"
 NINFO = 100
 
@@ -637,7 +639,8 @@ def run_ours(args):
     sites = L * L
 
     st = synthetic_state(model, L, seed=1 + rank)
-    lat = M.Lattice(mcode, params, L, L, 0, prec)
+    bc = args.bc
+    lat = M.Lattice(mcode, params, L, L, bc, prec)
     lat.upload_state(st)
     stream = torch.cuda.ExternalStream(lat.stream)
 
@@ -718,7 +721,7 @@ def run_ours(args):
     # result into pinned host memory; the host reuses a handle (and its
     # output buffers) only after synchronizing on it.
     NBUF = 3
-    lats = [lat] + [M.Lattice(mcode, params, L, L, 0, prec) for _ in range(NBUF - 1)]
+    lats = [lat] + [M.Lattice(mcode, params, L, L, bc, prec) for _ in range(NBUF - 1)]
     outsets = [outs]
     for x in lats[1:]:
         if lat.uses_fused:
@@ -799,9 +802,11 @@ def run_ours(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if args.precision == "fp32" else "f64",
             "data": "synthetic (seeded random director S=1, tanh phi disk R=L/4)",
-            "config": {"workload": f"{model} {args.precision.upper()} {L}x{L} periodic, "
+            "config": {"workload": f"{model} {args.precision.upper()} {L}x{L} "
+                                   f"{BC_NAMES.get(bc, 'periodic') if bc else 'periodic'}, "
                                    f"256^2-config physics, npc=1",
-                       "model": model, "LX": L, "LY": L, "precision": args.precision,
+                       "model": model, "LX": L, "LY": L, "bc": bc,
+                       "precision": args.precision,
                        "lattices": world,
                        "parallelism": "independent lattice per GPU" if world > 1 else "single GPU",
                        "l2": f"state {sites * bps // 2 / 1e6:.0f} MB per buffer > 126 MB L2, no flush",
@@ -834,6 +839,10 @@ def main():
     ap.add_argument("--model", default="lyotropic", choices=["lyotropic", "nematic", "go-or-grow"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--bc", type=int, default=0,
+                    help="walls (lyotropic 1/2: free-slip/no-slip channel, 3/4: box; "
+                         "nematic 1: channel); the FP64, ensemble and CPU records "
+                         "stay periodic and are skipped")
     ap.add_argument("--decomp", default="independent", choices=["independent", "slab"],
                     help="independent: a lattice per rank (weak scaling, default); slab: one "
                          "lattice split into x-slabs over the ranks (strong scaling)")
@@ -846,6 +855,8 @@ def main():
         args.size = 500 if args.model == "go-or-grow" else 4096
     if args.impl == "reference":
         return run_reference(args)
+    if args.bc:
+        args.no_fp64 = args.no_ensemble = args.no_cpu_baseline = True
     return run_ours(args)
 
 

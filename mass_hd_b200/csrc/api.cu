@@ -284,8 +284,8 @@ struct mass_lb_handle
   float* diag = nullptr;     // NDIAG planes, allocated on first use
   WallBand band[2];          // FP32 fused with walls: the band lattices
   int nbands = 0;
-  cudaStream_t bstream = nullptr;   // their work beside the fused kernel
-  cudaEvent_t band_in = nullptr, band_out = nullptr;
+  cudaStream_t bstream[2] = {};     // their work beside the fused kernel
+  cudaEvent_t band_in = nullptr, band_out[2] = {};
   bool has_prev = false;     // nxt holds the state before the last step
   bool derived_pending = false;   // unfused: the derived planes await replay_derived
   FusedConfig cfg{128, 256};
@@ -558,9 +558,13 @@ int init_bands(mass_lb_handle* h)
   h->nbands = walls_box(h) ? 2 : 1;
   int least = 0, greatest = 0;
   CU(cudaDeviceGetStreamPriorityRange(&least, &greatest), "priorities");
-  CU(cudaStreamCreateWithPriority(&h->bstream, cudaStreamNonBlocking, greatest), "band stream");
   CU(cudaEventCreateWithFlags(&h->band_in, cudaEventDisableTiming), "event");
-  CU(cudaEventCreateWithFlags(&h->band_out, cudaEventDisableTiming), "event");
+  for(int i = 0; i < h->nbands; ++i)
+  {
+    CU(cudaStreamCreateWithPriority(&h->bstream[i], cudaStreamNonBlocking, greatest),
+       "band stream");
+    CU(cudaEventCreateWithFlags(&h->band_out[i], cudaEventDisableTiming), "event");
+  }
   const int LX = static_cast<int>(h->LX), LY = static_cast<int>(h->LY);
   for(int i = 0; i < h->nbands; ++i)
   {
@@ -596,11 +600,13 @@ BandPtrs band_ptrs(const mass_lb_handle* h, const WallBand& b)
 }
 
 // The band part of one step of a fused lattice with walls, on stream `st`:
-// gather the bands from the state `from` and step them with the walls
-// (with `diag`, keeping the derived fields of the last UpdateQuantities).
-int band_compute(mass_lb_handle* h, const float* from, bool diag, cudaStream_t st)
+// gather bands [first, last) from the state `from` and step them with the
+// walls (with `diag`, keeping the derived fields of the last
+// UpdateQuantities).
+int band_compute(mass_lb_handle* h, int first, int last, const float* from, bool diag,
+                 cudaStream_t st)
 {
-  for(int i = 0; i < h->nbands; ++i)
+  for(int i = first; i < last; ++i)
   {
     WallBand& b = h->band[i];
     const int nb = blocks_for(static_cast<long long>(b.map.BX)*b.map.BY);
@@ -642,18 +648,22 @@ int band_emit(mass_lb_handle* h, float* to, bool diag, cudaStream_t st)
   return 0;
 }
 
-// One fused step of a walled lattice, cur -> nxt: the band work runs on the
-// high-priority band stream beside the warp-strip kernel (both only read
-// cur), and the step stream writes the band rows after both.
+// One fused step of a walled lattice, cur -> nxt: each band's work runs on
+// its own high-priority stream beside the warp-strip kernel (all of them
+// only read cur), and the step stream writes the band rows after them all.
 int fused_step_with_bands(mass_lb_handle* h)
 {
   CU(cudaEventRecord(h->band_in, h->stream), "band fork");
-  CU(cudaStreamWaitEvent(h->bstream, h->band_in, 0), "band fork");
-  if(int r = band_compute(h, h->cur, false, h->bstream)) return r;
-  CU(cudaEventRecord(h->band_out, h->bstream), "band join");
+  for(int i = 0; i < h->nbands; ++i)
+  {
+    CU(cudaStreamWaitEvent(h->bstream[i], h->band_in, 0), "band fork");
+    if(int r = band_compute(h, i, i + 1, h->cur, false, h->bstream[i])) return r;
+    CU(cudaEventRecord(h->band_out[i], h->bstream[i]), "band join");
+  }
   const FusedArgs a = fused_args(h, h->cur, h->nxt, false);
   CU(launch_fused_step(a, h->model, h->cfg, false, h->stream), "fused step");
-  CU(cudaStreamWaitEvent(h->stream, h->band_out, 0), "band join");
+  for(int i = 0; i < h->nbands; ++i)
+    CU(cudaStreamWaitEvent(h->stream, h->band_out[i], 0), "band join");
   return band_emit(h, h->nxt, false, h->stream);
 }
 
@@ -904,9 +914,12 @@ void mass_lb_destroy(mass_lb_handle* h)
   if(h->tot_ev) cudaEventDestroy(h->tot_ev);
   if(h->mq_copy) cudaStreamDestroy(h->mq_copy);
   if(h->xfer) { cudaStreamSynchronize(h->xfer); cudaStreamDestroy(h->xfer); }
-  if(h->bstream) { cudaStreamSynchronize(h->bstream); cudaStreamDestroy(h->bstream); }
+  for(int i = 0; i < 2; ++i)
+  {
+    if(h->bstream[i]) { cudaStreamSynchronize(h->bstream[i]); cudaStreamDestroy(h->bstream[i]); }
+    if(h->band_out[i]) cudaEventDestroy(h->band_out[i]);
+  }
   if(h->band_in) cudaEventDestroy(h->band_in);
-  if(h->band_out) cudaEventDestroy(h->band_out);
   if(h->xfer_in) cudaEventDestroy(h->xfer_in);
   if(h->xfer_out) cudaEventDestroy(h->xfer_out);
   if(h->order_ev) cudaEventDestroy(h->order_ev);
@@ -1280,7 +1293,7 @@ int mass_lb_download(mass_lb_handle* h, int field, double* out)
     CU(launch_fused_step(a, h->model, h->cfg, true, h->stream), "diag replay");
     if(h->nbands)
     {
-      if(int r = band_compute(h, h->nxt, true, h->stream)) return r;
+      if(int r = band_compute(h, 0, h->nbands, h->nxt, true, h->stream)) return r;
       if(int r = band_emit(h, nullptr, true, h->stream)) return r;
     }
     if(int r = check_err_flag(h)) return r;

@@ -783,8 +783,10 @@ bc_scalar_walls(Dims d, ScalarBC<T> job)
 {
   const int LX = d.LX, LY = d.LY;
   const int nwall = 2*LY + 2*LX;
-  for(int idx = blockIdx.x*blockDim.x + threadIdx.x; idx < nwall; idx += blockDim.x*gridDim.x)
+  // one thread per (ghost site, field)
+  for(int t = blockIdx.x*blockDim.x + threadIdx.x; t < nwall*job.nf; t += blockDim.x*gridDim.x)
   {
+    const int f = t / nwall, idx = t - f*nwall;
     int w, k;
     if(idx < LY) { w = W_LEFT; k = idx; }
     else if(idx < 2*LY) { w = W_RIGHT; k = idx - LY; }
@@ -793,49 +795,45 @@ bc_scalar_walls(Dims d, ScalarBC<T> job)
     const XY i = wall_xy(d, w, k);
     const bool pbc = job.mode == BCM_PBC ||
                      (job.mode == BCM_CHANNEL && (w == W_LEFT || w == W_RIGHT));
-    for(int f = 0; f < job.nf; ++f)
+    T* a = job.f[f];
+    if(pbc)
     {
-      T* a = job.f[f];
-      if(pbc)
-      {
-        const XY o = wall_xy(d, OPPv(w), k);
-        a[at(d, i)] = a[at(d, step_xy(d, o, w))];
-      }
-      else s_apply(d, a, i, OPPv(w), job.kind[f]);
+      const XY o = wall_xy(d, OPPv(w), k);
+      a[at(d, i)] = a[at(d, step_xy(d, o, w))];
     }
+    else s_apply(d, a, i, OPPv(w), job.kind[f]);
   }
 }
 
 template<typename T>
-__global__ void __launch_bounds__(32)
+__global__ void __launch_bounds__(64)
 bc_scalar_corners(Dims d, ScalarBC<T> job)
 {
-  if(threadIdx.x >= 4) return;
-  // order of the reference's corner calls does not matter: each corner
-  // reads a wall ghost or a domain site, never another corner
+  // one thread per (corner, field); the order of the reference's corner
+  // calls does not matter: each corner reads a wall ghost or a domain site,
+  // never another corner
+  const int t = threadIdx.x;
+  if(t >= 4*job.nf) return;
   const int cs[4] = {C_RIGHTBACK, C_RIGHTFRONT, C_LEFTBACK, C_LEFTFRONT};
-  const int c = cs[threadIdx.x];
+  const int c = cs[t & 3], f = t >> 2;
   const XY i = corner_xy(d, c);
-  for(int f = 0; f < job.nf; ++f)
+  T* a = job.f[f];
+  if(job.mode == BCM_PBC)
+    a[at(d, i)] = a[at(d, step_xy(d, corner_xy(d, OPPv(c)), c))];
+  else if(job.mode == BCM_CHANNEL)
   {
-    T* a = job.f[f];
-    if(job.mode == BCM_PBC)
-      a[at(d, i)] = a[at(d, step_xy(d, corner_xy(d, OPPv(c)), c))];
-    else if(job.mode == BCM_CHANNEL)
-    {
-      const int w = (c == C_RIGHTBACK || c == C_LEFTBACK) ? W_BACK : W_FRONT;
-      s_apply(d, a, i, OPPv(w), job.kind[f]);
-    }
-    else s_apply(d, a, i, OPPv(c), job.kind[f]);
+    const int w = (c == C_RIGHTBACK || c == C_LEFTBACK) ? W_BACK : W_FRONT;
+    s_apply(d, a, i, OPPv(w), job.kind[f]);
   }
+  else s_apply(d, a, i, OPPv(c), job.kind[f]);
 }
 
 template<typename T>
 void launch_bc_scalar(const Dims& d, const ScalarBC<T>& j, cudaStream_t st)
 {
-  const int n = 2*d.LY + 2*d.LX;
+  const int n = (2*d.LY + 2*d.LX)*j.nf;
   bc_scalar_walls<T><<<(n + 255)/256, 256, 0, st>>>(d, j);
-  bc_scalar_corners<T><<<1, 32, 0, st>>>(d, j);
+  bc_scalar_corners<T><<<1, 64, 0, st>>>(d, j);
 }
 
 template<typename T>
@@ -870,26 +868,24 @@ __global__ void __launch_bounds__(256)
 bc_lb_walls(Dims d, T* ff, T* fn, int kind)
 {
   const int LX = d.LX, LY = d.LY;
-  T* arrs[2] = {ff, fn};
-  for(int idx = blockIdx.x*blockDim.x + threadIdx.x; idx < 2*LY + 2*LX;
-      idx += blockDim.x*gridDim.x)
+  const int nwall = 2*LY + 2*LX;
+  // one thread per (ghost site, population array)
+  for(int t = blockIdx.x*blockDim.x + threadIdx.x; t < 2*nwall; t += blockDim.x*gridDim.x)
   {
+    const int a = t / nwall, idx = t - a*nwall;
+    T* f = a ? fn : ff;
     int w, k;
     if(idx < LY) { w = W_LEFT; k = idx; }
     else if(idx < 2*LY) { w = W_RIGHT; k = idx - LY; }
     else if(idx < 2*LY + LX) { w = W_FRONT; k = idx - 2*LY; }
     else { w = W_BACK; k = idx - 2*LY - LX; }
     const bool lr = (w == W_LEFT || w == W_RIGHT);
-    for(int a = 0; a < 2; ++a)
-    {
-      T* f = arrs[a];
-      if(kind == LBK_PBC || ((kind == LBK_FREESLIP_CHANNEL || kind == LBK_NOSLIP_CHANNEL) && lr))
-        f_pbc_node(d, f, wall_xy(d, w, k), step_xy(d, wall_xy(d, OPPv(w), k), w));
-      else if(kind == LBK_FREESLIP_CHANNEL || kind == LBK_FREESLIP_BOX)
-        f_wall(d, f, w, k, false);
-      else if(kind == LBK_NOSLIP_BOX && lr)
-        f_wall(d, f, w, k, true);
-    }
+    if(kind == LBK_PBC || ((kind == LBK_FREESLIP_CHANNEL || kind == LBK_NOSLIP_CHANNEL) && lr))
+      f_pbc_node(d, f, wall_xy(d, w, k), step_xy(d, wall_xy(d, OPPv(w), k), w));
+    else if(kind == LBK_FREESLIP_CHANNEL || kind == LBK_FREESLIP_BOX)
+      f_wall(d, f, w, k, false);
+    else if(kind == LBK_NOSLIP_BOX && lr)
+      f_wall(d, f, w, k, true);
   }
 }
 
@@ -898,12 +894,12 @@ __global__ void __launch_bounds__(256)
 bc_lb_noslip_fb(Dims d, T* ff, T* fn)
 {
   const int LX = d.LX;
-  T* arrs[2] = {ff, fn};
-  for(int idx = blockIdx.x*blockDim.x + threadIdx.x; idx < 2*LX; idx += blockDim.x*gridDim.x)
+  for(int t = blockIdx.x*blockDim.x + threadIdx.x; t < 4*LX; t += blockDim.x*gridDim.x)
   {
+    const int a = t / (2*LX), idx = t - a*2*LX;
     const int w = idx < LX ? W_FRONT : W_BACK;
     const int k = idx < LX ? idx : idx - LX;
-    for(int a = 0; a < 2; ++a) f_wall(d, arrs[a], w, k, true);
+    f_wall(d, a ? fn : ff, w, k, true);
   }
 }
 
@@ -911,29 +907,27 @@ template<typename T>
 __global__ void __launch_bounds__(32)
 bc_lb_corners(Dims d, T* ff, T* fn, int kind)
 {
-  if(threadIdx.x >= 4) return;
-  T* arrs[2] = {ff, fn};
+  // one thread per (corner, population array)
+  const int t = threadIdx.x;
+  if(t >= 8) return;
+  T* f = (t >> 2) ? fn : ff;
   const int cs[4] = {C_RIGHTBACK, C_RIGHTFRONT, C_LEFTBACK, C_LEFTFRONT};
-  const int c = cs[threadIdx.x];
+  const int c = cs[t & 3];
   const XY i = corner_xy(d, c);
-  for(int a = 0; a < 2; ++a)
+  if(kind == LBK_PBC)
+    f_pbc_node(d, f, i, step_xy(d, corner_xy(d, OPPv(c)), c));
+  else if(kind == LBK_FREESLIP_CHANNEL)
   {
-    T* f = arrs[a];
-    if(kind == LBK_PBC)
-      f_pbc_node(d, f, i, step_xy(d, corner_xy(d, OPPv(c)), c));
-    else if(kind == LBK_FREESLIP_CHANNEL)
-    {
-      const int w = (c == C_RIGHTBACK || c == C_LEFTBACK) ? W_BACK : W_FRONT;
-      const int p = c_proj[w][c];
-      const int v = OPPv(c);
-      const XY l = step_xy(d, corner_xy(d, c_refl[p][c]), p);
-      f[v*d.NE + at(d, i)] = f[v*d.NE + at(d, l)];
-    }
-    else
-    {
-      const int v = OPPv(c);
-      f[v*d.NE + at(d, i)] = f[c*d.NE + at(d, step_xy(d, i, v))];
-    }
+    const int w = (c == C_RIGHTBACK || c == C_LEFTBACK) ? W_BACK : W_FRONT;
+    const int p = c_proj[w][c];
+    const int v = OPPv(c);
+    const XY l = step_xy(d, corner_xy(d, c_refl[p][c]), p);
+    f[v*d.NE + at(d, i)] = f[v*d.NE + at(d, l)];
+  }
+  else
+  {
+    const int v = OPPv(c);
+    f[v*d.NE + at(d, i)] = f[c*d.NE + at(d, step_xy(d, i, v))];
   }
 }
 
@@ -942,9 +936,9 @@ bool lb_noslip(int kind) { return kind == LBK_NOSLIP_CHANNEL || kind == LBK_NOSL
 template<typename T>
 void launch_bc_lb(const Dims& d, T* ff, T* fn, int kind, cudaStream_t st)
 {
-  const int n = 2*d.LY + 2*d.LX;
+  const int n = 2*(2*d.LY + 2*d.LX);
   bc_lb_walls<T><<<(n + 255)/256, 256, 0, st>>>(d, ff, fn, kind);
-  if(lb_noslip(kind)) bc_lb_noslip_fb<T><<<(2*d.LX + 255)/256, 256, 0, st>>>(d, ff, fn);
+  if(lb_noslip(kind)) bc_lb_noslip_fb<T><<<(4*d.LX + 255)/256, 256, 0, st>>>(d, ff, fn);
   bc_lb_corners<T><<<1, 32, 0, st>>>(d, ff, fn, kind);
 }
 
