@@ -282,6 +282,9 @@ struct mass_lb_handle
   float* cur = nullptr;
   float* nxt = nullptr;
   float* diag = nullptr;     // NDIAG planes, allocated on first use
+  float* pred = nullptr;     // FP32 fused with npc > 1: fn, QNxx, QNyx[, phn] of the step
+  float* scratch = nullptr;  // its derived-field replay's throw-away outputs (NP planes)
+  bool diag_n_dev = false;   // the diagnostic n plane holds the density deviation
   WallBand band[2];          // FP32 fused with walls: the band lattices
   int nbands = 0;
   cudaStream_t bstream[2] = {};     // their work beside the fused kernel
@@ -465,7 +468,58 @@ FusedArgs fused_args(mass_lb_handle* h, const float* in, float* out, bool diag)
   a.p = h->model == GOG ? p32_of(h->P, h->s32.ph) : p32_of(h->P);
   // go-or-grow always reads its growth-rate plane (zero until a source is set)
   a.src = h->src_on || h->model == GOG ? h->src_fused : nullptr;
+  a.pred = !diag && h->P.npc > 1 ? h->pred : nullptr;
   return a;
+}
+
+// Lattices the CTA-strip kernel cannot step: a phi source, go-or-grow and
+// npc > 1 are in the warp-strip kernel only.
+bool warp_strip_only(const mass_lb_handle* h)
+{
+  return h->src_on || h->model == GOG || h->P.npc > 1;
+}
+
+// A further corrector (npc > 1) of a fused periodic lattice, `in` -> `out`:
+// the sweeps' corrector sub-step on a view of the fused planes (they agree
+// plane for plane with the sweeps' periodic layout) and of the predictor
+// values the warp-strip kernel wrote. With `diag` it also writes the
+// derived fields of its UpdateQuantities into the diagnostic planes.
+int extra_corrector(mass_lb_handle* h, const float* in, float* out, bool diag)
+{
+  const long long p = static_cast<long long>(h->LX)*h->LY;
+  State<float> v{};
+  v.ff = const_cast<float*>(in);
+  v.Qxx = const_cast<float*>(in) + 9*p;
+  v.Qyx = const_cast<float*>(in) + 10*p;
+  v.fn = h->pred;
+  v.QNxx = h->pred + 9*p;
+  v.QNyx = h->pred + 10*p;
+  v.ff_tmp = out;
+  v.Qxx_tmp = out + 9*p;
+  v.Qyx_tmp = out + 10*p;
+  if(h->model != NEM)
+  {
+    v.phi = const_cast<float*>(in) + 11*p;
+    v.phn = h->pred + 11*p;
+    v.phi_tmp = out + 11*p;
+    v.src = h->src_on ? h->src_fused : nullptr;
+  }
+  if(diag)
+  {
+    // the fused diagnostic plane order (fields n .. sigma_active_yx)
+    float* g = h->diag;
+    v.n = g; v.ux = g + p; v.uy = g + 2*p; v.Hxx = g + 5*p; v.Hyx = g + 6*p;
+    v.dxQxx = g + 8*p; v.dyQxx = g + 9*p; v.dxQyx = g + 10*p; v.dyQyx = g + 11*p;
+    v.sXX = g + 12*p; v.sYY = g + 13*p; v.sYX = g + 14*p; v.sXY = g + 15*p;
+    if(h->model != NEM)
+    {
+      v.uxp = g + 3*p; v.uyp = g + 4*p; v.MU = g + 7*p;
+      for(int k = 0; k < 7; ++k) v.diag[k] = g + (16 + k)*p;
+    }
+  }
+  if(corrector_substep_f32(h->d, h->P, v, diag, h->stream) != 0)
+    return cuda_fail(cudaGetLastError(), "corrector");
+  return 0;
 }
 
 // Moves an FP32 fused state into the unfused sweeps' state (allocated on
@@ -684,8 +738,7 @@ std::vector<FusedConfig> tile_candidates(const mass_lb_handle* h)
   for(int nt : {32, 64, 128, 256})
   {
     if(!fused_supported(static_cast<int>(h->LX), static_cast<int>(h->LY), nt)) continue;
-    // the phi source and go-or-grow are in the warp-strip kernel only
-    if((h->src_on || h->model == GOG) && nt != 32) continue;
+    if(warp_strip_only(h) && nt != 32) continue;
     for(int rows : {8, 16, 32, 64, 128, 256, 512, 1024})
     {
       if(rows > static_cast<int>(h->LX) && rows != 8) continue;
@@ -841,7 +894,8 @@ int mass_lb_create(const mass_lb_params* params, unsigned LX, unsigned LY,
     // the fused warp-strip kernel: every model with npc = 1, on periodic
     // lattices and, with the wall bands beside it, on walled ones; the rest
     // runs the unfused sweeps in FP32
-    h->fused = h->P.npc == 1 && (!h->wall || bands_fit(h)) &&
+    h->fused = (h->P.npc == 1 || (!h->wall && h->model != GOG)) &&
+               (!h->wall || bands_fit(h)) &&
                fused_supported(static_cast<int>(LX), static_cast<int>(LY), 64);
     if(h->fused)
     {
@@ -853,6 +907,11 @@ int mass_lb_create(const mass_lb_params* params, unsigned LX, unsigned LY,
         return bail(fail(MASS_LB_ECUDA, "memset"));
       if(h->wall)
         if(int r = init_bands(h)) return bail(r);
+      if(h->P.npc > 1)
+      {
+        const size_t np = static_cast<size_t>(h->model == NEM ? 11 : 12)*LX*LY;
+        if(int r = dalloc(h, &h->pred, np)) return bail(r);
+      }
       if(h->model == GOG)
       {
         // the growth-rate plane every go-or-grow step reads, zero until set
@@ -865,7 +924,8 @@ int mass_lb_create(const mass_lb_params* params, unsigned LX, unsigned LY,
       {
         int nt = 0, rows = 0;
         if(std::sscanf(env, "%d,%d", &nt, &rows) == 2 &&
-           fused_supported(static_cast<int>(LX), static_cast<int>(LY), nt) && rows > 0)
+           fused_supported(static_cast<int>(LX), static_cast<int>(LY), nt) && rows > 0 &&
+           (nt == 32 || !warp_strip_only(h)))
         {
           h->cfg = FusedConfig{nt, rows};
           h->tuned = true;
@@ -1152,6 +1212,13 @@ int mass_lb_step(mass_lb_handle* h, unsigned nsteps)
       {
         const FusedArgs a = fused_args(h, h->cur, h->nxt, false);
         CU(launch_fused_step(a, h->model, h->cfg, false, h->stream), "fused step");
+        // npc > 1: the further correctors; the last one's input stays in
+        // nxt after the swap below, for the derived-field replay
+        for(unsigned c = 2; c <= h->P.npc; ++c)
+        {
+          if(int r = extra_corrector(h, h->nxt, h->cur, false)) return r;
+          std::swap(h->cur, h->nxt);
+        }
       }
       std::swap(h->cur, h->nxt);
     }
@@ -1198,7 +1265,8 @@ static int get_primary(mass_lb_handle* h, int field, double* out, bool sync = tr
       {
         // derived fields from the replayed diagnostics, mass_lb_field order
         const int p = field - MASS_LB_N;
-        k_get_scalar<float><<<nb, 256, 0, h->io>>>(h->stage, h->diag + p*plane, x0, nrows, LY, 0, LY, 0.0);
+        k_get_scalar<float><<<nb, 256, 0, h->io>>>(h->stage, h->diag + p*plane, x0, nrows, LY, 0, LY,
+                                                   p == 0 && h->diag_n_dev ? h->P.rho : 0.0);
       }
     }
     else if(h->precision == MASS_LB_FP64)
@@ -1287,14 +1355,27 @@ int mass_lb_download(mass_lb_handle* h, int field, double* out)
     if(!h->has_prev)
       return fail(MASS_LB_EUNSUPPORTED, "derived fields need a step since the last upload");
     if(int r = ensure_diag_buffer(h)) return r;
-    // replay the last step from the retained input with the diagnostic
-    // outputs on (the replay does not write the state)
-    const FusedArgs a = fused_args(h, h->nxt, h->cur, true);
-    CU(launch_fused_step(a, h->model, h->cfg, true, h->stream), "diag replay");
-    if(h->nbands)
+    if(h->P.npc > 1)
     {
-      if(int r = band_compute(h, 0, h->nbands, h->nxt, true, h->stream)) return r;
-      if(int r = band_emit(h, nullptr, true, h->stream)) return r;
+      // the last corrector again, from its input (nxt) and the step's
+      // predictor values, its outputs thrown away
+      if(!h->scratch)
+        if(int r = dalloc(h, &h->scratch, static_cast<size_t>(nplanes(h))*h->LX*h->LY)) return r;
+      if(int r = extra_corrector(h, h->nxt, h->scratch, true)) return r;
+      h->diag_n_dev = true;
+    }
+    else
+    {
+      // replay the last step from the retained input with the diagnostic
+      // outputs on (the replay does not write the state)
+      const FusedArgs a = fused_args(h, h->nxt, h->cur, true);
+      CU(launch_fused_step(a, h->model, h->cfg, true, h->stream), "diag replay");
+      if(h->nbands)
+      {
+        if(int r = band_compute(h, 0, h->nbands, h->nxt, true, h->stream)) return r;
+        if(int r = band_emit(h, nullptr, true, h->stream)) return r;
+      }
+      h->diag_n_dev = false;
     }
     if(int r = check_err_flag(h)) return r;
   }
@@ -1554,9 +1635,11 @@ int mass_lb_launches_per_step(mass_lb_handle* h)
 {
   if(!h) return fail(MASS_LB_EINVAL, "null handle");
   // fused with walls: per band a gather, [chi,] the wall sweeps, a scatter
+  // npc > 1: a corrector sub-step per further corrector
   if(h->fused)
-    return 1 + h->nbands*(2 + (h->model == GOG ? 1 : 0) +
-                          launches_unfused(h->model, static_cast<int>(h->bc), 1));
+    return static_cast<int>(h->P.npc) +
+           h->nbands*(2 + (h->model == GOG ? 1 : 0) +
+                      launches_unfused(h->model, static_cast<int>(h->bc), 1));
   return launches_unfused(h->model, h->wall ? static_cast<int>(h->bc) : 0, h->P.npc);
 }
 
@@ -1578,6 +1661,9 @@ int mass_lb_set_tile(mass_lb_handle* h, int threads, int rows)
   if(threads == 0 && rows == 0) { h->tuned = false; return 0; }
   if(!fused_supported(static_cast<int>(h->LX), static_cast<int>(h->LY), threads) || rows <= 0)
     return fail(MASS_LB_EINVAL, "tile does not fit this lattice");
+  if(threads != 32 && warp_strip_only(h))
+    return fail(MASS_LB_EUNSUPPORTED,
+                "a phi source, go-or-grow and npc > 1 need the warp-strip kernel (threads = 32)");
   h->cfg = FusedConfig{threads, rows};
   h->tuned = true;
   return 0;

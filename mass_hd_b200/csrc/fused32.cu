@@ -627,7 +627,7 @@ cudaError_t launch_nt(const FusedArgs& a, int model, int rows, bool diag, cudaSt
 cudaError_t launch_fused_step(const FusedArgs& a, int model, FusedConfig cfg,
                               bool diag, cudaStream_t st)
 {
-  if(a.src && cfg.nt != 32) return cudaErrorInvalidValue;
+  if((a.src || a.pred) && cfg.nt != 32) return cudaErrorInvalidValue;
   switch(cfg.nt)
   {
     case 32:  return launch_fused_warp_step(a, model, cfg.rows, diag, st);

@@ -49,6 +49,8 @@ struct FusedArgs
   PairParams pp;       // filled by the warp-strip launcher
   const float* src;    // per-site phi source rate (LX*LY) or null; warp-strip kernel only
                        // (go-or-grow: the growth rate, always present)
+  float* pred;         // or null; warp-strip kernel, lyotropic and nematic: fn (9 planes),
+                       // QNxx, QNyx[, phn] of the step, for the further correctors of npc > 1
 };
 
 // Tile shapes the autotuner may pick.

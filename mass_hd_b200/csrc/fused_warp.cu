@@ -484,6 +484,7 @@ struct ItemView
   long long plane;
   int rows;
   const float* src;   // per-site phi source rate (SRC launches)
+  float* pred;        // PRED launches: fn (9 planes), QNxx, QNyx[, phn] per site
 };
 
 // Per-warp shared memory: input ring | delayed populations (3 rows) |
@@ -501,7 +502,7 @@ struct WarpSmem
 // Returns false if a bounded wait gave up. SRC adds the division models'
 // phi source, phi_tmp += phi*r after each UpdateFields
 // (src/models/lyotropic-with-division.cpp:121), in C and E.
-template<int MODEL, bool DIAG, bool SRC>
+template<int MODEL, bool DIAG, bool SRC, bool PRED = false>
 __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P, const int strip,
                                           const int chunk, float* ring, float* dpop, float* hrow,
                                           uint64_t* mbar, const int lane, unsigned& rowbase)
@@ -723,6 +724,35 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
 #pragma unroll
       for(int v = 0; v < 9; ++v)
         *reinterpret_cast<float2*>(hrow + ((i & 1)*9 + v)*COLS + 2*lane) = fma(hitau, fs[v], ns[v]).v;
+      if constexpr (PRED)
+      {
+        // what every further corrector of the step reads (npc > 1): the
+        // moved predictor populations fn and the half-step fields QN of
+        // this row, in the sweeps' plane order
+        const int xs = x0 - 5 + i;
+        if(xs >= x0 && xs < x0 + rows)
+        {
+          const long long pl = a.plane;
+          float* o = a.pred + static_cast<long long>(xs)*LY + yg;
+          constexpr int NPRED = MODEL == NEM ? 11 : 12;
+          f2 w[12];
+#pragma unroll
+          for(int v = 0; v < 9; ++v) w[v] = ns[v];
+          w[9] = qn1[0];
+          w[10] = qn1[1];
+          w[11] = qn1[2];
+          if(colx_ok && coly_ok)
+          {
+#pragma unroll
+            for(int k = 0; k < NPRED; ++k) *reinterpret_cast<float2*>(o + k*pl) = w[k].v;
+          }
+          else if(colx_ok)
+          {
+#pragma unroll
+            for(int k = 0; k < NPRED; ++k) o[k*pl] = w[k].v.x;
+          }
+        }
+      }
       if constexpr (DIAG)
       {
         const int xs = x0 - 5 + i;
@@ -864,7 +894,7 @@ __device__ __forceinline__ void warp_smem(float*& ring, float*& dpop, float*& hr
 }
 
 // One lattice: work item = blockIdx.x*WPB + warp.
-template<int MODEL, bool DIAG, bool SRC>
+template<int MODEL, bool DIAG, bool SRC, bool PRED>
 __global__ void __launch_bounds__(32*WPB, 2)
 fused_warp_kernel(const __grid_constant__ FusedArgs a, const int nitems)
 {
@@ -874,13 +904,13 @@ fused_warp_kernel(const __grid_constant__ FusedArgs a, const int nitems)
   float *ring, *dpop, *hrow;
   uint64_t* mbar;
   warp_smem<MODEL>(ring, dpop, hrow, mbar, warp, lane);
-  const ItemView v{a.in, a.out, a.diag, a.err, a.LX, a.LY, a.plane, a.rows, a.src};
+  const ItemView v{a.in, a.out, a.diag, a.err, a.LX, a.LY, a.plane, a.rows, a.src, a.pred};
   unsigned rowbase = 0;
   // chunk-major: the warps in flight together work down a few strips at
   // every height of the lattice (about 4 % faster than strip-major at 4096^2)
   const int nchunks = (a.LX + a.rows - 1)/a.rows;
-  warp_item<MODEL, DIAG, SRC>(v, a.pp, item / nchunks, item % nchunks, ring, dpop, hrow,
-                         mbar, lane, rowbase);
+  warp_item<MODEL, DIAG, SRC, PRED>(v, a.pp, item / nchunks, item % nchunks, ring, dpop, hrow,
+                                     mbar, lane, rowbase);
 }
 
 // Ensemble: persistent warps take (run, strip, chunk) items from a packed
@@ -908,7 +938,7 @@ fused_warp_ensemble_kernel(const EnsRun* __restrict__ runs, const int* __restric
     const EnsRun& R = runs[r];
     const int local = item - R.item0;
     const ItemView v{parity ? R.b : R.a, parity ? R.a : R.b, nullptr, err, R.LX, R.LY,
-                     R.plane, R.rows, nullptr};
+                     R.plane, R.rows, nullptr, nullptr};
     const int nchunks = (R.LX + R.rows - 1)/R.rows;   // chunk-major, as fused_warp_kernel
     if(!warp_item<MODEL, false, false>(v, c_ens_pp[R.slot], local / nchunks, local % nchunks,
                                 ring, dpop, hrow, mbar, lane, rowbase))
@@ -923,10 +953,10 @@ constexpr size_t smem_bytes()
          static_cast<size_t>(WPB)*RING*sizeof(uint64_t);
 }
 
-template<int MODEL, bool DIAG, bool SRC>
+template<int MODEL, bool DIAG, bool SRC, bool PRED = false>
 cudaError_t launch_t(const FusedArgs& a, int rows, cudaStream_t st)
 {
-  auto kern = fused_warp_kernel<MODEL, DIAG, SRC>;
+  auto kern = fused_warp_kernel<MODEL, DIAG, SRC, PRED>;
   static unsigned long long attr_set = 0;
   int dev = 0;
   cudaGetDevice(&dev);
@@ -1019,10 +1049,17 @@ int ensemble_grid(int model)
 cudaError_t launch_fused_warp_step(const FusedArgs& a, int model, int rows, bool diag,
                                    cudaStream_t st)
 {
+  // a non-diagnostic launch with a.pred set also writes the predictor
+  // values the further correctors of npc > 1 read (lyotropic, nematic)
+  const bool pred = !diag && a.pred;
   if(model == LYO)
   {
     if(a.src)
+    {
+      if(pred) return launch_t<LYO, false, true, true>(a, rows, st);
       return diag ? launch_t<LYO, true, true>(a, rows, st) : launch_t<LYO, false, true>(a, rows, st);
+    }
+    if(pred) return launch_t<LYO, false, false, true>(a, rows, st);
     return diag ? launch_t<LYO, true, false>(a, rows, st) : launch_t<LYO, false, false>(a, rows, st);
   }
   if(model == GOG)
@@ -1031,6 +1068,7 @@ cudaError_t launch_fused_warp_step(const FusedArgs& a, int model, int rows, bool
     if(!a.src) return cudaErrorInvalidValue;
     return diag ? launch_t<GOG, true, false>(a, rows, st) : launch_t<GOG, false, false>(a, rows, st);
   }
+  if(pred) return launch_t<NEM, false, false, true>(a, rows, st);
   return diag ? launch_t<NEM, true, false>(a, rows, st) : launch_t<NEM, false, false>(a, rows, st);
 }
 

@@ -1359,6 +1359,25 @@ int relax_unfused_f32(const Dims& d, const Params& P, State<float>& s, int bc,
   return relax_impl<float>(d, P, s, bc, nsteps, dt, relax_phi, relax_Q, sum_out, st);
 }
 
+int corrector_substep_f32(const Dims& d, const Params& P, const State<float>& s, bool diag,
+                          cudaStream_t st)
+{
+  switch(P.model)
+  {
+    case LYO:
+      if(diag) launch_substep<float, true, LYO, false, true>(d, P, s, 1, st);
+      else launch_substep<float, true, LYO, false, false>(d, P, s, 0, st);
+      break;
+    case NEM:
+      if(diag) launch_substep<float, true, NEM, false, true>(d, P, s, 1, st);
+      else launch_substep<float, true, NEM, false, false>(d, P, s, 0, st);
+      break;
+    default:
+      return -1;
+  }
+  return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
 int update_chi_f32(const Dims& d, State<float>& s, cudaStream_t st)
 {
   const dim3 blk(64, 4);

@@ -55,6 +55,13 @@ int relax_unfused_f32(const Dims& d, const Params& P, State<float>& s, int bc,
                       unsigned nsteps, double dt, int relax_phi, int relax_Q,
                       double* sum_out, cudaStream_t st);
 
+// One corrector sub-step (UpdateQuantities and the corrector UpdateFields)
+// of a periodic FP32 lattice, lyotropic or nematic: reads ff, Qxx, Qyx,
+// phi, fn, QNxx, QNyx, phn (and src), writes ff_tmp, Qxx_tmp, Qyx_tmp,
+// phi_tmp; with `diag`, also the derived fields of its UpdateQuantities.
+int corrector_substep_f32(const Dims& d, const Params& P, const State<float>& s, bool diag,
+                          cudaStream_t st);
+
 // chi = m/phi over the domain (after an upload of m or phi)
 int update_chi_f64(const Dims& d, State<double>& s, cudaStream_t st);
 int update_chi_f32(const Dims& d, State<float>& s, cudaStream_t st);
