@@ -731,7 +731,8 @@ int check_err_flag(mass_lb_handle* h)
 }
 
 // Candidate tiles for the autotuner: strip widths that fit the lattice and
-// chunk heights from 32 rows to the whole lattice.
+// chunk heights from 32 rows to the whole lattice, and from 2 rows on
+// lattices of up to 2 M sites.
 std::vector<FusedConfig> tile_candidates(const mass_lb_handle* h)
 {
   std::vector<FusedConfig> c;
@@ -739,7 +740,9 @@ std::vector<FusedConfig> tile_candidates(const mass_lb_handle* h)
   {
     if(!fused_supported(static_cast<int>(h->LX), static_cast<int>(h->LY), nt)) continue;
     if(warp_strip_only(h) && nt != 32) continue;
-    for(int rows : {8, 16, 32, 64, 128, 256, 512, 1024})
+    // 2 to 12 rows: on a small lattice the best chunk is the shortest whose
+    // warps still fit in one wave (500^2: 4 rows, 282 CTAs)
+    for(int rows : {2, 4, 6, 8, 12, 16, 32, 64, 128, 256, 512, 1024})
     {
       if(rows > static_cast<int>(h->LX) && rows != 8) continue;
       // short chunks only where a lattice has few strips to spread: each
