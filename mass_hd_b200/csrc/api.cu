@@ -134,20 +134,18 @@ inline int blocks_for(long long n)
 
 // ---- wall bands of a fused lattice ----------------------------------------
 // A fused FP32 lattice with walls steps in two parts. The warp-strip kernel
-// steps the whole lattice as if it were periodic. One Step() reaches 4
-// sites (predictor UpdateQuantities, UpdateFields and Move, corrector
-// UpdateQuantities and UpdateFields), so every site at least 4 sites from a
-// wall gets exactly what the wall step gives it: its dependence cone holds
-// no ghost value and no site whose update a wall changes. The sites nearer
-// a wall come from a band lattice: the kBandHalf rows next to each wall of
-// one axis, side by side, stepped by the wall-aware sweeps
-// (step_unfused_f32) with the lattice's own boundary kind. The band's
-// outer kBandKeep rows on each side are exact; the cut between its halves
-// reaches only rows that are discarded. Channels (walls across y) take one
-// band of LX x 2*kBandHalf sites, boxes a second of 2*kBandHalf x LY.
-constexpr int kBandHalf = 8;
-constexpr int kBandKeep = 4;
-
+// steps the whole lattice as if it were periodic. One Step() reaches
+// keep = 2 + 2*npc sites (predictor UpdateQuantities, UpdateFields and
+// Move, then UpdateQuantities and UpdateFields per corrector), so every site
+// at least `keep` sites from a wall gets exactly what the wall step gives
+// it: its dependence cone holds no ghost value and no site whose update a
+// wall changes. The sites nearer a wall come from a band lattice: the
+// half = 2*keep rows next to each wall of one axis, side by side, stepped
+// by the wall-aware sweeps (step_unfused_f32) with the lattice's own
+// boundary kind. The band's outer `keep` rows on each side are exact; the
+// cut between its halves reaches only rows that are discarded. Channels
+// (walls across y) take one band of LX x 2*half sites, boxes a second of
+// 2*half x LY.
 struct BandMap
 {
   int axis;            // 0: the band crosses y (walls front/back), 1: crosses x
@@ -156,6 +154,7 @@ struct BandMap
   int EY;              // the band's extended row (BY + 2, ghost ring g = 1)
   long long NE;        // the band's extended plane
   long long plane;     // LX*LY, the fused plane
+  int half, keep;      // rows taken next to each wall, rows kept
 };
 
 // band planes: ff (9 planes), the scalars Qxx, Qyx, [phi], [m] in the fused
@@ -177,9 +176,9 @@ struct BandDiag
   float rho;
 };
 
-__device__ __forceinline__ int band_row(int i, int N)
+__device__ __forceinline__ int band_row(const BandMap& m, int i, int N)
 {
-  return i < kBandHalf ? i : N - 2*kBandHalf + i;
+  return i < m.half ? i : N - 2*m.half + i;
 }
 
 // band site k -> fused index gi, band extended index bi; keep: the site is
@@ -188,12 +187,12 @@ __device__ __forceinline__ bool band_site(const BandMap& m, long long k, long lo
                                           long long& bi)
 {
   const int bx = static_cast<int>(k / m.BY), by = static_cast<int>(k % m.BY);
-  const int x = m.axis == 1 ? band_row(bx, m.LX) : bx;
-  const int y = m.axis == 0 ? band_row(by, m.LY) : by;
+  const int x = m.axis == 1 ? band_row(m, bx, m.LX) : bx;
+  const int y = m.axis == 0 ? band_row(m, by, m.LY) : by;
   gi = static_cast<long long>(x)*m.LY + y;
   bi = static_cast<long long>(bx + 1)*m.EY + (by + 1);
   const int r = m.axis == 0 ? by : bx;
-  return r < kBandKeep || r >= 2*kBandHalf - kBandKeep;
+  return r < m.keep || r >= 2*m.half - m.keep;
 }
 
 __global__ void __launch_bounds__(256)
@@ -288,7 +287,7 @@ struct mass_lb_handle
   WallBand band[2];          // FP32 fused with walls: the band lattices
   int nbands = 0;
   cudaStream_t bstream[2] = {};     // their work beside the fused kernel
-  cudaEvent_t band_in = nullptr, band_out[2] = {};
+  cudaEvent_t band_in = nullptr, band_read[2] = {}, band_out[2] = {};
   bool has_prev = false;     // nxt holds the state before the last step
   bool derived_pending = false;   // unfused: the derived planes await replay_derived
   FusedConfig cfg{128, 256};
@@ -517,7 +516,10 @@ int extra_corrector(mass_lb_handle* h, const float* in, float* out, bool diag)
       for(int k = 0; k < 7; ++k) v.diag[k] = g + (16 + k)*p;
     }
   }
-  if(corrector_substep_f32(h->d, h->P, v, diag, h->stream) != 0)
+  // the fused planes carry no ghost ring, walls or not: a periodic view
+  const int LX = static_cast<int>(h->LX), LY = static_cast<int>(h->LY);
+  const Dims d{LX, LY, 0, LX, LY, p};
+  if(corrector_substep_f32(d, h->P, v, diag, h->stream) != 0)
     return cuda_fail(cudaGetLastError(), "corrector");
   return 0;
 }
@@ -601,10 +603,15 @@ bool walls_box(const mass_lb_handle* h)
   return h->model != NEM && (h->bc == 3 || h->bc == 4);
 }
 
+// rows one step reaches (the band rows kept) and rows taken per wall
+int band_keep(const mass_lb_handle* h) { return 2 + 2*static_cast<int>(h->P.npc); }
+int band_half(const mass_lb_handle* h) { return 2*band_keep(h); }
+
 // the bands need two disjoint halves on every walled axis
 bool bands_fit(const mass_lb_handle* h)
 {
-  return h->LY >= 2u*kBandHalf && (!walls_box(h) || h->LX >= 2u*kBandHalf);
+  const unsigned n = 2u*band_half(h);
+  return h->LY >= n && (!walls_box(h) || h->LX >= n);
 }
 
 int init_bands(mass_lb_handle* h)
@@ -617,15 +624,17 @@ int init_bands(mass_lb_handle* h)
   {
     CU(cudaStreamCreateWithPriority(&h->bstream[i], cudaStreamNonBlocking, greatest),
        "band stream");
+    CU(cudaEventCreateWithFlags(&h->band_read[i], cudaEventDisableTiming), "event");
     CU(cudaEventCreateWithFlags(&h->band_out[i], cudaEventDisableTiming), "event");
   }
   const int LX = static_cast<int>(h->LX), LY = static_cast<int>(h->LY);
+  const int half = band_half(h), keep = band_keep(h);
   for(int i = 0; i < h->nbands; ++i)
   {
     WallBand& b = h->band[i];
-    const int BX = i == 0 ? LX : 2*kBandHalf, BY = i == 0 ? 2*kBandHalf : LY;
+    const int BX = i == 0 ? LX : 2*half, BY = i == 0 ? 2*half : LY;
     b.d = Dims{BX, BY, 1, BX + 2, BY + 2, static_cast<long long>(BX + 2)*(BY + 2)};
-    b.map = BandMap{i, LX, LY, BX, BY, BY + 2, b.d.NE, static_cast<long long>(LX)*LY};
+    b.map = BandMap{i, LX, LY, BX, BY, BY + 2, b.d.NE, static_cast<long long>(LX)*LY, half, keep};
     if(int r = alloc_state(h, b.s, b.d)) return r;
     if(int r = zero_state(h, b.s, b.d)) return r;
     if(h->model != NEM)
@@ -653,34 +662,33 @@ BandPtrs band_ptrs(const mass_lb_handle* h, const WallBand& b)
   return p;
 }
 
-// The band part of one step of a fused lattice with walls, on stream `st`:
-// gather bands [first, last) from the state `from` and step them with the
-// walls (with `diag`, keeping the derived fields of the last
-// UpdateQuantities).
-int band_compute(mass_lb_handle* h, int first, int last, const float* from, bool diag,
-                 cudaStream_t st)
+// Band i's part of one step of a fused lattice with walls, on stream `st`:
+// gather it from the state `from` (event band_read[i] marks the end of the
+// reads), then step it with the walls. The step also keeps the derived
+// fields of its last UpdateQuantities, which a download of derived fields
+// scatters (band_emit with diag) without stepping again.
+int band_compute(mass_lb_handle* h, int i, const float* from, cudaStream_t st)
 {
-  for(int i = first; i < last; ++i)
-  {
-    WallBand& b = h->band[i];
-    const int nb = blocks_for(static_cast<long long>(b.map.BX)*b.map.BY);
-    const BandPtrs p = band_ptrs(h, b);
-    k_band_gather<<<nb, 256, 0, st>>>(b.map, from, p);
-    CU(cudaGetLastError(), "band gather");
-    b.s.src = p.src;
-    b.s.conserve_phi = 0;
-    b.s.phisum = nullptr;
-    b.s.ph = h->s32.ph;
-    if(h->model == GOG && update_chi_f32(b.d, b.s, st))
-      return cuda_fail(cudaGetLastError(), "band chi");
-    if(step_unfused_f32(b.d, h->P, b.s, static_cast<int>(h->bc), 1, diag, st) != 0)
-      return cuda_fail(cudaGetLastError(), "band step");
-  }
+  WallBand& b = h->band[i];
+  const int nb = blocks_for(static_cast<long long>(b.map.BX)*b.map.BY);
+  const BandPtrs p = band_ptrs(h, b);
+  k_band_gather<<<nb, 256, 0, st>>>(b.map, from, p);
+  CU(cudaGetLastError(), "band gather");
+  CU(cudaEventRecord(h->band_read[i], st), "band gather");
+  b.s.src = p.src;
+  b.s.conserve_phi = 0;
+  b.s.phisum = nullptr;
+  b.s.ph = h->s32.ph;
+  if(h->model == GOG && update_chi_f32(b.d, b.s, st))
+    return cuda_fail(cudaGetLastError(), "band chi");
+  if(step_unfused_f32(b.d, h->P, b.s, static_cast<int>(h->bc), 1, true, st) != 0)
+    return cuda_fail(cudaGetLastError(), "band step");
   return 0;
 }
 
 // Then, on stream `st`: the bands' exact rows into the state `to` or, with
-// `diag`, their derived fields into the diagnostic planes.
+// `diag`, their derived fields into the diagnostic planes (whose n plane
+// holds the density, or its deviation after a corrector replay).
 int band_emit(mass_lb_handle* h, float* to, bool diag, cudaStream_t st)
 {
   for(int i = 0; i < h->nbands; ++i)
@@ -693,7 +701,7 @@ int band_emit(mass_lb_handle* h, float* to, bool diag, cudaStream_t st)
       const BandDiag dd{{s.n, s.ux, s.uy, s.uxp, s.uyp, s.Hxx, s.Hyx, s.MU, s.dxQxx, s.dyQxx,
                          s.dxQyx, s.dyQyx, s.sXX, s.sYY, s.sYX, s.sXY, s.diag[0], s.diag[1],
                          s.diag[2], s.diag[3], s.diag[4], s.diag[5], s.diag[6]},
-                        static_cast<float>(h->P.rho)};
+                        h->diag_n_dev ? 0.f : static_cast<float>(h->P.rho)};
       k_band_diag<<<nb, 256, 0, st>>>(b.map, h->diag, dd);
     }
     else k_band_scatter<<<nb, 256, 0, st>>>(b.map, to, band_ptrs(h, b));
@@ -702,20 +710,30 @@ int band_emit(mass_lb_handle* h, float* to, bool diag, cudaStream_t st)
   return 0;
 }
 
-// One fused step of a walled lattice, cur -> nxt: each band's work runs on
-// its own high-priority stream beside the warp-strip kernel (all of them
-// only read cur), and the step stream writes the band rows after them all.
+// One fused step of a walled lattice: each band's work runs on its own
+// high-priority stream beside the warp-strip kernel (both only read cur),
+// then any further correctors (npc > 1), which reuse cur once the bands
+// have read it; the step stream writes the band rows into the result,
+// which is in nxt at the end.
 int fused_step_with_bands(mass_lb_handle* h)
 {
   CU(cudaEventRecord(h->band_in, h->stream), "band fork");
   for(int i = 0; i < h->nbands; ++i)
   {
     CU(cudaStreamWaitEvent(h->bstream[i], h->band_in, 0), "band fork");
-    if(int r = band_compute(h, i, i + 1, h->cur, false, h->bstream[i])) return r;
+    if(int r = band_compute(h, i, h->cur, h->bstream[i])) return r;
     CU(cudaEventRecord(h->band_out[i], h->bstream[i]), "band join");
   }
   const FusedArgs a = fused_args(h, h->cur, h->nxt, false);
   CU(launch_fused_step(a, h->model, h->cfg, false, h->stream), "fused step");
+  for(unsigned c = 2; c <= h->P.npc; ++c)
+  {
+    if(c == 2)
+      for(int i = 0; i < h->nbands; ++i)
+        CU(cudaStreamWaitEvent(h->stream, h->band_read[i], 0), "band gather");
+    if(int r = extra_corrector(h, h->nxt, h->cur, false)) return r;
+    std::swap(h->cur, h->nxt);
+  }
   for(int i = 0; i < h->nbands; ++i)
     CU(cudaStreamWaitEvent(h->stream, h->band_out[i], 0), "band join");
   return band_emit(h, h->nxt, false, h->stream);
@@ -894,11 +912,10 @@ int mass_lb_create(const mass_lb_params* params, unsigned LX, unsigned LY,
   }
   else
   {
-    // the fused warp-strip kernel: every model with npc = 1, on periodic
-    // lattices and, with the wall bands beside it, on walled ones; the rest
-    // runs the unfused sweeps in FP32
-    h->fused = (h->P.npc == 1 || (!h->wall && h->model != GOG)) &&
-               (!h->wall || bands_fit(h)) &&
+    // the fused warp-strip kernel: every model with npc = 1 and lyotropic
+    // and nematic lattices with npc > 1, periodic or, with the wall bands
+    // beside it, walled; go-or-grow with npc > 1 runs the unfused sweeps
+    h->fused = (h->P.npc == 1 || h->model != GOG) && (!h->wall || bands_fit(h)) &&
                fused_supported(static_cast<int>(LX), static_cast<int>(LY), 64);
     if(h->fused)
     {
@@ -981,6 +998,7 @@ void mass_lb_destroy(mass_lb_handle* h)
   {
     if(h->bstream[i]) { cudaStreamSynchronize(h->bstream[i]); cudaStreamDestroy(h->bstream[i]); }
     if(h->band_out[i]) cudaEventDestroy(h->band_out[i]);
+    if(h->band_read[i]) cudaEventDestroy(h->band_read[i]);
   }
   if(h->band_in) cudaEventDestroy(h->band_in);
   if(h->xfer_in) cudaEventDestroy(h->xfer_in);
@@ -1373,13 +1391,11 @@ int mass_lb_download(mass_lb_handle* h, int field, double* out)
       // outputs on (the replay does not write the state)
       const FusedArgs a = fused_args(h, h->nxt, h->cur, true);
       CU(launch_fused_step(a, h->model, h->cfg, true, h->stream), "diag replay");
-      if(h->nbands)
-      {
-        if(int r = band_compute(h, 0, h->nbands, h->nxt, true, h->stream)) return r;
-        if(int r = band_emit(h, nullptr, true, h->stream)) return r;
-      }
       h->diag_n_dev = false;
     }
+    // the wall bands kept theirs when they stepped
+    if(h->nbands)
+      if(int r = band_emit(h, nullptr, true, h->stream)) return r;
     if(int r = check_err_flag(h)) return r;
   }
   return get_primary(h, field, out);
@@ -1642,7 +1658,7 @@ int mass_lb_launches_per_step(mass_lb_handle* h)
   if(h->fused)
     return static_cast<int>(h->P.npc) +
            h->nbands*(2 + (h->model == GOG ? 1 : 0) +
-                      launches_unfused(h->model, static_cast<int>(h->bc), 1));
+                      launches_unfused(h->model, static_cast<int>(h->bc), h->P.npc));
   return launches_unfused(h->model, h->wall ? static_cast<int>(h->bc) : 0, h->P.npc);
 }
 

@@ -36,6 +36,9 @@ DERIVED_LYO = ("ux_phi", "uy_phi", "MU", "sigma_bulk", "sigma_elastic_xx", "sigm
                "sigma_phase_field_xx", "sigma_phase_field_yx", "sigma_active_xx",
                "sigma_active_yx")
 CASES = [(O.LYOTROPIC, LYO_ALL, bc) for bc in (1, 2, 3, 4)] + [(O.NEMATIC, NEM_ALL, 1)]
+# two correctors: the bands keep 6 rows of 12-row halves
+CASES_NPC2 = [(O.LYOTROPIC, dict(LYO_ALL, npc=2), 1), (O.LYOTROPIC, dict(LYO_ALL, npc=2), 4),
+              (O.NEMATIC, dict(NEM_ALL, npc=2), 1)]
 
 
 def errors(a, b, model, rho=40.0):
@@ -56,7 +59,7 @@ def pair(model, params, LX, LY, bc, st):
     return a, b
 
 
-@pytest.mark.parametrize("model,params,bc", CASES)
+@pytest.mark.parametrize("model,params,bc", CASES + CASES_NPC2)
 def test_fused_walls_vs_fp64(model, params, bc):
     LX, LY = 72, 96
     st = O.synthetic_state(model, LX, LY, seed=50 + bc, flow=0.01)
@@ -75,7 +78,7 @@ def test_fused_walls_vs_fp64(model, params, bc):
         assert np.max(np.abs(x - y)) <= 1e-4 * scale + 1e-7, (bc, n)
 
 
-@pytest.mark.parametrize("model,params,bc", CASES)
+@pytest.mark.parametrize("model,params,bc", CASES + CASES_NPC2)
 def test_fused_walls_interior_is_the_periodic_step(model, params, bc):
     LX, LY = 40, 64
     st = O.synthetic_state(model, LX, LY, seed=70 + bc, flow=0.02)
@@ -87,8 +90,9 @@ def test_fused_walls_interior_is_the_periodic_step(model, params, bc):
     w.step(1)
     p.step(1)
     box = model != O.NEMATIC and bc in (3, 4)
+    k = 2 + 2 * params.get("npc", 1)     # rows one step reaches
     inner = np.zeros((LX, LY), dtype=bool)
-    inner[4 if box else 0:LX - 4 if box else LX, 4:LY - 4] = True
+    inner[k if box else 0:LX - k if box else LX, k:LY - k] = True
     for n in STATE[model]:
         x = w.get(n).reshape(LX, LY, -1)
         y = p.get(n).reshape(LX, LY, -1)
@@ -96,10 +100,10 @@ def test_fused_walls_interior_is_the_periodic_step(model, params, bc):
     # the walls act on the band rows
     fw = w.get("ff").reshape(LX, LY, 9)
     fp = p.get("ff").reshape(LX, LY, 9)
-    assert not np.array_equal(fw[:, :4], fp[:, :4])
-    assert not np.array_equal(fw[:, LY - 4:], fp[:, LY - 4:])
+    assert not np.array_equal(fw[:, :k], fp[:, :k])
+    assert not np.array_equal(fw[:, LY - k:], fp[:, LY - k:])
     if box:
-        assert not np.array_equal(fw[:4], fp[:4])
+        assert not np.array_equal(fw[:k], fp[:k])
 
 
 @pytest.mark.parametrize("bc", [2, 3])

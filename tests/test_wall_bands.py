@@ -7,19 +7,18 @@ A walled lattice steps as (1) the periodic step of the whole lattice and
 side, stepped with the lattice's own walls; the band's outer 4 rows per side
 replace the periodic result there (for boxes, a second band across x does
 the same for the left and right walls). mass_hd_b200/csrc/api.cu
-(k_band_gather, step_bands) does this on the device around the fused
+(k_band_gather, band_compute, band_emit) does this on the device around the fused
 kernel. Here the same splice, restated with the oracle, must equal the
 oracle's own walled step bit for bit, step after step, for every wall kind;
 with 7-row halves it must not (one Step() reaches 4 sites, so the kept rows
-need 4 more behind them).
+need 4 more behind them). With npc correctors a step reaches 2 + 2*npc
+sites; npc = 2 keeps 6 rows of 12-row halves.
 """
 import numpy as np
 import pytest
 
 from oracle import oracle as O
 from tests.helpers import LYO_ALL, NEM_ALL
-
-KEEP = 4
 
 
 def _names(model):
@@ -33,7 +32,7 @@ def _oracle(model, params, LX, LY, bc, fields):
     return o
 
 
-def spliced_step(model, params, cur, LX, LY, bc, half):
+def spliced_step(model, params, cur, LX, LY, bc, half, keep):
     """One walled step as the periodic step plus the wall bands."""
     names = _names(model)
     per = _oracle(model, params, LX, LY, 0, cur)
@@ -44,20 +43,20 @@ def spliced_step(model, params, cur, LX, LY, bc, half):
     yb.step(1)
     for k in names:
         r = yb.get(k).reshape(LX, 2 * half, -1)
-        nxt[k][:, :KEEP] = r[:, :KEEP]
-        nxt[k][:, LY - KEEP:] = r[:, 2 * half - KEEP:]
+        nxt[k][:, :keep] = r[:, :keep]
+        nxt[k][:, LY - keep:] = r[:, 2 * half - keep:]
     if model == O.LYOTROPIC and bc in (3, 4):
         xs = np.r_[0:half, LX - half:LX]
         xb = _oracle(model, params, 2 * half, LY, bc, {k: cur[k][xs] for k in names})
         xb.step(1)
         for k in names:
             r = xb.get(k).reshape(2 * half, LY, -1)
-            nxt[k][:KEEP] = r[:KEEP]
-            nxt[k][LX - KEEP:] = r[2 * half - KEEP:]
+            nxt[k][:keep] = r[:keep]
+            nxt[k][LX - keep:] = r[2 * half - keep:]
     return nxt
 
 
-def _run(model, params, LX, LY, bc, steps, half):
+def _run(model, params, LX, LY, bc, steps, half, keep=4):
     names = _names(model)
     st = O.synthetic_state(model, LX, LY, seed=31, flow=0.03)
     full = O.PortOracle(model, params, LX, LY, bc)
@@ -66,7 +65,7 @@ def _run(model, params, LX, LY, bc, steps, half):
     full.step(steps)
     cur = {k: np.asarray(st[k], dtype=np.float64).reshape(LX, LY, -1).copy() for k in names}
     for _ in range(steps):
-        cur = spliced_step(model, params, cur, LX, LY, bc, half)
+        cur = spliced_step(model, params, cur, LX, LY, bc, half, keep)
     return {k: (full.get(k).reshape(LX, LY, -1), cur[k]) for k in names}
 
 
@@ -80,4 +79,13 @@ def test_bands_splice_into_the_walled_step(model, params, bc):
 
 def test_narrower_bands_do_not():
     out = _run(O.LYOTROPIC, LYO_ALL, 22, 26, 4, 1, 7)
+    assert any(not np.array_equal(w, g) for w, g in out.values())
+
+
+@pytest.mark.parametrize("bc", [1, 4])
+def test_bands_with_two_correctors(bc):
+    p = dict(LYO_ALL, npc=2)
+    for k, (want, got) in _run(O.LYOTROPIC, p, 30, 32, bc, 2, 12, 6).items():
+        assert np.array_equal(want.view(np.uint64), got.view(np.uint64)), (bc, k)
+    out = _run(O.LYOTROPIC, p, 30, 32, bc, 1, 11, 6)
     assert any(not np.array_equal(w, g) for w, g in out.values())
