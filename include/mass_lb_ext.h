@@ -19,9 +19,11 @@ extern "C" {
  * (src/models/go-or-grow.cpp:208-216). */
 int mass_lb_upload_field(mass_lb_handle* h, int field, const double* src);
 
-/* Tile of the fused FP32 kernel: `threads` lattice columns per CTA strip
- * (64, 128 or 256; NT - 8 of them are output columns) and `rows` lattice
- * rows per CTA chunk. set_tile(h, 0, 0) re-enables the autotuner, which
+/* Tile of the fused FP32 kernel: `threads` = 32 selects the warp-strip
+ * kernel (64 columns per warp, 56 of them output columns); 64, 128 or 256
+ * the CTA-strip kernel with that many columns per CTA strip (NT - 8 output
+ * columns), which takes neither a phi source, go-or-grow nor npc > 1
+ * (MASS_LB_EUNSUPPORTED). `rows`: lattice rows per chunk. set_tile(h, 0, 0) re-enables the autotuner, which
  * otherwise runs once before the first step (timing every candidate tile on
  * the live state without advancing it). The environment variable
  * MASS_LB_TILE="threads,rows" fixes the tile at handle creation.
@@ -30,12 +32,15 @@ int mass_lb_get_tile(mass_lb_handle* h, int* threads, int* rows);
 int mass_lb_set_tile(mass_lb_handle* h, int threads, int rows);
 int mass_lb_autotune(mass_lb_handle* h);
 
-/* 1 if mass_lb_step runs the fused FP32 kernel (FP32, periodic lattice,
- * npc = 1, LY % 4 == 0, LY >= 64; every model), else 0. A go-or-grow or
- * division lattice leaves the fused kernel for the unfused FP32 sweeps when
- * conserve_phi is switched on (mass_lb_set_phi_conservation), which needs a
- * lattice-wide phi sum inside a sub-step; the dry relaxation of go-or-grow
- * runs on the sweeps and hands the state back. */
+/* 1 if mass_lb_step runs the fused FP32 kernel, else 0. FP32 lattices with
+ * LY % 4 == 0 and LY >= 64 take it: every model with npc = 1, lyotropic and
+ * nematic with npc > 1 (a corrector sub-step per further corrector),
+ * periodic or walled (walled: the rows next to the walls are stepped by the
+ * wall sweeps beside it; LY, and for boxes LX, at least 8 + 8*npc). A
+ * go-or-grow or division lattice leaves the fused kernel for the unfused
+ * FP32 sweeps when conserve_phi is switched on (mass_lb_set_phi_conservation),
+ * which needs a lattice-wide phi sum inside a sub-step; the dry relaxation
+ * of go-or-grow runs on the sweeps and hands the state back. */
 int mass_lb_uses_fused(mass_lb_handle* h);
 
 /* Device view of the fused FP32 state (read-only for the caller): `*planes`
@@ -155,8 +160,16 @@ int mass_lb_stream_wait(mass_lb_handle* h, mass_lb_handle* before);
  *   Lyotropic and nematic periodic lattices (MASS_LB_EUNSUPPORTED
  *   otherwise).
  * mass_lb_checks_rows: mass_lb_checks over rows [x0, x0 + nrows) only (the
- *   owned rows of a slab), for a sum over slabs. Synchronous. */
+ *   owned rows of a slab), for a sum over slabs. Synchronous.
+ * mass_lb_set_step_rows: from now on each step writes rows [x0, x0 + nrows)
+ *   only (a slab's owned rows; the halo rows' new values would be thrown
+ *   away by the next exchange), so the step costs what the owned rows cost.
+ *   The rows read still wrap periodically over the lattice. Rows outside
+ *   the range are left as they were two steps before. nrows = 0 restores
+ *   whole-lattice steps. FP32 fused periodic lattices with npc = 1
+ *   (MASS_LB_EUNSUPPORTED otherwise). */
 int mass_lb_rows_layout(mass_lb_handle* h, int* nplanes, int* elem_bytes);
+int mass_lb_set_step_rows(mass_lb_handle* h, unsigned x0, unsigned nrows);
 int mass_lb_get_rows(mass_lb_handle* h, unsigned x0, unsigned nrows, void* dst);
 int mass_lb_put_rows(mass_lb_handle* h, unsigned x0, unsigned nrows, const void* src);
 int mass_lb_checks_rows(mass_lb_handle* h, unsigned x0, unsigned nrows, double* fsum,

@@ -284,6 +284,7 @@ struct mass_lb_handle
   float* pred = nullptr;     // FP32 fused with npc > 1: fn, QNxx, QNyx[, phn] of the step
   float* scratch = nullptr;  // its derived-field replay's throw-away outputs (NP planes)
   bool diag_n_dev = false;   // the diagnostic n plane holds the density deviation
+  unsigned step_x0 = 0, step_nx = 0;   // fused: the rows a step writes (0 rows: all)
   WallBand band[2];          // FP32 fused with walls: the band lattices
   int nbands = 0;
   cudaStream_t bstream[2] = {};     // their work beside the fused kernel
@@ -468,6 +469,8 @@ FusedArgs fused_args(mass_lb_handle* h, const float* in, float* out, bool diag)
   // go-or-grow always reads its growth-rate plane (zero until a source is set)
   a.src = h->src_on || h->model == GOG ? h->src_fused : nullptr;
   a.pred = !diag && h->P.npc > 1 ? h->pred : nullptr;
+  a.xbase = static_cast<int>(h->step_x0);
+  a.xcount = static_cast<int>(h->step_nx ? h->step_nx : h->LX);
   return a;
 }
 
@@ -1486,9 +1489,36 @@ T* primary_plane(mass_lb_handle* h, State<T>& s, int q, long long* pitch)
   return base + off;
 }
 
+// Row r of plane q of the state, for r in [0, nrows): p[q] + r*pitch + y.
+template<typename T>
+struct RowPlanes
+{
+  T* p[13];
+};
+
+// state rows <-> packed [plane][row][y], one thread per value
+template<typename T>
+__global__ void __launch_bounds__(256)
+k_copy_rows(RowPlanes<T> pl, T* __restrict__ packed, int np, int nrows, int LY, long long pitch,
+            int to_rows)
+{
+  const long long per = static_cast<long long>(nrows)*LY, total = per*np;
+  for(long long k = blockIdx.x*256ll + threadIdx.x; k < total; k += 256ll*gridDim.x)
+  {
+    const int q = static_cast<int>(k / per);
+    const long long rem = k - q*per;
+    const long long r = rem / LY, y = rem - r*LY;
+    T* st = pl.p[q] + r*pitch + y;
+    if(to_rows) *st = packed[k];
+    else packed[k] = *st;
+  }
+}
+
 // Copies rows [x0, x0+nrows) of every primary plane between the handle's
 // state and a packed device buffer laid out [plane][row][y]. `to_rows`
-// selects the direction (packed -> state). The handle's stream orders it.
+// selects the direction (packed -> state). One kernel launch on the
+// handle's stream (strided copy-engine transfers of a few rows per plane
+// cost more than the bytes they move).
 int copy_rows(mass_lb_handle* h, unsigned x0, unsigned nrows, void* packed, bool to_rows)
 {
   if(!h || !packed) return fail(MASS_LB_EINVAL, "null argument");
@@ -1501,34 +1531,39 @@ int copy_rows(mass_lb_handle* h, unsigned x0, unsigned nrows, void* packed, bool
   if(to_rows)
     if(int r = settle_derived(h)) return r;
   const int NP = nplanes(h);
-  const size_t LY = h->LY;
+  const int LY = static_cast<int>(h->LY);
+  const long long total = static_cast<long long>(NP)*nrows*LY;
+  const int nb = blocks_for(total);
   if(h->fused)
   {
-    // planes of LX*LY floats: the rows of a plane are contiguous
-    const size_t width = nrows*LY*sizeof(float);
-    const size_t plane_b = static_cast<size_t>(h->LX)*LY*sizeof(float);
-    char* st = reinterpret_cast<char*>(h->cur) + static_cast<size_t>(x0)*LY*sizeof(float);
-    const cudaError_t e = to_rows
-      ? cudaMemcpy2DAsync(st, plane_b, packed, width, width, NP, cudaMemcpyDeviceToDevice, h->stream)
-      : cudaMemcpy2DAsync(packed, width, st, plane_b, width, NP, cudaMemcpyDeviceToDevice, h->stream);
-    CU(e, "row copy");
+    // planes of LX*LY floats
+    RowPlanes<float> pl{};
+    const long long plane = static_cast<long long>(h->LX)*LY;
+    for(int q = 0; q < NP; ++q) pl.p[q] = h->cur + q*plane + static_cast<long long>(x0)*LY;
+    k_copy_rows<float><<<nb, 256, 0, h->stream>>>(pl, static_cast<float*>(packed), NP,
+                                                  static_cast<int>(nrows), LY, LY, to_rows);
+    CU(cudaGetLastError(), "row copy");
     if(to_rows) h->has_prev = false;
     return 0;
   }
-  const size_t es = h->precision == MASS_LB_FP64 ? sizeof(double) : sizeof(float);
-  for(int q = 0; q < NP; ++q)
+  long long pitch = 0;
+  if(h->precision == MASS_LB_FP64)
   {
-    long long pitch = 0;
-    char* st = h->precision == MASS_LB_FP64
-      ? reinterpret_cast<char*>(primary_plane(h, h->s64, q, &pitch))
-      : reinterpret_cast<char*>(primary_plane(h, h->s32, q, &pitch));
-    st += static_cast<size_t>(x0)*pitch*es;
-    char* pk = static_cast<char*>(packed) + static_cast<size_t>(q)*nrows*LY*es;
-    const cudaError_t e = to_rows
-      ? cudaMemcpy2DAsync(st, pitch*es, pk, LY*es, LY*es, nrows, cudaMemcpyDeviceToDevice, h->stream)
-      : cudaMemcpy2DAsync(pk, LY*es, st, pitch*es, LY*es, nrows, cudaMemcpyDeviceToDevice, h->stream);
-    CU(e, "row copy");
+    RowPlanes<double> pl{};
+    for(int q = 0; q < NP; ++q)
+      pl.p[q] = primary_plane(h, h->s64, q, &pitch) + static_cast<long long>(x0)*pitch;
+    k_copy_rows<double><<<nb, 256, 0, h->stream>>>(pl, static_cast<double*>(packed), NP,
+                                                   static_cast<int>(nrows), LY, pitch, to_rows);
   }
+  else
+  {
+    RowPlanes<float> pl{};
+    for(int q = 0; q < NP; ++q)
+      pl.p[q] = primary_plane(h, h->s32, q, &pitch) + static_cast<long long>(x0)*pitch;
+    k_copy_rows<float><<<nb, 256, 0, h->stream>>>(pl, static_cast<float*>(packed), NP,
+                                                  static_cast<int>(nrows), LY, pitch, to_rows);
+  }
+  CU(cudaGetLastError(), "row copy");
   return 0;
 }
 
@@ -1558,6 +1593,21 @@ int mass_lb_rows_layout(mass_lb_handle* h, int* nplanes_out, int* elem_bytes)
   if(!h) return fail(MASS_LB_EINVAL, "null handle");
   if(nplanes_out) *nplanes_out = nplanes(h);
   if(elem_bytes) *elem_bytes = h->precision == MASS_LB_FP64 ? 8 : 4;
+  return 0;
+}
+
+int mass_lb_set_step_rows(mass_lb_handle* h, unsigned x0, unsigned nrows)
+{
+  if(!h) return fail(MASS_LB_EINVAL, "null handle");
+  if(nrows == 0) { h->step_x0 = h->step_nx = 0; return 0; }
+  if(!h->fused || h->wall || h->P.npc != 1 || h->in_ensemble)
+    return fail(MASS_LB_EUNSUPPORTED,
+                "row-range steps need a fused periodic lattice with npc = 1");
+  if(x0 >= h->LX || nrows > h->LX - x0)
+    return fail(MASS_LB_EINVAL, "row range outside the lattice");
+  h->step_x0 = x0;
+  h->step_nx = nrows;
+  h->has_prev = false;
   return 0;
 }
 

@@ -344,8 +344,8 @@ fused_step_kernel(const FusedArgs a)
   const int strip = blockIdx.x % a.nstrips;
   const int chunk = blockIdx.x / a.nstrips;
   const int y0 = strip*W;
-  const int x0 = chunk*a.rows;
-  const int rows = min(a.rows, a.LX - x0);
+  const int x0 = a.xbase + chunk*a.rows;
+  const int rows = min(a.rows, a.xbase + a.xcount - x0);
   const int LX = a.LX, LY = a.LY;
   const int nload = rows + 9;          // input rows x0-4 .. x0+rows+4
   const int ystart = (y0 - 4 + LY) % LY;
@@ -605,7 +605,7 @@ cudaError_t launch_t(const FusedArgs& a, int rows, cudaStream_t st)
     if(e != cudaSuccess) return e;
     attr_set |= bit;
   }
-  const int nchunks = (a.LX + rows - 1)/rows;
+  const int nchunks = (a.xcount + rows - 1)/rows;
   FusedArgs b = a;
   b.rows = rows;
   b.nstrips = (a.LY + (NT - 8) - 1)/(NT - 8);

@@ -51,6 +51,8 @@ struct FusedArgs
                        // (go-or-grow: the growth rate, always present)
   float* pred;         // or null; warp-strip kernel, lyotropic and nematic: fn (9 planes),
                        // QNxx, QNyx[, phn] of the step, for the further correctors of npc > 1
+  int xbase, xcount;   // the rows stepped, [xbase, xbase + xcount) with xcount >= 1; the
+                       // others are not written (inputs still wrap periodically over LX)
 };
 
 // Tile shapes the autotuner may pick.

@@ -485,6 +485,7 @@ struct ItemView
   int rows;
   const float* src;   // per-site phi source rate (SRC launches)
   float* pred;        // PRED launches: fn (9 planes), QNxx, QNyx[, phn] per site
+  int xbase, xcount;  // the rows stepped: [xbase, xbase + xcount)
 };
 
 // Per-warp shared memory: input ring | delayed populations (3 rows) |
@@ -509,8 +510,8 @@ __device__ __forceinline__ bool warp_item(const ItemView& a, const PairParams& P
 {
   constexpr int NP = MODEL == NEM ? 11 : MODEL == LYO ? 12 : 13;
   const int y0 = strip*WOUT;
-  const int x0 = chunk*a.rows;
-  const int rows = min(a.rows, a.LX - x0);
+  const int x0 = a.xbase + chunk*a.rows;
+  const int rows = min(a.rows, a.xbase + a.xcount - x0);
   const int LX = a.LX, LY = a.LY;
   const int nload = rows + 8;            // rows x0-4 .. x0+rows+3
   const int ystart = (y0 - 4 + LY) % LY;
@@ -904,11 +905,12 @@ fused_warp_kernel(const __grid_constant__ FusedArgs a, const int nitems)
   float *ring, *dpop, *hrow;
   uint64_t* mbar;
   warp_smem<MODEL>(ring, dpop, hrow, mbar, warp, lane);
-  const ItemView v{a.in, a.out, a.diag, a.err, a.LX, a.LY, a.plane, a.rows, a.src, a.pred};
+  const ItemView v{a.in, a.out, a.diag, a.err, a.LX, a.LY, a.plane, a.rows, a.src, a.pred,
+                   a.xbase, a.xcount};
   unsigned rowbase = 0;
   // chunk-major: the warps in flight together work down a few strips at
   // every height of the lattice (about 4 % faster than strip-major at 4096^2)
-  const int nchunks = (a.LX + a.rows - 1)/a.rows;
+  const int nchunks = (a.xcount + a.rows - 1)/a.rows;
   warp_item<MODEL, DIAG, SRC, PRED>(v, a.pp, item / nchunks, item % nchunks, ring, dpop, hrow,
                                      mbar, lane, rowbase);
 }
@@ -938,7 +940,7 @@ fused_warp_ensemble_kernel(const EnsRun* __restrict__ runs, const int* __restric
     const EnsRun& R = runs[r];
     const int local = item - R.item0;
     const ItemView v{parity ? R.b : R.a, parity ? R.a : R.b, nullptr, err, R.LX, R.LY,
-                     R.plane, R.rows, nullptr, nullptr};
+                     R.plane, R.rows, nullptr, nullptr, 0, R.LX};
     const int nchunks = (R.LX + R.rows - 1)/R.rows;   // chunk-major, as fused_warp_kernel
     if(!warp_item<MODEL, false, false>(v, c_ens_pp[R.slot], local / nchunks, local % nchunks,
                                 ring, dpop, hrow, mbar, lane, rowbase))
@@ -972,7 +974,7 @@ cudaError_t launch_t(const FusedArgs& a, int rows, cudaStream_t st)
   b.rows = rows;
   b.nstrips = (a.LY + WOUT - 1)/WOUT;
   b.pp = make_pp(a.p, MODEL);
-  const int nchunks = (a.LX + rows - 1)/rows;
+  const int nchunks = (a.xcount + rows - 1)/rows;
   const int nitems = b.nstrips*nchunks;
   const dim3 grid((nitems + WPB - 1)/WPB);
   kern<<<grid, 32*WPB, smem_bytes<MODEL>(), st>>>(b, nitems);

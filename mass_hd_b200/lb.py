@@ -143,6 +143,7 @@ def load_library(build_if_missing: bool = False):
         "mass_lb_upload_async": (C.c_int, [vp, dp, dp, dp, dp]),
         "mass_lb_download_async": (C.c_int, [vp, C.c_int, dp]),
         "mass_lb_stream_wait": (C.c_int, [vp, vp]),
+        "mass_lb_set_step_rows": (C.c_int, [vp, C.c_uint, C.c_uint]),
         "mass_lb_draw_masks_queued": (C.c_int, [vp, C.c_int] + [C.c_double] * 7),
         "mass_lb_mask_consumed": (C.c_int, [vp, C.POINTER(C.c_longlong)]),
         "mass_lb_mask_progress": (C.c_int, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_int)]),
@@ -391,6 +392,11 @@ class Lattice:
 
     def synchronize(self):
         _check(load_library().mass_lb_synchronize(self.h))
+
+    def set_step_rows(self, x0: int, nrows: int):
+        """mass_lb_set_step_rows: steps write rows [x0, x0 + nrows) only
+        (nrows = 0: the whole lattice again)."""
+        _check(load_library().mass_lb_set_step_rows(self.h, x0, nrows))
 
     def wait_for(self, before: "Lattice"):
         """mass_lb_stream_wait: work queued on this lattice from now on starts

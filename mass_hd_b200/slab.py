@@ -21,7 +21,10 @@ contiguous in every plane:
   in FP32. The halo rows' own updates are wrong (their neighbourhood wraps
   inside the slab) and are overwritten by the next exchange;
 * the conservation sums run over the owned rows (mass_lb_checks_rows) and
-  are summed over ranks in FP64.
+  are summed over ranks in FP64;
+* a fused slab steps its owned rows only (mass_lb_set_step_rows); the
+  halos' new values would be overwritten by the next exchange anyway.
+  Slabs take npc = 1 (a step with npc correctors reaches 2 + 2*npc rows).
 
 Transports: `DistExchange` sends the halo buffers with torch.distributed
 point-to-point operations (NCCL between GPUs, into each GPU's own receive
@@ -54,6 +57,13 @@ def partition(LX: int, world: int) -> List[Tuple[int, int]]:
     if world > 1 and min(n for _, n in out) < HALO:
         raise ValueError(f"{LX} rows over {world} ranks leaves a slab below {HALO} rows")
     return out
+
+
+def check_npc(params: dict):
+    """A step with npc correctors reaches 2 + 2*npc rows; the HALO rows
+    cover npc = 1."""
+    if int(params.get("npc", 1)) != 1:
+        raise ValueError("x-slabs hold 4 halo rows, one step's reach with npc = 1")
 
 
 def slab_rows(LX: int, x0: int, n: int) -> np.ndarray:
@@ -107,8 +117,14 @@ class LatticeSlab:
         import torch
 
         from mass_hd_b200 import lb
+        check_npc(params)
         self.LX, self.LY, self.x0, self.n = LX, LY, x0, n
         self.lat = lb.Lattice(model, params, n + 2 * HALO, LY, 0, precision)
+        if self.lat.uses_fused:
+            # the halo rows' new values would be overwritten by the next
+            # exchange: step the owned rows only (no partial chunk of the
+            # 8 extra rows)
+            self.lat.set_step_rows(HALO, n)
         self.nplanes, eb = self.lat.rows_layout()
         self.dtype = torch.float32 if eb == 4 else torch.float64
         self.device = torch.device("cuda", torch.cuda.current_device())

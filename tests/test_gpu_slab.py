@@ -119,3 +119,40 @@ def test_row_transfers_round_trip_and_refuse_bad_ranges():
     with pytest.raises(M.MassLBError):
         wall.get_rows(0, 4, buf.data_ptr())
     wall.close()
+
+
+def test_step_rows_write_their_range_only():
+    """mass_lb_set_step_rows: one step writes rows [x0, x0 + n) exactly as a
+    whole-lattice step does, and leaves the other rows as they were two steps
+    before (here: the uploaded state, since the ping-pong buffer holds it)."""
+    LX, LY = 40, 128
+    st = O.synthetic_state(M.LYOTROPIC, LX, LY, seed=8, flow=0.02)
+    a = M.Lattice(M.LYOTROPIC, LYO_ALL, LX, LY, 0, M.FP32)
+    b = M.Lattice(M.LYOTROPIC, LYO_ALL, LX, LY, 0, M.FP32)
+    for x in (a, b):
+        x.upload_state(st)
+        x.step(1)       # both buffers now hold the first step
+    a.set_step_rows(5, 23)
+    a.step(1)
+    b.step(1)
+    for k in FIELDS[M.LYOTROPIC]:
+        x = a.get(k).reshape(LX, LY, -1)
+        y = b.get(k).reshape(LX, LY, -1)
+        assert bits_equal(x[5:28], y[5:28]), k
+    c0 = M.Lattice(M.LYOTROPIC, LYO_ALL, LX, LY, 0, M.FP32)
+    c0.upload_state(st)
+    for k in FIELDS[M.LYOTROPIC]:
+        x = a.get(k).reshape(LX, LY, -1)
+        s0 = c0.get(k).reshape(LX, LY, -1)
+        assert bits_equal(x[:5], s0[:5]) and bits_equal(x[28:], s0[28:]), k
+    a.set_step_rows(0, 0)
+    a.step(1)
+    # walls and npc > 1 refuse a row range
+    w = M.Lattice(M.LYOTROPIC, LYO_ALL, 40, 128, 1, M.FP32)
+    with pytest.raises(M.MassLBError):
+        w.set_step_rows(4, 20)
+    c = M.Lattice(M.LYOTROPIC, dict(LYO_ALL, npc=2), 40, 128, 0, M.FP32)
+    with pytest.raises(M.MassLBError):
+        c.set_step_rows(4, 20)
+    with pytest.raises(M.MassLBError):
+        a.set_step_rows(30, 20)

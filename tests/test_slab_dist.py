@@ -186,3 +186,10 @@ def test_ensemble_runs_split_over_ranks_once_and_balanced():
     # more ranks than runs: some ranks get nothing, none gets a run twice
     share, load = E.partition_runs([(128, 128), (256, 256)], 4)
     assert sorted(i for s in share for i in s) == [0, 1] and load.count(0) == 2
+
+
+def test_slabs_take_one_corrector():
+    S.check_npc({"npc": 1})
+    S.check_npc({})
+    with pytest.raises(ValueError):
+        S.check_npc({"npc": 2})
