@@ -134,7 +134,8 @@ inline int blocks_for(long long n)
 
 // ---- wall bands of a fused lattice ----------------------------------------
 // A fused FP32 lattice with walls steps in two parts. The warp-strip kernel
-// steps the whole lattice as if it were periodic. One Step() reaches
+// (and, with npc > 1, the corrector sub-steps after it) steps the whole
+// lattice as if it were periodic. One Step() reaches
 // keep = 2 + 2*npc sites (predictor UpdateQuantities, UpdateFields and
 // Move, then UpdateQuantities and UpdateFields per corrector), so every site
 // at least `keep` sites from a wall gets exactly what the wall step gives
