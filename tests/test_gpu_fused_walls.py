@@ -185,3 +185,33 @@ def test_fused_walls_checkpoint_round_trip(tmp_path):
     b.step(5)
     for n in STATE[O.NEMATIC]:
         assert bits_equal(a.get(n), b.get(n)), n
+
+
+@pytest.mark.parametrize("bc", [2, 3])
+def test_fused_walls_go_or_grow_relaxation(bc):
+    """Go-or-grow's dry relaxation runs on the sweeps' state: a walled fused
+    lattice goes there through the ghost-ring layout and comes back, then
+    steps on, tracking the FP64 mode."""
+    from tests.test_gpu_go_or_grow import params
+    p = params(alpha=0.0, beta=0.0)
+    LX, LY = 64, 96
+    ref = O.RefOracle(O.GO_OR_GROW, params(**{"relax-steps": 0}), LX, LY, bc)
+    ref.configure(4)
+    st = {n: ref.get(n) for n in STATE[O.GO_OR_GROW]}
+    a = M.Lattice(M.GO_OR_GROW, p, LX, LY, bc, M.FP32)
+    b = M.Lattice(M.GO_OR_GROW, p, LX, LY, bc, M.FP64)
+    for lat in (a, b):
+        lat.upload_state(st)
+    ta = a.relax_free_energy(20, 0.8, True, True)
+    tb = b.relax_free_energy(20, 0.8, True, True)
+    assert a.uses_fused
+    assert ta == pytest.approx(tb, rel=1e-5)
+    for n in ("QQxx", "QQyx", "phi"):
+        assert rel_l2(a.get(n), b.get(n)) < 1e-5, n
+    a.step(10)
+    b.step(10)
+    for n in STATE[O.GO_OR_GROW]:
+        x, y = a.get(n), b.get(n)
+        if n == "ff":
+            x, y = ff_dev(x, 40.0), ff_dev(y, 40.0)
+        assert rel_l2(x, y) < 1e-4, n
