@@ -47,6 +47,17 @@ int mass_sg_conv3x3(const void* in, const void* w, int nout, int mode, int B, in
                     const float* bias, const void* resid, const void* aux, void* out, void* out2,
                     const float* resid_f, float* out_f, int* err, void* stream);
 
+/* mass_sg_conv3x3 that also writes the cycle counters of each CTA's MMA
+ * thread to `cycles` (device, 4 long longs per CTA, at most 4 x the SM
+ * count): cycles from start to done, to the last MMA issue, waiting for
+ * input slabs, waiting for drained accumulators. *ncta receives the
+ * number of CTAs launched. A profiling aid; same results as
+ * mass_sg_conv3x3. */
+int mass_sg_conv3x3_profile(const void* in, const void* w, int nout, int mode, int B, int H,
+                            int W, const float* bias, const void* resid, const void* aux,
+                            void* out, void* out2, const float* resid_f, float* out_f, int* err,
+                            long long* cycles, int* ncta, void* stream);
+
 /* dW[tap][ci][co] = sum_p x(p + tap)[ci] * dy(p)[co] (zeroes dW first). */
 int mass_sg_conv3x3_wgrad(const void* x, const void* dy, float* dW, int B, int H, int W,
                           int* err, void* stream);

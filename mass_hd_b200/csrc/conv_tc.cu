@@ -2,19 +2,25 @@
 //
 // Forward and input-gradient pass (conv3x3_kernel): D[128 pixels][NOUT] =
 // sum over 9 taps of A_tap[128 pixels][64 ci] * B_tap[NOUT][64 ci]^T. One
-// output tile is half a row of one image (128 consecutive x). For each of
-// the three input rows a tile needs, one TMA load (128-byte swizzle) brings
-// a slab of 136 pixels; the three taps of that row are the slab read from
-// pixel 0, 1 and 2 (descriptor start 128 bytes apart), so the input is
-// fetched once per row instead of once per tap. All 9 weight taps stay in
-// shared memory for the whole persistent kernel. Warp roles: warp 0 issues
-// TMA loads into a 5-slab ring, warp 1 issues tcgen05.mma (4 x K=16 per
-// tap) into two TMEM accumulators (alternate tiles), and warps 2-17 form
-// two epilogue groups, one per accumulator, so two tiles' epilogues run at
-// once. An epilogue drains its accumulator (tcgen05.ld), applies the fused
-// bias / GELU / residual / GELU' epilogue in packed FP32x2, stages the bf16
-// tile in swizzled shared memory and writes it (and its periodic ring row)
-// with TMA stores; residual and pre-activation inputs arrive as TMA tiles.
+// output tile is half a row of one image (128 consecutive x). A CTA marches
+// down strips of R output rows of one image half (R a divisor of H, up to
+// 16). For each padded input row of a strip (R + 2 of them), one TMA load
+// (128-byte swizzle) brings a slab of 136 pixels; the three taps of that
+// row are the slab read from pixel 0, 1 and 2 (descriptor start 128 bytes
+// apart). The slab feeds up to three output rows (tap rows ky = 0, 1, 2 of
+// output rows j, j-1, j-2), so each A operand (slab, tap column, 16-channel
+// step) goes once through the tensor core's A collector buffer and meets
+// the weights of every tap row that needs it: shared-memory operand reads
+// per output row drop from 36 A + 36 B to 12 A + 36 B. All 9 weight taps
+// stay in shared memory for the whole persistent kernel. Warp roles: warp
+// 0 issues TMA loads into a 5-slab ring, warp 1 issues tcgen05.mma into
+// four TMEM accumulators (output rows in flight, one per row modulo 4), and
+// warps 2-17 form two epilogue groups that take alternate output rows, so
+// two rows' epilogues run at once. An epilogue drains its accumulator
+// (tcgen05.ld), applies the fused bias / GELU / residual / GELU' epilogue
+// in packed FP32x2, stages the bf16 tile in swizzled shared memory and
+// writes it (and its periodic ring row) with TMA stores; residual and
+// pre-activation inputs arrive as TMA tiles.
 //
 // Weight gradient (conv3x3_wgrad_kernel): dW_tap[ci][co] = sum over pixels of
 // x(p + tap)[ci] * dy(p)[co]. K runs over pixels, so both operands are read
@@ -32,6 +38,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <mutex>
 
 namespace mlb {
@@ -61,12 +68,13 @@ struct ConvSmem
   static constexpr uint32_t OUT_OFF = A_OFF + NSTAGE*SLAB_BYTES;          // [group]
   static constexpr uint32_t AUX_OFF = OUT_OFF + (NOUT == 64 ? 2*TILE_BYTES : 0u);  // [group]
   static constexpr uint32_t BAR_OFF = AUX_OFF + (NOUT == 64 ? 2*TILE_BYTES : 0u);
-  static constexpr int NBAR = 2*NSTAGE + 8;  // full, empty, w, tfull[2], tempty[2], done, aux[2]
+  static constexpr int NACC = 4;             // TMEM accumulators (output rows in flight), a power of 2
+  static constexpr int NBAR = 2*NSTAGE + 2*NACC + 4;  // full, empty, w, tfull[NACC], tempty[NACC], done, aux[2]
   static constexpr uint32_t MISC_OFF = BAR_OFF + NBAR*8;
   static constexpr uint32_t BIAS_OFF = MISC_OFF + 16;
   static constexpr uint32_t BYTES = BIAS_OFF + 64*4;
   static constexpr uint32_t ALLOC = BYTES + 1024;            // room to align the base
-  static constexpr uint32_t TMEM_COLS = NOUT == 64 ? 128 : 32;
+  static constexpr uint32_t TMEM_COLS = NACC*NOUT;          // 256 or 64 columns
   static_assert(ALLOC <= 232448, "shared memory per CTA");
 };
 
@@ -142,6 +150,57 @@ __device__ __forceinline__ void unpack8(const uint4& u, float* f)
   }
 }
 
+// Output rows of one CTA: the CTA takes strips (image n, half-row column
+// xt, R consecutive rows from y0) item = blockIdx.x, + gridDim.x, ...; its
+// t-th output row is row t % R of its (t / R)-th strip. The coordinates are
+// recomputed from the kernel parameters where they are needed, so the
+// epilogue keeps no extra registers live (at 576 threads it has 96).
+__device__ __forceinline__ void strip_item(const ConvArgs& a, int it, int& n, int& x0, int& y0)
+{
+  const int xt_n = a.W >> 7, spi = a.H / a.rows;
+  const int xt = it % xt_n, s = it / xt_n;
+  x0 = xt << 7;
+  y0 = (s % spi)*a.rows;
+  n = s / spi;
+}
+__device__ __forceinline__ int strip_items(const ConvArgs& a)
+{
+  return a.B*(a.W >> 7)*(a.H / a.rows);
+}
+__device__ __forceinline__ void strip_row(const ConvArgs& a, int t, int& n, int& x0, int& y)
+{
+  int y0;
+  strip_item(a, static_cast<int>(blockIdx.x) + (t / a.rows)*static_cast<int>(gridDim.x), n, x0, y0);
+  y = y0 + t % a.rows;
+}
+
+// The MMAs of one input slab (padded row y0 + j of a strip) inside a strip:
+// the slab feeds output rows j, j-1, j-2 with tap rows ky = 0, 1, 2. For
+// each tap column kx and 16-channel step k, the slab's A operand goes once
+// through the collector buffer (fill, use, lastuse) and meets the weights
+// of the three tap rows. d0, d1, d2 are the accumulators of output rows j,
+// j-1, j-2.
+template<int NOUT>
+__device__ __forceinline__ void slab_mmas(uint32_t d0, uint32_t d1, uint32_t d2, uint64_t da,
+                                          uint64_t db, uint32_t idesc)
+{
+#pragma unroll
+  for(int kx = 0; kx < 3; ++kx)
+  {
+#pragma unroll
+    for(int k = 0; k < 4; ++k)
+    {
+      const uint64_t a = da + ((kx*128 + 32*k) >> 4);
+      const uint64_t b = db + ((kx*NOUT*128 + 32*k) >> 4);
+      // the first contribution to an output row (tap 0, first K step)
+      // overwrites the accumulator
+      mma_bf16_coll<1>(d0, a, b, idesc, (kx | k) != 0);
+      mma_bf16_coll<2>(d1, a, b + ((3*NOUT*128) >> 4), idesc, 1u);
+      mma_bf16_coll<3>(d2, a, b + ((6*NOUT*128) >> 4), idesc, 1u);
+    }
+  }
+}
+
 template<int NOUT, int MODE>
 __global__ void __launch_bounds__(CONV_THREADS, 1)
 conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmW,
@@ -150,6 +209,7 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
 {
   using L = ConvSmem<NOUT>;
   constexpr int STAGES = L::NSTAGE;
+  constexpr int NACC = L::NACC;
   constexpr bool HAS_AUX = MODE == CONV_FWD_RESID || MODE == CONV_BWD_RESID || MODE == CONV_BWD_GELU;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* sm = align1024(smem_raw);
@@ -161,29 +221,30 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
   uint64_t* full = bars;
   uint64_t* empty = bars + STAGES;
   uint64_t* wbar = bars + 2*STAGES;
-  uint64_t* tfull = wbar + 1;
-  uint64_t* tempty = wbar + 3;
-  uint64_t* done = wbar + 5;
-  uint64_t* abar0 = wbar + 6;       // [group]
+  uint64_t* tfull = wbar + 1;              // [NACC]
+  uint64_t* tempty = tfull + NACC;         // [NACC]
+  uint64_t* done = tempty + NACC;
+  uint64_t* abar0 = done + 1;              // [group]
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + L::MISC_OFF);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + L::MISC_OFF + 4);
   float* bias_sm = reinterpret_cast<float*>(sm + L::BIAS_OFF);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int H = a.H, W = a.W, xt_n = W >> 7;
-  const int ntiles = a.B*H*xt_n;
+  const int H = a.H, W = a.W, R = a.rows;
+  const int nitems = strip_items(a);
+  // this CTA's output rows
+  const int nrows = static_cast<int>(blockIdx.x) < nitems
+                  ? ((nitems - static_cast<int>(blockIdx.x) + static_cast<int>(gridDim.x) - 1)/
+                     static_cast<int>(gridDim.x))*R : 0;
 
   if(threadIdx.x == 0)
   {
     for(int s = 0; s < STAGES; ++s) { mbar_init(&full[s], 1); mbar_init(&empty[s], 1); }
     mbar_init(wbar, 1);
-    mbar_init(&tfull[0], 1);
-    mbar_init(&tfull[1], 1);
     // 64-channel kernels: one epilogue group of EPI_WARPS/2 warps releases
     // each accumulator; the output layer: every epilogue warp
     const uint32_t releases = NOUT == 64 ? EPI_WARPS/2 : EPI_WARPS;
-    mbar_init(&tempty[0], releases);
-    mbar_init(&tempty[1], releases);
+    for(int c = 0; c < NACC; ++c) { mbar_init(&tfull[c], 1); mbar_init(&tempty[c], releases); }
     mbar_init(done, 1);
     mbar_init(&abar0[0], 1);
     mbar_init(&abar0[1], 1);
@@ -213,16 +274,18 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
       mbar_expect_tx(wbar, L::W_BYTES);
       for(int t = 0; t < 9; ++t) tma_load_3d(Wsm + t*NOUT*128, &tmW, 0, 0, t, wbar);
       uint32_t it = 0;
-      for(int tile = blockIdx.x; tile < ntiles && !*abort_flag; tile += gridDim.x)
+      bool ok = true;
+      for(int item = blockIdx.x; ok && item < nitems && !*abort_flag; item += gridDim.x)
       {
-        const int xt = tile % xt_n, row = tile / xt_n;
-        const int y = row % H, n = row / H, x0 = xt << 7;
-        for(int ky = 0; ky < 3; ++ky, ++it)
+        int n, x0, y0;
+        strip_item(a, item, n, x0, y0);
+        // padded input rows y0 .. y0 + R + 1 feed output rows y0 .. y0 + R - 1
+        for(int j = 0; j < R + 2; ++j, ++it)
         {
           const uint32_t s = it % STAGES, ph = (it / STAGES) & 1u;
-          if(!mbar_wait(&empty[s], ph ^ 1u)) { give_up(); break; }
+          if(!mbar_wait(&empty[s], ph ^ 1u)) { give_up(); ok = false; break; }
           mbar_expect_tx(&full[s], SLAB_BYTES);
-          tma_load_4d(Asm + s*SLAB_BYTES, &tmX, 0, x0, y + ky, n, &full[s]);
+          tma_load_4d(Asm + s*SLAB_BYTES, &tmX, 0, x0, y0 + j, n, &full[s]);
         }
       }
       // loads still in flight after an abort land before the CTA exits
@@ -242,38 +305,84 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
       bool ok = mbar_wait(wbar, 0);
       if(!ok) give_up();
       const uint32_t wbase = smem_u32(Wsm), abase = smem_u32(Asm);
-      uint32_t it = 0, tcount = 0;
-      for(int tile = blockIdx.x; ok && tile < ntiles && !*abort_flag; tile += gridDim.x, ++tcount)
+      const uint64_t db = sw128_desc(wbase, 16, 1024);
+      // cycle counters of this thread (ConvArgs::cycles): waits for input
+      // slabs and for drained accumulators, and the span to the last issue
+      long long w_slab = 0, w_acc = 0;
+      const long long c_start = clock64();
+      uint32_t it = 0;
+      int t0 = 0;                    // this CTA's index of the strip's first output row
+      for(int item = blockIdx.x; ok && item < nitems && !*abort_flag; item += gridDim.x, t0 += R)
       {
-        const uint32_t acc = tcount & 1u, use = tcount >> 1;
-        if(!mbar_wait(&tempty[acc], (use & 1u) ^ 1u)) { give_up(); break; }
-        tc_fence_after();
-        const uint32_t d = tbase + acc*NOUT;
-        for(int ky = 0; ky < 3; ++ky, ++it)
+        for(int j = 0; j < R + 2; ++j, ++it)
         {
-          const uint32_t s = it % STAGES, ph = (it / STAGES) & 1u;
-          if(!mbar_wait(&full[s], ph)) { give_up(); ok = false; break; }
-          tc_fence_after();
-          // descriptors of this slab and weight row, advanced by plain adds
-          // (the start address sits in the low bits, in 16-byte units)
-          const uint64_t da = sw128_desc(abase + s*SLAB_BYTES, 16, 1024);
-          const uint64_t db = sw128_desc(wbase + 3*ky*NOUT*128, 16, 1024);
-#pragma unroll
-          for(int kx = 0; kx < 3; ++kx)
+          if(j < R)
           {
-            // tap (ky, kx): slab pixels kx .. kx+127
+            // output row j starts here: its accumulator must be drained
+            const int t = t0 + j;
+            const uint32_t acc = t % NACC, use = t / NACC;
+            const long long c0 = clock64();
+            const bool got = mbar_wait(&tempty[acc], (use & 1u) ^ 1u);
+            w_acc += clock64() - c0;
+            if(!got) { give_up(); ok = false; break; }
+            tc_fence_after();
+          }
+          const uint32_t s = it % STAGES, ph = (it / STAGES) & 1u;
+          const long long c0 = clock64();
+          const bool got = mbar_wait(&full[s], ph);
+          w_slab += clock64() - c0;
+          if(!got) { give_up(); ok = false; break; }
+          tc_fence_after();
+          // slab j feeds output rows j - ky for ky in [lo, hi]
+          const int lo = j >= R ? j - R + 1 : 0;
+          const int hi = j < 2 ? j : 2;
+          const uint32_t d0 = tbase + ((t0 + j) & (NACC - 1))*NOUT;
+          const uint32_t d1 = tbase + ((t0 + j - 1) & (NACC - 1))*NOUT;
+          const uint32_t d2 = tbase + ((t0 + j - 2) & (NACC - 1))*NOUT;
+          const uint64_t da = sw128_desc(abase + s*SLAB_BYTES, 16, 1024);
+          // the weight descriptor base, opaque to the compiler inside the
+          // loop: otherwise it hoists all 36 loop-invariant B descriptors
+          // into registers, and the kernel (96 registers at 576 threads)
+          // spills
+          uint64_t dbs;
+          asm volatile("mov.b64 %0, %1;" : "=l"(dbs) : "l"(db));
+          if(lo == 0 && hi == 2) slab_mmas<NOUT>(d0, d1, d2, da, dbs, IDESC);
+          else
+          {
+            // a strip's first two and last two slabs feed only the one or
+            // two output rows inside the strip: a compact loop without the
+            // collector (an unrolled variant per case costs registers)
+#pragma unroll 1
+            for(int ky = lo; ky <= hi; ++ky)
+            {
+              const uint32_t d = tbase + ((t0 + j - ky) & (NACC - 1))*NOUT;
+              const uint64_t dbk = sw128_desc(wbase + 3*ky*NOUT*128, 16, 1024);
 #pragma unroll
-            for(int k = 0; k < 4; ++k)
-              mma_bf16(d, da + ((kx*128 + 32*k) >> 4), db + ((kx*NOUT*128 + 32*k) >> 4), IDESC,
-                       (ky | kx | k) != 0);
+              for(int kx = 0; kx < 3; ++kx)
+              {
+#pragma unroll
+                for(int k = 0; k < 4; ++k)
+                  mma_bf16(d, da + ((kx*128 + 32*k) >> 4), dbk + ((kx*NOUT*128 + 32*k) >> 4), IDESC,
+                           (ky | kx | k) != 0);
+              }
+            }
           }
           mma_commit(&empty[s]);
+          // output row j - 2 has all its contributions
+          if(j >= 2) mma_commit(&tfull[(t0 + j - 2) & (NACC - 1)]);
         }
-        if(!ok) break;
-        mma_commit(&tfull[acc]);
       }
       mma_commit(done);
+      const long long c_issue = clock64() - c_start;
       if(!mbar_wait(done, 0)) give_up();
+      if(a.cycles)
+      {
+        long long* c = a.cycles + 4*blockIdx.x;
+        c[0] = clock64() - c_start;
+        c[1] = c_issue;
+        c[2] = w_slab;
+        c[3] = w_acc;
+      }
     }
   }
   else if constexpr(NOUT == 16)
@@ -282,14 +391,13 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
     // the first 16-column slice hold all 16 columns, the others only release
     const int q = warp & 3;
     const int c0 = ((warp - 2) >> 2)*16;
-    uint32_t tcount = 0;
-    for(int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++tcount)
+    for(int t = 0; t < nrows; ++t)
     {
       if(__any_sync(0xffffffffu, *abort_flag != 0)) break;
-      const uint32_t acc = tcount & 1u, use = tcount >> 1;
-      const int xt = tile % xt_n, row = tile / xt_n;
-      const int y = row % H, n = row / H;
-      const int x = (xt << 7) + q*32 + lane;
+      const uint32_t acc = t & (NACC - 1), use = t / NACC;
+      int n, x0, y;
+      strip_row(a, t, n, x0, y);
+      const int x = x0 + q*32 + lane;
       if(!__all_sync(0xffffffffu, mbar_wait(&tfull[acc], use & 1u)))
       {
         if(lane == 0) give_up();
@@ -312,15 +420,16 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
   }
   else
   {
-    // Two groups of 8 epilogue warps; group g drains accumulator g, i.e.
-    // every other tile, so two tiles' epilogues run at once. Within a group
-    // thread = pixel p = 32q + lane of the tile, channels c0..c0+31 (two
-    // warps per TMEM lane quarter). The output tile is staged in shared
-    // memory in the 128-byte-swizzled layout and written by TMA stores (row
-    // y and, on the first / last image row, the periodic ring row); the two
-    // ring columns are written directly by the threads of pixels 0 and W-1.
-    // Every branch that leaves the loop is agreed by all 256 threads of the
-    // group (named_and), so the group's named barrier is always met by all.
+    // Two groups of 8 epilogue warps; group g drains the output rows t = g,
+    // g + 2, ... of this CTA (accumulator t % NACC), so two rows' epilogues
+    // run at once. Within a group thread = pixel p = 32q + lane of the tile,
+    // channels c0..c0+31 (two warps per TMEM lane quarter). The output tile
+    // is staged in shared memory in the 128-byte-swizzled layout and written
+    // by TMA stores (row y and, on the first / last image row, the periodic
+    // ring row); the two ring columns are written directly by the threads of
+    // pixels 0 and W-1. Every branch that leaves the loop is agreed by all
+    // 256 threads of the group (named_and), so the group's named barrier is
+    // always met by all.
     constexpr int GROUP_N = 32*EPI_WARPS/2;
     const int e = warp - 2;
     const int g = e / (EPI_WARPS/2);
@@ -336,26 +445,26 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
     uint32_t off[4];
 #pragma unroll
     for(int k = 0; k < 4; ++k) off[k] = p*128u + ((((c0 >> 3) + k) ^ (p & 7)) << 4);
-    const int stride = 2*static_cast<int>(gridDim.x);
-    const int first = static_cast<int>(blockIdx.x) + g*static_cast<int>(gridDim.x);
     bool aux_pending = false;
     if constexpr(HAS_AUX)
     {
-      if(leader && first < ntiles)
+      if(leader && g < nrows)
       {
-        const int xt = first % xt_n, row = first / xt_n;
+        int n, x0, y;
+        strip_row(a, g, n, x0, y);
         mbar_expect_tx(abar, TILE_BYTES);
-        tma_load_4d(auxS, &tmR, 0, (xt << 7) + 1, row % H + 1, row / H, abar);
+        tma_load_4d(auxS, &tmR, 0, x0 + 1, y + 1, n, abar);
         aux_pending = true;
       }
     }
     uint32_t k = 0;
-    for(int tile = first; tile < ntiles; tile += stride, ++k)
+    for(int t = g; t < nrows; t += 2, ++k)
     {
-      const int xt = tile % xt_n, row = tile / xt_n;
-      const int y = row % H, n = row / H, x0 = xt << 7;
+      int n, x0, y;
+      strip_row(a, t, n, x0, y);
       const int x = x0 + p;
-      bool ok = *abort_flag == 0 && mbar_wait(&tfull[g], k & 1u);
+      const uint32_t acc = t & (NACC - 1), use = t / NACC;
+      bool ok = *abort_flag == 0 && mbar_wait(&tfull[acc], use & 1u);
       if constexpr(HAS_AUX) ok = ok && mbar_wait(abar, k & 1u);
       if(!named_and(bar_id, GROUP_N, ok))
       {
@@ -365,12 +474,12 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
       if constexpr(HAS_AUX) if(leader) aux_pending = false;
       tc_fence_after();
       float v[32];
-      const uint32_t taddr = tbase + (static_cast<uint32_t>(q*32) << 16) + g*NOUT + c0;
+      const uint32_t taddr = tbase + (static_cast<uint32_t>(q*32) << 16) + acc*NOUT + c0;
       tmem_ld16(taddr, v);
       tmem_ld16(taddr + 16, v + 16);
       tc_fence_before();
       __syncwarp();
-      if(lane == 0) mbar_arrive(&tempty[g]);
+      if(lane == 0) mbar_arrive(&tempty[acc]);
       float r[32];
       if constexpr(HAS_AUX)
       {
@@ -418,12 +527,12 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
       named_sync(bar_id, GROUP_N);
       if constexpr(HAS_AUX)
       {
-        const int nt = tile + stride;
-        if(leader && nt < ntiles)
+        if(leader && t + 2 < nrows)
         {
-          const int nxt = nt % xt_n, nrow = nt / xt_n;
+          int nn, nx0, ny;
+          strip_row(a, t + 2, nn, nx0, ny);
           mbar_expect_tx(abar, TILE_BYTES);
-          tma_load_4d(auxS, &tmR, 0, (nxt << 7) + 1, nrow % H + 1, nrow / H, abar);
+          tma_load_4d(auxS, &tmR, 0, nx0 + 1, ny + 1, nn, abar);
           aux_pending = true;
         }
       }
@@ -697,26 +806,50 @@ cudaError_t smem_attr(K kern, unsigned long long& set_mask, int bytes)
 template<int NOUT, int MODE>
 cudaError_t launch_mode(const CUtensorMap& tx, const CUtensorMap& tw, const CUtensorMap& to,
                         const CUtensorMap& to2, const CUtensorMap& tr, const ConvArgs& a,
-                        cudaStream_t st)
+                        cudaStream_t st, int* ncta)
 {
   static unsigned long long attr = 0;
   auto kern = conv3x3_kernel<NOUT, MODE>;
   const cudaError_t e = smem_attr(kern, attr, static_cast<int>(ConvSmem<NOUT>::ALLOC));
   if(e != cudaSuccess) return e;
-  const int ntiles = a.B*a.H*(a.W >> 7);
-  const int grid = std::min(ntiles, sm_count());
+  const int nitems = a.B*(a.W >> 7)*(a.H / a.rows);
+  const int grid = std::min(nitems, sm_count());
+  if(ncta) *ncta = grid;
   kern<<<grid, CONV_THREADS, ConvSmem<NOUT>::ALLOC, st>>>(tx, tw, to, to2, tr, a);
   return cudaGetLastError();
+}
+
+// Strip height R of the forward / input-gradient kernel: a divisor of H of
+// at most 16, so that every strip is whole. Each input slab serves up to
+// three output rows of its strip, so taller strips read fewer A operands
+// per output row; they also make fewer strips. A problem that fills less
+// than one wave at R = 1 takes the tallest strips; otherwise the tallest
+// that still gives every SM two strips or more. MASS_SG_CONV_ROWS, a
+// divisor of H from 1 to 64, fixes R.
+int strip_rows(int B, int H, int W)
+{
+  if(const char* e = std::getenv("MASS_SG_CONV_ROWS"))
+  {
+    const int r = std::atoi(e);
+    if(r >= 1 && r <= 64 && H % r == 0) return r;
+  }
+  const long long rows = static_cast<long long>(B)*H*(W >> 7);
+  const long long sms = sm_count();
+  for(int r = std::min(16, H); r > 1; --r)
+    if(H % r == 0 && (rows <= sms || rows/r >= 2*sms)) return r;
+  return 1;
 }
 
 } // namespace
 
 cudaError_t conv3x3_launch(const __nv_bfloat16* in, const __nv_bfloat16* w, int nout, int mode,
-                           const ConvArgs& a, cudaStream_t st)
+                           const ConvArgs& args, cudaStream_t st, int* ncta)
 {
-  if(a.B < 1 || a.H < 1 || a.W < 128 || (a.W & 127)) return cudaErrorInvalidValue;
+  if(args.B < 1 || args.H < 1 || args.W < 128 || (args.W & 127)) return cudaErrorInvalidValue;
   if((nout == 16) != (mode == CONV_FWD_OUT) || (nout != 16 && nout != 64))
     return cudaErrorInvalidValue;
+  ConvArgs a = args;
+  a.rows = strip_rows(a.B, a.H, a.W);
   CUtensorMap tx, tw, to, to2, tr;
   if(!map_activation(&tx, in, a.B, a.H, a.W, SLAB_PX) || !map_weights(&tw, w, nout))
     return cudaErrorInvalidValue;
@@ -731,13 +864,13 @@ cudaError_t conv3x3_launch(const __nv_bfloat16* in, const __nv_bfloat16* w, int 
     return cudaErrorInvalidValue;
   switch(mode)
   {
-    case CONV_FWD_BIAS: return launch_mode<64, CONV_FWD_BIAS>(tx, tw, to, to2, tr, a, st);
-    case CONV_FWD_GELU: return launch_mode<64, CONV_FWD_GELU>(tx, tw, to, to2, tr, a, st);
-    case CONV_FWD_RESID: return launch_mode<64, CONV_FWD_RESID>(tx, tw, to, to2, tr, a, st);
-    case CONV_FWD_OUT: return launch_mode<16, CONV_FWD_OUT>(tx, tw, to, to2, tr, a, st);
-    case CONV_BWD_GELU: return launch_mode<64, CONV_BWD_GELU>(tx, tw, to, to2, tr, a, st);
-    case CONV_BWD_RESID: return launch_mode<64, CONV_BWD_RESID>(tx, tw, to, to2, tr, a, st);
-    case CONV_BWD_PLAIN: return launch_mode<64, CONV_BWD_PLAIN>(tx, tw, to, to2, tr, a, st);
+    case CONV_FWD_BIAS: return launch_mode<64, CONV_FWD_BIAS>(tx, tw, to, to2, tr, a, st, ncta);
+    case CONV_FWD_GELU: return launch_mode<64, CONV_FWD_GELU>(tx, tw, to, to2, tr, a, st, ncta);
+    case CONV_FWD_RESID: return launch_mode<64, CONV_FWD_RESID>(tx, tw, to, to2, tr, a, st, ncta);
+    case CONV_FWD_OUT: return launch_mode<16, CONV_FWD_OUT>(tx, tw, to, to2, tr, a, st, ncta);
+    case CONV_BWD_GELU: return launch_mode<64, CONV_BWD_GELU>(tx, tw, to, to2, tr, a, st, ncta);
+    case CONV_BWD_RESID: return launch_mode<64, CONV_BWD_RESID>(tx, tw, to, to2, tr, a, st, ncta);
+    case CONV_BWD_PLAIN: return launch_mode<64, CONV_BWD_PLAIN>(tx, tw, to, to2, tr, a, st, ncta);
     default: return cudaErrorInvalidValue;
   }
 }

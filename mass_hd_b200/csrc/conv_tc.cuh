@@ -40,12 +40,18 @@ struct ConvArgs
   const float* resid_f;              // [B][H][W][5] (FWD_OUT)
   float* out_f;                      // [B][H][W][5] (FWD_OUT)
   int* err;                          // bit 1: a bounded wait gave up
+  int rows = 0;                      // strip height; conv3x3_launch sets it
+  // optional, 4 per CTA (grid = min(strips, SMs)): the MMA thread's cycles
+  // from start to done, to its last issue, waiting for input slabs, waiting
+  // for drained accumulators
+  long long* cycles = nullptr;
 };
 
 // in: padded NHWC64; w: forward weights [9][nout][64] (nout 64 or 16) or the
 // input-gradient weights [9][64][64] (nout 64).
+// *ncta (if given) receives the number of CTAs launched.
 cudaError_t conv3x3_launch(const __nv_bfloat16* in, const __nv_bfloat16* w, int nout, int mode,
-                           const ConvArgs& a, cudaStream_t st);
+                           const ConvArgs& a, cudaStream_t st, int* ncta = nullptr);
 
 // dW[tap][ci][co] += sum over pixels of x(p + tap offset)[ci] * dy(p)[co];
 // x and dy padded NHWC64; dW fp32 [9][64][64], accumulated with atomics

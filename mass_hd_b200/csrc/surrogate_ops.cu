@@ -267,9 +267,11 @@ Norm make_norm(const float* mean, const float* scale)
 
 extern "C" {
 
-int mass_sg_conv3x3(const void* in, const void* w, int nout, int mode, int B, int H, int W,
-                    const float* bias, const void* resid, const void* aux, void* out, void* out2,
-                    const float* resid_f, float* out_f, int* err, void* stream)
+namespace {
+int conv_call(const void* in, const void* w, int nout, int mode, int B, int H, int W,
+              const float* bias, const void* resid, const void* aux, void* out, void* out2,
+              const float* resid_f, float* out_f, int* err, long long* cycles, int* ncta,
+              void* stream)
 {
   if(!in || !w || !err) return sg_fail(MASS_LB_EINVAL, "null argument");
   if(!dims_ok(B, H, W)) return sg_fail(MASS_LB_EINVAL, "need B, H >= 1 and W a multiple of 128");
@@ -286,9 +288,29 @@ int mass_sg_conv3x3(const void* in, const void* w, int nout, int mode, int B, in
   ConvArgs a{B, H, W, bias, static_cast<const __nv_bfloat16*>(resid),
              static_cast<const __nv_bfloat16*>(aux), static_cast<__nv_bfloat16*>(out),
              static_cast<__nv_bfloat16*>(out2), resid_f, out_f, err};
+  a.cycles = cycles;
   return sg_cuda(conv3x3_launch(static_cast<const __nv_bfloat16*>(in),
                                 static_cast<const __nv_bfloat16*>(w), nout, mode, a,
-                                static_cast<cudaStream_t>(stream)), "conv3x3");
+                                static_cast<cudaStream_t>(stream), ncta), "conv3x3");
+}
+} // namespace
+
+int mass_sg_conv3x3(const void* in, const void* w, int nout, int mode, int B, int H, int W,
+                    const float* bias, const void* resid, const void* aux, void* out, void* out2,
+                    const float* resid_f, float* out_f, int* err, void* stream)
+{
+  return conv_call(in, w, nout, mode, B, H, W, bias, resid, aux, out, out2, resid_f, out_f, err,
+                   nullptr, nullptr, stream);
+}
+
+int mass_sg_conv3x3_profile(const void* in, const void* w, int nout, int mode, int B, int H,
+                            int W, const float* bias, const void* resid, const void* aux,
+                            void* out, void* out2, const float* resid_f, float* out_f, int* err,
+                            long long* cycles, int* ncta, void* stream)
+{
+  if(!cycles || !ncta) return sg_fail(MASS_LB_EINVAL, "null cycles or ncta");
+  return conv_call(in, w, nout, mode, B, H, W, bias, resid, aux, out, out2, resid_f, out_f, err,
+                   cycles, ncta, stream);
 }
 
 int mass_sg_conv3x3_wgrad(const void* x, const void* dy, float* dW, int B, int H, int W, int* err,

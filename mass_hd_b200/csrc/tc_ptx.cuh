@@ -174,6 +174,37 @@ __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a_desc, uint6
     "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
     :: "r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate));
 }
+// The same MMA with the A-operand collector buffer: COLL 1 fills it from
+// shared memory (A read as usual, then kept), 2 reads A from it, 3 reads A
+// from it for the last time. A run fill, use..., lastuse lets consecutive
+// MMAs that share A (same descriptor) but take different B read A from
+// shared memory once.
+template<int COLL>
+__device__ __forceinline__ void mma_bf16_coll(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc,
+                                              uint32_t idesc, uint32_t accumulate)
+{
+  static_assert(COLL >= 0 && COLL <= 3, "collector usage");
+  if constexpr(COLL == 0)
+    mma_bf16(d_tmem, a_desc, b_desc, idesc, accumulate);
+  else if constexpr(COLL == 1)
+    asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16.collector::a::fill [%0], %1, %2, %3, p;\n\t}"
+      :: "r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate));
+  else if constexpr(COLL == 2)
+    asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16.collector::a::use [%0], %1, %2, %3, p;\n\t}"
+      :: "r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate));
+  else
+    asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16.collector::a::lastuse [%0], %1, %2, %3, p;\n\t}"
+      :: "r"(d_tmem), "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate));
+}
 // arrive on `bar` once every tcgen05.mma issued so far by this thread is done
 __device__ __forceinline__ void mma_commit(uint64_t* bar)
 {

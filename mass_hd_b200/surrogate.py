@@ -57,6 +57,8 @@ def library():
     fl = C.POINTER(C.c_float)
     sig = {
         "mass_sg_conv3x3": [vp, vp, i, i, i, i, i, vp, vp, vp, vp, vp, vp, vp, vp, vp],
+        "mass_sg_conv3x3_profile": [vp, vp, i, i, i, i, i, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
+                                    vp],
         "mass_sg_conv3x3_wgrad": [vp, vp, vp, i, i, i, vp, vp],
         "mass_sg_bias_grad": [vp, vp, i, i, i, vp],
         "mass_sg_pack": [vp, vp, vp, i, i, i, vp, vp, vp, vp],

@@ -19,6 +19,7 @@ Each prints one JSON object.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import sys
@@ -55,6 +56,21 @@ def _time(fn, iters=20, warmup=3):
     return s.elapsed_time(e) / iters
 
 
+def mma_thread_cycles(net, L) -> dict:
+    """Median over CTAs of the forward kernel's MMA-thread cycle counters
+    (mass_sg_conv3x3_profile), for the GELU-epilogue convolution."""
+    cyc = torch.zeros(4 * 1024, dtype=torch.int64, device="cuda")
+    ncta = ctypes.c_int(0)
+    G._call("mass_sg_conv3x3_profile", G._p(net.h[0]), G._p(L.wt), 64, G.FWD_GELU, net.B, net.H,
+            net.W, G._p(L.b), None, None, G._p(net.u[0]), G._p(net.t[0]), None, None,
+            G._p(net.err), G._p(cyc), ctypes.addressof(ncta), G._stream())
+    torch.cuda.synchronize()
+    c = cyc[:4 * ncta.value].view(-1, 4).cpu().numpy()
+    med = np.median(c, axis=0)
+    return {"ctas": ncta.value, "cycles_total": int(med[0]), "cycles_to_last_issue": int(med[1]),
+            "waiting_for_slabs": int(med[2]), "waiting_for_accumulators": int(med[3])}
+
+
 def bench(batch=32, size=256) -> dict:
     P = G.Params(seed=0)
     net = G.Net(P, batch, size, size, train=True)
@@ -79,6 +95,7 @@ def bench(batch=32, size=256) -> dict:
     for k, fn in cases.items():
         ms = _time(fn)
         out[k] = {"ms": ms, "tflops": flop / ms / 1e9, "frac_of_peak": flop / ms / 1e9 / peak}
+    out["fwd_gelu"]["mma_thread"] = mma_thread_cycles(net, L)
 
     def step():
         net.forward()

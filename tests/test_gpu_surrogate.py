@@ -147,6 +147,64 @@ def test_backward_modes(B, H, W):
     assert rel_l2(core(host(out)), ref + r) < 3e-3
 
 
+@pytest.mark.parametrize("rows", [1, 2, 3, 8, 24])
+def test_strip_heights(rows, monkeypatch):
+    """Each CTA marches down strips of `rows` output rows and reuses every
+    input slab's A operand for the up to three output rows it feeds. Every
+    strip height gives the same convolution: 8 x 24 x 256 has 384 half-row
+    tiles, so strips of 1 or 2 rows put several strips on one CTA (the four
+    accumulators wrap) and 3, 8 and 24 rows cover the strip edges."""
+    monkeypatch.setenv("MASS_SG_CONV_ROWS", str(rows))
+    B, H, W = 8, 24, 256
+    rng = np.random.default_rng(rows)
+    x = S.bf16(rng.normal(size=(B, H, W, 64)))
+    w = S.bf16(rng.normal(0, 0.05, (64, 9, 64)))
+    bias = rng.normal(0, 0.1, 64)
+    r = S.bf16(rng.normal(size=(B, H, W, 64)))
+    X, Wt, R = dev_bf16(to_padded(x)), dev_bf16(fwd_weights(w, 64)), dev_bf16(to_padded(r))
+    out, _, _ = run_conv(X, Wt, 64, G.FWD_RESID, bias, resid=R)
+    o = host(out)
+    check_ring(o)
+    assert rel_l2(core(o), S.conv(x, w) + bias + r) < 3e-3
+    Wd = dev_bf16(dgrad_weights(w))
+    out, _, _ = run_conv(X, Wd, 64, G.BWD_GELU, aux=R)
+    assert rel_l2(core(host(out)), S.conv_input_grad(x, w) * S.gelu_grad(r)) < 3e-3
+    w5 = S.bf16(rng.normal(0, 0.05, (5, 9, 64)))
+    b16 = np.zeros(16)
+    b16[:5] = bias[:5]
+    _, _, of = run_conv(X, dev_bf16(fwd_weights(w5, 16)), 16, G.FWD_OUT, b16)
+    assert rel_l2(of.cpu().numpy(), S.conv(x, w5) + bias[:5]) < 1e-5
+
+
+def test_profile_entry_point_matches_and_counts():
+    """mass_sg_conv3x3_profile gives mass_sg_conv3x3's output bit for bit and
+    fills 4 cycle counters per CTA (total >= span to the last issue >= each
+    wait)."""
+    import ctypes
+    B, H, W = 4, 32, 256
+    rng = np.random.default_rng(5)
+    x = S.bf16(rng.normal(size=(B, H, W, 64)))
+    w = S.bf16(rng.normal(0, 0.05, (64, 9, 64)))
+    bias = rng.normal(0, 0.1, 64)
+    X, Wt = dev_bf16(to_padded(x)), dev_bf16(fwd_weights(w, 64))
+    ref, ref2, _ = run_conv(X, Wt, 64, G.FWD_GELU, bias)
+    out, out2 = torch.zeros_like(X), torch.zeros_like(X)
+    b = torch.tensor(bias, dtype=torch.float32).cuda()
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    cyc = torch.zeros(4 * 1024, dtype=torch.int64, device="cuda")
+    ncta = ctypes.c_int(0)
+    G._call("mass_sg_conv3x3_profile", G._p(X), G._p(Wt), 64, G.FWD_GELU, B, H, W, G._p(b), None,
+            None, G._p(out), G._p(out2), None, None, G._p(err), G._p(cyc), ctypes.addressof(ncta),
+            G._stream())
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    assert torch.equal(out, ref) and torch.equal(out2, ref2)
+    c = cyc[:4 * ncta.value].view(-1, 4).cpu().numpy()
+    assert ncta.value >= 1
+    assert (c[:, 0] >= c[:, 1]).all() and (c[:, 1] > 0).all()
+    assert (c[:, 1] >= c[:, 2]).all() and (c[:, 1] >= c[:, 3]).all()
+
+
 @pytest.mark.parametrize("B,H,W", SIZES)
 def test_weight_gradient(B, H, W):
     rng = np.random.default_rng(13)
