@@ -24,10 +24,11 @@
 //
 // Weight gradient (conv3x3_wgrad_kernel): dW_tap[ci][co] = sum over pixels of
 // x(p + tap)[ci] * dy(p)[co]. K runs over pixels, so both operands are read
-// MN-major straight from the NHWC tiles. A CTA owns a pair of taps (M = 2 x
-// 64 input channels, two TMA tiles LBO apart) for a contiguous range of
-// pixel tiles, accumulates in TMEM and adds its partial sums to dW with
-// atomics.
+// MN-major straight from the NHWC tiles. A CTA computes all 9 taps (five tap
+// pairs, M = 2 x 64 input channels, the pair's tiles LBO apart in the three
+// input slabs of a block) for a contiguous range of 128-pixel blocks,
+// accumulates in TMEM and adds its partial sums to dW with vector
+// reductions.
 //
 // Every mbarrier wait is bounded (about a second); on time-out the role sets
 // an error bit, the others stop at their next wait, outstanding MMAs are
@@ -589,13 +590,27 @@ conv3x3_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ 
 }
 
 // ---- weight gradient ---------------------------------------------------------
+//
+// A CTA computes all 9 taps for a contiguous range of 128-pixel blocks. Per
+// block one stage holds the three 136-pixel input slabs of padded rows y,
+// y+1, y+2 (tap (ky, kx) of the block is slab ky read from pixel kx) and the
+// dy tile: 68 KB of TMA writes for 40 MMAs, instead of 48 KB for every 8
+// when a CTA owned one tap pair. A = two taps' input tiles, MN-major (M = 2
+// x 64 input channels, the second group LBO bytes after the first, K =
+// pixels), B = the dy tile; five tap pairs, five accumulators:
+//   (0,0)+(0,1) and (1,0)+(1,1) and (2,0)+(2,1): one slab, LBO 128 B;
+//   (0,2)+(1,2): slabs 0 and 1, LBO one slab;
+//   (2,2) + a second group that is read but not kept (LBO 128 B, pixels
+//   3..130 of slab 2, inside the slab).
 
-constexpr int WG_STAGES = 4;
-constexpr uint32_t WG_STAGE = 3*TILE_BYTES;     // x tap a, x tap b, dy
+constexpr int WG_STAGES = 3;
+constexpr uint32_t WG_SLABS = 3*SLAB_BYTES;
+constexpr uint32_t WG_STAGE = WG_SLABS + TILE_BYTES;     // three x slabs, dy
 constexpr uint32_t WG_BAR_OFF = WG_STAGES*WG_STAGE;
 constexpr uint32_t WG_MISC_OFF = WG_BAR_OFF + (2*WG_STAGES + 1)*8;
 constexpr uint32_t WG_ALLOC = WG_MISC_OFF + 16 + 1024;
-constexpr int WG_GROUPS = 5;                     // tap pairs {0,1} {2,3} {4,5} {6,7} {8}
+constexpr int WG_PAIRS = 5;
+static_assert(WG_ALLOC <= 232448, "shared memory per CTA");
 
 struct WgradArgs
 {
@@ -603,6 +618,25 @@ struct WgradArgs
   float* dW;
   int* err;
 };
+
+// tap of M group h (0 or 1) of pair p; -1: read but not kept
+__device__ __forceinline__ int wg_tap(int p, int h)
+{
+  switch(p)
+  {
+    case 0: return h;          // (0,0), (0,1)
+    case 1: return 3 + h;      // (1,0), (1,1)
+    case 2: return 6 + h;      // (2,0), (2,1)
+    case 3: return h ? 5 : 2;  // (0,2), (1,2)
+    default: return h ? -1 : 8;
+  }
+}
+
+__device__ __forceinline__ void red_add4(float* p, float a, float b, float c, float d)
+{
+  asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};"
+               :: "l"(p), "f"(a), "f"(b), "f"(c), "f"(d) : "memory");
+}
 
 __global__ void __launch_bounds__(WG_THREADS, 1)
 conv3x3_wgrad_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_constant__ CUtensorMap tmD,
@@ -617,8 +651,7 @@ conv3x3_wgrad_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_const
   volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + WG_MISC_OFF + 4);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int g = blockIdx.x % WG_GROUPS, chunk = blockIdx.x / WG_GROUPS;
-  const int ta = 2*g, tb = 2*g + 1 < 9 ? 2*g + 1 : 8;
+  const int chunk = blockIdx.x;
   const int xt_n = a.W >> 7;
   const long long nblocks = static_cast<long long>(a.B)*a.H*xt_n;
   const int b0 = static_cast<int>(chunk*nblocks/a.nchunks);
@@ -632,7 +665,7 @@ conv3x3_wgrad_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_const
     fence_barrier_init();
     fence_proxy_async();
   }
-  if(warp == 1) tmem_alloc(tmem_slot, 64);
+  if(warp == 1) tmem_alloc(tmem_slot, 512);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -657,9 +690,8 @@ conv3x3_wgrad_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_const
         if(!mbar_wait(&empty[s], ph ^ 1u)) { give_up(); break; }
         uint8_t* st = sm + s*WG_STAGE;
         mbar_expect_tx(&full[s], WG_STAGE);
-        tma_load_4d(st, &tmX, 0, x0 + ta % 3, y + ta / 3, n, &full[s]);
-        tma_load_4d(st + TILE_BYTES, &tmX, 0, x0 + tb % 3, y + tb / 3, n, &full[s]);
-        tma_load_4d(st + 2*TILE_BYTES, &tmD, 0, x0 + 1, y + 1, n, &full[s]);
+        for(int ky = 0; ky < 3; ++ky) tma_load_4d(st + ky*SLAB_BYTES, &tmX, 0, x0, y + ky, n, &full[s]);
+        tma_load_4d(st + WG_SLABS, &tmD, 0, x0 + 1, y + 1, n, &full[s]);
       }
       if(*abort_flag)
         for(uint32_t k = 0; k < WG_STAGES && k < it; ++k)
@@ -673,9 +705,7 @@ conv3x3_wgrad_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_const
   {
     if(lane == 0)
     {
-      // A = the two x tiles (M = 2 x 64 input channels, MN groups one tile
-      // apart, K = pixels in 8-row groups 1024 B apart); B = the dy tile
-      // (N = 64 output channels, one MN group)
+      // both operands MN-major: K = pixels in 8-row groups 1024 B apart
       constexpr uint32_t IDESC = idesc_bf16_f32(128, 64, 1, 1);
       const uint32_t base = smem_u32(sm);
       uint32_t it = 0;
@@ -685,12 +715,22 @@ conv3x3_wgrad_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_const
         if(!mbar_wait(&full[s], ph)) { give_up(); break; }
         tc_fence_after();
         const uint32_t st = base + s*WG_STAGE;
-        const uint64_t da = sw128_desc(st, TILE_BYTES, 1024);
-        const uint64_t db = sw128_desc(st + 2*TILE_BYTES, 1024, 1024);
+        const uint64_t db = sw128_desc(st + WG_SLABS, 1024, 1024);
+        const uint64_t da[WG_PAIRS] = {
+          sw128_desc(st, 128, 1024),
+          sw128_desc(st + SLAB_BYTES, 128, 1024),
+          sw128_desc(st + 2*SLAB_BYTES, 128, 1024),
+          sw128_desc(st + 256, SLAB_BYTES, 1024),
+          sw128_desc(st + 2*SLAB_BYTES + 256, 128, 1024)};
+        const uint32_t first = blk == b0;
 #pragma unroll
-        for(int kk = 0; kk < 8; ++kk)
-          mma_bf16(tbase, da + ((kk*2048) >> 4), db + ((kk*2048) >> 4), IDESC,
-                   (blk != b0) || (kk != 0));
+        for(int p = 0; p < WG_PAIRS; ++p)
+        {
+#pragma unroll
+          for(int kk = 0; kk < 8; ++kk)
+            mma_bf16(tbase + p*64, da[p] + ((kk*2048) >> 4), db + ((kk*2048) >> 4), IDESC,
+                     !(first && kk == 0));
+        }
         mma_commit(&empty[s]);
       }
       mma_commit(done);
@@ -699,8 +739,8 @@ conv3x3_wgrad_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_const
   }
   else if(b1 > b0)
   {
+    // warps 2-5: TMEM lane quarter q = warp % 4 holds M rows 32q .. 32q+31
     const int q = warp & 3;
-    // warp-uniform: tcgen05.ld needs all 32 lanes
     if(!__all_sync(0xffffffffu, mbar_wait(done, 0)))
     {
       if(lane == 0) give_up();
@@ -710,17 +750,20 @@ conv3x3_wgrad_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_const
       tc_fence_after();
       const int m = q*32 + lane;
       const int h = m >> 6, ci = m & 63;
-      const int tap = h ? tb : ta;
-      float v[64];
-      const uint32_t taddr = tbase + (static_cast<uint32_t>(q*32) << 16);
-      tmem_ld32(taddr, v);
-      tmem_ld32(taddr + 32, v + 32);
       const bool aborted = __any_sync(0xffffffffu, *abort_flag != 0);
-      if(!(h == 1 && tb == ta) && !aborted)
+      const uint32_t taddr = tbase + (static_cast<uint32_t>(q*32) << 16);
+      for(int p = 0; p < WG_PAIRS; ++p)
       {
-        float* dst = a.dW + (static_cast<size_t>(tap)*64 + ci)*64;
+        float v[64];
+        tmem_ld32(taddr + p*64, v);
+        tmem_ld32(taddr + p*64 + 32, v + 32);
+        const int tap = wg_tap(p, h);
+        if(tap >= 0 && !aborted)
+        {
+          float* dst = a.dW + (static_cast<size_t>(tap)*64 + ci)*64;
 #pragma unroll
-        for(int co = 0; co < 64; ++co) atomicAdd(dst + co, v[co]);
+          for(int co = 0; co < 64; co += 4) red_add4(dst + co, v[co], v[co + 1], v[co + 2], v[co + 3]);
+        }
       }
     }
   }
@@ -730,7 +773,7 @@ conv3x3_wgrad_kernel(const __grid_constant__ CUtensorMap tmX, const __grid_const
   if(warp == 1)
   {
     tc_fence_after();
-    tmem_dealloc(tbase, 64);
+    tmem_dealloc(tbase, 512);
     tmem_relinquish();
   }
 }
@@ -880,17 +923,16 @@ cudaError_t conv3x3_wgrad_launch(const __nv_bfloat16* x, const __nv_bfloat16* dy
 {
   if(B < 1 || H < 1 || W < 128 || (W & 127)) return cudaErrorInvalidValue;
   CUtensorMap tx, td;
-  if(!map_activation(&tx, x, B, H, W, 128) || !map_activation(&td, dy, B, H, W, 128))
+  if(!map_activation(&tx, x, B, H, W, SLAB_PX) || !map_activation(&td, dy, B, H, W, 128))
     return cudaErrorInvalidValue;
   static unsigned long long attr = 0;
   const cudaError_t e = smem_attr(conv3x3_wgrad_kernel, attr, static_cast<int>(WG_ALLOC));
   if(e != cudaSuccess) return e;
   const long long nblocks = static_cast<long long>(B)*H*(W >> 7);
-  // chunks per tap pair: all CTAs in one wave (one CTA fits an SM)
-  const int nchunks = static_cast<int>(std::max<long long>(1, std::min<long long>(
-    nblocks, std::max(1, sm_count()/WG_GROUPS))));
+  // one CTA per SM (one fits), each a contiguous range of blocks
+  const int nchunks = static_cast<int>(std::max<long long>(1, std::min<long long>(nblocks, sm_count())));
   WgradArgs a{B, H, W, nchunks, dW, err};
-  conv3x3_wgrad_kernel<<<WG_GROUPS*nchunks, WG_THREADS, WG_ALLOC, st>>>(tx, td, a);
+  conv3x3_wgrad_kernel<<<nchunks, WG_THREADS, WG_ALLOC, st>>>(tx, td, a);
   return cudaGetLastError();
 }
 
