@@ -864,11 +864,14 @@ cudaError_t launch_mode(const CUtensorMap& tx, const CUtensorMap& tw, const CUte
 
 // Strip height R of the forward / input-gradient kernel: a divisor of H of
 // at most 16, so that every strip is whole. Each input slab serves up to
-// three output rows of its strip, so taller strips read fewer A operands
-// per output row; they also make fewer strips. A problem that fills less
-// than one wave at R = 1 takes the tallest strips; otherwise the tallest
-// that still gives every SM two strips or more. MASS_SG_CONV_ROWS, a
-// divisor of H from 1 to 64, fixes R.
+// three output rows of its strip, so taller strips load fewer slabs per
+// output row (R + 2 per R rows), but they make fewer, longer work items.
+// R minimises the busiest CTA's time: its output rows (whole strips per CTA
+// times R) times the cost of a row, 0.724 + 0.245 (R + 2)/R, a fit to the
+// measured time per row on B200 (strips of 1, 4, 8 and 16 rows at 32 x 256
+// x 256: 1.46, 1.07, 1.02 and 1.00). At 32 x 256 x 256 that is 16 rows; at
+// 16 x 256 x 256, 8 rows (56 rows per CTA against 64 with 16-row strips).
+// MASS_SG_CONV_ROWS, a divisor of H from 1 to 64, fixes R.
 int strip_rows(int B, int H, int W)
 {
   if(const char* e = std::getenv("MASS_SG_CONV_ROWS"))
@@ -876,11 +879,19 @@ int strip_rows(int B, int H, int W)
     const int r = std::atoi(e);
     if(r >= 1 && r <= 64 && H % r == 0) return r;
   }
-  const long long rows = static_cast<long long>(B)*H*(W >> 7);
+  const long long halves = static_cast<long long>(B)*(W >> 7);
   const long long sms = sm_count();
-  for(int r = std::min(16, H); r > 1; --r)
-    if(H % r == 0 && (rows <= sms || rows/r >= 2*sms)) return r;
-  return 1;
+  int best = 1;
+  double best_cost = -1.0;
+  for(int r = 1; r <= std::min(16, H); ++r)
+  {
+    if(H % r) continue;
+    const long long items = halves*(H / r);
+    const double rows = static_cast<double>((items + sms - 1)/sms*r);
+    const double cost = rows*(0.724 + 0.245*(r + 2)/r);
+    if(best_cost < 0.0 || cost <= best_cost) { best = r; best_cost = cost; }
+  }
+  return best;
 }
 
 } // namespace
