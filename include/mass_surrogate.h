@@ -58,6 +58,13 @@ int mass_sg_conv3x3_profile(const void* in, const void* w, int nout, int mode, i
                             void* out, void* out2, const float* resid_f, float* out_f, int* err,
                             long long* cycles, int* ncta, void* stream);
 
+/* The strip height mass_sg_conv3x3 uses for B images of H x W on a GPU
+ * with nsm SMs: each CTA marches down strips of that many output rows (a
+ * divisor of H, at most 16), loading each input row once per strip. Host
+ * arithmetic, no GPU needed; the environment variable MASS_SG_CONV_ROWS,
+ * which mass_sg_conv3x3 honours, is not read here. */
+int mass_sg_conv_strip_rows(int B, int H, int W, int nsm);
+
 /* dW[tap][ci][co] = sum_p x(p + tap)[ci] * dy(p)[co] (zeroes dW first). */
 int mass_sg_conv3x3_wgrad(const void* x, const void* dy, float* dW, int B, int H, int W,
                           int* err, void* stream);

@@ -879,8 +879,16 @@ int strip_rows(int B, int H, int W)
     const int r = std::atoi(e);
     if(r >= 1 && r <= 64 && H % r == 0) return r;
   }
+  return conv3x3_strip_rows(B, H, W, sm_count());
+}
+
+} // namespace
+
+int conv3x3_strip_rows(int B, int H, int W, int nsm)
+{
+  if(B < 1 || H < 1 || W < 128 || nsm < 1) return 1;
   const long long halves = static_cast<long long>(B)*(W >> 7);
-  const long long sms = sm_count();
+  const long long sms = nsm;
   int best = 1;
   double best_cost = -1.0;
   for(int r = 1; r <= std::min(16, H); ++r)
@@ -893,8 +901,6 @@ int strip_rows(int B, int H, int W)
   }
   return best;
 }
-
-} // namespace
 
 cudaError_t conv3x3_launch(const __nv_bfloat16* in, const __nv_bfloat16* w, int nout, int mode,
                            const ConvArgs& args, cudaStream_t st, int* ncta)

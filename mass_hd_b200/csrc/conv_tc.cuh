@@ -49,6 +49,11 @@ struct ConvArgs
 
 // in: padded NHWC64; w: forward weights [9][nout][64] (nout 64 or 16) or the
 // input-gradient weights [9][64][64] (nout 64).
+// Strip height the forward / input-gradient kernel uses for B images of H x
+// W on a GPU with nsm SMs (host arithmetic only; MASS_SG_CONV_ROWS, which
+// conv3x3_launch honours, is not read here).
+int conv3x3_strip_rows(int B, int H, int W, int nsm);
+
 // *ncta (if given) receives the number of CTAs launched.
 cudaError_t conv3x3_launch(const __nv_bfloat16* in, const __nv_bfloat16* w, int nout, int mode,
                            const ConvArgs& a, cudaStream_t st, int* ncta = nullptr);

@@ -303,6 +303,11 @@ int mass_sg_conv3x3(const void* in, const void* w, int nout, int mode, int B, in
                    nullptr, nullptr, stream);
 }
 
+int mass_sg_conv_strip_rows(int B, int H, int W, int nsm)
+{
+  return conv3x3_strip_rows(B, H, W, nsm);
+}
+
 int mass_sg_conv3x3_profile(const void* in, const void* w, int nout, int mode, int B, int H,
                             int W, const float* bias, const void* resid, const void* aux,
                             void* out, void* out2, const float* resid_f, float* out_f, int* err,
