@@ -5,7 +5,7 @@ f_v - t_v*rho so the rest state cannot hide errors):
   * 1 step:   <= 2e-5 on every state field
   * 10 steps: <= 1e-4
 These are the FP32 rounding of the step arithmetic; the measured per-field
-errors are printed with -s. Long runs diverge chaotically and are judged
+errors are printed with -s. Long runs diverge chaotically and are compared
 statistically (tests/test_gpu_stats.py).
 
 Also checked: every tile shape of the fused kernel gives bit-identical

@@ -4,7 +4,7 @@ The FP64 mode keeps the reference's evaluation order with no FMA
 contraction, so it must agree with the reference's double-precision build
 bit for bit: against the golden fixtures the reference itself produced, and
 against the CPU restatement on fresh seeded states for 100 steps (the
-north-star bound is <= 1e-10 relative L2 per field; the test asserts exact
+required bound is <= 1e-10 relative L2 per field; the test asserts exact
 equality and reports the bound).
 """
 import numpy as np
