@@ -30,7 +30,9 @@ The line also carries `fp64`: the FP64 mode (bit-identical to the
 reference's double-precision build) timed on the same seeded lattice, the
 like-for-like counterpart of the reference's FP64 CPU build; and
 `ensemble`: the 96-run batched sweep against the same runs one after
-another (a bounded sample of 200 steps per run).
+another (a bounded sample of 200 steps per run); and `surrogate`: the
+learned surrogate's tcgen05 convolutions at the training shape, each with
+its fraction of the measured BF16 peak, and its training step.
 
 --impl reference times the reference's own OpenMP build of the same step
 (oracle/_ref, compiled from the reference sources) on the host cores, on a
@@ -563,6 +565,28 @@ def ensemble_record(steps: int = 200, nruns: int = 96) -> dict:
                     f"{steps} steps per run as a bounded sample of the 10k-step sweep"}
 
 
+def surrogate_record() -> dict:
+    """The learned surrogate's tensor-core convolutions at the training shape
+    (batch 32, 256^2, 64 channels in and out, BF16 operands, FP32
+    accumulation): CUDA-event time of each convolution kind with its
+    fraction of the measured BF16 peak, and of one training step and one
+    forward pass (mass_hd_b200.surrogate_run bench). An auxiliary record:
+    if it fails, the line carries the error instead."""
+    try:
+        from mass_hd_b200 import surrogate_run as R
+        r = R.bench()
+        rec = {"batch": r["batch"], "size": r["size"], "gflop_per_conv": r["gflop_per_conv"],
+               "peak_tflops": r["peak_tflops"], "peak_kind": r["peak_kind"]}
+        for k in ("fwd_gelu", "fwd_resid", "dgrad_gelu", "wgrad"):
+            rec[k] = {"ms": r[k]["ms"], "tflops": r[k]["tflops"], "frac": r[k]["frac_of_peak"]}
+        rec["fwd_gelu"]["mma_thread"] = r["fwd_gelu"].get("mma_thread")
+        rec["train_step_ms"] = r["train_step"]["ms"]
+        rec["forward_images_per_s"] = r["forward"]["images_per_s"]
+        return rec
+    except Exception as e:
+        return {"error": f"{type(e).__name__}: {e}"}
+
+
 def run_ours_slab(args):
     """--decomp slab: ONE lattice of size^2 split into x-slabs over the ranks
     (strong scaling), halo rows exchanged before every step over NCCL
@@ -788,6 +812,9 @@ def run_ours(args):
     ens = None
     if model == "lyotropic" and world == 1 and not args.no_ensemble:
         ens = ensemble_record()
+    sg = None
+    if model == "lyotropic" and world == 1 and not args.no_surrogate:
+        sg = surrogate_record()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -818,6 +845,7 @@ def run_ours(args):
             "cpu_baseline": cpu,
             "fp64": fp64,
             "ensemble": ens,
+            "surrogate": sg,
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
@@ -850,13 +878,15 @@ def main():
                     help="skip the batched-ensemble record beside the lyotropic line")
     ap.add_argument("--no-fp64", action="store_true",
                     help="skip the FP64-mode record beside the FP32 line")
+    ap.add_argument("--no-surrogate", action="store_true",
+                    help="skip the surrogate-convolution record beside the lyotropic line")
     args = ap.parse_args()
     if args.size is None:
         args.size = 500 if args.model == "go-or-grow" else 4096
     if args.impl == "reference":
         return run_reference(args)
     if args.bc:
-        args.no_fp64 = args.no_ensemble = args.no_cpu_baseline = True
+        args.no_fp64 = args.no_ensemble = args.no_cpu_baseline = args.no_surrogate = True
     return run_ours(args)
 
 
