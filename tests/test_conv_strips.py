@@ -1,7 +1,11 @@
-"""Strip height of the surrogate's forward / input-gradient convolution
-(mass_sg_conv_strip_rows, host arithmetic, no GPU): each CTA marches down
-strips of that many output rows of one image half, so the height must
-divide H, stay within 16, and balance the strips over the SMs."""
+"""Host logic of the surrogate's convolution entry points, no GPU needed.
+
+The strip height (mass_sg_conv_strip_rows): each CTA of the forward /
+input-gradient kernel marches down strips of that many output rows of one
+image half, so the height must divide H, stay within 16, and balance the
+strips over the SMs. And the argument checks of mass_sg_conv3x3 and
+mass_sg_conv3x3_profile, which reject bad shapes, modes and missing
+buffers before any device work."""
 import ctypes
 import math
 
@@ -52,3 +56,38 @@ def test_degenerate_arguments_fall_back_to_one_row():
     assert strip_rows(0, 256, 256, 148) == 1
     assert strip_rows(4, 256, 64, 148) == 1
     assert strip_rows(4, 256, 256, 0) == 1
+
+
+def _conv_fn(name):
+    lib = ctypes.CDLL(M.library_path())
+    f = getattr(lib, name)
+    vp, i = ctypes.c_void_p, ctypes.c_int
+    f.argtypes = [vp, vp, i, i, i, i, i] + [vp] * 8 + ([vp, vp] if name.endswith("profile") else []) + [vp]
+    f.restype = ctypes.c_int
+    return f
+
+
+# Argument checks run on the host before any device work, so they can be
+# exercised without a GPU: fake non-null pointers never reach a kernel.
+P = ctypes.c_void_p(64)
+
+
+@pytest.mark.parametrize("name", ["mass_sg_conv3x3", "mass_sg_conv3x3_profile"])
+@pytest.mark.parametrize("nout,mode,B,H,W,why", [
+    (64, 1, 1, 8, 100, "W not a multiple of 128"),
+    (64, 1, 0, 8, 128, "no image"),
+    (64, 9, 1, 8, 128, "unknown mode"),
+    (16, 1, 1, 8, 128, "nout 16 outside the output layer"),
+    (64, 3, 1, 8, 128, "the output layer with nout 64"),
+])
+def test_convolution_rejects_bad_arguments(name, nout, mode, B, H, W, why):
+    f = _conv_fn(name)
+    extra = [P, P] if name.endswith("profile") else []
+    r = f(P, P, nout, mode, B, H, W, P, P, P, P, P, P, P, P, *extra, None)
+    assert r < 0, why
+
+
+def test_profile_needs_its_counter_buffers():
+    f = _conv_fn("mass_sg_conv3x3_profile")
+    assert f(P, P, 64, 1, 1, 8, 128, P, P, P, P, P, P, P, P, None, P, None) < 0
+    assert f(P, P, 64, 1, 1, 8, 128, P, P, P, P, P, P, P, P, P, None, None) < 0
